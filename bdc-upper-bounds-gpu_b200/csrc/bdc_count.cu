@@ -1,0 +1,445 @@
+// bdc_count.cu -- the exact subsequence-count path and the two passes of one BA
+// iteration that are built on it.
+//
+// Reference path (Pintz45/BDC-Upper-Bounds-GPU, backend/BAA.cu):
+//   total_transitions   340-395  N(x,y) by the split identity
+//   compute_den_kernel  429-485  q(y) = sum_x p(x) W(y|x)  (atomics per pair)
+//   compute_log_W_gpu   487-530  ln p(x) + D(x)
+//   compute_KL_kernel   533-571  D(x) = sum_y W ln(W/q)
+//
+// B200 design (differs from the reference on purpose):
+//   * no per-x DP + unranking: every thread owns a fixed structured set of
+//     2^{TB+BB} output words y (TB top bits x BB bottom bits, the middle bits
+//     are the thread's index in its x-group) and evaluates the DENSE row
+//     N(x, y) for its y's.  For split point j the distinct half-table entries
+//     of those y's are loaded once and reused by all products (register
+//     tiling of the Kronecker-sum structure N = sum_j A_j (x) B_{k-j});
+//   * the q pass accumulates sum_x |O(x)| p(x) N(x,y) per raw y in registers
+//     (no atomics) and folds orbits once at the end:
+//         q(rep r) = sum_{y in O(r)} acc[y] / (|O(r)| C(n,k));
+//   * the D pass uses the p-independent entropy term h(x) = sum_y W ln W,
+//     computed once per handle, so that each pair costs one multiply-add:
+//         D(x) = h(x) - (1/C) sum_y N(x,y) ln q(y).
+#include <utility>
+
+#include "bdc_common.cuh"
+#include "bdc_engine.cuh"
+#include "bdc_kernels.cuh"
+
+namespace bdc {
+
+// ------------------------------------------------------------ pair counts
+__global__ void k_count_pairs(Split s, HalfTables A, HalfTables B, const uint32_t* __restrict__ xs,
+                              const uint32_t* __restrict__ ys, int64_t npairs,
+                              uint32_t* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npairs;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = split_count(s, A, B, xs[i], ys[i]);
+}
+
+// ------------------------------------------------------- dense count tiles
+// Thread-owned y set: y(t, b) = (t << (K - TB)) | (g << BB) | b with
+// t < 2^TB, b < 2^BB and g the thread's index inside its x-group of
+// 2^{K-TB-BB} threads.
+template <int K, int TB, int BB>
+struct Tile {
+    static constexpr int T = 1 << TB;
+    static constexpr int NB = 1 << BB;
+    static constexpr int YPT = T * NB;
+    static constexpr int MID = K - TB - BB;
+    static constexpr int GROUP = 1 << MID;  // threads per x
+    static_assert(MID >= 0, "tile larger than the output alphabet");
+
+    __device__ __forceinline__ static uint32_t y_of(uint32_t g, int t, int b) {
+        return ((uint32_t)t << (K - TB)) | (g << BB) | (uint32_t)b;
+    }
+};
+
+// One split point J of the dense row: N[t][b] += A_J[xh][y >> M] * B_M[xl][y & (2^M-1)].
+template <int K, int TB, int BB, int J>
+__device__ __forceinline__ void tile_term(const Split& s, const uint16_t* __restrict__ ar,
+                                          const uint16_t* __restrict__ br, uint32_t xh, uint32_t xl,
+                                          uint32_t g, uint32_t (&N)[1 << TB][1 << BB]) {
+    constexpr int M = K - J;
+    constexpr int T = 1 << TB, NB = 1 << BB;
+    // distinct entries along t and b for the A (high) and B (low) halves
+    constexpr int AT = (J >= TB) ? T : (1 << J);
+    constexpr int AB = (M >= BB) ? 1 : (1 << (BB - M));
+    constexpr int BT = (J >= TB) ? 1 : (1 << (TB - J));
+    constexpr int BN = (M >= BB) ? NB : (1 << M);
+    if (J < s.jlo || J > s.jhi) return;  // uniform across the grid
+    const bool idA = (J == s.n1);
+    const bool idB = (M == s.n2);
+    uint32_t av[AT][AB], bv[BT][BN];
+#pragma unroll
+    for (int ta = 0; ta < AT; ++ta)
+#pragma unroll
+        for (int ba = 0; ba < AB; ++ba) {
+            const int t = (J >= TB) ? ta : (ta << (TB - J));
+            const int b = (M >= BB) ? 0 : (ba << M);
+            const uint32_t yh = Tile<K, TB, BB>::y_of(g, t, b) >> M;
+            av[ta][ba] = idA ? (uint32_t)(xh == yh) : (uint32_t)__ldg(ar + bundle_offset(J) + yh);
+        }
+#pragma unroll
+    for (int tb = 0; tb < BT; ++tb)
+#pragma unroll
+        for (int bb = 0; bb < BN; ++bb) {
+            const int t = (J >= TB) ? 0 : tb;
+            const uint32_t yl = Tile<K, TB, BB>::y_of(g, t, bb) & low_mask(M);
+            bv[tb][bb] = idB ? (uint32_t)(xl == yl) : (uint32_t)__ldg(br + bundle_offset(M) + yl);
+        }
+#pragma unroll
+    for (int t = 0; t < T; ++t)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int ai = (J >= TB) ? t : (t >> (TB - J));
+            const int aj = (M >= BB) ? 0 : (b >> M);
+            const int bi = (J >= TB) ? 0 : (t & (BT - 1));
+            const int bj = (M >= BB) ? b : (b & (BN - 1));
+            N[t][b] += av[ai][aj] * bv[bi][bj];
+        }
+}
+
+template <int K, int TB, int BB, int... Js>
+__device__ __forceinline__ void tile_row_impl(const Split& s, const uint16_t* ar, const uint16_t* br,
+                                              uint32_t xh, uint32_t xl, uint32_t g,
+                                              uint32_t (&N)[1 << TB][1 << BB],
+                                              std::integer_sequence<int, Js...>) {
+    (tile_term<K, TB, BB, Js>(s, ar, br, xh, xl, g, N), ...);
+}
+
+// Dense counts N(x, y(t,b)) for all of this thread's y.
+template <int K, int TB, int BB>
+__device__ __forceinline__ void tile_row(const Split& s, const HalfTables& A, const HalfTables& B,
+                                         uint32_t x, uint32_t g, uint32_t (&N)[1 << TB][1 << BB]) {
+#pragma unroll
+    for (int t = 0; t < (1 << TB); ++t)
+#pragma unroll
+        for (int b = 0; b < (1 << BB); ++b) N[t][b] = 0u;
+    const uint32_t xh = x >> s.n2, xl = x & low_mask(s.n2);
+    const uint16_t* ar = A.rows + (size_t)xh * A.stride;
+    const uint16_t* br = B.rows + (size_t)xl * B.stride;
+    tile_row_impl<K, TB, BB>(s, ar, br, xh, xl, g, N, std::make_integer_sequence<int, K + 1>{});
+}
+
+// ------------------------------------------------------------- q pass
+// acc[y] = sum over this CTA's x of |O(x)| p(x) N(x,y), written per CTA to
+// part[blockIdx.x][y]; k_qfold reduces over CTAs.
+template <int K, int TB, int BB>
+__global__ void __launch_bounds__(256) k_qpass(Split s, HalfTables A, HalfTables B,
+                                               const uint32_t* __restrict__ reps,
+                                               const double* __restrict__ p_buf0,
+                                               const double* __restrict__ p_buf1, int64_t R,
+                                               double* __restrict__ part, const DevState* st,
+                                               int use_state) {
+    using TL = Tile<K, TB, BB>;
+    if (use_state && st->done) return;
+    const double* __restrict__ p = (use_state && st->cur) ? p_buf1 : p_buf0;
+    const int groups_per_cta = blockDim.x / TL::GROUP;
+    const int grp = threadIdx.x / TL::GROUP;
+    const uint32_t g = threadIdx.x % TL::GROUP;
+    const int64_t ngroups = (int64_t)gridDim.x * groups_per_cta;
+    const int64_t gid = (int64_t)blockIdx.x * groups_per_cta + grp;
+    const int64_t chunk = (R + ngroups - 1) / ngroups;
+    const int64_t i0 = gid * chunk;
+    const int64_t i1 = (i0 + chunk < R) ? i0 + chunk : R;
+
+    double acc[TL::T][TL::NB];
+#pragma unroll
+    for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+        for (int b = 0; b < TL::NB; ++b) acc[t][b] = 0.0;
+
+    for (int64_t i = i0; i < i1; ++i) {
+        const uint32_t x = __ldg(reps + i);
+        const double w = (double)orbit_size(x, s.n) * __ldg(p + i);
+        uint32_t N[TL::T][TL::NB];
+        tile_row<K, TB, BB>(s, A, B, x, g, N);
+#pragma unroll
+        for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+            for (int b = 0; b < TL::NB; ++b) acc[t][b] = fma(w, (double)N[t][b], acc[t][b]);
+    }
+
+    // reduce the CTA's groups (same g => same y set) in shared memory
+    extern __shared__ double sh_acc[];  // [1 << K]
+    for (int y = threadIdx.x; y < (1 << K); y += blockDim.x) sh_acc[y] = 0.0;
+    __syncthreads();
+    for (int gg = 0; gg < groups_per_cta; ++gg) {
+        if (grp == gg) {
+#pragma unroll
+            for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+                for (int b = 0; b < TL::NB; ++b) sh_acc[TL::y_of(g, t, b)] += acc[t][b];
+        }
+        __syncthreads();
+    }
+    double* out = part + (size_t)blockIdx.x * (1 << K);
+    for (int y = threadIdx.x; y < (1 << K); y += blockDim.x) out[y] = sh_acc[y];
+}
+
+// ------------------------------------------------------------- D / h pass
+// MODE 0: D(x) = h(x) - (1/C) sum_y N(x,y) ln q(rep y)       -> out_d[i]
+// MODE 1: h(x) = (1/C) sum_y N ln N - ln C                    -> out_d[i]
+template <int K, int TB, int BB, int MODE>
+__global__ void __launch_bounds__(256) k_dpass(Split s, HalfTables A, HalfTables B,
+                                               const uint32_t* __restrict__ reps, int64_t R,
+                                               const double* __restrict__ lnq,
+                                               const double* __restrict__ h,
+                                               double inv_c, double log_c,
+                                               double* __restrict__ out_d, uint32_t* __restrict__ out_nnz,
+                                               const DevState* st, int use_state) {
+    using TL = Tile<K, TB, BB>;
+    if (use_state && st->done) return;
+    const int groups_per_cta = blockDim.x / TL::GROUP;
+    const int grp = threadIdx.x / TL::GROUP;
+    const uint32_t g = threadIdx.x % TL::GROUP;
+    const int64_t ngroups = (int64_t)gridDim.x * groups_per_cta;
+    const int64_t gid = (int64_t)blockIdx.x * groups_per_cta + grp;
+    const int64_t chunk = (R + ngroups - 1) / ngroups;
+    const int64_t i0 = gid * chunk;
+    const int64_t i1 = (i0 + chunk < R) ? i0 + chunk : R;
+    const int lane = threadIdx.x & 31;
+
+    double lq[TL::T][TL::NB];
+    if (MODE == 0) {
+#pragma unroll
+        for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+            for (int b = 0; b < TL::NB; ++b)
+                lq[t][b] = __ldg(lnq + orbit_rep(TL::y_of(g, t, b), K));
+    }
+
+    // per-warp partial sums of the group's x, folded every XC rows
+    constexpr int XC = 32;
+    constexpr int WPG = (TL::GROUP + 31) / 32;  // warps per group
+    __shared__ double sh_part[XC][8];            // [x slot][warp of the CTA]
+    __shared__ uint32_t sh_nz[XC][8];
+    const int warp = threadIdx.x >> 5;
+    // All groups of a CTA run the same number of rounds so that the
+    // barriers below are uniform.
+    for (int64_t r0 = 0; r0 < chunk; r0 += XC) {
+        for (int xs = 0; xs < XC; ++xs) {
+            const int64_t i = i0 + r0 + xs;
+            double v = 0.0;
+            uint32_t nz = 0;
+            if (i < i1) {
+                const uint32_t x = __ldg(reps + i);
+                uint32_t N[TL::T][TL::NB];
+                tile_row<K, TB, BB>(s, A, B, x, g, N);
+#pragma unroll
+                for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+                    for (int b = 0; b < TL::NB; ++b) {
+                        if (MODE == 0) {
+                            v = fma((double)N[t][b], lq[t][b], v);
+                        } else {
+                            const uint32_t c = N[t][b];
+                            if (c) {
+                                v = fma((double)c, log((double)c), v);
+                                ++nz;
+                            }
+                        }
+                    }
+            }
+            if (TL::GROUP <= 32) {
+                // the group is a lane-aligned slice of one warp
+#pragma unroll
+                for (int off = TL::GROUP / 2; off > 0; off >>= 1) {
+                    v += __shfl_xor_sync(0xFFFFFFFFu, v, off);
+                    if (MODE == 1) nz += __shfl_xor_sync(0xFFFFFFFFu, nz, off);
+                }
+                if (g == 0 && i < i1) {
+                    out_d[i] = (MODE == 0) ? (__ldg(h + i) - v * inv_c) : (v * inv_c - log_c);
+                    if (MODE == 1) out_nnz[i] = nz;
+                }
+            } else {
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    v += __shfl_xor_sync(0xFFFFFFFFu, v, off);
+                    if (MODE == 1) nz += __shfl_xor_sync(0xFFFFFFFFu, nz, off);
+                }
+                if (lane == 0) {
+                    sh_part[xs][warp] = v;
+                    sh_nz[xs][warp] = nz;
+                }
+            }
+        }
+        if (TL::GROUP > 32) {
+            __syncthreads();
+            if (threadIdx.x < XC * groups_per_cta) {
+                const int gg = threadIdx.x / XC, xs = threadIdx.x % XC;
+                const int64_t gi0 = ((int64_t)blockIdx.x * groups_per_cta + gg) * chunk;
+                const int64_t gi1 = (gi0 + chunk < R) ? gi0 + chunk : R;
+                const int64_t i = gi0 + r0 + xs;
+                if (i < gi1) {
+                    double v = 0.0;
+                    uint32_t nz = 0;
+                    for (int w = 0; w < WPG; ++w) {
+                        v += sh_part[xs][gg * WPG + w];
+                        nz += sh_nz[xs][gg * WPG + w];
+                    }
+                    out_d[i] = (MODE == 0) ? (__ldg(h + i) - v * inv_c) : (v * inv_c - log_c);
+                    if (MODE == 1) out_nnz[i] = nz;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// -------------------------------------------------------------- q fold
+// lnq[r] = ln( sum_{y in O(r)} sum_c part[c][y] / (|O(r)| C) ) for
+// representative slots r < 2^{k-1}; 0 for other slots and for q == 0.
+// One warp per slot; fixed lane-strided order, so the result is deterministic.
+__global__ void k_qfold(const double* __restrict__ part, int nparts, int k, double inv_c,
+                        double* __restrict__ lnq, double* __restrict__ q_out, const DevState* st,
+                        int use_state) {
+    if (use_state && st->done) return;
+    const int nq = (k >= 1) ? (1 << (k - 1)) : 1;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int ny = 1 << k;
+    for (int r = warp; r < nq; r += nwarps) {
+        if (!is_rep((uint32_t)r, k)) {
+            if (lane == 0) { lnq[r] = 0.0; if (q_out) q_out[r] = 0.0; }
+            continue;
+        }
+        uint32_t mem[4];
+        int nm = 0;
+        const uint32_t rv = reverse_bits((uint32_t)r, k);
+        const uint32_t cv = complement_bits((uint32_t)r, k);
+        const uint32_t rcv = reverse_bits(cv, k);
+        mem[nm++] = (uint32_t)r;
+        if (rv != (uint32_t)r) mem[nm++] = rv;
+        if (cv != (uint32_t)r && cv != rv) mem[nm++] = cv;
+        if (rcv != (uint32_t)r && rcv != rv && rcv != cv) mem[nm++] = rcv;
+        double acc = 0.0;
+        for (int c = lane; c < nparts; c += 32) {
+            const double* row = part + (size_t)c * ny;
+            for (int e = 0; e < nm; ++e) acc += row[mem[e]];
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, off);
+        if (lane == 0) {
+            const double q = acc * inv_c / (double)orbit_size((uint32_t)r, k);
+            lnq[r] = (q != 0.0) ? log(q) : 0.0;
+            if (q_out) q_out[r] = q;
+        }
+    }
+}
+
+// ------------------------------------------------------------ dispatch
+// (TB, BB) per output length K: 16 words per thread for K >= 4.
+// (TB, BB) per output length K: 16 words per thread for 4 <= K <= 12, and
+// larger tiles above so that an x-group never exceeds 256 threads.
+template <int K>
+struct TileChoice {
+    static constexpr int TB = (K >= 13) ? 3 : (K >= 4) ? 2 : (K >= 2 ? 1 : 0);
+    static constexpr int BB = (K >= 14) ? 3 : (K >= 4) ? 2 : (K >= 2 ? 1 : 0);
+};
+
+template <int K>
+static int cta_threads() {
+    constexpr int G = Tile<K, TileChoice<K>::TB, TileChoice<K>::BB>::GROUP;
+    return G >= 256 ? G : 256;
+}
+
+template <int K>
+static cudaError_t launch_qpass_k(const CountLaunch& L, const double* p0, const double* p1,
+                                  double* part, const DevState* st, int use_state) {
+    constexpr int TB = TileChoice<K>::TB, BB = TileChoice<K>::BB;
+    const int threads = cta_threads<K>();
+    const size_t shm = sizeof(double) << K;
+    auto kern = k_qpass<K, TB, BB>;
+    if (shm > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<L.grid, threads, shm, L.stream>>>(L.s, L.A, L.B, L.reps, p0, p1, L.R, part, st, use_state);
+    return cudaGetLastError();
+}
+
+template <int K, int MODE>
+static cudaError_t launch_dpass_k(const CountLaunch& L, const double* lnq, const double* h,
+                                  double inv_c, double log_c, double* out, uint32_t* nnz,
+                                  const DevState* st, int use_state) {
+    constexpr int TB = TileChoice<K>::TB, BB = TileChoice<K>::BB;
+    const int threads = cta_threads<K>();
+    k_dpass<K, TB, BB, MODE><<<L.grid, threads, 0, L.stream>>>(L.s, L.A, L.B, L.reps, L.R, lnq, h,
+                                                               inv_c, log_c, out, nnz, st, use_state);
+    return cudaGetLastError();
+}
+
+#define BDC_K_CASES(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14)
+
+int count_group_size(int k) {
+    switch (k) {
+#define C_(K) case K: return Tile<K, TileChoice<K>::TB, TileChoice<K>::BB>::GROUP;
+        BDC_K_CASES(C_)
+#undef C_
+        default: return 0;
+    }
+}
+
+int count_cta_threads(int k) {
+    switch (k) {
+#define C_(K) case K: return cta_threads<K>();
+        BDC_K_CASES(C_)
+#undef C_
+        default: return 0;
+    }
+}
+
+cudaError_t launch_qpass(const CountLaunch& L, const double* p0, const double* p1, double* part,
+                         const DevState* st, int use_state) {
+    switch (L.s.k) {
+#define C_(K) case K: return launch_qpass_k<K>(L, p0, p1, part, st, use_state);
+        BDC_K_CASES(C_)
+#undef C_
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_dpass(const CountLaunch& L, const double* lnq, const double* h, double inv_c,
+                         double log_c, double* out, const DevState* st, int use_state) {
+    switch (L.s.k) {
+#define C_(K) case K: return launch_dpass_k<K, 0>(L, lnq, h, inv_c, log_c, out, nullptr, st, use_state);
+        BDC_K_CASES(C_)
+#undef C_
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_hpass(const CountLaunch& L, double inv_c, double log_c, double* out, uint32_t* nnz) {
+    switch (L.s.k) {
+#define C_(K) case K: return launch_dpass_k<K, 1>(L, nullptr, nullptr, inv_c, log_c, out, nnz, nullptr, 0);
+        BDC_K_CASES(C_)
+#undef C_
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_qfold(const double* part, int nparts, int k, double inv_c, double* lnq,
+                         double* q_out, const DevState* st, int use_state, cudaStream_t stream) {
+    const int nq = (k >= 1) ? (1 << (k - 1)) : 1;
+    const int warps = nq;
+    const int threads = 256;
+    int blocks = (warps * 32 + threads - 1) / threads;
+    if (blocks > 4096) blocks = 4096;
+    k_qfold<<<blocks, threads, 0, stream>>>(part, nparts, k, inv_c, lnq, q_out, st, use_state);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_count_pairs(const Split& s, const HalfTables& A, const HalfTables& B,
+                               const uint32_t* xs, const uint32_t* ys, int64_t npairs,
+                               uint32_t* out, cudaStream_t stream) {
+    if (npairs <= 0) return cudaSuccess;
+    int64_t blocks = (npairs + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    k_count_pairs<<<(int)blocks, 256, 0, stream>>>(s, A, B, xs, ys, npairs, out);
+    return cudaGetLastError();
+}
+
+}  // namespace bdc

@@ -1,0 +1,80 @@
+// bdc_engine.cuh -- the handle behind bdc_handle_t and the engine interface.
+#pragma once
+
+#include <string>
+
+#include "bdc_common.cuh"
+#include "bdc_kernels.cuh"
+
+struct FactoredState;  // bdc_factored.cu
+
+struct bdc_handle {
+    // problem
+    int n = 0, k = 0;
+    bdc::Split s{};
+    double C = 0, inv_c = 0, log_c = 0;
+    int64_t R = 0;
+    // placement / options
+    int device = 0;
+    int engine = BDC_ENGINE_COUNT;
+    int verbose = 0;
+    int num_sms = 148;
+    std::string cache_dir;
+    cudaStream_t stream = nullptr;      // where work is queued
+    cudaStream_t own_stream = nullptr;  // created by the handle
+    size_t bytes = 0;  // device bytes held
+    // tables
+    uint32_t* d_reps = nullptr;
+    uint16_t* d_bundle_hi = nullptr;
+    uint16_t* d_bundle_lo = nullptr;  // equal to d_bundle_hi when n is even
+    bdc::HalfTables A{}, B{};
+    // per-representative vectors
+    double* d_p[2] = {nullptr, nullptr};
+    double* d_h = nullptr;     // sum_y W ln W
+    double* d_d = nullptr;     // D(x)
+    double* d_logw = nullptr;  // scratch
+    // output side
+    double* d_lnq = nullptr;   // [2^{k-1}]
+    double* d_q = nullptr;     // [2^{k-1}]
+    double* d_qpart = nullptr; // [grid][2^k]
+    // reductions / state
+    double* d_red = nullptr;
+    double* d_scalar = nullptr;
+    bdc::DevState* d_st = nullptr;
+    bdc::DevState* h_st = nullptr;  // pinned mirror
+    int grid_count = 0;
+    int nb_upd = 0;
+    bool p_set = false;
+    int64_t nonzero_pairs = 0;  // sum over reps of distinct length-k subsequences
+    // factored engine
+    FactoredState* fac = nullptr;
+};
+
+namespace bdc {
+
+bdc_status fail(bdc_status st, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+
+int select_engine(int requested, int n, int k);
+bdc_status engine_init(bdc_handle* H);
+void engine_free(bdc_handle* H);
+bdc_status engine_after_set_p(bdc_handle* H);
+bdc_status engine_current_p(bdc_handle* H, const double** p);
+bdc_status engine_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats);
+bdc_status engine_log_q(bdc_handle* H);       // ln q of the current p into H->d_lnq
+bdc_status engine_divergence(bdc_handle* H);  // D from H->d_lnq into H->d_d
+
+CountLaunch count_launch(const bdc_handle* H);
+UpdateLaunch update_launch(const bdc_handle* H, double a);
+bdc_status engine_profile(bdc_handle* H, int iters, bdc_profile_t* out);
+int count_group_size(int k);
+
+// factored engine (bdc_factored.cu)
+bool factored_supports(int n, int k);
+bdc_status factored_init(bdc_handle* H);
+void factored_free(bdc_handle* H);
+bdc_status factored_load_p(bdc_handle* H);                 // d_p[0] -> dense state
+bdc_status factored_store_p(bdc_handle* H, double* p_out);  // dense state -> p per rep
+bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats);
+bdc_status factored_profile(bdc_handle* H, int iters, bdc_profile_t* out);
+
+}  // namespace bdc

@@ -1,0 +1,257 @@
+// bdc_update.cu -- the normalised BA update, the stopping statistic and the
+// reported scalars, as three streaming kernels over the representatives.
+//
+// Reference (Pintz45/BDC-Upper-Bounds-GPU):
+//   backend/BAA.cu:590-639   baa_iteration: max logW, exp(logW - max),
+//                            sum |O| exp(..), divide (four Thrust passes and a
+//                            host round trip of every vector)
+//   backend/BAA.cu:916-946   compute_max_deviation: max log2 p' - log2 p
+//   backend/BAA.cu:820-913   compute_rate: sum |O| p KL
+//   backend/main_BAA.cu:73   the loop runs while (mx >= a)
+//
+// Here everything stays resident: each kernel streams the R-vectors once,
+// reduces per block, and the last block to finish folds the block partials
+// in a fixed order (deterministic) into DevState.  DevState::done makes every
+// later kernel a no-op once mx < a, so a chunk of iterations can be queued or
+// captured in a graph without a host round trip per iteration.
+#include <cfloat>
+
+#include "bdc_common.cuh"
+#include "bdc_kernels.cuh"
+
+namespace bdc {
+
+constexpr int kUpdThreads = 256;
+
+__device__ __forceinline__ double log_keep0(double v) { return v != 0.0 ? log(v) : 0.0; }
+
+template <typename Op>
+__device__ __forceinline__ double block_reduce(double v, Op op, double ident) {
+    __shared__ double sh[kUpdThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = op(v, __shfl_xor_sync(0xFFFFFFFFu, v, off));
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double r = ident;
+    if (threadIdx.x < 32) {
+        r = (lane < kUpdThreads / 32) ? sh[lane] : ident;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) r = op(r, __shfl_xor_sync(0xFFFFFFFFu, r, off));
+    }
+    return r;  // valid in thread 0
+}
+
+struct OpMax {
+    __device__ double operator()(double a, double b) const {
+        // NaN propagates: a NaN deviation stops the loop as in the reference
+        // (while (mx >= a) is false for NaN)
+        if (a != a) return a;
+        if (b != b) return b;
+        return a > b ? a : b;
+    }
+};
+struct OpSum {
+    __device__ double operator()(double a, double b) const { return a + b; }
+};
+
+// true in exactly one block: the last one to arrive
+__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    return is_last;
+}
+
+// fold nb partials (strided by `stride` doubles) with op in a fixed order
+template <typename Op>
+__device__ __forceinline__ double fold_partials(const double* part, int nb, Op op, double ident) {
+    double v = ident;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) v = op(v, ((volatile const double*)part)[b]);
+    return block_reduce(v, op, ident);
+}
+
+// stage 1: logW = ln p + D; block max logW, max D, sum |O| p D, any zero p
+__global__ void __launch_bounds__(kUpdThreads)
+k_upd_logw(int n, const uint32_t* __restrict__ reps, int64_t R, const double* __restrict__ p0,
+           const double* __restrict__ p1, const double* __restrict__ d, double* __restrict__ logw,
+           double* __restrict__ part, DevState* st) {
+    if (st->done) return;
+    const double* __restrict__ p = st->cur ? p1 : p0;
+    double mlw = -DBL_MAX, md = -DBL_MAX, rate = 0.0, zero = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double pi = p[i];
+        const double di = d[i];
+        const double lw = log_keep0(pi) + di;
+        logw[i] = lw;
+        mlw = OpMax()(mlw, lw);
+        md = OpMax()(md, di);
+        rate = fma((double)orbit_size(reps[i], n) * pi, di, rate);
+        if (pi == 0.0) zero = 1.0;
+    }
+    const int nb = gridDim.x;
+    double r0 = block_reduce(mlw, OpMax(), -DBL_MAX);
+    double r1 = block_reduce(md, OpMax(), -DBL_MAX);
+    double r2 = block_reduce(rate, OpSum(), 0.0);
+    double r3 = block_reduce(zero, OpMax(), 0.0);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = r0;
+        part[nb + blockIdx.x] = r1;
+        part[2 * nb + blockIdx.x] = r2;
+        part[3 * nb + blockIdx.x] = r3;
+    }
+    if (!last_block(&st->ticket[0])) return;
+    r0 = fold_partials(part, nb, OpMax(), -DBL_MAX);
+    r1 = fold_partials(part + nb, nb, OpMax(), -DBL_MAX);
+    r2 = fold_partials(part + 2 * nb, nb, OpSum(), 0.0);
+    r3 = fold_partials(part + 3 * nb, nb, OpMax(), 0.0);
+    if (threadIdx.x == 0) {
+        st->max_logw = r0;
+        st->max_d = r1;
+        st->rate = r2;
+        st->zero_p = (r3 != 0.0);
+        st->shift = r0;
+        st->ticket[0] = 0;
+    }
+}
+
+// stage 2: e = exp(logW - max) into the other buffer; Z = sum |O| e
+__global__ void __launch_bounds__(kUpdThreads)
+k_upd_exp(int n, const uint32_t* __restrict__ reps, int64_t R, double* __restrict__ p0,
+          double* __restrict__ p1, const double* __restrict__ logw, double* __restrict__ part,
+          DevState* st) {
+    if (st->done) return;
+    double* __restrict__ pn = st->cur ? p0 : p1;
+    const double shift = st->shift;
+    double z = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double e = exp(logw[i] - shift);
+        pn[i] = e;
+        z = fma((double)orbit_size(reps[i], n), e, z);
+    }
+    const int nb = gridDim.x;
+    double r = block_reduce(z, OpSum(), 0.0);
+    if (threadIdx.x == 0) part[4 * nb + blockIdx.x] = r;
+    if (!last_block(&st->ticket[1])) return;
+    r = fold_partials(part + 4 * nb, nb, OpSum(), 0.0);
+    if (threadIdx.x == 0) {
+        st->log_z = log(r);
+        st->lse = st->shift + log(r);
+        st->ticket[1] = 0;
+    }
+}
+
+// stage 3: p' = e / Z; mx = max log2 p' - log2 p; flip buffers; stop test
+__global__ void __launch_bounds__(kUpdThreads)
+k_upd_norm(int64_t R, double* __restrict__ p0, double* __restrict__ p1, double* __restrict__ part,
+           double a, DevState* st) {
+    if (st->done) return;
+    double* __restrict__ pn = st->cur ? p0 : p1;
+    const double* __restrict__ pc = st->cur ? p1 : p0;
+    const double z = exp(st->log_z);
+    double mx = -DBL_MAX;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = pn[i] / z;
+        pn[i] = v;
+        mx = OpMax()(mx, log2(v) - log2(pc[i]));
+    }
+    const int nb = gridDim.x;
+    double r = block_reduce(mx, OpMax(), -DBL_MAX);
+    if (threadIdx.x == 0) part[5 * nb + blockIdx.x] = r;
+    if (!last_block(&st->ticket[2])) return;
+    r = fold_partials(part + 5 * nb, nb, OpMax(), -DBL_MAX);
+    if (threadIdx.x == 0) {
+        st->mx = r;
+        st->cur ^= 1;
+        st->iter += 1;
+        st->done = !(r >= a);
+        st->ticket[2] = 0;
+    }
+}
+
+cudaError_t launch_update(const UpdateLaunch& U) {
+    k_upd_logw<<<U.nblocks, kUpdThreads, 0, U.stream>>>(U.n, U.reps, U.R, U.p0, U.p1, U.d, U.logw,
+                                                        U.part, U.st);
+    k_upd_exp<<<U.nblocks, kUpdThreads, 0, U.stream>>>(U.n, U.reps, U.R, U.p0, U.p1, U.logw, U.part,
+                                                       U.st);
+    k_upd_norm<<<U.nblocks, kUpdThreads, 0, U.stream>>>(U.R, U.p0, U.p1, U.part, U.a, U.st);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- helpers
+__global__ void k_logw(int n, const uint32_t* __restrict__ reps, int64_t R,
+                       const double* __restrict__ p, const double* __restrict__ d,
+                       double* __restrict__ logw) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R;
+         i += (int64_t)gridDim.x * blockDim.x)
+        logw[i] = log_keep0(p[i]) + d[i];
+}
+
+cudaError_t launch_logw(int n, const uint32_t* reps, int64_t R, const double* p, const double* d,
+                        double* logw, cudaStream_t stream) {
+    int64_t b = (R + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    if (b < 1) b = 1;
+    k_logw<<<(int)b, 256, 0, stream>>>(n, reps, R, p, d, logw);
+    return cudaGetLastError();
+}
+
+// single-kernel sum |O| p D (two kernels: block partials, then one block)
+__global__ void __launch_bounds__(kUpdThreads)
+k_rate_part(int n, const uint32_t* __restrict__ reps, int64_t R, const double* __restrict__ p,
+            const double* __restrict__ d, double* __restrict__ part) {
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R;
+         i += (int64_t)gridDim.x * blockDim.x)
+        s = fma((double)orbit_size(reps[i], n) * p[i], d[i], s);
+    s = block_reduce(s, OpSum(), 0.0);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(kUpdThreads)
+k_fold_sum(const double* __restrict__ part, int nb, double* out) {
+    const double s = fold_partials(part, nb, OpSum(), 0.0);
+    if (threadIdx.x == 0) *out = s;
+}
+
+__global__ void __launch_bounds__(kUpdThreads)
+k_fold_max(const double* __restrict__ part, int nb, double* out) {
+    const double s = fold_partials(part, nb, OpMax(), -DBL_MAX);
+    if (threadIdx.x == 0) *out = s;
+}
+
+cudaError_t launch_rate(int n, const uint32_t* reps, int64_t R, const double* p, const double* d,
+                        double* part, int nblocks, double* out, cudaStream_t stream) {
+    k_rate_part<<<nblocks, kUpdThreads, 0, stream>>>(n, reps, R, p, d, part);
+    k_fold_sum<<<1, kUpdThreads, 0, stream>>>(part, nblocks, out);
+    return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(kUpdThreads)
+k_maxdev_part(const double* __restrict__ p, const double* __restrict__ pb, int64_t R,
+              double* __restrict__ part) {
+    double m = -DBL_MAX;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R;
+         i += (int64_t)gridDim.x * blockDim.x)
+        m = OpMax()(m, log2(p[i]) - log2(pb[i]));
+    m = block_reduce(m, OpMax(), -DBL_MAX);
+    if (threadIdx.x == 0) part[blockIdx.x] = m;
+}
+
+cudaError_t launch_max_dev(const double* p, const double* pb, int64_t R, double* part, int nblocks,
+                           double* out, cudaStream_t stream) {
+    k_maxdev_part<<<nblocks, kUpdThreads, 0, stream>>>(p, pb, R, part);
+    k_fold_max<<<1, kUpdThreads, 0, stream>>>(part, nblocks, out);
+    return cudaGetLastError();
+}
+
+}  // namespace bdc

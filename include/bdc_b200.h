@@ -1,0 +1,177 @@
+/*
+ * bdc_b200.h -- C ABI of the B200 Blahut-Arimoto (BA) engine for the binary
+ * deletion channel BDC_{n,k}: inputs are the 2^n binary strings of length n,
+ * outputs the 2^k strings of length k, W(y|x) = N(x,y) / C(n,k) with N(x,y)
+ * the number of occurrences of y as a subsequence of x.
+ *
+ * Plain C types only (no torch, no C++).  Every function returns a
+ * bdc_status; on failure bdc_last_error() gives a one-line reason.  Nothing
+ * calls exit().
+ *
+ * Layouts (identical to the reference, Pintz45/BDC-Upper-Bounds-GPU):
+ *   p[R]       probability of EACH string of an orbit, one entry per canonical
+ *              representative in ascending order (backend/main_BAA.cu:46-64);
+ *              R = number of orbits of {id, reverse, complement, rev-compl}
+ *   ln q[2^{k-1}]  ln of the output marginal, indexed by the representative's
+ *              value; non-representative slots and q == 0 hold 0
+ *              (backend/BAA.cu:649-652, 573-580)
+ *   cache_n_k  binary uint32 little endian, 2^{n+k} entries, index (x<<k)|y
+ *              (backend/cache_io.h:7-44)
+ *   dist_n_k.txt   one "%.17g" probability per line, same order as p
+ *              (backend/main_BAA.cu:84-91, 113-119)
+ */
+#ifndef BDC_B200_H
+#define BDC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    BDC_OK = 0,
+    BDC_ERR_ARG = 1,          /* bad argument: NULL, size mismatch, n/k out of range */
+    BDC_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    BDC_ERR_IO = 3,           /* cache or distribution file missing, short or malformed */
+    BDC_ERR_NOMEM = 4,        /* the device has too little free memory */
+    BDC_ERR_STATE = 5,        /* call out of order (no handle loaded, no p set) */
+    BDC_ERR_UNSUPPORTED = 6,  /* (n,k) outside what this build supports */
+    BDC_ERR_NUMERIC = 7       /* non-finite input or result */
+} bdc_status;
+
+typedef enum {
+    BDC_ENGINE_AUTO = 0,      /* the fastest engine that supports (n,k) */
+    BDC_ENGINE_COUNT = 1,     /* split-identity count path: q pass + D pass per iteration */
+    BDC_ENGINE_FACTORED = 2   /* Kronecker-factored passes (FP64 matrix products) */
+} bdc_engine;
+
+typedef struct {
+    int engine;               /* bdc_engine */
+    int device;               /* CUDA device ordinal */
+    const char* cache_dir;    /* directory holding cache_n_k files (the reference's
+                                 transition_counts/); NULL builds the half tables on
+                                 the device with the GPU generator */
+    int verbose;              /* print load/progress lines to stdout */
+} bdc_options;
+
+typedef struct {
+    int64_t iters;            /* iterations done by this call */
+    int64_t total_iters;      /* iterations since the distribution was set */
+    double mx;                /* max_x log2 p'(x) - log2 p(x) of the last iteration (bits) */
+    double upper_bound;       /* max_x D(x) of the last iteration's D pass (bits): C <= this */
+    double rate;              /* sum_x p(x) D(x) of that iterate (bits) = I(p;W) */
+    double lse;               /* log2 sum_x p(x) 2^{D(x)} of that iterate (bits) */
+    int converged;            /* 1 when the last mx < a (the loop of main_BAA.cu:73 ends) */
+} bdc_stats;
+
+typedef struct bdc_handle* bdc_handle_t;
+
+void bdc_default_options(bdc_options* opts);
+const char* bdc_last_error(void);
+const char* bdc_version(void);
+
+/* ---------------------------------------------------------------- handle
+ * Replaces load_cache (backend/BAA.cu:183-188, decl. BAA.cuh:29) and its parts
+ * load_gpu_cache / compute_normalizers / load_log_counts (BAA.cu:27-178): the
+ * handle owns every device buffer, for one (n,k), until bdc_destroy.
+ * 1 <= k <= n <= 32 for the count engine; the factored engine needs k < n. */
+bdc_status bdc_create(int n, int k, const bdc_options* opts, bdc_handle_t* out);
+bdc_status bdc_destroy(bdc_handle_t h);
+bdc_status bdc_info(bdc_handle_t h, int* n, int* k, int64_t* num_reps, int* engine);
+
+/* canonical representatives, ascending (backend/main_BAA.cu:46-50) */
+bdc_status bdc_get_reps(bdc_handle_t h, uint32_t* reps, int64_t num_reps);
+
+/* starting distribution (backend/main_BAA.cu:59-65); not renormalised,
+ * like the reference.  Zero entries follow the reference's ln 0 = 0 rule. */
+bdc_status bdc_set_p(bdc_handle_t h, const double* p, int64_t num_reps);
+bdc_status bdc_set_p_uniform(bdc_handle_t h);           /* p = 1 / 2^n */
+bdc_status bdc_get_p(bdc_handle_t h, double* p, int64_t num_reps);
+/* device-pointer forms (the caller's memory on the handle's device) */
+bdc_status bdc_set_p_device(bdc_handle_t h, const double* p_dev, int64_t num_reps);
+bdc_status bdc_get_p_device(bdc_handle_t h, double* p_dev, int64_t num_reps);
+
+/* The BA loop body (backend/main_BAA.cu:73-109 with baa_iteration,
+ * BAA.cu:590-639 and compute_max_deviation, BAA.cu:916-946): runs iterations
+ * until mx < a or max_iters iterations, all on the device.  stats may be NULL. */
+bdc_status bdc_iterate(bdc_handle_t h, int64_t max_iters, double a, bdc_stats* stats);
+
+/* One reference-shaped iteration with host vectors: p_in -> p_out, like
+ * baa_iteration (BAA.cu:590-639, decl. BAA.cuh:295); p_out may equal p_in. */
+bdc_status bdc_baa_iteration(bdc_handle_t h, const double* p_in, double* p_out, int64_t num_reps);
+
+/* compute_all_log_D (BAA.cu:642-724, decl. BAA.cuh:314): ln q of the current p */
+bdc_status bdc_log_q(bdc_handle_t h, double* lnq, int64_t nq);
+/* compute_all_log_W (BAA.cu:727-814, decl. BAA.cuh:342): ln p + D for the
+ * current p and a caller-given ln q (NULL: ln q of the current p) */
+bdc_status bdc_log_w(bdc_handle_t h, const double* lnq, double* logw, int64_t num_reps);
+/* compute_KL_kernel (BAA.cu:533-571, decl. BAA.cuh:266): D(x) in nats for a
+ * caller-given ln q (NULL: ln q of the current p) */
+bdc_status bdc_divergence(bdc_handle_t h, const double* lnq, double* d, int64_t num_reps);
+/* compute_rate (BAA.cu:836-913, decl. BAA.cuh:348): sum |O| p D in nats with
+ * ln q of the current p */
+bdc_status bdc_rate(bdc_handle_t h, double* rate_nats);
+/* compute_max_deviation (BAA.cu:916-946, decl. BAA.cuh:361) on host vectors */
+bdc_status bdc_max_deviation(bdc_handle_t h, const double* p, const double* p_before,
+                             int64_t num_reps, double* mx);
+
+/* exact counts N(x,y) by the split identity (total_transitions, BAA.cu:340-395)
+ * for npairs host pairs; out[i] = N(xs[i], ys[i]) */
+bdc_status bdc_counts(bdc_handle_t h, const uint32_t* xs, const uint32_t* ys, int64_t npairs,
+                      uint32_t* out);
+
+/* ----------------------------------------------------------- measurement
+ * Algorithmic work of one pass over the channel matrix: nonzero_pairs =
+ * sum over representatives x of the number of distinct length-k
+ * subsequences of x (the pairs the reference enumerates, BAA.cu:460), and
+ * split_terms = number of split points j of total_transitions (BAA.cu:355). */
+bdc_status bdc_work(bdc_handle_t h, int64_t* nonzero_pairs, int* split_terms);
+
+typedef struct {
+    double ms_q;        /* q pass (count engine) or q-side products (factored) */
+    double ms_fold;     /* orbit fold of q and ln q */
+    double ms_d;        /* D pass (count engine) or D-side products + update (factored) */
+    double ms_update;   /* normalisation, mx and stop test */
+    double ms_iter;     /* whole iteration */
+    int iters;          /* iterations averaged */
+} bdc_profile_t;
+
+/* Runs `iters` iterations (a = -inf, so none stops early) with CUDA events
+ * around each pass on the handle's stream; averages in milliseconds.  The
+ * iterate advances like bdc_iterate. */
+bdc_status bdc_profile(bdc_handle_t h, int iters, bdc_profile_t* out);
+
+/* Run the handle's work on a caller-owned cudaStream_t (NULL: the handle's
+ * own stream), e.g. to order it with a framework's stream or to time it with
+ * events recorded on that stream. */
+bdc_status bdc_set_stream(bdc_handle_t h, void* cuda_stream);
+
+/* Device throughput probe: kind 0 = int32 multiply-add (IMAD), 1 = FP64 FMA,
+ * 2 = FP32 FMA.  Runs a register-resident chain kernel on `device` for about
+ * `ms` milliseconds and returns operations per second (one multiply-add = 1
+ * operation).  Used as the measured denominator of roofline fractions. */
+bdc_status bdc_peak_probe(int device, int kind, double ms, double* ops_per_s);
+
+/* ------------------------------------------------------- cache generator
+ * The table cache_{n,k} of generate_bit_transition_cache.cpp:46-77, computed on
+ * the device: out holds 2^{n+k} uint32, index (x << k) | y.  n + k <= 34. */
+bdc_status bdc_generate_cache(int n, int k, int device, uint32_t* out);
+
+/* ------------------------------------------------------------ file formats */
+/* read a cache_n_k file (cache_io.h:29-44): exactly 2^{n+k} entries */
+bdc_status bdc_read_cache_file(const char* path, int n, int k, uint32_t* out);
+/* write a cache_n_k file (cache_io.h:17-26) */
+bdc_status bdc_write_cache_file(const char* path, int n, int k, const uint32_t* data);
+/* read a dist file (main_BAA.cu:3-18); *count gets the number of values.
+ * With out == NULL only counts. */
+bdc_status bdc_read_dist_file(const char* path, double* out, int64_t cap, int64_t* count);
+/* write a dist file with "%.17g\n" per value, via a temporary file and rename */
+bdc_status bdc_write_dist_file(const char* path, const double* p, int64_t count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BDC_B200_H */
