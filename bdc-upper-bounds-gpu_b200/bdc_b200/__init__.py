@@ -56,7 +56,8 @@ class Options(ctypes.Structure):
 
 class Profile(ctypes.Structure):
     _fields_ = [("ms_q", ctypes.c_double), ("ms_fold", ctypes.c_double), ("ms_d", ctypes.c_double),
-                ("ms_update", ctypes.c_double), ("ms_iter", ctypes.c_double), ("iters", ctypes.c_int)]
+                ("ms_update", ctypes.c_double), ("ms_iter", ctypes.c_double), ("ms_main", ctypes.c_double),
+                ("work_main", ctypes.c_double), ("launches", ctypes.c_int), ("iters", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}

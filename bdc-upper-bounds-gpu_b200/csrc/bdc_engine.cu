@@ -90,7 +90,7 @@ int select_engine(int requested, int n, int k) {
     switch (requested) {
         case BDC_ENGINE_COUNT: return BDC_ENGINE_COUNT;
         case BDC_ENGINE_FACTORED: return factored_supports(n, k) ? BDC_ENGINE_FACTORED : -1;
-        case BDC_ENGINE_AUTO: return factored_supports(n, k) ? BDC_ENGINE_FACTORED : BDC_ENGINE_COUNT;
+        case BDC_ENGINE_AUTO: return BDC_ENGINE_COUNT;
         default: return -1;
     }
 }
@@ -368,6 +368,9 @@ bdc_status engine_profile(bdc_handle* H, int iters, bdc_profile_t* out) {
     out->ms_d = acc[2] / iters;
     out->ms_update = acc[3] / iters;
     out->ms_iter = tot / iters;
+    out->ms_main = out->ms_d;
+    out->work_main = (double)H->nonzero_pairs * (double)(H->s.jhi - H->s.jlo + 1);
+    out->launches = 6;
     out->iters = iters;
     return BDC_OK;
 }

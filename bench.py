@@ -197,7 +197,7 @@ def ours_arm(args) -> None:
     # warm-up, then K iterations timed with events on the stream the engine uses
     E.iterate(args.warmup, float("-inf"))
     prof = E.profile(2)
-    launches_per_iter = 6 if E.engine == "count" else prof.get("launches", 0)
+    launches_per_iter = prof["launches"]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         barrier()
@@ -238,18 +238,25 @@ def ours_arm(args) -> None:
     imad = bdc_b200.peak_probe("imad", local)
     dfma = bdc_b200.peak_probe("dfma", local)
     if E.engine == "count":
-        dom = "q pass" if prof["ms_q"] >= prof["ms_d"] else "D pass"
-        dom_ms = max(prof["ms_q"], prof["ms_d"])
-        work = pairs * S
-        roofline = {"bound": "int32 multiply-add pipe", "kernel": f"k_dpass/k_qpass ({dom})",
-                    "achieved": work / (dom_ms / 1e3) / 1e12, "peak": imad / 1e12, "unit": "Tops/s",
-                    "frac": work / (dom_ms / 1e3) / imad, "traffic": None,
-                    "work_per_launch": f"{pairs} nonzero (x,y) pairs x {S} split terms = {work:.3e} multiply-adds",
+        achieved = prof["work_main"] / (prof["ms_main"] / 1e3)
+        roofline = {"bound": "int32 multiply-add pipe (no tensor cores: exact integer counts)",
+                    "kernel": "k_dpass (D pass; the q pass k_qpass is the same count loop)",
+                    "achieved": achieved / 1e12, "peak": imad / 1e12, "unit": "Tops/s",
+                    "frac": achieved / imad, "traffic": None,
+                    "work_per_launch": f"{pairs} nonzero (x,y) pairs x {S} split terms = "
+                                       f"{prof['work_main']:.4e} multiply-adds",
                     "peak_source": "bdc_peak_probe int32 IMAD chain, measured in this run"}
     else:
-        roofline = prof.get("roofline", {})
+        achieved = prof["work_main"] / (prof["ms_main"] / 1e3)
+        roofline = {"bound": "fp64 FMA pipe (CUDA cores; sm_100 tensor cores have no FP64)",
+                    "kernel": "k_gemm_tile<128,128,8,4,2,1> (G = LA*RB fused with the BA update)",
+                    "achieved": achieved / 1e12, "peak": 2 * dfma / 1e12, "unit": "TFLOP/s",
+                    "frac": achieved / (2 * dfma), "traffic": None,
+                    "work_per_launch": f"2*H1*H2*K = {prof['work_main']:.4e} flops "
+                                       f"(H1=H2={1 << ((args.n + 1) // 2)}, K = sum of the term widths)",
+                    "peak_source": "bdc_peak_probe FP64 FMA chain, measured in this run (2 flops per FMA)"}
     upd_bytes = R * 72
-    roofline_update = {"bound": "hbm", "achieved": upd_bytes / (prof["ms_update"] / 1e3) / 1e9,
+    roofline_update = None if E.engine != "count" else {"bound": "hbm", "achieved": upd_bytes / (prof["ms_update"] / 1e3) / 1e9,
                        "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                        "frac": upd_bytes / (prof["ms_update"] / 1e3) / 1e9 / peaks.get("hbm_gbs"),
                        "traffic": None, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_src})",
@@ -270,7 +277,7 @@ def ours_arm(args) -> None:
                    "parallelism": f"replicas x{world}",
                    "l2": "working set per iteration > L2 (p, D, logW, h vectors of 33.6 MB each + 32 MB tables)"},
         "gpu_launches": launches_per_iter * args.steps,
-        "profile_ms": {k2: prof[k2] for k2 in ("ms_q", "ms_fold", "ms_d", "ms_update", "ms_iter")},
+        "profile_ms": {k2: prof[k2] for k2 in ("ms_q", "ms_fold", "ms_d", "ms_update", "ms_iter", "ms_main")},
         "roofline": roofline, "roofline_update": roofline_update,
         "peaks_measured": {"int32_madd_tops": imad / 1e12, "fp64_fma_tflops": 2 * dfma / 1e12},
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
@@ -281,6 +288,18 @@ def ours_arm(args) -> None:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def kernels_only(args) -> None:
+    """Engine set-up and `steps` iterations, nothing else: the command that
+    the ncu captures under profiles/ run."""
+    import bdc_b200
+    E = bdc_b200.Engine(args.n, args.k, engine=args.engine)
+    E.set_uniform()
+    st = E.iterate(args.steps, float("-inf"))
+    print(json.dumps({"engine": E.engine, "n": args.n, "k": args.k, "iters": st["iters"],
+                      "upper_bound_bits": st["upper_bound"]}))
+    E.close()
 
 
 def main() -> None:
@@ -294,10 +313,13 @@ def main() -> None:
     ap.add_argument("--engine", default="auto")
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mode", choices=["bench", "kernels"], default="bench")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.mode == "kernels":
+        kernels_only(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         ours_arm(args)

@@ -135,6 +135,11 @@ typedef struct {
     double ms_d;        /* D pass (count engine) or D-side products + update (factored) */
     double ms_update;   /* normalisation, mx and stop test */
     double ms_iter;     /* whole iteration */
+    double ms_main;     /* the dominant kernel alone: the D pass (count engine) or
+                           the fused D-side product G = LA * RB (factored engine) */
+    double work_main;   /* its algorithmic work per launch: split-term multiply-adds
+                           over the nonzero pairs (count) or FP64 flops (factored) */
+    int launches;       /* kernel launches per iteration */
     int iters;          /* iterations averaged */
 } bdc_profile_t;
 

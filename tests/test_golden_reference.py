@@ -1,0 +1,127 @@
+"""Parity with the reference's own BA outputs (tests/golden/ref_ba/*.npz,
+produced by backend/BAA.cu compiled unchanged and run on a B200, see
+tests/golden/make_golden.py).
+
+The CPU oracle is checked here without a GPU; the CUDA engine is checked
+against the same vectors under -m gpu.  Tolerances: ln q, logW and KL
+absolute 1e-11 (values of size 1..30, FP64 sums in a different order than the
+reference's atomics), p' relative 1e-11, mx absolute 1e-11, rate 1e-12.
+"""
+import glob
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "ref_ba", "*.npz")))
+NAMES = [os.path.basename(f)[7:-4] for f in FIXTURES]
+ATOL = 1e-11
+RTOL = 1e-11
+
+
+def vec(z, key):
+    """(indices or None, values) of a stored vector."""
+    if f"{key}.full" in z:
+        return None, z[f"{key}.full"]
+    return z[f"{key}.idx"], z[f"{key}.val"]
+
+
+def check_vec(z, key, got, rtol=0.0, atol=ATOL):
+    idx, val = vec(z, key)
+    g = got if idx is None else got[idx]
+    np.testing.assert_allclose(g, val, rtol=rtol, atol=atol, err_msg=key)
+    if idx is not None:
+        assert abs(np.sum(got) - float(z[f"{key}.sum"])) <= 1e-9 * max(1.0, abs(float(z[f"{key}.sum"]))), key
+
+
+def start_of(z):
+    sys.path.insert(0, GOLDEN)
+    from make_golden import start_vector
+    import oracle as O
+    n = int(z["n"])
+    spec = eval(str(z["start"]))
+    p0 = start_vector(n, spec)
+    if p0 is None:
+        p0 = np.full(len(O.canonicals(n)), 1.0 / (1 << n))
+    check_vec(z, "p_0", p0, rtol=0, atol=0)
+    return p0
+
+
+class OracleRunner:
+    def __init__(self, n, k, O):
+        self.n, self.k, self.O = n, k, O
+        self.reps = O.canonicals(n)
+
+    def step(self, p):
+        pn, lnq, lw = self.O.ba_iteration(self.n, self.k, p, self.reps)
+        return lnq, lw, pn, self.O.max_deviation(pn, p)
+
+    def final(self, p):
+        lnq = self.O.log_q(self.n, self.k, p, self.reps)
+        kl = self.O.kl(self.n, self.k, lnq, self.reps)
+        return lnq, kl, self.O.rate(self.n, self.k, lnq, p, self.reps)
+
+
+class EngineRunner:
+    def __init__(self, n, k, bdc, engine):
+        self.E = bdc.Engine(n, k, engine=engine)
+
+    def step(self, p):
+        self.E.set_p(p)
+        lnq = self.E.log_q()
+        lw = self.E.log_w()
+        st = self.E.iterate(1, float("-inf"))
+        pn = self.E.get_p()
+        return lnq, lw, pn, st["mx"]
+
+    def final(self, p):
+        self.E.set_p(p)
+        lnq = self.E.log_q()
+        return lnq, self.E.divergence(lnq), self.E.rate()
+
+
+def run_chain(z, runner, p):
+    iters = int(z["iters"])
+    for t in range(iters):
+        lnq, lw, pn, mx = runner.step(p)
+        check_vec(z, f"lnq_{t}", lnq)
+        check_vec(z, f"logw_{t}", lw)
+        check_vec(z, f"p_{t + 1}", pn, rtol=RTOL, atol=0)
+        ref_mx = float(z["mx"][t])
+        if np.isinf(ref_mx):
+            assert np.isinf(mx) and mx > 0
+        else:
+            assert abs(mx - ref_mx) < ATOL, (t, mx, ref_mx)
+        # continue from the reference's own iterate where it is stored in full
+        idx, val = vec(z, f"p_{t + 1}")
+        p = val if idx is None else pn
+    lnq, kl, rate = runner.final(p)
+    check_vec(z, "lnq_final", lnq)
+    check_vec(z, "kl_final", kl)
+    assert abs(rate - float(z["rate_nats"])) < 1e-12
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_matches_reference_ba(O, name):
+    z = np.load(os.path.join(GOLDEN, "ref_ba", f"ref_ba_{name}.npz"))
+    p0 = start_of(z)
+    run_chain(z, OracleRunner(int(z["n"]), int(z["k"]), O), p0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine", ["count", "factored"])
+@pytest.mark.parametrize("name", NAMES)
+def test_engine_matches_reference_ba(bdc, O, name, engine):
+    z = np.load(os.path.join(GOLDEN, "ref_ba", f"ref_ba_{name}.npz"))
+    n, k = int(z["n"]), int(z["k"])
+    if engine == "factored" and k >= n:
+        pytest.skip("the factored engine needs k < n")
+    p0 = start_of(z)
+    r = EngineRunner(n, k, bdc, engine)
+    try:
+        run_chain(z, r, p0)
+    finally:
+        r.E.close()
