@@ -90,7 +90,7 @@ int select_engine(int requested, int n, int k) {
     switch (requested) {
         case BDC_ENGINE_COUNT: return BDC_ENGINE_COUNT;
         case BDC_ENGINE_FACTORED: return factored_supports(n, k) ? BDC_ENGINE_FACTORED : -1;
-        case BDC_ENGINE_AUTO: return BDC_ENGINE_COUNT;
+        case BDC_ENGINE_AUTO: return factored_supports(n, k) ? BDC_ENGINE_FACTORED : BDC_ENGINE_COUNT;
         default: return -1;
     }
 }

@@ -34,6 +34,43 @@ namespace bdc {
 
 constexpr int kErrShift = 1;  // DevState::error: exp shift out of range, re-scale
 
+// q-side small product of one term: Q_t = sum_s a(s) (x) b(s), the outer
+// products of a(s) = a + s*a_stride (2^j entries) and b(s) = b + s*b_stride
+// (2^m entries), s over the contracted half (L terms: a = column of U_t,
+// b = row of B_m; R terms: a = row of A_j, b = row of V_t).
+struct OuterDesc {
+    const void* a;
+    const void* b;
+    int64_t a_stride, b_stride;
+    int a_u16, b_u16;
+    int j, m;
+    int S;           // length of the contracted range
+    int term;        // slice of qparts
+};
+
+// D-side small product of one term, one s at a time (Lq_t = ln q as 2^j x 2^m):
+//   L: out_s[yh] = sum_yl Lq_t[yh][yl] B_m[s][yl]   (column s of M_t -> RB)
+//   R: out_s[yl] = sum_yh A_j[s][yh] Lq_t[yh][yl]   (row s of N_t -> LA)
+struct MatvecDesc {
+    const uint16_t* v;  // bundle rows: v(s) = v + s * v_stride
+    int64_t v_stride;
+    double* out;        // element i of s at out[s * s_stride + i * i_stride]
+    int64_t s_stride, i_stride;
+    int j, m, left;
+    int S;
+    int cta_begin;
+};
+
+// how the fold reads Q_t: 0 = split slices in qparts, 1 = U^T rows (the
+// identity B of an L term), 2 = V rows (the identity A of an R term); the
+// identity terms of the D side are written by the fold as copies of ln q.
+struct FoldTerm {
+    int kind;
+    int j, m, off;
+    int idB_left;   // L term with identity B_m: RB rows [off, off+2^j) = Lq_t
+    int idA_right;  // R term with identity A_j: LA columns [KL+off, +2^m) = Lq_t
+};
+
 struct Term {
     int j, m;       // split point and the low sub-length k - j
     int left;       // 1: L term (contract x_hi first), 0: R term
@@ -51,21 +88,23 @@ struct FactoredState {
     double* hx = nullptr;     // [2^n]  h(x) at representatives
     double* LA = nullptr;     // [H1][Kp]  = [AL | NR]
     double* RB = nullptr;     // [Kp][H2]  = [ML ; BR^T]
-    double* UL = nullptr;     // [KL][H2]
+    double* UL = nullptr;     // [H2][KL]  (U^T: column c of AL^T Pw is row-contiguous)
     double* VR = nullptr;     // [H1][KR]
-    double* ulpart = nullptr; // [S1][KL][H2]
+    double* ulpart = nullptr; // [S1][H2][KL]
     double* vrpart = nullptr; // [S2][H1][KR]
     int S1 = 1, S2 = 1;
-    double* qparts = nullptr; // [T][2^k]
+    double* qparts = nullptr; // [T][QS][2^k]
+    int QS = 1;               // split of the s range of the small q products
     double* lnq_full = nullptr;  // [2^k]
     double* epart = nullptr;  // [ctas][4]
     int ctas_g = 0;
     // launch plans
     bdc::GemmDesc* d_big = nullptr;  int n_big = 0, tiles_big = 0;     // UL, VR partials
-    bdc::GemmDesc* d_qrows = nullptr; int n_qrows = 0, tiles_qrows = 0;
-    bdc::GemmDesc* d_qtile = nullptr; int n_qtile = 0, tiles_qtile = 0;
-    bdc::GemmDesc* d_drows = nullptr; int n_drows = 0, tiles_drows = 0;
-    bdc::GemmDesc* d_dtile = nullptr; int n_dtile = 0, tiles_dtile = 0;
+    bdc::OuterDesc* d_qsmall = nullptr; int n_qsmall = 0;   // q-side small products
+    bdc::MatvecDesc* d_dsmall = nullptr; int n_dsmall = 0;  // D-side small products
+    int dsmall_chunk = 64;                                  // s values per CTA
+    int ctas_dsmall = 0, smem_dsmall = 0;
+    bdc::FoldTerm* d_fold = nullptr;                        // per term: how the fold reads Q_t
     bdc::GemmDesc* d_g = nullptr;
     int launches_per_iter = 0;
 };
@@ -215,7 +254,8 @@ __global__ void __launch_bounds__(256) k_gemm_tile(const GemmDesc* __restrict__ 
     // ---- BA epilogue: rows are x_hi, columns x_lo, x = (x_hi << n2) | x_lo
     const double shift = st->shift;
     const double lnz = st->log_z;
-    double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0;
+    const double inv_z = exp(-lnz);
+    double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0, zero = 0.0;
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
         const int m = m0 + mbase + (i >> 1) * 8 + (i & 1);
@@ -228,7 +268,10 @@ __global__ void __launch_bounds__(256) k_gemm_tile(const GemmDesc* __restrict__ 
             if (!is_rep(x, ep.n)) continue;
             const double o = (double)orbit_size(x, ep.n);
             const double D = __ldg(ep.hx + x) - acc[i][j] * ep.inv_c;
-            const double lnp = ep.Lt[x] - lnz;
+            // an entry that is exactly 0 takes ln p = 0, as the reference's
+            // apply_log_kernel leaves ln 0 at 0 (backend/BAA.cu:573-580)
+            const double pw = ep.Pw[x];
+            const double lnp = (pw == 0.0) ? 0.0 : ep.Lt[x] - lnz;
             const double lw = lnp + D - shift;
             const double e = exp(lw);
             ep.Lt[x] = lw;
@@ -236,97 +279,161 @@ __global__ void __launch_bounds__(256) k_gemm_tile(const GemmDesc* __restrict__ 
             mD = fmax(mD, D);
             mL = fmax(mL, lw);
             sE = fma(o, e, sE);
-            sR = fma(o * exp(lnp), D, sR);
+            sR = fma(pw * inv_z, D, sR);
+            if (pw == 0.0) zero = 1.0;
         }
     }
-    // CTA reduction of the four partials
-    __shared__ double red[4][8];
+    // CTA reduction of the five partials
+    __shared__ double red[5][8];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         mD = fmax(mD, __shfl_xor_sync(0xFFFFFFFFu, mD, off));
         mL = fmax(mL, __shfl_xor_sync(0xFFFFFFFFu, mL, off));
         sE += __shfl_xor_sync(0xFFFFFFFFu, sE, off);
         sR += __shfl_xor_sync(0xFFFFFFFFu, sR, off);
+        zero = fmax(zero, __shfl_xor_sync(0xFFFFFFFFu, zero, off));
     }
     if (lane == 0) {
         red[0][warp] = mD;
         red[1][warp] = sE;
         red[2][warp] = mL;
         red[3][warp] = sR;
+        red[4][warp] = zero;
     }
     __syncthreads();
     if (tid == 0) {
-        double a0 = red[0][0], a1 = red[1][0], a2 = red[2][0], a3 = red[3][0];
+        double a0 = red[0][0], a1 = red[1][0], a2 = red[2][0], a3 = red[3][0], a4 = red[4][0];
         for (int w = 1; w < 8; ++w) {
             a0 = fmax(a0, red[0][w]);
             a1 += red[1][w];
             a2 = fmax(a2, red[2][w]);
             a3 += red[3][w];
+            a4 = fmax(a4, red[4][w]);
         }
-        double* p = ep.part + (size_t)blockIdx.x * 4;
+        double* p = ep.part + (size_t)blockIdx.x * 8;
         p[0] = a0;
         p[1] = a1;
         p[2] = a2;
         p[3] = a3;
+        p[4] = a4;
     }
 }
 
-// --------------------------------------------------------- few-row GEMM
-// Output rows M <= 8.  CTA = 64 columns x 4 K-slices; the chunk of B is
-// staged in shared memory whatever its storage order; A is broadcast.
-constexpr int kRowsMax = 8;
-constexpr int kRowsCols = 64;
-constexpr int kRowsKC = 32;
+// ------------------------------------------------- q-side small products
+// CTA = one (term, split of the s range); thread t owns OPT consecutive
+// outputs o = y = yh * 2^m + yl of Q_t and accumulates a(s)[yh] * b(s)[yl].
+__device__ __forceinline__ double ld_any(const void* p, int u16, int64_t i) {
+    return u16 ? (double)__ldg((const uint16_t*)p + i) : __ldg((const double*)p + i);
+}
 
-__global__ void __launch_bounds__(256) k_gemm_rows(const GemmDesc* __restrict__ descs, int ndesc,
-                                                   const DevState* st) {
+template <int OPT>
+__global__ void __launch_bounds__(256) k_qsmall(const OuterDesc* __restrict__ descs, int QS, int k,
+                                                double* __restrict__ qparts, const DevState* st) {
     if (gated(st)) return;
-    const int di = find_desc(descs, ndesc, blockIdx.x);
-    const GemmDesc& d = descs[di];
-    const Operand A = d.A, B = d.B;
-    const int M = d.M, N = d.N, K = d.K;
-    const int t = blockIdx.x - d.tile_begin;
-    const int n0 = t * kRowsCols;
-    __shared__ double As[kRowsMax][kRowsKC];
-    __shared__ double Bs[kRowsKC][kRowsCols + 1];
-    __shared__ double red[4][kRowsMax][kRowsCols];
-    const int tid = threadIdx.x;
-    const int col = tid & (kRowsCols - 1);
-    const int ks = tid >> 6;  // 0..3
-    const bool b_cols = !contiguous_in_rows(B);
-    double acc[kRowsMax];
+    const OuterDesc& d = descs[blockIdx.x / QS];
+    const int split = blockIdx.x % QS;
+    const int ny = 1 << k;
+    const int s0 = (int)((int64_t)d.S * split / QS), s1 = (int)((int64_t)d.S * (split + 1) / QS);
+    const int o0 = threadIdx.x * OPT;
+    if (o0 >= ny) return;
+    const int m = d.m;
+    const int mask = (1 << m) - 1;
+    double acc[OPT];
 #pragma unroll
-    for (int r = 0; r < kRowsMax; ++r) acc[r] = 0.0;
-    for (int k0 = 0; k0 < K; k0 += kRowsKC) {
-        for (int e = tid; e < kRowsMax * kRowsKC; e += 256) {
-            const int r = e / kRowsKC, kk = e % kRowsKC;
-            As[r][kk] = (r < M && k0 + kk < K) ? op_load(A, r, k0 + kk) : 0.0;
-        }
-        for (int e = tid; e < kRowsKC * kRowsCols; e += 256) {
-            const int kk = b_cols ? e / kRowsCols : e % kRowsKC;
-            const int nn = b_cols ? e % kRowsCols : e / kRowsKC;
-            const int n = n0 + nn, k = k0 + kk;
-            Bs[kk][nn] = (n < N && k < K) ? op_load(B, k, n) : 0.0;
-        }
-        __syncthreads();
+    for (int i = 0; i < OPT; ++i) acc[i] = 0.0;
+    if ((1 << m) >= OPT) {
+        // one yh, OPT consecutive yl
+        const int yh = o0 >> m, yl0 = o0 & mask;
+        for (int s = s0; s < s1; ++s) {
+            const double av = ld_any(d.a, d.a_u16, (int64_t)s * d.a_stride + yh);
+            const int64_t bb = (int64_t)s * d.b_stride + yl0;
 #pragma unroll
-        for (int kk = ks; kk < kRowsKC; kk += 4) {
-            const double b = Bs[kk][col];
-#pragma unroll
-            for (int r = 0; r < kRowsMax; ++r) acc[r] = fma(As[r][kk], b, acc[r]);
+            for (int i = 0; i < OPT; ++i) acc[i] = fma(av, ld_any(d.b, d.b_u16, bb + i), acc[i]);
         }
-        __syncthreads();
+    } else {
+        // OPT / 2^m consecutive yh, all 2^m yl
+        const int yh0 = o0 >> m;
+        for (int s = s0; s < s1; ++s) {
+            const int64_t ab = (int64_t)s * d.a_stride + yh0, bb = (int64_t)s * d.b_stride;
+#pragma unroll
+            for (int i = 0; i < OPT; ++i)
+                acc[i] = fma(ld_any(d.a, d.a_u16, ab + (i >> m)), ld_any(d.b, d.b_u16, bb + (i & mask)),
+                             acc[i]);
+        }
     }
+    double* out = qparts + ((size_t)d.term * QS + split) * ny + o0;
 #pragma unroll
-    for (int r = 0; r < kRowsMax; ++r) red[ks][r][col] = acc[r];
+    for (int i = 0; i < OPT; ++i) out[i] = acc[i];
+}
+
+// ------------------------------------------------- D-side small products
+// CTA = one term and a chunk of s; Lq_t staged in shared memory with row
+// stride 2^m + 1; one warp per s.
+__global__ void __launch_bounds__(256) k_dsmall(const MatvecDesc* __restrict__ descs, int nd, int chunk,
+                                                const double* __restrict__ lnq_full, const DevState* st) {
+    if (gated(st)) return;
+    int di = 0;
+    while (di + 1 < nd && descs[di + 1].cta_begin <= (int)blockIdx.x) ++di;
+    const MatvecDesc& d = descs[di];
+    const int c = blockIdx.x - d.cta_begin;
+    const int nj = 1 << d.j, nm = 1 << d.m;
+    const int rs = nm + 1;
+    extern __shared__ double lq[];  // [nj][nm + 1]
+    for (int e = threadIdx.x; e < nj * nm; e += blockDim.x) lq[(e >> d.m) * rs + (e & (nm - 1))] = lnq_full[e];
     __syncthreads();
-    for (int e = tid; e < kRowsMax * kRowsCols; e += 256) {
-        const int r = e / kRowsCols, c = e % kRowsCols;
-        const int n = n0 + c;
-        if (r >= M || n >= N) continue;
-        const double v = d.alpha * (red[0][r][c] + red[1][r][c] + red[2][r][c] + red[3][r][c]);
-        double* cp = d.C + (int64_t)r * d.ldc_m + (int64_t)n * d.ldc_n;
-        *cp = d.accumulate ? *cp + v : v;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sb = c * chunk, se = min(sb + chunk, d.S);
+    for (int s = sb + warp; s < se; s += 8) {
+        const uint16_t* v = d.v + (int64_t)s * d.v_stride;
+        double* out = d.out + (int64_t)s * d.s_stride;
+        if (d.left) {
+            // out[yh] = sum_yl Lq[yh][yl] v[yl]
+            if (nj >= 32) {
+                for (int yh = lane; yh < nj; yh += 32) {
+                    double acc = 0.0;
+                    const double* row = lq + yh * rs;
+                    for (int yl = 0; yl < nm; ++yl) acc = fma(row[yl], (double)__ldg(v + yl), acc);
+                    out[(int64_t)yh * d.i_stride] = acc;
+                }
+            } else {
+                for (int yh = 0; yh < nj; ++yh) {
+                    double acc = 0.0;
+                    const double* row = lq + yh * rs;
+                    for (int yl = lane; yl < nm; yl += 32) acc = fma(row[yl], (double)__ldg(v + yl), acc);
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, off);
+                    if (lane == 0) out[(int64_t)yh * d.i_stride] = acc;
+                }
+            }
+        } else {
+            // out[yl] = sum_yh v[yh] Lq[yh][yl]
+            if (nm >= 32) {
+                for (int yl = lane; yl < nm; yl += 32) {
+                    double acc = 0.0;
+                    for (int yh = 0; yh < nj; ++yh) acc = fma((double)__ldg(v + yh), lq[yh * rs + yl], acc);
+                    out[(int64_t)yl * d.i_stride] = acc;
+                }
+            } else {
+                double acc[32];
+#pragma unroll
+                for (int yl = 0; yl < 32; ++yl) acc[yl] = 0.0;
+                for (int yh = lane; yh < nj; yh += 32) {
+                    const double vv = (double)__ldg(v + yh);
+                    const double* row = lq + yh * rs;
+#pragma unroll
+                    for (int yl = 0; yl < 32; ++yl)
+                        if (yl < nm) acc[yl] = fma(vv, row[yl], acc[yl]);
+                }
+#pragma unroll
+                for (int yl = 0; yl < 32; ++yl) {
+                    if (yl >= nm) break;
+                    double a = acc[yl];
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xFFFFFFFFu, a, off);
+                    if (lane == 0) out[(int64_t)yl * d.i_stride] = a;
+                }
+            }
+        }
     }
 }
 
@@ -351,10 +458,27 @@ __global__ void k_sum_parts(const double* __restrict__ a, int sa, int64_t na, do
     }
 }
 
-// acc[y] = sum_t qparts[t][y]; q(rep r) = sum_{y in O(r)} acc[y] / (|O(r)| C Z);
-// ln q with the reference's 0 for q == 0; expanded to every y.
-__global__ void k_fold_q(const double* __restrict__ qparts, int T, int k, double inv_c,
-                         double* __restrict__ lnq_full, double* __restrict__ lnq, const DevState* st) {
+// q(rep r) = sum_{y in O(r)} acc[y] / (|O(r)| C Z) with acc[y] = sum over
+// terms of Q_t[y] (split slices, or U^T / V rows for identity terms); ln q
+// with the reference's 0 for q == 0 (backend/BAA.cu:573-580), expanded to
+// every y, and copied into RB / LA where a D-side product is the identity.
+__device__ __forceinline__ double term_value(const FoldTerm& f, const double* qparts, int QS, int t, int ny,
+                                             const double* ULt, int KL, const double* VR, int KR, uint32_t y) {
+    if (f.kind == 0) {
+        double a = 0.0;
+        const double* q = qparts + (size_t)t * QS * ny + y;
+        for (int sp = 0; sp < QS; ++sp) a += q[(size_t)sp * ny];
+        return a;
+    }
+    const uint32_t yh = y >> f.m, yl = y & ((1u << f.m) - 1u);
+    if (f.kind == 1) return ULt[(size_t)yl * KL + f.off + yh];  // Q_t = U_t
+    return VR[(size_t)yh * KR + f.off + yl];                    // Q_t = V_t
+}
+
+__global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ qparts, int QS,
+                         const double* __restrict__ ULt, int KL, const double* __restrict__ VR, int KR, int k,
+                         double inv_c, double* __restrict__ lnq_full, double* __restrict__ lnq,
+                         double* __restrict__ RB, int H2, double* __restrict__ LA, int Kp, const DevState* st) {
     if (gated(st)) return;
     const int ny = 1 << k;
     const double inv_z = exp(-st->log_z);
@@ -369,29 +493,37 @@ __global__ void k_fold_q(const double* __restrict__ qparts, int T, int k, double
         if (rcv != r && rcv != rv && rcv != cv) mem[nm++] = rcv;
         double acc = 0.0;
         for (int e = 0; e < nm; ++e)
-            for (int t = 0; t < T; ++t) acc += qparts[(size_t)t * ny + mem[e]];
+            for (int t = 0; t < T; ++t) acc += term_value(terms[t], qparts, QS, t, ny, ULt, KL, VR, KR, mem[e]);
         const double q = acc * inv_c * inv_z / (double)nm;
         const double lq = (q != 0.0) ? log(q) : 0.0;
         lnq_full[y] = lq;
         if ((uint32_t)y == r) lnq[y] = lq;  // representatives are < 2^{k-1}
+        for (int t = 0; t < T; ++t) {
+            const FoldTerm& f = terms[t];
+            const uint32_t yh = (uint32_t)y >> f.m, yl = (uint32_t)y & ((1u << f.m) - 1u);
+            if (f.idB_left) RB[(size_t)(f.off + yh) * H2 + yl] = lq;   // M_t = Lq_t
+            if (f.idA_right) LA[(size_t)yh * Kp + KL + f.off + yl] = lq;  // N_t = Lq_t
+        }
     }
 }
 
 __global__ void __launch_bounds__(256)
 k_fac_finalize(const double* __restrict__ part, int nb, double a, DevState* st) {
     if (gated(st)) return;
-    __shared__ double red[4][256];
-    double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0;
+    __shared__ double red[5][256];
+    double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0, zero = 0.0;
     for (int b = threadIdx.x; b < nb; b += 256) {
-        mD = fmax(mD, part[(size_t)b * 4 + 0]);
-        sE += part[(size_t)b * 4 + 1];
-        mL = fmax(mL, part[(size_t)b * 4 + 2]);
-        sR += part[(size_t)b * 4 + 3];
+        mD = fmax(mD, part[(size_t)b * 8 + 0]);
+        sE += part[(size_t)b * 8 + 1];
+        mL = fmax(mL, part[(size_t)b * 8 + 2]);
+        sR += part[(size_t)b * 8 + 3];
+        zero = fmax(zero, part[(size_t)b * 8 + 4]);
     }
     red[0][threadIdx.x] = mD;
     red[1][threadIdx.x] = sE;
     red[2][threadIdx.x] = mL;
     red[3][threadIdx.x] = sR;
+    red[4][threadIdx.x] = zero;
     __syncthreads();
     for (int s = 128; s > 0; s >>= 1) {
         if (threadIdx.x < s) {
@@ -399,6 +531,7 @@ k_fac_finalize(const double* __restrict__ part, int nb, double a, DevState* st) 
             red[1][threadIdx.x] += red[1][threadIdx.x + s];
             red[2][threadIdx.x] = fmax(red[2][threadIdx.x], red[2][threadIdx.x + s]);
             red[3][threadIdx.x] += red[3][threadIdx.x + s];
+            red[4][threadIdx.x] = fmax(red[4][threadIdx.x], red[4][threadIdx.x + s]);
         }
         __syncthreads();
     }
@@ -407,6 +540,7 @@ k_fac_finalize(const double* __restrict__ part, int nb, double a, DevState* st) 
     sE = red[1][0];
     mL = red[2][0];
     sR = red[3][0];
+    st->zero_p = (red[4][0] != 0.0);
     if (!(sE > 0.0) || !isfinite(sE) || mL > 600.0 || mL < -600.0) {
         st->error = kErrShift;  // e over/underflowed: re-scale from Lt, then finish
         st->max_logw = mL;      // relative to shift; k_fac_rescale subtracts it
@@ -561,31 +695,12 @@ __global__ void k_fill_tables(int H1, int H2, int Kp, const uint16_t* __restrict
 }
 
 // ------------------------------------------------------------ planning
-using TileBig = void (*)(const GemmDesc*, int, BaEpilogue, const DevState*);
-
 static Operand op_f64(const double* p, int64_t ld, int trans) {
     Operand o;
     o.ptr = p;
     o.ld = ld;
     o.kind = OP_F64;
     o.trans = trans;
-    return o;
-}
-static Operand op_u16(const uint16_t* p, int64_t ld, int trans) {
-    Operand o;
-    o.ptr = p;
-    o.ld = ld;
-    o.kind = OP_U16;
-    o.trans = trans;
-    return o;
-}
-static Operand op_eye() {
-    Operand o;
-    o.kind = OP_EYE;
-    return o;
-}
-static Operand op_t(Operand o) {
-    if (o.kind != OP_EYE) o.trans ^= 1;
     return o;
 }
 
@@ -604,26 +719,6 @@ static GemmDesc make_desc(Operand A, Operand B, double* C, int64_t ldc_m, int64_
     return d;
 }
 
-// C^T = B^T A^T: the same product with the roles of rows and columns swapped
-static GemmDesc transposed(const GemmDesc& d) {
-    GemmDesc t = make_desc(op_t(d.B), op_t(d.A), d.C, d.ldc_n, d.ldc_m, d.N, d.M, d.K);
-    t.alpha = d.alpha;
-    t.accumulate = d.accumulate;
-    return t;
-}
-
-struct Plan {
-    std::vector<GemmDesc> rows, tiles;
-};
-
-// route one small product to the few-row kernel (after transposing if it is
-// the column count that is small) or to the 64x64 tile kernel
-static void route(Plan& P, const GemmDesc& d) {
-    if (d.M <= kRowsMax) P.rows.push_back(d);
-    else if (d.N <= kRowsMax) P.rows.push_back(transposed(d));
-    else P.tiles.push_back(d);
-}
-
 static int assign_tiles(std::vector<GemmDesc>& v, int bm, int bn) {
     int t = 0;
     for (auto& d : v) {
@@ -635,28 +730,23 @@ static int assign_tiles(std::vector<GemmDesc>& v, int bm, int bn) {
     return t;
 }
 
-static int assign_rows(std::vector<GemmDesc>& v) {
-    int t = 0;
-    for (auto& d : v) {
-        d.tiles_m = 1;
-        d.tiles_n = (d.N + kRowsCols - 1) / kRowsCols;
-        d.tile_begin = t;
-        t += d.tiles_n;
-    }
-    return t;
-}
-
-static cudaError_t upload(std::vector<GemmDesc>& v, GemmDesc** dst) {
+template <typename T>
+static cudaError_t upload(const std::vector<T>& v, T** dst) {
     if (v.empty()) return cudaSuccess;
-    cudaError_t e = cudaMalloc(dst, sizeof(GemmDesc) * v.size());
+    cudaError_t e = cudaMalloc(dst, sizeof(T) * v.size());
     if (e != cudaSuccess) return e;
-    return cudaMemcpy(*dst, v.data(), sizeof(GemmDesc) * v.size(), cudaMemcpyHostToDevice);
+    return cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
 }
 
 bool factored_supports(int n, int k) {
-    // needs k < n (W is not the identity), half lengths that fit the uint16
+    // needs k < n (W is not the identity), half tables that fit the uint16
     // bundles, and a dense 2^n state that fits comfortably in device memory
-    return k >= 1 && k < n && n >= 4 && n <= 28 && k <= 14;
+    return k >= 1 && k < n && n >= 2 && n <= 28 && k <= 14;
+}
+
+static int qsmall_opt(int k) {
+    const int ny = 1 << k;
+    return ny >= 256 ? ny / 256 : 1;
 }
 
 bdc_status factored_init(bdc_handle* H) {
@@ -678,12 +768,10 @@ bdc_status factored_init(bdc_handle* H) {
         t.left = t.idB ? 1 : (t.idA ? 0 : (j <= t.m));
         F->terms.push_back(t);
     }
-    for (auto& t : F->terms) {
+    for (auto& t : F->terms)
         if (t.left) { t.off = KL; KL += 1 << t.j; }
-    }
-    for (auto& t : F->terms) {
+    for (auto& t : F->terms)
         if (!t.left) { t.off = KR; KR += 1 << t.m; }
-    }
     F->KL = KL;
     F->KR = KR;
     F->Kp = (KL + KR + 7) / 8 * 8;
@@ -691,8 +779,14 @@ bdc_status factored_init(bdc_handle* H) {
     const int64_t NX = (int64_t)1 << H->n;
     const int ny = 1 << k;
     const int H1 = F->H1, H2 = F->H2, Kp = F->Kp;
+    const int KLa = KL > 0 ? KL : 1, KRa = KR > 0 ? KR : 1;
 
-    // device buffers
+    // small q products: split the contracted range so the launch fills the GPU
+    int n_outer = 0;
+    for (auto& t : F->terms) n_outer += (t.left ? !t.idB : !t.idA);
+    F->QS = n_outer > 0 ? std::max(1, std::min(64, (H->num_sms * 4) / n_outer)) : 1;
+    while (F->QS > 1 && (std::min(H1, H2) / F->QS) < 16) F->QS /= 2;
+
     auto al = [&](double** p, size_t cnt) -> cudaError_t {
         H->bytes += cnt * sizeof(double);
         return cudaMalloc(p, cnt * sizeof(double) + 16);
@@ -702,35 +796,39 @@ bdc_status factored_init(bdc_handle* H) {
     BDC_CUDA_TRY(al(&F->hx, NX));
     BDC_CUDA_TRY(al(&F->LA, (size_t)H1 * Kp));
     BDC_CUDA_TRY(al(&F->RB, (size_t)Kp * H2));
-    BDC_CUDA_TRY(al(&F->UL, (size_t)(KL > 0 ? KL : 1) * H2));
-    BDC_CUDA_TRY(al(&F->VR, (size_t)H1 * (KR > 0 ? KR : 1)));
-    // split-K so that the two thin products fill the GPU
-    F->S1 = KL > 0 ? std::max(1, std::min(32, (H->num_sms * 4) / std::max(1, ((KL + 127) / 128) * ((H2 + 127) / 128)))) : 1;
-    F->S2 = KR > 0 ? std::max(1, std::min(32, (H->num_sms * 4) / std::max(1, ((H1 + 127) / 128) * ((KR + 127) / 128)))) : 1;
-    while (F->S1 > 1 && H1 % F->S1) --F->S1;
-    while (F->S2 > 1 && H2 % F->S2) --F->S2;
-    BDC_CUDA_TRY(al(&F->ulpart, (size_t)F->S1 * (KL > 0 ? KL : 1) * H2));
-    BDC_CUDA_TRY(al(&F->vrpart, (size_t)F->S2 * H1 * (KR > 0 ? KR : 1)));
-    BDC_CUDA_TRY(al(&F->qparts, (size_t)F->T * ny));
+    BDC_CUDA_TRY(al(&F->UL, (size_t)H2 * KLa));
+    BDC_CUDA_TRY(al(&F->VR, (size_t)H1 * KRa));
+    // split-K of the two thin products so that they fill the GPU
+    const int tiles_ul = ((KL + 127) / 128) * ((H2 + 127) / 128);
+    const int tiles_vr = ((H1 + 127) / 128) * ((KR + 127) / 128);
+    F->S1 = KL > 0 ? std::max(1, std::min(32, (H->num_sms * 4) / std::max(1, tiles_ul))) : 1;
+    F->S2 = KR > 0 ? std::max(1, std::min(32, (H->num_sms * 4) / std::max(1, tiles_vr))) : 1;
+    while (F->S1 > 1 && (H1 % F->S1 || H1 / F->S1 < 8)) --F->S1;
+    while (F->S2 > 1 && (H2 % F->S2 || H2 / F->S2 < 8)) --F->S2;
+    BDC_CUDA_TRY(al(&F->ulpart, (size_t)F->S1 * H2 * KLa));
+    BDC_CUDA_TRY(al(&F->vrpart, (size_t)F->S2 * H1 * KRa));
+    BDC_CUDA_TRY(al(&F->qparts, (size_t)F->T * F->QS * ny));
     BDC_CUDA_TRY(al(&F->lnq_full, (size_t)ny));
     F->ctas_g = ((H1 + 127) / 128) * ((H2 + 127) / 128);
-    BDC_CUDA_TRY(al(&F->epart, (size_t)std::max(F->ctas_g, 2 * H->nb_upd) * 4));
+    BDC_CUDA_TRY(al(&F->epart, (size_t)std::max(F->ctas_g * 2, 2 * H->nb_upd) * 4));
     BDC_CUDA_TRY(cudaMemsetAsync(F->LA, 0, sizeof(double) * H1 * Kp, H->stream));
     BDC_CUDA_TRY(cudaMemsetAsync(F->RB, 0, sizeof(double) * Kp * H2, H->stream));
     BDC_CUDA_TRY(cudaMemsetAsync(F->hx, 0, sizeof(double) * NX, H->stream));
     BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
     BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
+    BDC_CUDA_TRY(cudaMemsetAsync(F->qparts, 0, sizeof(double) * F->T * F->QS * ny, H->stream));
 
-    // constant table columns
+    // constant table columns of LA (AL) and rows of RB (BR^T)
     {
-        std::vector<int> colmap(KL + KR);
+        std::vector<int> colmap(KL + KR + 1);
         for (auto& t : F->terms) {
             if (t.left) for (int c = 0; c < (1 << t.j); ++c) colmap[t.off + c] = bundle_offset(t.j) + c;
             else for (int c = 0; c < (1 << t.m); ++c) colmap[KL + t.off + c] = bundle_offset(t.m) + c;
         }
         int* d_cm = nullptr;
-        BDC_CUDA_TRY(cudaMalloc(&d_cm, sizeof(int) * (colmap.size() + 1)));
+        BDC_CUDA_TRY(cudaMalloc(&d_cm, sizeof(int) * colmap.size()));
         BDC_CUDA_TRY(cudaMemcpy(d_cm, colmap.data(), sizeof(int) * colmap.size(), cudaMemcpyHostToDevice));
+        // a left term's A_j or a right term's B_m is never the identity
         k_fill_tables<<<H->num_sms * 8, 256, 0, H->stream>>>(H1, H2, Kp, H->A.rows, H->A.stride, H->B.rows,
                                                             H->B.stride, d_cm, KL, KR, F->LA, F->RB);
         BDC_CUDA_TRY(cudaGetLastError());
@@ -740,15 +838,16 @@ bdc_status factored_init(bdc_handle* H) {
     k_scatter<<<H->num_sms * 8, 256, 0, H->stream>>>(H->d_reps, H->R, H->d_h, F->hx);
     BDC_CUDA_TRY(cudaGetLastError());
 
-    // ---- plan 1: UL = AL^T Pw and VR = Pw BR, split over the contraction
+    // ---- the two thin products, split over the contraction:
+    //   U^T (H2 x KL) = (AL^T Pw)^T and V (H1 x KR) = Pw BR
     std::vector<GemmDesc> big;
     if (KL > 0) {
         const int kc = H1 / F->S1;
         for (int sidx = 0; sidx < F->S1; ++sidx) {
-            // A(m = col c, kk = x_hi) = LA[x_hi * Kp + c]; B(kk = x_hi, n = x_lo) = Pw
+            // A(m = c, kk = x_hi) = LA[x_hi * Kp + c]; B(kk = x_hi, n = x_lo) = Pw; C(c, x_lo) -> U^T[x_lo][c]
             Operand A = op_f64(F->LA + (int64_t)sidx * kc * Kp, Kp, 1);
             Operand B = op_f64(F->Pw + (int64_t)sidx * kc * H2, H2, 0);
-            big.push_back(make_desc(A, B, F->ulpart + (size_t)sidx * KL * H2, H2, 1, KL, H2, kc));
+            big.push_back(make_desc(A, B, F->ulpart + (size_t)sidx * H2 * KL, 1, KL, KL, H2, kc));
         }
     }
     if (KR > 0) {
@@ -764,55 +863,102 @@ bdc_status factored_init(bdc_handle* H) {
     F->tiles_big = assign_tiles(big, 128, 128);
     BDC_CUDA_TRY(upload(big, &F->d_big));
 
-    // ---- plan 2: q parts Q_t (2^j x 2^m, row-major = flat y order)
-    Plan pq, pd;
+    // ---- per-term small products and the fold plan
+    std::vector<OuterDesc> outer;
+    std::vector<MatvecDesc> mv;
+    std::vector<FoldTerm> fold;
+    int cta = 0;
     for (int ti = 0; ti < F->T; ++ti) {
         const Term& t = F->terms[ti];
-        const int nj = 1 << t.j, nm = 1 << t.m;
-        double* C = F->qparts + (size_t)ti * ny;
+        FoldTerm f{};
+        f.j = t.j;
+        f.m = t.m;
+        f.off = t.off;
         if (t.left) {
-            Operand A = op_f64(F->UL + (int64_t)t.off * H2, H2, 0);  // U_t(yh, x_lo)
-            Operand B = t.idB ? op_eye() : op_u16(H->B.rows + bundle_offset(t.m), H->B.stride, 0);
-            route(pq, make_desc(A, B, C, nm, 1, nj, nm, H2));
+            if (t.idB) {
+                f.kind = 1;       // Q_t = U_t
+                f.idB_left = 1;   // M_t = Lq_t
+            } else {
+                OuterDesc o{};
+                o.a = F->UL + t.off;                       // a(s)[yh] = U^T[s][off + yh]
+                o.a_stride = KL;
+                o.a_u16 = 0;
+                o.b = H->B.rows + bundle_offset(t.m);      // b(s)[yl] = B_m[s][yl]
+                o.b_stride = H->B.stride;
+                o.b_u16 = 1;
+                o.j = t.j;
+                o.m = t.m;
+                o.S = H2;
+                o.term = ti;
+                outer.push_back(o);
+                MatvecDesc d{};
+                d.v = H->B.rows + bundle_offset(t.m);
+                d.v_stride = H->B.stride;
+                d.out = F->RB + (int64_t)t.off * H2;       // M_t[yh][s] -> RB[off + yh][s]
+                d.s_stride = 1;
+                d.i_stride = H2;
+                d.j = t.j;
+                d.m = t.m;
+                d.left = 1;
+                d.S = H2;
+                d.cta_begin = cta;
+                cta += (H2 + F->dsmall_chunk - 1) / F->dsmall_chunk;
+                mv.push_back(d);
+            }
         } else {
-            Operand A = t.idA ? op_eye() : op_u16(H->A.rows + bundle_offset(t.j), H->A.stride, 1);
-            Operand B = op_f64(F->VR + t.off, KR, 0);  // V_t(x_hi, yl)
-            route(pq, make_desc(A, B, C, nm, 1, nj, nm, H1));
+            if (t.idA) {
+                f.kind = 2;        // Q_t = V_t
+                f.idA_right = 1;   // N_t = Lq_t
+            } else {
+                OuterDesc o{};
+                o.a = H->A.rows + bundle_offset(t.j);      // a(s)[yh] = A_j[s][yh]
+                o.a_stride = H->A.stride;
+                o.a_u16 = 1;
+                o.b = F->VR + t.off;                       // b(s)[yl] = V[s][off + yl]
+                o.b_stride = KR;
+                o.b_u16 = 0;
+                o.j = t.j;
+                o.m = t.m;
+                o.S = H1;
+                o.term = ti;
+                outer.push_back(o);
+                MatvecDesc d{};
+                d.v = H->A.rows + bundle_offset(t.j);
+                d.v_stride = H->A.stride;
+                d.out = F->LA + KL + t.off;                // N_t[s][yl] -> LA[s][KL + off + yl]
+                d.s_stride = Kp;
+                d.i_stride = 1;
+                d.j = t.j;
+                d.m = t.m;
+                d.left = 0;
+                d.S = H1;
+                d.cta_begin = cta;
+                cta += (H1 + F->dsmall_chunk - 1) / F->dsmall_chunk;
+                mv.push_back(d);
+            }
         }
-        // D-side operands
-        Operand Lq = op_f64(F->lnq_full, nm, 0);  // Lq_t(yh, yl)
-        if (t.left) {
-            // M_t (2^j x H2) = Lq_t B_m^T -> RB rows [off, off + 2^j)
-            Operand B = t.idB ? op_eye() : op_u16(H->B.rows + bundle_offset(t.m), H->B.stride, 1);
-            route(pd, make_desc(Lq, B, F->RB + (int64_t)t.off * H2, H2, 1, nj, H2, nm));
-        } else {
-            // N_t (H1 x 2^m) = A_j Lq_t -> LA columns [KL + off, + 2^m)
-            Operand A = t.idA ? op_eye() : op_u16(H->A.rows + bundle_offset(t.j), H->A.stride, 0);
-            route(pd, make_desc(A, Lq, F->LA + KL + t.off, Kp, 1, H1, nm, nj));
-        }
+        fold.push_back(f);
     }
-    F->n_qrows = (int)pq.rows.size();
-    F->tiles_qrows = assign_rows(pq.rows);
-    F->n_qtile = (int)pq.tiles.size();
-    F->tiles_qtile = assign_tiles(pq.tiles, 64, 64);
-    F->n_drows = (int)pd.rows.size();
-    F->tiles_drows = assign_rows(pd.rows);
-    F->n_dtile = (int)pd.tiles.size();
-    F->tiles_dtile = assign_tiles(pd.tiles, 64, 64);
-    BDC_CUDA_TRY(upload(pq.rows, &F->d_qrows));
-    BDC_CUDA_TRY(upload(pq.tiles, &F->d_qtile));
-    BDC_CUDA_TRY(upload(pd.rows, &F->d_drows));
-    BDC_CUDA_TRY(upload(pd.tiles, &F->d_dtile));
+    F->n_qsmall = (int)outer.size();
+    F->n_dsmall = (int)mv.size();
+    F->ctas_dsmall = cta;
+    int max_smem = 0;
+    for (auto& d : mv) max_smem = std::max(max_smem, (int)(sizeof(double) * (1 << d.j) * ((1 << d.m) + 1)));
+    F->smem_dsmall = max_smem;
+    if (max_smem > 48 * 1024)
+        BDC_CUDA_TRY(cudaFuncSetAttribute(k_dsmall, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+    BDC_CUDA_TRY(upload(outer, &F->d_qsmall));
+    BDC_CUDA_TRY(upload(mv, &F->d_dsmall));
+    BDC_CUDA_TRY(upload(fold, &F->d_fold));
 
-    // ---- plan 3: G = LA RB with the BA epilogue
+    // ---- G = LA RB with the BA epilogue
     {
         std::vector<GemmDesc> g;
         g.push_back(make_desc(op_f64(F->LA, Kp, 0), op_f64(F->RB, H2, 0), nullptr, 0, 0, H1, H2, Kp));
         assign_tiles(g, 128, 128);
         BDC_CUDA_TRY(upload(g, &F->d_g));
     }
-    F->launches_per_iter = 1 + 1 + (F->n_qrows > 0) + (F->n_qtile > 0) + 1 + (F->n_drows > 0) +
-                           (F->n_dtile > 0) + 1 + 1;
+    F->launches_per_iter = (F->n_big > 0 ? 2 : 1) + (F->n_qsmall > 0) + 1 + (F->n_dsmall > 0) + 1 + 1;
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
 }
@@ -823,7 +969,11 @@ void factored_free(bdc_handle* H) {
     for (double* p : {F->Pw, F->Lt, F->hx, F->LA, F->RB, F->UL, F->VR, F->ulpart, F->vrpart, F->qparts,
                       F->lnq_full, F->epart})
         cudaFree(p);
-    for (GemmDesc* p : {F->d_big, F->d_qrows, F->d_qtile, F->d_drows, F->d_dtile, F->d_g}) cudaFree(p);
+    cudaFree(F->d_big);
+    cudaFree(F->d_g);
+    cudaFree(F->d_qsmall);
+    cudaFree(F->d_dsmall);
+    cudaFree(F->d_fold);
     delete F;
     H->fac = nullptr;
 }
@@ -845,34 +995,50 @@ static BaEpilogue make_epilogue(bdc_handle* H) {
 // the stages of one iteration, each gated by DevState::done / error
 enum Stage { ST_QBIG = 0, ST_QSMALL, ST_FOLD, ST_DSMALL, ST_G, ST_FIN, ST_COUNT };
 
+static cudaError_t launch_qsmall(bdc_handle* H) {
+    FactoredState* F = H->fac;
+    const int grid = F->n_qsmall * F->QS;
+    switch (qsmall_opt(H->k)) {
+        case 1: k_qsmall<1><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
+        case 2: k_qsmall<2><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
+        case 4: k_qsmall<4><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
+        case 8: k_qsmall<8><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
+        case 16: k_qsmall<16><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
+        case 32: k_qsmall<32><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
+        case 64: k_qsmall<64><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
     FactoredState* F = H->fac;
     cudaStream_t s = H->stream;
     const BaEpilogue ep = make_epilogue(H);
     switch (stage) {
         case ST_QBIG: {
-            if (F->n_big > 0)
+            if (F->n_big > 0) {
                 k_gemm_tile<128, 128, 8, 4, 2, 0><<<F->tiles_big, 256, 0, s>>>(F->d_big, F->n_big, ep, H->d_st);
-            const int64_t na = (int64_t)F->KL * F->H2, nb = (int64_t)F->H1 * F->KR;
-            k_sum_parts<<<H->num_sms * 4, 256, 0, s>>>(F->ulpart, F->S1, F->KL > 0 ? na : 0, F->UL, F->vrpart,
-                                                       F->S2, F->KR > 0 ? nb : 0, F->VR, H->d_st);
+                const int64_t na = (int64_t)F->KL * F->H2, nb = (int64_t)F->H1 * F->KR;
+                k_sum_parts<<<H->num_sms * 4, 256, 0, s>>>(F->ulpart, F->S1, F->KL > 0 ? na : 0, F->UL, F->vrpart,
+                                                           F->S2, F->KR > 0 ? nb : 0, F->VR, H->d_st);
+            }
             break;
         }
         case ST_QSMALL:
-            if (F->n_qrows > 0) k_gemm_rows<<<F->tiles_qrows, 256, 0, s>>>(F->d_qrows, F->n_qrows, H->d_st);
-            if (F->n_qtile > 0)
-                k_gemm_tile<64, 64, 16, 4, 2, 0><<<F->tiles_qtile, 256, 0, s>>>(F->d_qtile, F->n_qtile, ep, H->d_st);
+            if (F->n_qsmall > 0) return launch_qsmall(H);
             break;
         case ST_FOLD: {
             const int ny = 1 << H->k;
-            k_fold_q<<<(ny + 255) / 256, 256, 0, s>>>(F->qparts, F->T, H->k, H->inv_c, F->lnq_full, H->d_lnq,
-                                                     H->d_st);
+            k_fold_q<<<(ny + 255) / 256, 256, 0, s>>>(F->d_fold, F->T, F->qparts, F->QS, F->UL, F->KL, F->VR, F->KR,
+                                                     H->k, H->inv_c, F->lnq_full, H->d_lnq, F->RB, F->H2, F->LA,
+                                                     F->Kp, H->d_st);
             break;
         }
         case ST_DSMALL:
-            if (F->n_drows > 0) k_gemm_rows<<<F->tiles_drows, 256, 0, s>>>(F->d_drows, F->n_drows, H->d_st);
-            if (F->n_dtile > 0)
-                k_gemm_tile<64, 64, 16, 4, 2, 0><<<F->tiles_dtile, 256, 0, s>>>(F->d_dtile, F->n_dtile, ep, H->d_st);
+            if (F->n_dsmall > 0)
+                k_dsmall<<<F->ctas_dsmall, 256, F->smem_dsmall, s>>>(F->d_dsmall, F->n_dsmall, F->dsmall_chunk,
+                                                                     F->lnq_full, H->d_st);
             break;
         case ST_G:
             k_gemm_tile<128, 128, 8, 4, 2, 1><<<F->ctas_g, 256, 0, s>>>(F->d_g, 1, ep, H->d_st);

@@ -195,20 +195,36 @@ def test_factored_equals_count_engine(bdc, O, n, k):
 
 
 def test_factored_rescales_extreme_start(bdc, O):
-    """A start whose probabilities span 600 orders of magnitude forces the
-    exp shift out of range in the first fused update; the engine re-scales
-    and still matches the oracle."""
+    """An unnormalised start scaled by 1e-280 (the reference does not
+    renormalise its input) puts exp(logW - shift) far out of range in the
+    first fused update; the engine re-scales and still matches the oracle."""
+    from bdc_b200 import dist
     n, k = 12, 6
     reps = O.canonicals(n)
-    rng = np.random.default_rng(3)
-    p0 = np.exp(-rng.uniform(0, 1400, len(reps)))
-    p0[0] = 1.0
+    p0 = dist.dirichlet_start(n, 1.0, 5) * 1e-280
     ref = O.run_ba(n, k, p0, reps, -1.0, 3)
     with bdc.Engine(n, k, engine="factored") as E:
         E.set_p(p0)
         st = E.iterate(3, -1.0)
         assert st["iters"] == 3
-        p = E.get_p()
-        big = ref["p"] > 1e-250
-        np.testing.assert_allclose(p[big], ref["p"][big], rtol=1e-9, atol=0)
-        assert abs(st["upper_bound"] - ref["ub_bits"][-1]) < 1e-9
+        np.testing.assert_allclose(E.get_p(), ref["p"], rtol=1e-11, atol=0)
+        assert abs(st["upper_bound"] - ref["ub_bits"][-1]) < 1e-11
+        assert abs(st["mx"] - ref["mx"][-1]) < 1e-11
+
+
+def test_underflowed_entries_reenter_like_reference(bdc, O):
+    """Entries that are exactly 0 take ln p = 0 (backend/BAA.cu:573-580) in
+    every iteration, in both engines, as in the oracle."""
+    from bdc_b200 import dist
+    n, k = 10, 5
+    reps = O.canonicals(n)
+    p0 = dist.dirichlet_start(n, 1.0, 9)
+    p0[::7] = 0.0
+    ref = O.run_ba(n, k, p0, reps, -1.0, 4)
+    for engine in ("count", "factored"):
+        with bdc.Engine(n, k, engine=engine) as E:
+            E.set_p(p0)
+            st = E.iterate(1, -1.0)
+            assert np.isinf(st["mx"])
+            st = E.iterate(3, -1.0)
+            np.testing.assert_allclose(E.get_p(), ref["p"], rtol=1e-11, atol=0)
