@@ -82,18 +82,20 @@ struct Term {
 
 struct FactoredState {
     int H1 = 0, H2 = 0, KL = 0, KR = 0, Kp = 0, T = 0;
+    int H1h = 0;              // rows that hold representatives: x_hi < H1 / 2
     std::vector<bdc::Term> terms;
-    double* Pw = nullptr;     // [2^n]  |O(x)| e(x) at representatives, 0 elsewhere
-    double* Lt = nullptr;     // [2^n]  ln e(x) (p = e / Z)
-    double* hx = nullptr;     // [2^n]  h(x) at representatives
-    double* LA = nullptr;     // [H1][Kp]  = [AL | NR]
+    double* Pw = nullptr;     // [2^{n-1}]  |O(x)| e(x) at representatives, 0 elsewhere
+    double* Lt = nullptr;     // [2^{n-1}]  ln e(x) (p = e / Z)
+    double* hx = nullptr;     // [2^{n-1}]  h(x) at representatives
+    double* LA = nullptr;     // [H1h][Kp]  = [AL | NR]
     double* RB = nullptr;     // [Kp][H2]  = [ML ; BR^T]
     double* UL = nullptr;     // [H2][KL]  (U^T: column c of AL^T Pw is row-contiguous)
-    double* VR = nullptr;     // [H1][KR]
+    double* VR = nullptr;     // [H1h][KR]
     double* ulpart = nullptr; // [S1][H2][KL]
-    double* vrpart = nullptr; // [S2][H1][KR]
+    double* vrpart = nullptr; // [S2][H1h][KR]
     int S1 = 1, S2 = 1;
     double* qparts = nullptr; // [T][QS][2^k]
+    double* qsum = nullptr;   // [T][2^k]  qparts summed over the splits
     int QS = 1;               // split of the s range of the small q products
     double* lnq_full = nullptr;  // [2^k]
     double* epart = nullptr;  // [ctas][4]
@@ -268,10 +270,13 @@ __global__ void __launch_bounds__(256) k_gemm_tile(const GemmDesc* __restrict__ 
             if (!is_rep(x, ep.n)) continue;
             const double o = (double)orbit_size(x, ep.n);
             const double D = __ldg(ep.hx + x) - acc[i][j] * ep.inv_c;
-            // an entry that is exactly 0 takes ln p = 0, as the reference's
-            // apply_log_kernel leaves ln 0 at 0 (backend/BAA.cu:573-580)
+            // an entry that is exactly 0 in the caller's distribution (Lt holds
+            // NaN) takes ln p = 0, as the reference's apply_log_kernel leaves
+            // ln 0 at 0 (backend/BAA.cu:573-580); later iterates keep exact logs
             const double pw = ep.Pw[x];
-            const double lnp = (pw == 0.0) ? 0.0 : ep.Lt[x] - lnz;
+            const double lt = ep.Lt[x];
+            const bool zero_in = (lt != lt);
+            const double lnp = zero_in ? 0.0 : lt - lnz;
             const double lw = lnp + D - shift;
             const double e = exp(lw);
             ep.Lt[x] = lw;
@@ -280,7 +285,7 @@ __global__ void __launch_bounds__(256) k_gemm_tile(const GemmDesc* __restrict__ 
             mL = fmax(mL, lw);
             sE = fma(o, e, sE);
             sR = fma(pw * inv_z, D, sR);
-            if (pw == 0.0) zero = 1.0;
+            if (zero_in) zero = 1.0;
         }
     }
     // CTA reduction of the five partials
@@ -462,22 +467,38 @@ __global__ void k_sum_parts(const double* __restrict__ a, int sa, int64_t na, do
 // terms of Q_t[y] (split slices, or U^T / V rows for identity terms); ln q
 // with the reference's 0 for q == 0 (backend/BAA.cu:573-580), expanded to
 // every y, and copied into RB / LA where a D-side product is the identity.
-__device__ __forceinline__ double term_value(const FoldTerm& f, const double* qparts, int QS, int t, int ny,
-                                             const double* ULt, int KL, const double* VR, int KR, uint32_t y) {
-    if (f.kind == 0) {
-        double a = 0.0;
+// phase 1: qsum[t][y] = sum over the splits of qparts[t][split][y]
+__global__ void k_qsum(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ qparts, int QS, int k,
+                       double* __restrict__ qsum, const DevState* st) {
+    if (gated(st)) return;
+    const int ny = 1 << k;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < T * ny; e += gridDim.x * blockDim.x) {
+        const int t = e / ny, y = e % ny;
+        if (terms[t].kind != 0) continue;
         const double* q = qparts + (size_t)t * QS * ny + y;
+        double a = 0.0;
         for (int sp = 0; sp < QS; ++sp) a += q[(size_t)sp * ny];
-        return a;
+        qsum[e] = a;
     }
-    const uint32_t yh = y >> f.m, yl = y & ((1u << f.m) - 1u);
-    if (f.kind == 1) return ULt[(size_t)yl * KL + f.off + yh];  // Q_t = U_t
-    return VR[(size_t)yh * KR + f.off + yl];                    // Q_t = V_t
 }
 
-__global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ qparts, int QS,
-                         const double* __restrict__ ULt, int KL, const double* __restrict__ VR, int KR, int k,
-                         double inv_c, double* __restrict__ lnq_full, double* __restrict__ lnq,
+// Q_t[y] from the split sums, or from U^T / V for identity terms (V holds
+// only the rows x_hi < H1h; the rows above are zero)
+__device__ __forceinline__ double term_value(const FoldTerm& f, const double* qsum, int t, int ny,
+                                             const double* ULt, int KL, const double* VR, int KR, int H1h,
+                                             uint32_t y) {
+    if (f.kind == 0) return qsum[(size_t)t * ny + y];
+    const uint32_t yh = y >> f.m, yl = y & ((1u << f.m) - 1u);
+    if (f.kind == 1) return ULt[(size_t)yl * KL + f.off + yh];  // Q_t = U_t
+    return yh < (uint32_t)H1h ? VR[(size_t)yh * KR + f.off + yl] : 0.0;  // Q_t = V_t
+}
+
+// phase 2: q(rep r) = sum_{y in O(r)} sum_t Q_t[y] / (|O(r)| C Z); ln q with
+// the reference's 0 for q == 0 (backend/BAA.cu:573-580), expanded to every
+// y, and copied into RB / LA where a D-side product is the identity.
+__global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ qsum,
+                         const double* __restrict__ ULt, int KL, const double* __restrict__ VR, int KR, int H1h,
+                         int k, double inv_c, double* __restrict__ lnq_full, double* __restrict__ lnq,
                          double* __restrict__ RB, int H2, double* __restrict__ LA, int Kp, const DevState* st) {
     if (gated(st)) return;
     const int ny = 1 << k;
@@ -493,7 +514,7 @@ __global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double
         if (rcv != r && rcv != rv && rcv != cv) mem[nm++] = rcv;
         double acc = 0.0;
         for (int e = 0; e < nm; ++e)
-            for (int t = 0; t < T; ++t) acc += term_value(terms[t], qparts, QS, t, ny, ULt, KL, VR, KR, mem[e]);
+            for (int t = 0; t < T; ++t) acc += term_value(terms[t], qsum, t, ny, ULt, KL, VR, KR, H1h, mem[e]);
         const double q = acc * inv_c * inv_z / (double)nm;
         const double lq = (q != 0.0) ? log(q) : 0.0;
         lnq_full[y] = lq;
@@ -501,8 +522,8 @@ __global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double
         for (int t = 0; t < T; ++t) {
             const FoldTerm& f = terms[t];
             const uint32_t yh = (uint32_t)y >> f.m, yl = (uint32_t)y & ((1u << f.m) - 1u);
-            if (f.idB_left) RB[(size_t)(f.off + yh) * H2 + yl] = lq;   // M_t = Lq_t
-            if (f.idA_right) LA[(size_t)yh * Kp + KL + f.off + yl] = lq;  // N_t = Lq_t
+            if (f.idB_left) RB[(size_t)(f.off + yh) * H2 + yl] = lq;  // M_t = Lq_t
+            if (f.idA_right && yh < (uint32_t)H1h) LA[(size_t)yh * Kp + KL + f.off + yl] = lq;  // N_t = Lq_t
         }
     }
 }
@@ -620,8 +641,9 @@ k_fac_load(const uint32_t* __restrict__ reps, int64_t R, int n, const double* __
         const uint32_t x = reps[i];
         const double v = p[i];
         Pw[x] = (double)orbit_size(x, n) * v;
-        const double l = (v != 0.0) ? log(v) : 0.0;  // ln 0 = 0 (backend/BAA.cu:573-580)
-        Lt[x] = l;
+        // ln 0 = 0 (backend/BAA.cu:573-580): marked with NaN for the epilogue
+        const double l = (v != 0.0) ? log(v) : 0.0;
+        Lt[x] = (v != 0.0) ? l : __longlong_as_double(0x7ff8000000000000ll);
         mx = fmax(mx, l);
         if (v == 0.0) zero = 1;
     }
@@ -755,6 +777,9 @@ bdc_status factored_init(bdc_handle* H) {
     const Split& s = H->s;
     F->H1 = 1 << s.n1;
     F->H2 = 1 << s.n2;
+    // every representative is <= its complement, so its top bit is 0 and
+    // x_hi < H1 / 2: only those rows of the iterate and of G are needed
+    F->H1h = F->H1 / 2;
     const int k = H->k;
     // terms and their association
     int KL = 0, KR = 0;
@@ -776,9 +801,9 @@ bdc_status factored_init(bdc_handle* H) {
     F->KR = KR;
     F->Kp = (KL + KR + 7) / 8 * 8;
     F->T = (int)F->terms.size();
-    const int64_t NX = (int64_t)1 << H->n;
+    const int64_t NX = (int64_t)1 << (H->n - 1);
     const int ny = 1 << k;
-    const int H1 = F->H1, H2 = F->H2, Kp = F->Kp;
+    const int H1 = F->H1h, H2 = F->H2, Kp = F->Kp;  // H1: the rows kept
     const int KLa = KL > 0 ? KL : 1, KRa = KR > 0 ? KR : 1;
 
     // small q products: split the contracted range so the launch fills the GPU
@@ -808,6 +833,7 @@ bdc_status factored_init(bdc_handle* H) {
     BDC_CUDA_TRY(al(&F->ulpart, (size_t)F->S1 * H2 * KLa));
     BDC_CUDA_TRY(al(&F->vrpart, (size_t)F->S2 * H1 * KRa));
     BDC_CUDA_TRY(al(&F->qparts, (size_t)F->T * F->QS * ny));
+    BDC_CUDA_TRY(al(&F->qsum, (size_t)F->T * ny));
     BDC_CUDA_TRY(al(&F->lnq_full, (size_t)ny));
     F->ctas_g = ((H1 + 127) / 128) * ((H2 + 127) / 128);
     BDC_CUDA_TRY(al(&F->epart, (size_t)std::max(F->ctas_g * 2, 2 * H->nb_upd) * 4));
@@ -839,7 +865,7 @@ bdc_status factored_init(bdc_handle* H) {
     BDC_CUDA_TRY(cudaGetLastError());
 
     // ---- the two thin products, split over the contraction:
-    //   U^T (H2 x KL) = (AL^T Pw)^T and V (H1 x KR) = Pw BR
+    //   U^T (H2 x KL) = (AL^T Pw)^T and V (H1h x KR) = Pw BR
     std::vector<GemmDesc> big;
     if (KL > 0) {
         const int kc = H1 / F->S1;
@@ -958,7 +984,7 @@ bdc_status factored_init(bdc_handle* H) {
         assign_tiles(g, 128, 128);
         BDC_CUDA_TRY(upload(g, &F->d_g));
     }
-    F->launches_per_iter = (F->n_big > 0 ? 2 : 1) + (F->n_qsmall > 0) + 1 + (F->n_dsmall > 0) + 1 + 1;
+    F->launches_per_iter = (F->n_big > 0 ? 2 : 0) + (F->n_qsmall > 0) + 2 + (F->n_dsmall > 0) + 1 + 1;
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
 }
@@ -967,7 +993,7 @@ void factored_free(bdc_handle* H) {
     FactoredState* F = H->fac;
     if (!F) return;
     for (double* p : {F->Pw, F->Lt, F->hx, F->LA, F->RB, F->UL, F->VR, F->ulpart, F->vrpart, F->qparts,
-                      F->lnq_full, F->epart})
+                      F->qsum, F->lnq_full, F->epart})
         cudaFree(p);
     cudaFree(F->d_big);
     cudaFree(F->d_g);
@@ -1019,7 +1045,7 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
         case ST_QBIG: {
             if (F->n_big > 0) {
                 k_gemm_tile<128, 128, 8, 4, 2, 0><<<F->tiles_big, 256, 0, s>>>(F->d_big, F->n_big, ep, H->d_st);
-                const int64_t na = (int64_t)F->KL * F->H2, nb = (int64_t)F->H1 * F->KR;
+                const int64_t na = (int64_t)F->KL * F->H2, nb = (int64_t)F->H1h * F->KR;
                 k_sum_parts<<<H->num_sms * 4, 256, 0, s>>>(F->ulpart, F->S1, F->KL > 0 ? na : 0, F->UL, F->vrpart,
                                                            F->S2, F->KR > 0 ? nb : 0, F->VR, H->d_st);
             }
@@ -1030,9 +1056,11 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             break;
         case ST_FOLD: {
             const int ny = 1 << H->k;
-            k_fold_q<<<(ny + 255) / 256, 256, 0, s>>>(F->d_fold, F->T, F->qparts, F->QS, F->UL, F->KL, F->VR, F->KR,
-                                                     H->k, H->inv_c, F->lnq_full, H->d_lnq, F->RB, F->H2, F->LA,
-                                                     F->Kp, H->d_st);
+            const int nqs = (F->T * ny + 255) / 256;
+            k_qsum<<<nqs < 4096 ? nqs : 4096, 256, 0, s>>>(F->d_fold, F->T, F->qparts, F->QS, H->k, F->qsum, H->d_st);
+            k_fold_q<<<(ny + 63) / 64, 64, 0, s>>>(F->d_fold, F->T, F->qsum, F->UL, F->KL, F->VR, F->KR, F->H1h, H->k,
+                                                  H->inv_c, F->lnq_full, H->d_lnq, F->RB, F->H2, F->LA, F->Kp,
+                                                  H->d_st);
             break;
         }
         case ST_DSMALL:
@@ -1060,7 +1088,7 @@ static cudaError_t enqueue_iteration(bdc_handle* H, double a) {
 
 bdc_status factored_load_p(bdc_handle* H) {
     FactoredState* F = H->fac;
-    const int64_t NX = (int64_t)1 << H->n;
+    const int64_t NX = (int64_t)1 << (H->n - 1);  // representatives have x < 2^{n-1}
     BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
     const int nb = H->nb_upd;
     k_fac_load<<<nb, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, H->d_p[0], F->Pw, F->Lt, F->epart, H->d_st);
@@ -1159,7 +1187,7 @@ bdc_status factored_profile(bdc_handle* H, int iters, bdc_profile_t* out) {
     out->ms_update = acc[ST_FIN] / iters;
     out->ms_iter = tot / iters;
     out->ms_main = acc[ST_G] / iters;
-    out->work_main = 2.0 * (double)F->H1 * (double)F->H2 * (double)(F->KL + F->KR);
+    out->work_main = 2.0 * (double)F->H1h * (double)F->H2 * (double)(F->KL + F->KR);
     out->launches = F->launches_per_iter;
     out->iters = iters;
     return BDC_OK;
