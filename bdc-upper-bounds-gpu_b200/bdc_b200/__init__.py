@@ -320,9 +320,10 @@ def generate_cache(n: int, k: int, device: int = 0) -> np.ndarray:
 
 
 def peak_probe(kind: str, device: int = 0, ms: float = 50.0) -> float:
-    """Measured operations/s of one arithmetic pipe: "imad", "dfma" or "ffma"."""
+    """Measured multiply-adds/s of one arithmetic path: "imad", "dfma",
+    "ffma" or "dmma" (FP64 mma.sync)."""
     r = ctypes.c_double()
-    _check(library().bdc_peak_probe(device, {"imad": 0, "dfma": 1, "ffma": 2}[kind], ms, ctypes.byref(r)),
+    _check(library().bdc_peak_probe(device, {"imad": 0, "dfma": 1, "ffma": 2, "dmma": 3}[kind], ms, ctypes.byref(r)),
            "bdc_peak_probe")
     return r.value
 

@@ -1,65 +1,43 @@
 // bdc_factored.cu -- the factored engine: one BA iteration as FP64 matrix
 // products over the half tables, with the BA update fused into the largest one.
 //
-// Reference path replaced (Pintz45/BDC-Upper-Bounds-GPU): the same iteration
-// as backend/BAA.cu:590-639 (q pass 429-485, D pass 487-530, normalisation
+// Reference path replaced (Pintz45/BDC-Upper-Bounds-GPU): the iteration of
+// backend/BAA.cu:590-639 (q pass 429-485, D pass 487-530, normalisation
 // 590-639, max deviation 916-946).  The reference evaluates N(x,y) pair by
 // pair through the split identity (total_transitions, BAA.cu:340-395):
 //     N(x, y) = sum_j A_j[x_hi][y_hi] * B_{k-j}[x_lo][y_lo],
-// A_j = cache_{n1,j}, B_m = cache_{n2,m}.  For fixed j this is a Kronecker
+// A_j = cache_{n1,j}, B_m = cache_{n2,m}.  For a fixed j this is a Kronecker
 // product, so with the iterate laid out as a 2^{n1} x 2^{n2} matrix P:
-//   q-side:  Q_j = A_j^T P B_{k-j}                    (2^j x 2^{k-j} block of q)
-//   D-side:  G   = sum_j A_j Lq_j B_{k-j}^T,  D(x) = h(x) - G(x) / C(n,k)
+//   q side:  Q_j = A_j^T P B_{k-j}                (the 2^j x 2^{k-j} block of q)
+//   D side:  G   = sum_j A_j Lq_j B_{k-j}^T,  D(x) = h(x) - G(x) / C(n,k)
 // with Lq_j = ln q reshaped to 2^j x 2^{k-j} and h(x) = sum_y W ln W (from
-// the count path, once per handle).  Each term is evaluated in the cheaper
-// association: "L" terms (2^j <= 2^{k-j}) contract x_hi first, "R" terms
-// contract x_lo first.  Per iteration:
-//   1. UL = AL^T Pw, VR = Pw BR        (Pw = |O(x)| p(x) at representatives,
-//                                        0 elsewhere; AL, BR = the L / R tables)
+// the count path, once per handle).  Each term uses the cheaper association:
+// "L" terms (2^j <= 2^{k-j}) contract x_hi first, "R" terms contract x_lo
+// first.  Every representative is <= its complement, so its top bit is 0 and
+// only the rows x_hi < H1/2 of the iterate and of G exist.  Per iteration:
+//   1. U^T = (AL^T Pw)^T, V = Pw BR      (Pw = |O(x)| p(x) at representatives,
+//                                          0 elsewhere; AL, BR: L / R tables)
 //   2. Q_t = U_t B_m (L), A_j^T V_t (R) -> q parts; fold orbits -> ln q
 //   3. M_t = Lq_t B_m^T (L), N_t = A_j Lq_t (R) -> operands of step 4
 //   4. G = [AL | NR] [ML ; BR^T] with the BA update as epilogue: D, logW,
 //      exp(logW - shift), the new iterate (in place) and block partials of
 //      max D, sum |O| e, max logW, sum |O| p D
 //   5. one-block finalize: ln Z, mx, upper bound, stop test, next shift.
-// Counts are exact (integers <= 2^16 widened to FP64); all sums are FP64.
+// All products run on the FP64 tensor-core path (bdc_mma.cuh).  Counts are
+// exact integers < 2^16 widened to FP64; all sums are FP64.  The tile shape
+// and split of the large products are picked at set-up by timing candidates.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <vector>
 
 #include "bdc_engine.cuh"
 #include "bdc_gemm.cuh"
+#include "bdc_mma.cuh"
 
 namespace bdc {
 
 constexpr int kErrShift = 1;  // DevState::error: exp shift out of range, re-scale
-
-// q-side small product of one term: Q_t = sum_s a(s) (x) b(s), the outer
-// products of a(s) = a + s*a_stride (2^j entries) and b(s) = b + s*b_stride
-// (2^m entries), s over the contracted half (L terms: a = column of U_t,
-// b = row of B_m; R terms: a = row of A_j, b = row of V_t).
-struct OuterDesc {
-    const void* a;
-    const void* b;
-    int64_t a_stride, b_stride;
-    int a_u16, b_u16;
-    int j, m;
-    int S;           // length of the contracted range
-    int term;        // slice of qparts
-};
-
-// D-side small product of one term, one s at a time (Lq_t = ln q as 2^j x 2^m):
-//   L: out_s[yh] = sum_yl Lq_t[yh][yl] B_m[s][yl]   (column s of M_t -> RB)
-//   R: out_s[yl] = sum_yh A_j[s][yh] Lq_t[yh][yl]   (row s of N_t -> LA)
-struct MatvecDesc {
-    const uint16_t* v;  // bundle rows: v(s) = v + s * v_stride
-    int64_t v_stride;
-    double* out;        // element i of s at out[s * s_stride + i * i_stride]
-    int64_t s_stride, i_stride;
-    int j, m, left;
-    int S;
-    int cta_begin;
-};
 
 // how the fold reads Q_t: 0 = split slices in qparts, 1 = U^T rows (the
 // identity B of an L term), 2 = V rows (the identity A of an R term); the
@@ -78,6 +56,16 @@ struct Term {
     int idA, idB;   // A_j / B_m is the identity (j == n1 / m == n2)
 };
 
+// tile configurations of the FP64 tensor-core products (BM x BN, warps WM x WN)
+enum MmaConfig { CFG_128x128 = 0, CFG_128x64, CFG_64x128, CFG_64x64, CFG_128x16, CFG_16x128, CFG_COUNT };
+static const int kCfgBM[CFG_COUNT] = {128, 128, 64, 64, 128, 16};
+static const int kCfgBN[CFG_COUNT] = {128, 64, 128, 64, 16, 128};
+
+struct Launch {
+    GemmDesc* d = nullptr;   // device descriptors
+    int n = 0, tiles = 0, cfg = CFG_64x64;
+};
+
 }  // namespace bdc
 
 struct FactoredState {
@@ -89,40 +77,26 @@ struct FactoredState {
     double* hx = nullptr;     // [2^{n-1}]  h(x) at representatives
     double* LA = nullptr;     // [H1h][Kp]  = [AL | NR]
     double* RB = nullptr;     // [Kp][H2]  = [ML ; BR^T]
-    double* UL = nullptr;     // [H2][KL]  (U^T: column c of AL^T Pw is row-contiguous)
+    double* UL = nullptr;     // [H2][KL]  (U^T)
     double* VR = nullptr;     // [H1h][KR]
     double* ulpart = nullptr; // [S1][H2][KL]
     double* vrpart = nullptr; // [S2][H1h][KR]
     int S1 = 1, S2 = 1;
     double* qparts = nullptr; // [T][QS][2^k]
     double* qsum = nullptr;   // [T][2^k]  qparts summed over the splits
-    int QS = 1;               // split of the s range of the small q products
+    int QS = 1;               // split of the contraction of the small q products
     double* lnq_full = nullptr;  // [2^k]
-    double* epart = nullptr;  // [ctas][4]
+    double* epart = nullptr;  // [ctas][8]
     int ctas_g = 0;
-    // launch plans
-    bdc::GemmDesc* d_big = nullptr;  int n_big = 0, tiles_big = 0;     // UL, VR partials
-    bdc::OuterDesc* d_qsmall = nullptr; int n_qsmall = 0;   // q-side small products
-    bdc::MatvecDesc* d_dsmall = nullptr; int n_dsmall = 0;  // D-side small products
-    int dsmall_chunk = 64;                                  // s values per CTA
-    int ctas_dsmall = 0, smem_dsmall = 0;
-    bdc::FoldTerm* d_fold = nullptr;                        // per term: how the fold reads Q_t
-    bdc::GemmDesc* d_g = nullptr;
+    bdc::Launch ul, vr, g;
+    std::vector<bdc::Launch> qsmall, dsmall;
+    bdc::FoldTerm* d_fold = nullptr;
     int launches_per_iter = 0;
 };
 
 namespace bdc {
 
-// ---------------------------------------------------------------- helpers
-__device__ __forceinline__ double op_load(const Operand& o, int64_t r, int64_t c) {
-    if (o.kind == OP_EYE) return r == c ? 1.0 : 0.0;
-    const int64_t idx = o.trans ? c * o.ld + r : r * o.ld + c;
-    if (o.kind == OP_U16) return (double)__ldg((const uint16_t*)o.ptr + idx);
-    return __ldg((const double*)o.ptr + idx);
-}
-
-// element (r, c) is contiguous along c (row-major storage) unless transposed
-__device__ __forceinline__ bool contiguous_in_rows(const Operand& o) { return o.trans != 0; }
+__device__ __forceinline__ bool gated(const DevState* st) { return st && (st->done || st->error); }
 
 __device__ __forceinline__ int find_desc(const GemmDesc* d, int nd, int t) {
     int i = 0;
@@ -130,165 +104,93 @@ __device__ __forceinline__ int find_desc(const GemmDesc* d, int nd, int t) {
     return i;
 }
 
-__device__ __forceinline__ bool gated(const DevState* st) { return st && (st->done || st->error); }
-
-// ------------------------------------------------------------ tiled GEMM
-// 256 threads = WARPS_M x WARPS_N warps; a warp is 4 (m) x 8 (n) lanes; a
-// thread owns rows mbase + q*8 + {0,1} (q < TM/2) and columns
-// nbase + q*16 + {0,1} (q < TN/2), so that each shared-memory fragment load
-// is one 16-byte access per lane with broadcast (A) or contiguous (B) lanes.
-template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int EPI>
-__global__ void __launch_bounds__(256) k_gemm_tile(const GemmDesc* __restrict__ descs, int ndesc,
-                                                   BaEpilogue ep, const DevState* st) {
-    constexpr int TM = BM / (WARPS_M * 4);
-    constexpr int TN = BN / (WARPS_N * 8);
-    static_assert(WARPS_M * WARPS_N == 8, "256 threads");
-    static_assert(TM % 2 == 0 && TN % 2 == 0, "pairs");
-    constexpr int A_PER = BK * BM / 256;
-    constexpr int B_PER = BK * BN / 256;
+// ------------------------------------------------ products: plain store
+template <int BM, int BN, int WM, int WN>
+__global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ descs, int ndesc,
+                                                   const DevState* st) {
+    using C = MmaCfg<BM, BN, WM, WN>;
     if (gated(st)) return;
-    const int di = find_desc(descs, ndesc, blockIdx.x);
-    const GemmDesc& d = descs[di];
-    const Operand A = d.A, B = d.B;
-    const int M = d.M, N = d.N, K = d.K;
+    extern __shared__ __align__(16) double smem[];
+    const GemmDesc& d = descs[find_desc(descs, ndesc, blockIdx.x)];
     const int t = blockIdx.x - d.tile_begin;
     const int m0 = (t / d.tiles_n) * BM, n0 = (t % d.tiles_n) * BN;
-
-    __shared__ __align__(16) double As[2][BK][BM];
-    __shared__ __align__(16) double Bs[2][BK][BN];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wm = warp / WARPS_N, wn = warp % WARPS_N;
-    const int mbase = wm * (BM / WARPS_M) + (lane >> 3) * 2;
-    const int nbase = wn * (BN / WARPS_N) + (lane & 7) * 2;
-    const bool a_rows = contiguous_in_rows(A);   // A(m,k) contiguous along m
-    const bool b_cols = !contiguous_in_rows(B);  // B(k,n) contiguous along n
-
-    double ra[A_PER], rb[B_PER];
-    auto gload = [&](int k0) {
+    double acc[C::MT][C::NT][2];
+    mma_mainloop<BM, BN, WM, WN>(d, m0, n0, smem, acc);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tq = lane & 3;
+    const int wm0 = (warp / WN) * (8 * C::MT), wn0 = (warp % WN) * (8 * C::NT);
 #pragma unroll
-        for (int i = 0; i < A_PER; ++i) {
-            const int e = tid + i * 256;
-            const int kk = a_rows ? e / BM : e % BK;
-            const int mm = a_rows ? e % BM : e / BK;
-            const int m = m0 + mm, k = k0 + kk;
-            ra[i] = (m < M && k < K) ? op_load(A, m, k) : 0.0;
-        }
+    for (int i = 0; i < C::MT; ++i) {
+        const int m = m0 + wm0 + i * 8 + g;
+        if (m >= d.M) continue;
 #pragma unroll
-        for (int i = 0; i < B_PER; ++i) {
-            const int e = tid + i * 256;
-            const int kk = b_cols ? e / BN : e % BK;
-            const int nn = b_cols ? e % BN : e / BK;
-            const int n = n0 + nn, k = k0 + kk;
-            rb[i] = (n < N && k < K) ? op_load(B, k, n) : 0.0;
-        }
-    };
-    auto sstore = [&](int buf) {
+        for (int j = 0; j < C::NT; ++j)
 #pragma unroll
-        for (int i = 0; i < A_PER; ++i) {
-            const int e = tid + i * 256;
-            const int kk = a_rows ? e / BM : e % BK;
-            const int mm = a_rows ? e % BM : e / BK;
-            As[buf][kk][mm] = ra[i];
-        }
-#pragma unroll
-        for (int i = 0; i < B_PER; ++i) {
-            const int e = tid + i * 256;
-            const int kk = b_cols ? e / BN : e % BK;
-            const int nn = b_cols ? e % BN : e / BK;
-            Bs[buf][kk][nn] = rb[i];
-        }
-    };
-
-    double acc[TM][TN];
-#pragma unroll
-    for (int i = 0; i < TM; ++i)
-#pragma unroll
-        for (int j = 0; j < TN; ++j) acc[i][j] = 0.0;
-
-    const int nk = (K + BK - 1) / BK;
-    gload(0);
-    sstore(0);
-    __syncthreads();
-    for (int s = 0; s < nk; ++s) {
-        const int cur = s & 1;
-        if (s + 1 < nk) gload((s + 1) * BK);
-#pragma unroll
-        for (int kk = 0; kk < BK; ++kk) {
-            double a[TM], b[TN];
-#pragma unroll
-            for (int q = 0; q < TM / 2; ++q) {
-                const double2 v = *reinterpret_cast<const double2*>(&As[cur][kk][mbase + q * 8]);
-                a[2 * q] = v.x;
-                a[2 * q + 1] = v.y;
-            }
-#pragma unroll
-            for (int q = 0; q < TN / 2; ++q) {
-                const double2 v = *reinterpret_cast<const double2*>(&Bs[cur][kk][nbase + q * 16]);
-                b[2 * q] = v.x;
-                b[2 * q + 1] = v.y;
-            }
-#pragma unroll
-            for (int i = 0; i < TM; ++i)
-#pragma unroll
-                for (int j = 0; j < TN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-        if (s + 1 < nk) sstore(cur ^ 1);
-        __syncthreads();
-    }
-
-    if (EPI == 0) {
-#pragma unroll
-        for (int i = 0; i < TM; ++i) {
-            const int m = m0 + mbase + (i >> 1) * 8 + (i & 1);
-            if (m >= M) continue;
-#pragma unroll
-            for (int j = 0; j < TN; ++j) {
-                const int n = n0 + nbase + (j >> 1) * 16 + (j & 1);
-                if (n >= N) continue;
+            for (int h = 0; h < 2; ++h) {
+                const int n = n0 + wn0 + j * 8 + 2 * tq + h;
+                if (n >= d.N) continue;
                 double* c = d.C + (int64_t)m * d.ldc_m + (int64_t)n * d.ldc_n;
-                const double v = d.alpha * acc[i][j];
+                const double v = d.alpha * acc[i][j][h];
                 *c = d.accumulate ? *c + v : v;
             }
-        }
-        return;
     }
+}
 
-    // ---- BA epilogue: rows are x_hi, columns x_lo, x = (x_hi << n2) | x_lo
+// ------------------------------------------- the G product + BA update
+// rows are x_hi, columns x_lo, x = (x_hi << n2) | x_lo; only representatives
+// are updated; block partials [max D, sum |O| e, max (logW - shift),
+// sum |O| p D, input-zero flag] go to ep.part[blockIdx.x * 8 + 0..4].
+template <int BM, int BN, int WM, int WN>
+__global__ void __launch_bounds__(256) k_mma_ba(const GemmDesc* __restrict__ descs, BaEpilogue ep,
+                                                const DevState* st) {
+    using C = MmaCfg<BM, BN, WM, WN>;
+    if (gated(st)) return;
+    extern __shared__ __align__(16) double smem[];
+    const GemmDesc& d = descs[0];
+    const int t = blockIdx.x;
+    const int m0 = (t / d.tiles_n) * BM, n0 = (t % d.tiles_n) * BN;
+    double acc[C::MT][C::NT][2];
+    mma_mainloop<BM, BN, WM, WN>(d, m0, n0, smem, acc);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, tq = lane & 3;
+    const int wm0 = (warp / WN) * (8 * C::MT), wn0 = (warp % WN) * (8 * C::NT);
     const double shift = st->shift;
     const double lnz = st->log_z;
     const double inv_z = exp(-lnz);
     double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0, zero = 0.0;
 #pragma unroll
-    for (int i = 0; i < TM; ++i) {
-        const int m = m0 + mbase + (i >> 1) * 8 + (i & 1);
-        if (m >= M) continue;
+    for (int i = 0; i < C::MT; ++i) {
+        const int m = m0 + wm0 + i * 8 + g;
+        if (m >= d.M) continue;
 #pragma unroll
-        for (int j = 0; j < TN; ++j) {
-            const int n = n0 + nbase + (j >> 1) * 16 + (j & 1);
-            if (n >= N) continue;
-            const uint32_t x = ((uint32_t)m << ep.n2) | (uint32_t)n;
-            if (!is_rep(x, ep.n)) continue;
-            const double o = (double)orbit_size(x, ep.n);
-            const double D = __ldg(ep.hx + x) - acc[i][j] * ep.inv_c;
-            // an entry that is exactly 0 in the caller's distribution (Lt holds
-            // NaN) takes ln p = 0, as the reference's apply_log_kernel leaves
-            // ln 0 at 0 (backend/BAA.cu:573-580); later iterates keep exact logs
-            const double pw = ep.Pw[x];
-            const double lt = ep.Lt[x];
-            const bool zero_in = (lt != lt);
-            const double lnp = zero_in ? 0.0 : lt - lnz;
-            const double lw = lnp + D - shift;
-            const double e = exp(lw);
-            ep.Lt[x] = lw;
-            ep.Pw[x] = o * e;
-            mD = fmax(mD, D);
-            mL = fmax(mL, lw);
-            sE = fma(o, e, sE);
-            sR = fma(pw * inv_z, D, sR);
-            if (zero_in) zero = 1.0;
-        }
+        for (int j = 0; j < C::NT; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int n = n0 + wn0 + j * 8 + 2 * tq + h;
+                if (n >= d.N) continue;
+                const uint32_t x = ((uint32_t)m << ep.n2) | (uint32_t)n;
+                if (!is_rep(x, ep.n)) continue;
+                const double o = (double)orbit_size(x, ep.n);
+                const double D = __ldg(ep.hx + x) - acc[i][j][h] * ep.inv_c;
+                // an entry that is exactly 0 in the caller's distribution (Lt
+                // holds NaN) takes ln p = 0, as the reference's apply_log_kernel
+                // leaves ln 0 at 0 (backend/BAA.cu:573-580); later iterates keep
+                // exact logarithms
+                const double pw = ep.Pw[x];
+                const double lt = ep.Lt[x];
+                const bool zero_in = (lt != lt);
+                const double lnp = zero_in ? 0.0 : lt - lnz;
+                const double lw = lnp + D - shift;
+                const double e = exp(lw);
+                ep.Lt[x] = lw;
+                ep.Pw[x] = o * e;
+                mD = fmax(mD, D);
+                mL = fmax(mL, lw);
+                sE = fma(o, e, sE);
+                sR = fma(pw * inv_z, D, sR);
+                if (zero_in) zero = 1.0;
+            }
     }
-    // CTA reduction of the five partials
     __shared__ double red[5][8];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -306,7 +208,7 @@ __global__ void __launch_bounds__(256) k_gemm_tile(const GemmDesc* __restrict__ 
         red[4][warp] = zero;
     }
     __syncthreads();
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
         double a0 = red[0][0], a1 = red[1][0], a2 = red[2][0], a3 = red[3][0], a4 = red[4][0];
         for (int w = 1; w < 8; ++w) {
             a0 = fmax(a0, red[0][w]);
@@ -324,122 +226,72 @@ __global__ void __launch_bounds__(256) k_gemm_tile(const GemmDesc* __restrict__ 
     }
 }
 
-// ------------------------------------------------- q-side small products
-// CTA = one (term, split of the s range); thread t owns OPT consecutive
-// outputs o = y = yh * 2^m + yl of Q_t and accumulates a(s)[yh] * b(s)[yl].
-__device__ __forceinline__ double ld_any(const void* p, int u16, int64_t i) {
-    return u16 ? (double)__ldg((const uint16_t*)p + i) : __ldg((const double*)p + i);
+#define BDC_CFG_ARGS_128x128 128, 128, 2, 4
+#define BDC_CFG_ARGS_128x64 128, 64, 4, 2
+#define BDC_CFG_ARGS_64x128 64, 128, 2, 4
+#define BDC_CFG_ARGS_64x64 64, 64, 2, 4
+#define BDC_CFG_ARGS_128x16 128, 16, 8, 1
+#define BDC_CFG_ARGS_16x128 16, 128, 1, 8
+
+static int cfg_smem(int cfg) {
+    switch (cfg) {
+        case CFG_128x128: return mma_smem_bytes<BDC_CFG_ARGS_128x128>();
+        case CFG_128x64: return mma_smem_bytes<BDC_CFG_ARGS_128x64>();
+        case CFG_64x128: return mma_smem_bytes<BDC_CFG_ARGS_64x128>();
+        case CFG_64x64: return mma_smem_bytes<BDC_CFG_ARGS_64x64>();
+        case CFG_128x16: return mma_smem_bytes<BDC_CFG_ARGS_128x16>();
+        case CFG_16x128: return mma_smem_bytes<BDC_CFG_ARGS_16x128>();
+    }
+    return 0;
 }
 
-template <int OPT>
-__global__ void __launch_bounds__(256) k_qsmall(const OuterDesc* __restrict__ descs, int QS, int k,
-                                                double* __restrict__ qparts, const DevState* st) {
-    if (gated(st)) return;
-    const OuterDesc& d = descs[blockIdx.x / QS];
-    const int split = blockIdx.x % QS;
-    const int ny = 1 << k;
-    const int s0 = (int)((int64_t)d.S * split / QS), s1 = (int)((int64_t)d.S * (split + 1) / QS);
-    const int o0 = threadIdx.x * OPT;
-    if (o0 >= ny) return;
-    const int m = d.m;
-    const int mask = (1 << m) - 1;
-    double acc[OPT];
-#pragma unroll
-    for (int i = 0; i < OPT; ++i) acc[i] = 0.0;
-    if ((1 << m) >= OPT) {
-        // one yh, OPT consecutive yl
-        const int yh = o0 >> m, yl0 = o0 & mask;
-        for (int s = s0; s < s1; ++s) {
-            const double av = ld_any(d.a, d.a_u16, (int64_t)s * d.a_stride + yh);
-            const int64_t bb = (int64_t)s * d.b_stride + yl0;
-#pragma unroll
-            for (int i = 0; i < OPT; ++i) acc[i] = fma(av, ld_any(d.b, d.b_u16, bb + i), acc[i]);
-        }
-    } else {
-        // OPT / 2^m consecutive yh, all 2^m yl
-        const int yh0 = o0 >> m;
-        for (int s = s0; s < s1; ++s) {
-            const int64_t ab = (int64_t)s * d.a_stride + yh0, bb = (int64_t)s * d.b_stride;
-#pragma unroll
-            for (int i = 0; i < OPT; ++i)
-                acc[i] = fma(ld_any(d.a, d.a_u16, ab + (i >> m)), ld_any(d.b, d.b_u16, bb + (i & mask)),
-                             acc[i]);
-        }
+static cudaError_t set_smem_attrs() {
+    static bool done = false;
+    if (done) return cudaSuccess;
+#define SET_(NAME, ARGS)                                                                       \
+    {                                                                                          \
+        cudaError_t e = cudaFuncSetAttribute(NAME<ARGS>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                             mma_smem_bytes<ARGS>());                          \
+        if (e != cudaSuccess) return e;                                                        \
     }
-    double* out = qparts + ((size_t)d.term * QS + split) * ny + o0;
-#pragma unroll
-    for (int i = 0; i < OPT; ++i) out[i] = acc[i];
+    SET_(k_mma_store, BDC_CFG_ARGS_128x128)
+    SET_(k_mma_store, BDC_CFG_ARGS_128x64)
+    SET_(k_mma_store, BDC_CFG_ARGS_64x128)
+    SET_(k_mma_store, BDC_CFG_ARGS_64x64)
+    SET_(k_mma_store, BDC_CFG_ARGS_128x16)
+    SET_(k_mma_store, BDC_CFG_ARGS_16x128)
+    SET_(k_mma_ba, BDC_CFG_ARGS_128x128)
+    SET_(k_mma_ba, BDC_CFG_ARGS_128x64)
+    SET_(k_mma_ba, BDC_CFG_ARGS_64x128)
+#undef SET_
+    done = true;
+    return cudaSuccess;
 }
 
-// ------------------------------------------------- D-side small products
-// CTA = one term and a chunk of s; Lq_t staged in shared memory with row
-// stride 2^m + 1; one warp per s.
-__global__ void __launch_bounds__(256) k_dsmall(const MatvecDesc* __restrict__ descs, int nd, int chunk,
-                                                const double* __restrict__ lnq_full, const DevState* st) {
-    if (gated(st)) return;
-    int di = 0;
-    while (di + 1 < nd && descs[di + 1].cta_begin <= (int)blockIdx.x) ++di;
-    const MatvecDesc& d = descs[di];
-    const int c = blockIdx.x - d.cta_begin;
-    const int nj = 1 << d.j, nm = 1 << d.m;
-    const int rs = nm + 1;
-    extern __shared__ double lq[];  // [nj][nm + 1]
-    for (int e = threadIdx.x; e < nj * nm; e += blockDim.x) lq[(e >> d.m) * rs + (e & (nm - 1))] = lnq_full[e];
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int sb = c * chunk, se = min(sb + chunk, d.S);
-    for (int s = sb + warp; s < se; s += 8) {
-        const uint16_t* v = d.v + (int64_t)s * d.v_stride;
-        double* out = d.out + (int64_t)s * d.s_stride;
-        if (d.left) {
-            // out[yh] = sum_yl Lq[yh][yl] v[yl]
-            if (nj >= 32) {
-                for (int yh = lane; yh < nj; yh += 32) {
-                    double acc = 0.0;
-                    const double* row = lq + yh * rs;
-                    for (int yl = 0; yl < nm; ++yl) acc = fma(row[yl], (double)__ldg(v + yl), acc);
-                    out[(int64_t)yh * d.i_stride] = acc;
-                }
-            } else {
-                for (int yh = 0; yh < nj; ++yh) {
-                    double acc = 0.0;
-                    const double* row = lq + yh * rs;
-                    for (int yl = lane; yl < nm; yl += 32) acc = fma(row[yl], (double)__ldg(v + yl), acc);
-#pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, off);
-                    if (lane == 0) out[(int64_t)yh * d.i_stride] = acc;
-                }
-            }
-        } else {
-            // out[yl] = sum_yh v[yh] Lq[yh][yl]
-            if (nm >= 32) {
-                for (int yl = lane; yl < nm; yl += 32) {
-                    double acc = 0.0;
-                    for (int yh = 0; yh < nj; ++yh) acc = fma((double)__ldg(v + yh), lq[yh * rs + yl], acc);
-                    out[(int64_t)yl * d.i_stride] = acc;
-                }
-            } else {
-                double acc[32];
-#pragma unroll
-                for (int yl = 0; yl < 32; ++yl) acc[yl] = 0.0;
-                for (int yh = lane; yh < nj; yh += 32) {
-                    const double vv = (double)__ldg(v + yh);
-                    const double* row = lq + yh * rs;
-#pragma unroll
-                    for (int yl = 0; yl < 32; ++yl)
-                        if (yl < nm) acc[yl] = fma(vv, row[yl], acc[yl]);
-                }
-#pragma unroll
-                for (int yl = 0; yl < 32; ++yl) {
-                    if (yl >= nm) break;
-                    double a = acc[yl];
-#pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xFFFFFFFFu, a, off);
-                    if (lane == 0) out[(int64_t)yl * d.i_stride] = a;
-                }
-            }
-        }
+static cudaError_t launch_store(const Launch& L, cudaStream_t s, const DevState* st) {
+    if (L.n == 0 || L.tiles == 0) return cudaSuccess;
+    const int sm = cfg_smem(L.cfg);
+    switch (L.cfg) {
+        case CFG_128x128: k_mma_store<BDC_CFG_ARGS_128x128><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
+        case CFG_128x64: k_mma_store<BDC_CFG_ARGS_128x64><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
+        case CFG_64x128: k_mma_store<BDC_CFG_ARGS_64x128><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
+        case CFG_64x64: k_mma_store<BDC_CFG_ARGS_64x64><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
+        case CFG_128x16: k_mma_store<BDC_CFG_ARGS_128x16><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
+        case CFG_16x128: k_mma_store<BDC_CFG_ARGS_16x128><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
+        default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_ba(const Launch& L, const BaEpilogue& ep, cudaStream_t s, const DevState* st) {
+    const int sm = cfg_smem(L.cfg);
+    switch (L.cfg) {
+        case CFG_128x128: k_mma_ba<BDC_CFG_ARGS_128x128><<<L.tiles, 256, sm, s>>>(L.d, ep, st); break;
+        case CFG_128x64: k_mma_ba<BDC_CFG_ARGS_128x64><<<L.tiles, 256, sm, s>>>(L.d, ep, st); break;
+        case CFG_64x128: k_mma_ba<BDC_CFG_ARGS_64x128><<<L.tiles, 256, sm, s>>>(L.d, ep, st); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------ small kernels
@@ -726,6 +578,15 @@ static Operand op_f64(const double* p, int64_t ld, int trans) {
     return o;
 }
 
+static Operand op_u16(const uint16_t* p, int64_t ld, int trans) {
+    Operand o;
+    o.ptr = p;
+    o.ld = ld;
+    o.kind = OP_U16;
+    o.trans = trans;
+    return o;
+}
+
 static GemmDesc make_desc(Operand A, Operand B, double* C, int64_t ldc_m, int64_t ldc_n, int M, int N, int K) {
     GemmDesc d{};
     d.A = A;
@@ -741,37 +602,119 @@ static GemmDesc make_desc(Operand A, Operand B, double* C, int64_t ldc_m, int64_
     return d;
 }
 
-static int assign_tiles(std::vector<GemmDesc>& v, int bm, int bn) {
+// the operand restricted to contraction indices >= k0
+static Operand k_offset(Operand o, bool is_a, int64_t k0) {
+    if (o.kind == OP_EYE || k0 == 0) return o;
+    const int64_t step = is_a ? (o.trans ? k0 * o.ld : k0) : (o.trans ? k0 : k0 * o.ld);
+    if (o.kind == OP_U16) o.ptr = (const uint16_t*)o.ptr + step;
+    else o.ptr = (const double*)o.ptr + step;
+    return o;
+}
+
+// S products over consecutive slices of the contraction, output s at C + s * cstride
+static void split_k(std::vector<GemmDesc>& out, const GemmDesc& d, int S, int64_t cstride) {
+    for (int s = 0; s < S; ++s) {
+        const int64_t k0 = (int64_t)d.K * s / S, k1 = (int64_t)d.K * (s + 1) / S;
+        GemmDesc e = d;
+        e.A = k_offset(d.A, true, k0);
+        e.B = k_offset(d.B, false, k0);
+        e.K = (int)(k1 - k0);
+        e.C = d.C + s * cstride;
+        out.push_back(e);
+    }
+}
+
+static int assign_tiles(std::vector<GemmDesc>& v, int cfg) {
     int t = 0;
     for (auto& d : v) {
-        d.tiles_m = (d.M + bm - 1) / bm;
-        d.tiles_n = (d.N + bn - 1) / bn;
+        d.tiles_m = (d.M + kCfgBM[cfg] - 1) / kCfgBM[cfg];
+        d.tiles_n = (d.N + kCfgBN[cfg] - 1) / kCfgBN[cfg];
         d.tile_begin = t;
         t += d.tiles_m * d.tiles_n;
     }
     return t;
 }
 
-template <typename T>
-static cudaError_t upload(const std::vector<T>& v, T** dst) {
+static cudaError_t make_launch(Launch& L, std::vector<GemmDesc> v, int cfg) {
+    if (L.d) cudaFree(L.d);
+    L.d = nullptr;
+    L.cfg = cfg;
+    L.n = (int)v.size();
+    L.tiles = assign_tiles(v, cfg);
     if (v.empty()) return cudaSuccess;
-    cudaError_t e = cudaMalloc(dst, sizeof(T) * v.size());
+    cudaError_t e = cudaMalloc(&L.d, sizeof(GemmDesc) * v.size());
     if (e != cudaSuccess) return e;
-    return cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+    return cudaMemcpy(L.d, v.data(), sizeof(GemmDesc) * v.size(), cudaMemcpyHostToDevice);
+}
+
+// tile shape for a small product from its shape
+static int small_cfg(int M, int N) {
+    if (N <= 16) return CFG_128x16;
+    if (M <= 16) return CFG_16x128;
+    return CFG_64x64;
+}
+
+template <typename F>
+static float time_ms(bdc_handle* H, F&& launch) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    launch();  // warm-up
+    cudaEventRecord(a, H->stream);
+    for (int r = 0; r < 3; ++r) launch();
+    cudaEventRecord(b, H->stream);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return (cudaGetLastError() == cudaSuccess) ? ms / 3.f : 1e30f;
+}
+
+// chooses tile shape and split of one of the thin products by timing them
+static bdc_status tune_thin(bdc_handle* H, Launch& L, const GemmDesc& base, int64_t cstride, int max_split,
+                            int kmin, const char* what, int* split_out) {
+    const int cfgs[4] = {CFG_128x128, CFG_128x64, CFG_64x128, CFG_64x64};
+    float best = 1e30f;
+    int best_cfg = CFG_64x64, best_s = 1;
+    for (int ci = 0; ci < 4; ++ci) {
+        for (int S = 1; S <= max_split; S *= 2) {
+            if (base.K / S < kmin) break;
+            std::vector<GemmDesc> v;
+            split_k(v, base, S, cstride);
+            Launch T;
+            BDC_CUDA_TRY(make_launch(T, v, cfgs[ci]));
+            if (T.tiles > 64 * H->num_sms) {
+                cudaFree(T.d);
+                continue;
+            }
+            const float ms = time_ms(H, [&] { launch_store(T, H->stream, nullptr); });
+            cudaFree(T.d);
+            if (ms < best) {
+                best = ms;
+                best_cfg = cfgs[ci];
+                best_s = S;
+            }
+        }
+    }
+    std::vector<GemmDesc> v;
+    split_k(v, base, best_s, cstride);
+    BDC_CUDA_TRY(make_launch(L, v, best_cfg));
+    *split_out = best_s;
+    if (H->verbose)
+        printf("bdc: tuned %s: tile %dx%d, split %d, %.1f us\n", what, kCfgBM[best_cfg], kCfgBN[best_cfg], best_s,
+               best * 1e3f);
+    return BDC_OK;
 }
 
 bool factored_supports(int n, int k) {
     // needs k < n (W is not the identity), half tables that fit the uint16
-    // bundles, and a dense 2^n state that fits comfortably in device memory
+    // bundles, and a dense 2^{n-1} state that fits comfortably in device memory
     return k >= 1 && k < n && n >= 2 && n <= 28 && k <= 14;
 }
 
-static int qsmall_opt(int k) {
-    const int ny = 1 << k;
-    return ny >= 256 ? ny / 256 : 1;
-}
-
 bdc_status factored_init(bdc_handle* H) {
+    BDC_CUDA_TRY(set_smem_attrs());
     FactoredState* F = new FactoredState();
     H->fac = F;
     const Split& s = H->s;
@@ -781,7 +724,6 @@ bdc_status factored_init(bdc_handle* H) {
     // x_hi < H1 / 2: only those rows of the iterate and of G are needed
     F->H1h = F->H1 / 2;
     const int k = H->k;
-    // terms and their association
     int KL = 0, KR = 0;
     for (int j = s.jlo; j <= s.jhi; ++j) {
         Term t{};
@@ -805,12 +747,7 @@ bdc_status factored_init(bdc_handle* H) {
     const int ny = 1 << k;
     const int H1 = F->H1h, H2 = F->H2, Kp = F->Kp;  // H1: the rows kept
     const int KLa = KL > 0 ? KL : 1, KRa = KR > 0 ? KR : 1;
-
-    // small q products: split the contracted range so the launch fills the GPU
-    int n_outer = 0;
-    for (auto& t : F->terms) n_outer += (t.left ? !t.idB : !t.idA);
-    F->QS = n_outer > 0 ? std::max(1, std::min(64, (H->num_sms * 4) / n_outer)) : 1;
-    while (F->QS > 1 && (std::min(H1, H2) / F->QS) < 16) F->QS /= 2;
+    const int max_split = 16;
 
     auto al = [&](double** p, size_t cnt) -> cudaError_t {
         H->bytes += cnt * sizeof(double);
@@ -823,28 +760,18 @@ bdc_status factored_init(bdc_handle* H) {
     BDC_CUDA_TRY(al(&F->RB, (size_t)Kp * H2));
     BDC_CUDA_TRY(al(&F->UL, (size_t)H2 * KLa));
     BDC_CUDA_TRY(al(&F->VR, (size_t)H1 * KRa));
-    // split-K of the two thin products so that they fill the GPU
-    const int tiles_ul = ((KL + 127) / 128) * ((H2 + 127) / 128);
-    const int tiles_vr = ((H1 + 127) / 128) * ((KR + 127) / 128);
-    F->S1 = KL > 0 ? std::max(1, std::min(32, (H->num_sms * 4) / std::max(1, tiles_ul))) : 1;
-    F->S2 = KR > 0 ? std::max(1, std::min(32, (H->num_sms * 4) / std::max(1, tiles_vr))) : 1;
-    while (F->S1 > 1 && (H1 % F->S1 || H1 / F->S1 < 8)) --F->S1;
-    while (F->S2 > 1 && (H2 % F->S2 || H2 / F->S2 < 8)) --F->S2;
-    BDC_CUDA_TRY(al(&F->ulpart, (size_t)F->S1 * H2 * KLa));
-    BDC_CUDA_TRY(al(&F->vrpart, (size_t)F->S2 * H1 * KRa));
-    BDC_CUDA_TRY(al(&F->qparts, (size_t)F->T * F->QS * ny));
-    BDC_CUDA_TRY(al(&F->qsum, (size_t)F->T * ny));
+    BDC_CUDA_TRY(al(&F->ulpart, (size_t)max_split * H2 * KLa));
+    BDC_CUDA_TRY(al(&F->vrpart, (size_t)max_split * H1 * KRa));
     BDC_CUDA_TRY(al(&F->lnq_full, (size_t)ny));
-    F->ctas_g = ((H1 + 127) / 128) * ((H2 + 127) / 128);
-    BDC_CUDA_TRY(al(&F->epart, (size_t)std::max(F->ctas_g * 2, 2 * H->nb_upd) * 4));
     BDC_CUDA_TRY(cudaMemsetAsync(F->LA, 0, sizeof(double) * H1 * Kp, H->stream));
     BDC_CUDA_TRY(cudaMemsetAsync(F->RB, 0, sizeof(double) * Kp * H2, H->stream));
     BDC_CUDA_TRY(cudaMemsetAsync(F->hx, 0, sizeof(double) * NX, H->stream));
     BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
     BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
-    BDC_CUDA_TRY(cudaMemsetAsync(F->qparts, 0, sizeof(double) * F->T * F->QS * ny, H->stream));
+    BDC_CUDA_TRY(cudaMemsetAsync(F->lnq_full, 0, sizeof(double) * ny, H->stream));
 
-    // constant table columns of LA (AL) and rows of RB (BR^T)
+    // constant table columns of LA (AL) and rows of RB (BR^T); a left term's
+    // A_j or a right term's B_m is never the identity
     {
         std::vector<int> colmap(KL + KR + 1);
         for (auto& t : F->terms) {
@@ -854,7 +781,6 @@ bdc_status factored_init(bdc_handle* H) {
         int* d_cm = nullptr;
         BDC_CUDA_TRY(cudaMalloc(&d_cm, sizeof(int) * colmap.size()));
         BDC_CUDA_TRY(cudaMemcpy(d_cm, colmap.data(), sizeof(int) * colmap.size(), cudaMemcpyHostToDevice));
-        // a left term's A_j or a right term's B_m is never the identity
         k_fill_tables<<<H->num_sms * 8, 256, 0, H->stream>>>(H1, H2, Kp, H->A.rows, H->A.stride, H->B.rows,
                                                             H->B.stride, d_cm, KL, KR, F->LA, F->RB);
         BDC_CUDA_TRY(cudaGetLastError());
@@ -864,127 +790,130 @@ bdc_status factored_init(bdc_handle* H) {
     k_scatter<<<H->num_sms * 8, 256, 0, H->stream>>>(H->d_reps, H->R, H->d_h, F->hx);
     BDC_CUDA_TRY(cudaGetLastError());
 
-    // ---- the two thin products, split over the contraction:
-    //   U^T (H2 x KL) = (AL^T Pw)^T and V (H1h x KR) = Pw BR
-    std::vector<GemmDesc> big;
+    // ---- the two thin products: U^T (H2 x KL) = (AL^T Pw)^T, V (H1h x KR) = Pw BR
     if (KL > 0) {
-        const int kc = H1 / F->S1;
-        for (int sidx = 0; sidx < F->S1; ++sidx) {
-            // A(m = c, kk = x_hi) = LA[x_hi * Kp + c]; B(kk = x_hi, n = x_lo) = Pw; C(c, x_lo) -> U^T[x_lo][c]
-            Operand A = op_f64(F->LA + (int64_t)sidx * kc * Kp, Kp, 1);
-            Operand B = op_f64(F->Pw + (int64_t)sidx * kc * H2, H2, 0);
-            big.push_back(make_desc(A, B, F->ulpart + (size_t)sidx * H2 * KL, 1, KL, KL, H2, kc));
-        }
+        // A(m = c, kk = x_hi) = LA[x_hi * Kp + c]; B(kk = x_hi, n = x_lo) = Pw; C(c, x_lo) -> U^T[x_lo][c]
+        GemmDesc d = make_desc(op_f64(F->LA, Kp, 1), op_f64(F->Pw, H2, 0), F->ulpart, 1, KL, KL, H2, H1);
+        bdc_status rc = tune_thin(H, F->ul, d, (int64_t)H2 * KL, max_split, 16, "U = AL^T Pw", &F->S1);
+        if (rc != BDC_OK) return rc;
     }
     if (KR > 0) {
-        const int kc = H2 / F->S2;
-        for (int sidx = 0; sidx < F->S2; ++sidx) {
-            // A(m = x_hi, kk = x_lo) = Pw; B(kk = x_lo, n = c) = RB[(KL + c) * H2 + x_lo]
-            Operand A = op_f64(F->Pw + (int64_t)sidx * kc, H2, 0);
-            Operand B = op_f64(F->RB + (int64_t)KL * H2 + (int64_t)sidx * kc, H2, 1);
-            big.push_back(make_desc(A, B, F->vrpart + (size_t)sidx * H1 * KR, KR, 1, H1, KR, kc));
-        }
+        // A(m = x_hi, kk = x_lo) = Pw; B(kk = x_lo, n = c) = RB[(KL + c) * H2 + x_lo]
+        GemmDesc d = make_desc(op_f64(F->Pw, H2, 0), op_f64(F->RB + (int64_t)KL * H2, H2, 1), F->vrpart, KR, 1,
+                               H1, KR, H2);
+        bdc_status rc = tune_thin(H, F->vr, d, (int64_t)H1 * KR, max_split, 16, "V = Pw BR", &F->S2);
+        if (rc != BDC_OK) return rc;
     }
-    F->n_big = (int)big.size();
-    F->tiles_big = assign_tiles(big, 128, 128);
-    BDC_CUDA_TRY(upload(big, &F->d_big));
 
     // ---- per-term small products and the fold plan
-    std::vector<OuterDesc> outer;
-    std::vector<MatvecDesc> mv;
+    std::vector<GemmDesc> qs[CFG_COUNT], ds[CFG_COUNT];
     std::vector<FoldTerm> fold;
-    int cta = 0;
+    std::vector<std::pair<int, GemmDesc>> qprod;  // (term, product) before splitting
     for (int ti = 0; ti < F->T; ++ti) {
         const Term& t = F->terms[ti];
+        const int nj = 1 << t.j, nm = 1 << t.m;
         FoldTerm f{};
         f.j = t.j;
         f.m = t.m;
         f.off = t.off;
-        if (t.left) {
-            if (t.idB) {
-                f.kind = 1;       // Q_t = U_t
-                f.idB_left = 1;   // M_t = Lq_t
-            } else {
-                OuterDesc o{};
-                o.a = F->UL + t.off;                       // a(s)[yh] = U^T[s][off + yh]
-                o.a_stride = KL;
-                o.a_u16 = 0;
-                o.b = H->B.rows + bundle_offset(t.m);      // b(s)[yl] = B_m[s][yl]
-                o.b_stride = H->B.stride;
-                o.b_u16 = 1;
-                o.j = t.j;
-                o.m = t.m;
-                o.S = H2;
-                o.term = ti;
-                outer.push_back(o);
-                MatvecDesc d{};
-                d.v = H->B.rows + bundle_offset(t.m);
-                d.v_stride = H->B.stride;
-                d.out = F->RB + (int64_t)t.off * H2;       // M_t[yh][s] -> RB[off + yh][s]
-                d.s_stride = 1;
-                d.i_stride = H2;
-                d.j = t.j;
-                d.m = t.m;
-                d.left = 1;
-                d.S = H2;
-                d.cta_begin = cta;
-                cta += (H2 + F->dsmall_chunk - 1) / F->dsmall_chunk;
-                mv.push_back(d);
-            }
+        Operand Lq = op_f64(F->lnq_full, nm, 0);  // Lq_t(yh, yl)
+        if (t.left && t.idB) {
+            f.kind = 1;       // Q_t = U_t
+            f.idB_left = 1;   // M_t = Lq_t
+        } else if (!t.left && t.idA) {
+            f.kind = 2;        // Q_t = V_t
+            f.idA_right = 1;   // N_t = Lq_t
+        } else if (t.left) {
+            // Q_t = U_t B_m: U_t(yh, x_lo) = U^T[x_lo][off + yh]; B_m(x_lo, yl)
+            qprod.push_back({ti, make_desc(op_f64(F->UL + t.off, KL, 1),
+                                           op_u16(H->B.rows + bundle_offset(t.m), H->B.stride, 0), nullptr, nm, 1,
+                                           nj, nm, H2)});
+            // M_t = Lq_t B_m^T -> RB rows [off, off + 2^j)
+            GemmDesc d = make_desc(Lq, op_u16(H->B.rows + bundle_offset(t.m), H->B.stride, 1),
+                                   F->RB + (int64_t)t.off * H2, H2, 1, nj, H2, nm);
+            ds[small_cfg(d.M, d.N)].push_back(d);
         } else {
-            if (t.idA) {
-                f.kind = 2;        // Q_t = V_t
-                f.idA_right = 1;   // N_t = Lq_t
-            } else {
-                OuterDesc o{};
-                o.a = H->A.rows + bundle_offset(t.j);      // a(s)[yh] = A_j[s][yh]
-                o.a_stride = H->A.stride;
-                o.a_u16 = 1;
-                o.b = F->VR + t.off;                       // b(s)[yl] = V[s][off + yl]
-                o.b_stride = KR;
-                o.b_u16 = 0;
-                o.j = t.j;
-                o.m = t.m;
-                o.S = H1;
-                o.term = ti;
-                outer.push_back(o);
-                MatvecDesc d{};
-                d.v = H->A.rows + bundle_offset(t.j);
-                d.v_stride = H->A.stride;
-                d.out = F->LA + KL + t.off;                // N_t[s][yl] -> LA[s][KL + off + yl]
-                d.s_stride = Kp;
-                d.i_stride = 1;
-                d.j = t.j;
-                d.m = t.m;
-                d.left = 0;
-                d.S = H1;
-                d.cta_begin = cta;
-                cta += (H1 + F->dsmall_chunk - 1) / F->dsmall_chunk;
-                mv.push_back(d);
-            }
+            // Q_t = A_j^T V_t: A_j^T(yh, x_hi) = A_j[x_hi][yh]; V_t(x_hi, yl) = V[x_hi][off + yl]
+            qprod.push_back({ti, make_desc(op_u16(H->A.rows + bundle_offset(t.j), H->A.stride, 1),
+                                           op_f64(F->VR + t.off, KR, 0), nullptr, nm, 1, nj, nm, H1)});
+            // N_t = A_j Lq_t -> LA columns [KL + off, + 2^m) of the rows x_hi < H1h
+            GemmDesc d = make_desc(op_u16(H->A.rows + bundle_offset(t.j), H->A.stride, 0), Lq,
+                                   F->LA + KL + t.off, Kp, 1, H1, nm, nj);
+            ds[small_cfg(d.M, d.N)].push_back(d);
         }
         fold.push_back(f);
     }
-    F->n_qsmall = (int)outer.size();
-    F->n_dsmall = (int)mv.size();
-    F->ctas_dsmall = cta;
-    int max_smem = 0;
-    for (auto& d : mv) max_smem = std::max(max_smem, (int)(sizeof(double) * (1 << d.j) * ((1 << d.m) + 1)));
-    F->smem_dsmall = max_smem;
-    if (max_smem > 48 * 1024)
-        BDC_CUDA_TRY(cudaFuncSetAttribute(k_dsmall, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
-    BDC_CUDA_TRY(upload(outer, &F->d_qsmall));
-    BDC_CUDA_TRY(upload(mv, &F->d_dsmall));
-    BDC_CUDA_TRY(upload(fold, &F->d_fold));
-
-    // ---- G = LA RB with the BA epilogue
-    {
-        std::vector<GemmDesc> g;
-        g.push_back(make_desc(op_f64(F->LA, Kp, 0), op_f64(F->RB, H2, 0), nullptr, 0, 0, H1, H2, Kp));
-        assign_tiles(g, 128, 128);
-        BDC_CUDA_TRY(upload(g, &F->d_g));
+    // one split count for all small q products: enough CTAs to fill the GPU
+    int qtiles = 0, kmin = 1 << 30;
+    for (auto& pq : qprod) {
+        const int c = small_cfg(pq.second.M, pq.second.N);
+        qtiles += ((pq.second.M + kCfgBM[c] - 1) / kCfgBM[c]) * ((pq.second.N + kCfgBN[c] - 1) / kCfgBN[c]);
+        kmin = std::min(kmin, pq.second.K);
     }
-    F->launches_per_iter = (F->n_big > 0 ? 2 : 0) + (F->n_qsmall > 0) + 2 + (F->n_dsmall > 0) + 1 + 1;
+    F->QS = 1;
+    if (qtiles > 0)
+        while (F->QS < 16 && qtiles * F->QS * 2 <= 4 * H->num_sms && kmin / (F->QS * 2) >= 64) F->QS *= 2;
+    BDC_CUDA_TRY(al(&F->qparts, (size_t)F->T * F->QS * ny));
+    BDC_CUDA_TRY(al(&F->qsum, (size_t)F->T * ny));
+    BDC_CUDA_TRY(cudaMemsetAsync(F->qparts, 0, sizeof(double) * F->T * F->QS * ny, H->stream));
+    for (auto& pq : qprod) {
+        GemmDesc d = pq.second;
+        d.C = F->qparts + (size_t)pq.first * F->QS * ny;
+        split_k(qs[small_cfg(d.M, d.N)], d, F->QS, ny);
+    }
+    for (int c = 0; c < CFG_COUNT; ++c) {
+        if (!qs[c].empty()) {
+            F->qsmall.emplace_back();
+            BDC_CUDA_TRY(make_launch(F->qsmall.back(), qs[c], c));
+        }
+        if (!ds[c].empty()) {
+            F->dsmall.emplace_back();
+            BDC_CUDA_TRY(make_launch(F->dsmall.back(), ds[c], c));
+        }
+    }
+    {
+        BDC_CUDA_TRY(cudaMalloc(&F->d_fold, sizeof(FoldTerm) * fold.size()));
+        BDC_CUDA_TRY(cudaMemcpy(F->d_fold, fold.data(), sizeof(FoldTerm) * fold.size(), cudaMemcpyHostToDevice));
+    }
+
+    // ---- G = LA RB with the BA epilogue; the tile shape is tuned on the
+    // zero state (set_p re-initialises everything it touches)
+    {
+        const int cfgs[3] = {CFG_128x128, CFG_128x64, CFG_64x128};
+        int ctas_max = 0;
+        for (int c : cfgs) ctas_max = std::max(ctas_max, ((H1 + kCfgBM[c] - 1) / kCfgBM[c]) * ((H2 + kCfgBN[c] - 1) / kCfgBN[c]));
+        BDC_CUDA_TRY(al(&F->epart, (size_t)std::max(ctas_max, H->nb_upd) * 8));
+        float best = 1e30f;
+        int best_cfg = CFG_128x64;
+        GemmDesc d = make_desc(op_f64(F->LA, Kp, 0), op_f64(F->RB, H2, 0), nullptr, 0, 0, H1, H2, Kp);
+        BaEpilogue ep{};
+        ep.n = H->n;
+        ep.n2 = H->s.n2;
+        ep.hx = F->hx;
+        ep.Lt = F->Lt;
+        ep.Pw = F->Pw;
+        ep.inv_c = H->inv_c;
+        ep.part = F->epart;
+        for (int c : cfgs) {
+            Launch T;
+            BDC_CUDA_TRY(make_launch(T, {d}, c));
+            const float ms = time_ms(H, [&] { launch_ba(T, ep, H->stream, H->d_st); });
+            cudaFree(T.d);
+            if (ms < best) {
+                best = ms;
+                best_cfg = c;
+            }
+        }
+        BDC_CUDA_TRY(make_launch(F->g, {d}, best_cfg));
+        F->ctas_g = F->g.tiles;
+        if (H->verbose)
+            printf("bdc: tuned G: tile %dx%d, %.1f us\n", kCfgBM[best_cfg], kCfgBN[best_cfg], best * 1e3f);
+        BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
+        BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
+        BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
+    }
+    F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + (int)F->qsmall.size() + 2 +
+                           (int)F->dsmall.size() + 1 + 1;
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
 }
@@ -995,10 +924,9 @@ void factored_free(bdc_handle* H) {
     for (double* p : {F->Pw, F->Lt, F->hx, F->LA, F->RB, F->UL, F->VR, F->ulpart, F->vrpart, F->qparts,
                       F->qsum, F->lnq_full, F->epart})
         cudaFree(p);
-    cudaFree(F->d_big);
-    cudaFree(F->d_g);
-    cudaFree(F->d_qsmall);
-    cudaFree(F->d_dsmall);
+    for (Launch* L : {&F->ul, &F->vr, &F->g}) cudaFree(L->d);
+    for (auto& L : F->qsmall) cudaFree(L.d);
+    for (auto& L : F->dsmall) cudaFree(L.d);
     cudaFree(F->d_fold);
     delete F;
     H->fac = nullptr;
@@ -1021,38 +949,23 @@ static BaEpilogue make_epilogue(bdc_handle* H) {
 // the stages of one iteration, each gated by DevState::done / error
 enum Stage { ST_QBIG = 0, ST_QSMALL, ST_FOLD, ST_DSMALL, ST_G, ST_FIN, ST_COUNT };
 
-static cudaError_t launch_qsmall(bdc_handle* H) {
-    FactoredState* F = H->fac;
-    const int grid = F->n_qsmall * F->QS;
-    switch (qsmall_opt(H->k)) {
-        case 1: k_qsmall<1><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
-        case 2: k_qsmall<2><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
-        case 4: k_qsmall<4><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
-        case 8: k_qsmall<8><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
-        case 16: k_qsmall<16><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
-        case 32: k_qsmall<32><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
-        case 64: k_qsmall<64><<<grid, 256, 0, H->stream>>>(F->d_qsmall, F->QS, H->k, F->qparts, H->d_st); break;
-        default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
-}
-
 static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
     FactoredState* F = H->fac;
     cudaStream_t s = H->stream;
-    const BaEpilogue ep = make_epilogue(H);
+    cudaError_t e = cudaSuccess;
     switch (stage) {
         case ST_QBIG: {
-            if (F->n_big > 0) {
-                k_gemm_tile<128, 128, 8, 4, 2, 0><<<F->tiles_big, 256, 0, s>>>(F->d_big, F->n_big, ep, H->d_st);
-                const int64_t na = (int64_t)F->KL * F->H2, nb = (int64_t)F->H1h * F->KR;
-                k_sum_parts<<<H->num_sms * 4, 256, 0, s>>>(F->ulpart, F->S1, F->KL > 0 ? na : 0, F->UL, F->vrpart,
-                                                           F->S2, F->KR > 0 ? nb : 0, F->VR, H->d_st);
-            }
+            e = launch_store(F->ul, s, H->d_st);
+            if (e == cudaSuccess) e = launch_store(F->vr, s, H->d_st);
+            if (e != cudaSuccess) return e;
+            const int64_t na = (int64_t)F->KL * F->H2, nb = (int64_t)F->H1h * F->KR;
+            k_sum_parts<<<H->num_sms * 4, 256, 0, s>>>(F->ulpart, F->S1, F->KL > 0 ? na : 0, F->UL, F->vrpart,
+                                                       F->S2, F->KR > 0 ? nb : 0, F->VR, H->d_st);
             break;
         }
         case ST_QSMALL:
-            if (F->n_qsmall > 0) return launch_qsmall(H);
+            for (auto& L : F->qsmall)
+                if ((e = launch_store(L, s, H->d_st)) != cudaSuccess) return e;
             break;
         case ST_FOLD: {
             const int ny = 1 << H->k;
@@ -1064,13 +977,11 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             break;
         }
         case ST_DSMALL:
-            if (F->n_dsmall > 0)
-                k_dsmall<<<F->ctas_dsmall, 256, F->smem_dsmall, s>>>(F->d_dsmall, F->n_dsmall, F->dsmall_chunk,
-                                                                     F->lnq_full, H->d_st);
+            for (auto& L : F->dsmall)
+                if ((e = launch_store(L, s, H->d_st)) != cudaSuccess) return e;
             break;
         case ST_G:
-            k_gemm_tile<128, 128, 8, 4, 2, 1><<<F->ctas_g, 256, 0, s>>>(F->d_g, 1, ep, H->d_st);
-            break;
+            return launch_ba(F->g, make_epilogue(H), s, H->d_st);
         case ST_FIN:
             k_fac_finalize<<<1, 256, 0, s>>>(F->epart, F->ctas_g, a, H->d_st);
             break;

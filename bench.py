@@ -294,7 +294,7 @@ def kernels_only(args) -> None:
     """Engine set-up and `steps` iterations, nothing else: the command that
     the ncu captures under profiles/ run."""
     import bdc_b200
-    E = bdc_b200.Engine(args.n, args.k, engine=args.engine)
+    E = bdc_b200.Engine(args.n, args.k, engine=args.engine, verbose=True)
     E.set_uniform()
     st = E.iterate(args.steps, float("-inf"))
     print(json.dumps({"engine": E.engine, "n": args.n, "k": args.k, "iters": st["iters"],

@@ -154,7 +154,7 @@ bdc_status bdc_profile(bdc_handle_t h, int iters, bdc_profile_t* out);
 bdc_status bdc_set_stream(bdc_handle_t h, void* cuda_stream);
 
 /* Device throughput probe: kind 0 = int32 multiply-add (IMAD), 1 = FP64 FMA,
- * 2 = FP32 FMA.  Runs a register-resident chain kernel on `device` for about
+ * 2 = FP32 FMA, 3 = FP64 tensor-core multiply-add (mma.sync m8n8k4).  Runs a register-resident chain kernel on `device` for about
  * `ms` milliseconds and returns operations per second (one multiply-add = 1
  * operation).  Used as the measured denominator of roofline fractions. */
 bdc_status bdc_peak_probe(int device, int kind, double ms, double* ops_per_s);
