@@ -45,6 +45,8 @@ constexpr int kErrShift = 1;  // DevState::error: exp shift out of range, re-sca
 struct FoldTerm {
     int kind;
     int j, m, off;
+    int64_t qoff;   // kind 0: first split slice of Q_t in qparts
+    int qs;         // kind 0: number of split slices
     int idB_left;   // L term with identity B_m: RB rows [off, off+2^j) = Lq_t
     int idA_right;  // R term with identity A_j: LA columns [KL+off, +2^m) = Lq_t
 };
@@ -66,6 +68,15 @@ struct Launch {
     int n = 0, tiles = 0, cfg = CFG_64x64;
 };
 
+// sum of S split slices [S][M][N] into a strided destination
+struct SumDesc {
+    const double* part;
+    double* dst;
+    int64_t ldc_m, ldc_n;
+    int S, M, N;
+    int64_t begin;    // first element index of this product in the launch
+};
+
 }  // namespace bdc
 
 struct FactoredState {
@@ -82,9 +93,12 @@ struct FactoredState {
     double* ulpart = nullptr; // [S1][H2][KL]
     double* vrpart = nullptr; // [S2][H1h][KR]
     int S1 = 1, S2 = 1;
-    double* qparts = nullptr; // [T][QS][2^k]
+    double* qparts = nullptr; // split slices of the small q products (FoldTerm::qoff)
     double* qsum = nullptr;   // [T][2^k]  qparts summed over the splits
-    int QS = 1;               // split of the contraction of the small q products
+    double* dparts = nullptr; // split slices of the small D products
+    bdc::SumDesc* d_dsum = nullptr;
+    int n_dsum = 0;
+    int64_t dsum_elems = 0;
     double* lnq_full = nullptr;  // [2^k]
     double* epart = nullptr;  // [ctas][8]
     int ctas_g = 0;
@@ -319,18 +333,35 @@ __global__ void k_sum_parts(const double* __restrict__ a, int sa, int64_t na, do
 // terms of Q_t[y] (split slices, or U^T / V rows for identity terms); ln q
 // with the reference's 0 for q == 0 (backend/BAA.cu:573-580), expanded to
 // every y, and copied into RB / LA where a D-side product is the identity.
-// phase 1: qsum[t][y] = sum over the splits of qparts[t][split][y]
-__global__ void k_qsum(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ qparts, int QS, int k,
+// phase 1: qsum[t][y] = sum over the split slices of Q_t
+__global__ void k_qsum(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ qparts, int k,
                        double* __restrict__ qsum, const DevState* st) {
     if (gated(st)) return;
     const int ny = 1 << k;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < T * ny; e += gridDim.x * blockDim.x) {
         const int t = e / ny, y = e % ny;
-        if (terms[t].kind != 0) continue;
-        const double* q = qparts + (size_t)t * QS * ny + y;
+        const FoldTerm& f = terms[t];
+        if (f.kind != 0) continue;
+        const double* q = qparts + f.qoff + y;
         double a = 0.0;
-        for (int sp = 0; sp < QS; ++sp) a += q[(size_t)sp * ny];
+        for (int sp = 0; sp < f.qs; ++sp) a += q[(size_t)sp * ny];
         qsum[e] = a;
+    }
+}
+
+// D-side split sums into RB / LA
+__global__ void k_dsum(const SumDesc* __restrict__ descs, int nd, int64_t total, const DevState* st) {
+    if (gated(st)) return;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        int i = 0;
+        while (i + 1 < nd && descs[i + 1].begin <= e) ++i;
+        const SumDesc& d = descs[i];
+        const int64_t l = e - d.begin;
+        const int64_t mn = (int64_t)d.M * d.N;
+        const int m = (int)(l / d.N), n = (int)(l % d.N);
+        double a = 0.0;
+        for (int sp = 0; sp < d.S; ++sp) a += d.part[sp * mn + l];
+        d.dst[(int64_t)m * d.ldc_m + (int64_t)n * d.ldc_n] = a;
     }
 }
 
@@ -805,10 +836,16 @@ bdc_status factored_init(bdc_handle* H) {
         if (rc != BDC_OK) return rc;
     }
 
-    // ---- per-term small products and the fold plan
+    // ---- per-term small products and the fold plan.  Each small product is
+    // split over its contraction so that a CTA runs at most ~8 k-slices
+    // (their shapes are thin: 2^j x 2^{k-j} outputs over a 2^{n/2} contraction,
+    // or 2^{n/2} x 2^{k-j} over 2^j); q-side slices are summed by the fold,
+    // D-side slices by k_dsum into RB / LA.
+    auto split_of = [](int K) { return std::max(1, std::min(32, K / 128)); };
     std::vector<GemmDesc> qs[CFG_COUNT], ds[CFG_COUNT];
     std::vector<FoldTerm> fold;
-    std::vector<std::pair<int, GemmDesc>> qprod;  // (term, product) before splitting
+    std::vector<SumDesc> dsum;
+    std::vector<std::pair<int, GemmDesc>> qprod, dprod;  // (term, product) before splitting
     for (int ti = 0; ti < F->T; ++ti) {
         const Term& t = F->terms[ti];
         const int nj = 1 << t.j, nm = 1 << t.m;
@@ -829,37 +866,70 @@ bdc_status factored_init(bdc_handle* H) {
                                            op_u16(H->B.rows + bundle_offset(t.m), H->B.stride, 0), nullptr, nm, 1,
                                            nj, nm, H2)});
             // M_t = Lq_t B_m^T -> RB rows [off, off + 2^j)
-            GemmDesc d = make_desc(Lq, op_u16(H->B.rows + bundle_offset(t.m), H->B.stride, 1),
-                                   F->RB + (int64_t)t.off * H2, H2, 1, nj, H2, nm);
-            ds[small_cfg(d.M, d.N)].push_back(d);
+            dprod.push_back({ti, make_desc(Lq, op_u16(H->B.rows + bundle_offset(t.m), H->B.stride, 1),
+                                           F->RB + (int64_t)t.off * H2, H2, 1, nj, H2, nm)});
         } else {
             // Q_t = A_j^T V_t: A_j^T(yh, x_hi) = A_j[x_hi][yh]; V_t(x_hi, yl) = V[x_hi][off + yl]
             qprod.push_back({ti, make_desc(op_u16(H->A.rows + bundle_offset(t.j), H->A.stride, 1),
                                            op_f64(F->VR + t.off, KR, 0), nullptr, nm, 1, nj, nm, H1)});
             // N_t = A_j Lq_t -> LA columns [KL + off, + 2^m) of the rows x_hi < H1h
-            GemmDesc d = make_desc(op_u16(H->A.rows + bundle_offset(t.j), H->A.stride, 0), Lq,
-                                   F->LA + KL + t.off, Kp, 1, H1, nm, nj);
-            ds[small_cfg(d.M, d.N)].push_back(d);
+            dprod.push_back({ti, make_desc(op_u16(H->A.rows + bundle_offset(t.j), H->A.stride, 0), Lq,
+                                           F->LA + KL + t.off, Kp, 1, H1, nm, nj)});
         }
         fold.push_back(f);
     }
-    // one split count for all small q products: enough CTAs to fill the GPU
-    int qtiles = 0, kmin = 1 << 30;
-    for (auto& pq : qprod) {
-        const int c = small_cfg(pq.second.M, pq.second.N);
-        qtiles += ((pq.second.M + kCfgBM[c] - 1) / kCfgBM[c]) * ((pq.second.N + kCfgBN[c] - 1) / kCfgBN[c]);
-        kmin = std::min(kmin, pq.second.K);
+    int64_t qelems = 0;
+    for (auto& pq : qprod) qelems += (int64_t)split_of(pq.second.K) * ny;
+    int64_t delems = 0;
+    for (auto& pd : dprod) {
+        const int S = split_of(pd.second.K);
+        if (S > 1) delems += (int64_t)S * pd.second.M * pd.second.N;
     }
-    F->QS = 1;
-    if (qtiles > 0)
-        while (F->QS < 16 && qtiles * F->QS * 2 <= 4 * H->num_sms && kmin / (F->QS * 2) >= 64) F->QS *= 2;
-    BDC_CUDA_TRY(al(&F->qparts, (size_t)F->T * F->QS * ny));
+    BDC_CUDA_TRY(al(&F->qparts, (size_t)std::max<int64_t>(qelems, 1)));
     BDC_CUDA_TRY(al(&F->qsum, (size_t)F->T * ny));
-    BDC_CUDA_TRY(cudaMemsetAsync(F->qparts, 0, sizeof(double) * F->T * F->QS * ny, H->stream));
+    BDC_CUDA_TRY(al(&F->dparts, (size_t)std::max<int64_t>(delems, 1)));
+    BDC_CUDA_TRY(cudaMemsetAsync(F->qparts, 0, sizeof(double) * std::max<int64_t>(qelems, 1), H->stream));
+    int64_t qo = 0;
     for (auto& pq : qprod) {
         GemmDesc d = pq.second;
-        d.C = F->qparts + (size_t)pq.first * F->QS * ny;
-        split_k(qs[small_cfg(d.M, d.N)], d, F->QS, ny);
+        const int S = split_of(d.K);
+        d.C = F->qparts + qo;
+        fold[pq.first].qoff = qo;
+        fold[pq.first].qs = S;
+        split_k(qs[small_cfg(d.M, d.N)], d, S, ny);
+        qo += (int64_t)S * ny;
+    }
+    int64_t dpo = 0, dbegin = 0;
+    for (auto& pd : dprod) {
+        GemmDesc d = pd.second;
+        const int S = split_of(d.K);
+        if (S == 1) {
+            ds[small_cfg(d.M, d.N)].push_back(d);
+            continue;
+        }
+        SumDesc sd{};
+        sd.part = F->dparts + dpo;
+        sd.dst = d.C;
+        sd.ldc_m = d.ldc_m;
+        sd.ldc_n = d.ldc_n;
+        sd.S = S;
+        sd.M = d.M;
+        sd.N = d.N;
+        sd.begin = dbegin;
+        dsum.push_back(sd);
+        // slices are dense [S][M][N]
+        d.C = F->dparts + dpo;
+        d.ldc_m = d.N;
+        d.ldc_n = 1;
+        split_k(ds[small_cfg(d.M, d.N)], d, S, (int64_t)d.M * d.N);
+        dpo += (int64_t)S * d.M * d.N;
+        dbegin += (int64_t)d.M * d.N;
+    }
+    F->n_dsum = (int)dsum.size();
+    F->dsum_elems = dbegin;
+    if (!dsum.empty()) {
+        BDC_CUDA_TRY(cudaMalloc(&F->d_dsum, sizeof(SumDesc) * dsum.size()));
+        BDC_CUDA_TRY(cudaMemcpy(F->d_dsum, dsum.data(), sizeof(SumDesc) * dsum.size(), cudaMemcpyHostToDevice));
     }
     for (int c = 0; c < CFG_COUNT; ++c) {
         if (!qs[c].empty()) {
@@ -913,7 +983,7 @@ bdc_status factored_init(bdc_handle* H) {
         BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
     }
     F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + (int)F->qsmall.size() + 2 +
-                           (int)F->dsmall.size() + 1 + 1;
+                           (int)F->dsmall.size() + (F->n_dsum > 0) + 1 + 1;
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
 }
@@ -922,8 +992,9 @@ void factored_free(bdc_handle* H) {
     FactoredState* F = H->fac;
     if (!F) return;
     for (double* p : {F->Pw, F->Lt, F->hx, F->LA, F->RB, F->UL, F->VR, F->ulpart, F->vrpart, F->qparts,
-                      F->qsum, F->lnq_full, F->epart})
+                      F->qsum, F->dparts, F->lnq_full, F->epart})
         cudaFree(p);
+    cudaFree(F->d_dsum);
     for (Launch* L : {&F->ul, &F->vr, &F->g}) cudaFree(L->d);
     for (auto& L : F->qsmall) cudaFree(L.d);
     for (auto& L : F->dsmall) cudaFree(L.d);
@@ -970,7 +1041,7 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
         case ST_FOLD: {
             const int ny = 1 << H->k;
             const int nqs = (F->T * ny + 255) / 256;
-            k_qsum<<<nqs < 4096 ? nqs : 4096, 256, 0, s>>>(F->d_fold, F->T, F->qparts, F->QS, H->k, F->qsum, H->d_st);
+            k_qsum<<<nqs < 4096 ? nqs : 4096, 256, 0, s>>>(F->d_fold, F->T, F->qparts, H->k, F->qsum, H->d_st);
             k_fold_q<<<(ny + 63) / 64, 64, 0, s>>>(F->d_fold, F->T, F->qsum, F->UL, F->KL, F->VR, F->KR, F->H1h, H->k,
                                                   H->inv_c, F->lnq_full, H->d_lnq, F->RB, F->H2, F->LA, F->Kp,
                                                   H->d_st);
@@ -979,6 +1050,11 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
         case ST_DSMALL:
             for (auto& L : F->dsmall)
                 if ((e = launch_store(L, s, H->d_st)) != cudaSuccess) return e;
+            if (F->n_dsum > 0) {
+                int64_t b = (F->dsum_elems + 255) / 256;
+                if (b > H->num_sms * 8) b = H->num_sms * 8;
+                k_dsum<<<(int)b, 256, 0, s>>>(F->d_dsum, F->n_dsum, F->dsum_elems, H->d_st);
+            }
             break;
         case ST_G:
             return launch_ba(F->g, make_epilogue(H), s, H->d_st);
