@@ -77,9 +77,9 @@ __host__ __device__ inline uint32_t binom(uint32_t n, uint32_t k) {
 
 // ------------------------------------------------------------ half tables
 // Half-table "bundles": for a half length h the device holds one row per
-// half-string v (2^h rows); the row concatenates cache_{h,m}[v][.] for
-// m = 0 .. mmax, so that cache_{h,m}[v][w] sits at row(v)[(2^m - 1) + w].
-// Rows are padded to a stride of 2^{mmax+1} entries (16-byte multiple).
+// half-string v (2^h rows); the row holds cache_{h,m}[v][.] for m = 0 .. mmax
+// at row(v)[2^m + w] (entry 0 is unused), so every segment with m >= 3 starts
+// on a 16-byte boundary.  The row stride is 2^{mmax+1} entries.
 // Entries are uint16 (exact: every count in a half table of length <= 17
 // is < 65536).  m == h (the whole half) is an equality test, never stored.
 struct HalfTables {
@@ -89,7 +89,7 @@ struct HalfTables {
     int stride = 0;                  // entries per row
 };
 
-__host__ __device__ __forceinline__ int bundle_offset(int m) { return (1 << m) - 1; }
+__host__ __device__ __forceinline__ int bundle_offset(int m) { return 1 << m; }
 
 // the split of x = x_hi || x_lo and of y at split point j (backend/BAA.cu:340-395)
 struct Split {

@@ -65,16 +65,40 @@ static const int kCfgBN[CFG_COUNT] = {128, 64, 128, 64, 16, 128};
 
 struct Launch {
     GemmDesc* d = nullptr;   // device descriptors
+    int* map = nullptr;      // CTA -> descriptor index
     int n = 0, tiles = 0, cfg = CFG_64x64;
 };
 
-// sum of S split slices [S][M][N] into a strided destination
-struct SumDesc {
-    const double* part;
-    double* dst;
-    int64_t ldc_m, ldc_n;
-    int S, M, N;
-    int64_t begin;    // first element index of this product in the launch
+// q side thin product of one term over a slice [s0, s1) of its contraction:
+//   out[i][w] += sum_s small(s)[i] * wide(s)[w]   (i < SMALL, w < WIDE)
+// with small(s) = small + s * small_stride, wide(s) = wide + s * wide_stride;
+// out element (i, w) at out[i * WIDE + w] (L terms: i = yh, w = yl) or
+// out[w * SMALL + i] (R terms: i = yl, w = yh), i.e. Q_t in flat y order.
+struct ThinQ {
+    const void* small;
+    const void* wide;
+    int64_t small_stride, wide_stride;
+    int small_u16, wide_u16;
+    int SMALL, WIDE;
+    int s0, s1;
+    double* out;
+    int out_trans;
+};
+
+// D side thin product of one term, one output row per table row s:
+//   out[s][i] = sum_w wide(s)[w] * Lq'[w][i]      (i < SMALL, w < WIDE)
+// wide(s) = a half-table row (uint16); Lq'[w][i] = ln q at y = i * WIDE + w
+// (L terms, i = yh) or y = w * SMALL + i (R terms, i = yl); out at
+// out[s * out_s + i * out_i] (RB rows or LA columns).
+struct ThinD {
+    const uint16_t* wide;
+    int64_t wide_stride;
+    int SMALL, WIDE;
+    int rows;
+    int lq_trans;
+    double* out;
+    int64_t out_s, out_i;
+    int cta_begin;
 };
 
 }  // namespace bdc
@@ -95,37 +119,38 @@ struct FactoredState {
     int S1 = 1, S2 = 1;
     double* qparts = nullptr; // split slices of the small q products (FoldTerm::qoff)
     double* qsum = nullptr;   // [T][2^k]  qparts summed over the splits
-    double* dparts = nullptr; // split slices of the small D products
-    bdc::SumDesc* d_dsum = nullptr;
-    int n_dsum = 0;
-    int64_t dsum_elems = 0;
+    // thin per-term products, grouped by the small size (index log2 SMALL)
+    bdc::ThinQ* d_thinq[8] = {};
+    int n_thinq[8] = {};
+    bdc::ThinD* d_thind[8] = {};
+    int n_thind[8] = {}, ctas_thind[8] = {};
     double* lnq_full = nullptr;  // [2^k]
     double* epart = nullptr;  // [ctas][8]
     int ctas_g = 0;
     bdc::Launch ul, vr, g;
-    std::vector<bdc::Launch> qsmall, dsmall;
     bdc::FoldTerm* d_fold = nullptr;
     int launches_per_iter = 0;
+    // independent thin products run as parallel branches
+    cudaStream_t side[8] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[8] = {};
+    // a captured chunk of kGraphIters iterations for the threshold graph_a
+    cudaGraphExec_t graph = nullptr;
+    double graph_a = 0.0;
 };
 
 namespace bdc {
 
 __device__ __forceinline__ bool gated(const DevState* st) { return st && (st->done || st->error); }
 
-__device__ __forceinline__ int find_desc(const GemmDesc* d, int nd, int t) {
-    int i = 0;
-    while (i + 1 < nd && d[i + 1].tile_begin <= t) ++i;
-    return i;
-}
 
 // ------------------------------------------------ products: plain store
 template <int BM, int BN, int WM, int WN>
-__global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ descs, int ndesc,
+__global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ descs, const int* __restrict__ map,
                                                    const DevState* st) {
     using C = MmaCfg<BM, BN, WM, WN>;
     if (gated(st)) return;
     extern __shared__ __align__(16) double smem[];
-    const GemmDesc& d = descs[find_desc(descs, ndesc, blockIdx.x)];
+    const GemmDesc& d = descs[map[blockIdx.x]];
     const int t = blockIdx.x - d.tile_begin;
     const int m0 = (t / d.tiles_n) * BM, n0 = (t % d.tiles_n) * BN;
     double acc[C::MT][C::NT][2];
@@ -286,12 +311,12 @@ static cudaError_t launch_store(const Launch& L, cudaStream_t s, const DevState*
     if (L.n == 0 || L.tiles == 0) return cudaSuccess;
     const int sm = cfg_smem(L.cfg);
     switch (L.cfg) {
-        case CFG_128x128: k_mma_store<BDC_CFG_ARGS_128x128><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
-        case CFG_128x64: k_mma_store<BDC_CFG_ARGS_128x64><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
-        case CFG_64x128: k_mma_store<BDC_CFG_ARGS_64x128><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
-        case CFG_64x64: k_mma_store<BDC_CFG_ARGS_64x64><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
-        case CFG_128x16: k_mma_store<BDC_CFG_ARGS_128x16><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
-        case CFG_16x128: k_mma_store<BDC_CFG_ARGS_16x128><<<L.tiles, 256, sm, s>>>(L.d, L.n, st); break;
+        case CFG_128x128: k_mma_store<BDC_CFG_ARGS_128x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
+        case CFG_128x64: k_mma_store<BDC_CFG_ARGS_128x64><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
+        case CFG_64x128: k_mma_store<BDC_CFG_ARGS_64x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
+        case CFG_64x64: k_mma_store<BDC_CFG_ARGS_64x64><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
+        case CFG_128x16: k_mma_store<BDC_CFG_ARGS_128x16><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
+        case CFG_16x128: k_mma_store<BDC_CFG_ARGS_16x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -306,6 +331,192 @@ static cudaError_t launch_ba(const Launch& L, const BaEpilogue& ep, cudaStream_t
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+// ------------------------------------------------------ thin products
+__device__ __forceinline__ double ld_val(const void* p, int u16, int64_t i) {
+    return u16 ? (double)__ldg((const uint16_t*)p + i) : __ldg((const double*)p + i);
+}
+
+// q side: CTA = (descriptor, block of 256 wide indices); blockDim 256.  The
+// small side of a chunk of 64 rows is staged in shared memory and broadcast;
+// each thread streams its wide column (coalesced across the warp) with 8 row
+// loads in flight.  When WIDE < 256 the spare threads take every
+// (256 / WIDE)-th row and the partial sums are added in shared memory.
+template <int SMALL>
+__global__ void __launch_bounds__(256) k_thin_q(const ThinQ* __restrict__ descs, int nblk, const DevState* st) {
+    if (gated(st)) return;
+    const ThinQ& d = descs[blockIdx.x / nblk];
+    const int wb = blockIdx.x % nblk;
+    const int lanes_w = d.WIDE < 256 ? d.WIDE : 256;  // threads along w
+    const int rows_par = 256 / lanes_w;               // threads along s
+    const int tw = threadIdx.x % lanes_w, ts = threadIdx.x / lanes_w;
+    const int w = wb * 256 + tw;
+    const bool active = (w < d.WIDE) && (ts < rows_par);
+    constexpr int CH = 64, U = 8;
+    __shared__ double sm[CH][SMALL];
+    double acc[SMALL];
+#pragma unroll
+    for (int i = 0; i < SMALL; ++i) acc[i] = 0.0;
+    for (int c0 = d.s0; c0 < d.s1; c0 += CH) {
+        const int nrow = min(CH, d.s1 - c0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < CH * SMALL; e += 256) {
+            const int r = e / SMALL, i = e % SMALL;
+            sm[r][i] = (r < nrow) ? ld_val(d.small, d.small_u16, (int64_t)(c0 + r) * d.small_stride + i) : 0.0;
+        }
+        __syncthreads();
+        if (active) {
+            for (int r0 = ts; r0 < nrow; r0 += rows_par * U) {
+                double wv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int r = r0 + u * rows_par;
+                    wv[u] = (r < nrow) ? ld_val(d.wide, d.wide_u16, (int64_t)(c0 + r) * d.wide_stride + w) : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int r = min(r0 + u * rows_par, CH - 1);  // rows past nrow carry weight 0
+#pragma unroll
+                    for (int i = 0; i < SMALL; ++i) acc[i] = fma(sm[r][i], wv[u], acc[i]);
+                }
+            }
+        }
+    }
+    if (rows_par > 1) {
+        // add the rows_par partial sums of each w (fixed order)
+        __shared__ double red[256];
+        for (int i = 0; i < SMALL; ++i) {
+            __syncthreads();
+            red[threadIdx.x] = active ? acc[i] : 0.0;
+            __syncthreads();
+            if (ts == 0 && w < d.WIDE) {
+                double a = 0.0;
+                for (int q = 0; q < rows_par; ++q) a += red[q * lanes_w + tw];
+                acc[i] = a;
+            }
+        }
+        if (ts != 0) return;
+    }
+    if (w >= d.WIDE) return;
+#pragma unroll
+    for (int i = 0; i < SMALL; ++i) {
+        if (d.out_trans) d.out[(int64_t)w * SMALL + i] = acc[i];
+        else d.out[(int64_t)i * d.WIDE + w] = acc[i];
+    }
+}
+
+// D side: CTA = 16 table rows of one descriptor (64 threads, 4 lanes per
+// row); ln q of the term is staged in shared memory as Lq'[w][i] and read
+// with broadcasts while each lane walks a quarter of its row in 16-byte
+// pieces, two in flight; the 4 partial sums of a row are added by shuffles.
+constexpr int kThinDRows = 16;
+
+template <int SMALL>
+__global__ void __launch_bounds__(64) k_thin_d(const ThinD* __restrict__ descs, int nd,
+                                               const double* __restrict__ lnq_full, const DevState* st) {
+    if (gated(st)) return;
+    int lo = 0, hi = nd - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].cta_begin <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const ThinD& d = descs[lo];
+    const int q = threadIdx.x & 3;
+    const int row = (blockIdx.x - d.cta_begin) * kThinDRows + (threadIdx.x >> 2);
+    extern __shared__ double lqs[];  // [WIDE][SMALL]
+    const int ny = SMALL * d.WIDE;
+    for (int e = threadIdx.x; e < ny; e += 64) {
+        const int w = e / SMALL, i = e % SMALL;
+        lqs[e] = d.lq_trans ? lnq_full[w * SMALL + i] : lnq_full[i * d.WIDE + w];
+    }
+    __syncthreads();
+    const bool live = row < d.rows;
+    double acc[SMALL];
+#pragma unroll
+    for (int i = 0; i < SMALL; ++i) acc[i] = 0.0;
+    const uint16_t* v = d.wide + (int64_t)(live ? row : 0) * d.wide_stride;
+    if (live && (d.WIDE & 31) == 0 && ((uintptr_t)v & 15) == 0) {
+        // lane q takes the 8-entry pieces q, q + 4, q + 8, ...
+        for (int w0 = q * 8; w0 < d.WIDE; w0 += 64) {
+            uint4 pc[2];
+            pc[0] = __ldg(reinterpret_cast<const uint4*>(v + w0));
+            pc[1] = (w0 + 32 < d.WIDE) ? __ldg(reinterpret_cast<const uint4*>(v + w0 + 32)) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t pk[4] = {pc[h].x, pc[h].y, pc[h].z, pc[h].w};
+                const int wb = w0 + 32 * h;
+                if (wb >= d.WIDE) break;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const double wv = (double)((pk[u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+                    const double* lr = lqs + (wb + u) * SMALL;
+#pragma unroll
+                    for (int i = 0; i < SMALL; ++i) acc[i] = fma(wv, lr[i], acc[i]);
+                }
+            }
+        }
+    } else if (live) {
+        for (int w = q; w < d.WIDE; w += 4) {
+            const double wv = (double)__ldg(v + w);
+            const double* lr = lqs + w * SMALL;
+#pragma unroll
+            for (int i = 0; i < SMALL; ++i) acc[i] = fma(wv, lr[i], acc[i]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < SMALL; ++i) {
+        acc[i] += __shfl_xor_sync(0xFFFFFFFFu, acc[i], 1);
+        acc[i] += __shfl_xor_sync(0xFFFFFFFFu, acc[i], 2);
+    }
+    if (!live || q != 0) return;
+    double* o = d.out + (int64_t)row * d.out_s;
+#pragma unroll
+    for (int i = 0; i < SMALL; ++i) o[(int64_t)i * d.out_i] = acc[i];
+}
+
+static cudaError_t launch_thin_q(int lg, const ThinQ* d, int n, int ny, cudaStream_t s, const DevState* st) {
+    const int small = 1 << lg, wide = ny / small;
+    const int nblk = (wide + 255) / 256;
+    const int grid = n * nblk;
+    switch (lg) {
+        case 0: k_thin_q<1><<<grid, 256, 0, s>>>(d, nblk, st); break;
+        case 1: k_thin_q<2><<<grid, 256, 0, s>>>(d, nblk, st); break;
+        case 2: k_thin_q<4><<<grid, 256, 0, s>>>(d, nblk, st); break;
+        case 3: k_thin_q<8><<<grid, 256, 0, s>>>(d, nblk, st); break;
+        case 4: k_thin_q<16><<<grid, 256, 0, s>>>(d, nblk, st); break;
+        case 5: k_thin_q<32><<<grid, 256, 0, s>>>(d, nblk, st); break;
+        case 6: k_thin_q<64><<<grid, 256, 0, s>>>(d, nblk, st); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_thin_d(int lg, const ThinD* d, int n, int ctas, int ny, const double* lnq_full,
+                                 cudaStream_t s, const DevState* st) {
+    const size_t sm = sizeof(double) * ny;
+    switch (lg) {
+        case 0: k_thin_d<1><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
+        case 1: k_thin_d<2><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
+        case 2: k_thin_d<4><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
+        case 3: k_thin_d<8><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
+        case 4: k_thin_d<16><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
+        case 5: k_thin_d<32><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
+        case 6: k_thin_d<64><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+static cudaError_t set_thin_smem(int ny) {
+    const int sm = (int)sizeof(double) * ny;
+    if (sm <= 48 * 1024) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+#define SET_(S) if (e == cudaSuccess) e = cudaFuncSetAttribute(k_thin_d<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    SET_(1) SET_(2) SET_(4) SET_(8) SET_(16) SET_(32) SET_(64)
+#undef SET_
+    return e;
 }
 
 // ------------------------------------------------------------ small kernels
@@ -346,22 +557,6 @@ __global__ void k_qsum(const FoldTerm* __restrict__ terms, int T, const double* 
         double a = 0.0;
         for (int sp = 0; sp < f.qs; ++sp) a += q[(size_t)sp * ny];
         qsum[e] = a;
-    }
-}
-
-// D-side split sums into RB / LA
-__global__ void k_dsum(const SumDesc* __restrict__ descs, int nd, int64_t total, const DevState* st) {
-    if (gated(st)) return;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        int i = 0;
-        while (i + 1 < nd && descs[i + 1].begin <= e) ++i;
-        const SumDesc& d = descs[i];
-        const int64_t l = e - d.begin;
-        const int64_t mn = (int64_t)d.M * d.N;
-        const int m = (int)(l / d.N), n = (int)(l % d.N);
-        double a = 0.0;
-        for (int sp = 0; sp < d.S; ++sp) a += d.part[sp * mn + l];
-        d.dst[(int64_t)m * d.ldc_m + (int64_t)n * d.ldc_n] = a;
     }
 }
 
@@ -609,15 +804,6 @@ static Operand op_f64(const double* p, int64_t ld, int trans) {
     return o;
 }
 
-static Operand op_u16(const uint16_t* p, int64_t ld, int trans) {
-    Operand o;
-    o.ptr = p;
-    o.ld = ld;
-    o.kind = OP_U16;
-    o.trans = trans;
-    return o;
-}
-
 static GemmDesc make_desc(Operand A, Operand B, double* C, int64_t ldc_m, int64_t ldc_n, int M, int N, int K) {
     GemmDesc d{};
     d.A = A;
@@ -666,23 +852,27 @@ static int assign_tiles(std::vector<GemmDesc>& v, int cfg) {
     return t;
 }
 
-static cudaError_t make_launch(Launch& L, std::vector<GemmDesc> v, int cfg) {
-    if (L.d) cudaFree(L.d);
+static void free_launch(Launch& L) {
+    cudaFree(L.d);
+    cudaFree(L.map);
     L.d = nullptr;
+    L.map = nullptr;
+}
+
+static cudaError_t make_launch(Launch& L, std::vector<GemmDesc> v, int cfg) {
+    free_launch(L);
     L.cfg = cfg;
     L.n = (int)v.size();
     L.tiles = assign_tiles(v, cfg);
     if (v.empty()) return cudaSuccess;
+    std::vector<int> map(L.tiles);
+    for (int i = 0; i < (int)v.size(); ++i)
+        for (int t = 0; t < v[i].tiles_m * v[i].tiles_n; ++t) map[v[i].tile_begin + t] = i;
     cudaError_t e = cudaMalloc(&L.d, sizeof(GemmDesc) * v.size());
-    if (e != cudaSuccess) return e;
-    return cudaMemcpy(L.d, v.data(), sizeof(GemmDesc) * v.size(), cudaMemcpyHostToDevice);
-}
-
-// tile shape for a small product from its shape
-static int small_cfg(int M, int N) {
-    if (N <= 16) return CFG_128x16;
-    if (M <= 16) return CFG_16x128;
-    return CFG_64x64;
+    if (e == cudaSuccess) e = cudaMemcpy(L.d, v.data(), sizeof(GemmDesc) * v.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&L.map, sizeof(int) * map.size());
+    if (e == cudaSuccess) e = cudaMemcpy(L.map, map.data(), sizeof(int) * map.size(), cudaMemcpyHostToDevice);
+    return e;
 }
 
 template <typename F>
@@ -716,11 +906,11 @@ static bdc_status tune_thin(bdc_handle* H, Launch& L, const GemmDesc& base, int6
             Launch T;
             BDC_CUDA_TRY(make_launch(T, v, cfgs[ci]));
             if (T.tiles > 64 * H->num_sms) {
-                cudaFree(T.d);
+                free_launch(T);
                 continue;
             }
             const float ms = time_ms(H, [&] { launch_store(T, H->stream, nullptr); });
-            cudaFree(T.d);
+            free_launch(T);
             if (ms < best) {
                 best = ms;
                 best_cfg = cfgs[ci];
@@ -836,111 +1026,133 @@ bdc_status factored_init(bdc_handle* H) {
         if (rc != BDC_OK) return rc;
     }
 
-    // ---- per-term small products and the fold plan.  Each small product is
-    // split over its contraction so that a CTA runs at most ~8 k-slices
-    // (their shapes are thin: 2^j x 2^{k-j} outputs over a 2^{n/2} contraction,
-    // or 2^{n/2} x 2^{k-j} over 2^j); q-side slices are summed by the fold,
-    // D-side slices by k_dsum into RB / LA.
-    auto split_of = [](int K) { return std::max(1, std::min(32, K / 128)); };
-    std::vector<GemmDesc> qs[CFG_COUNT], ds[CFG_COUNT];
+    // ---- per-term thin products and the fold plan.  q side: Q_t as a sum of
+    // outer products over the contracted half, split into slices so that the
+    // launch fills the GPU (the fold sums the slices); D side: one row-dot
+    // per half-table row.  Terms whose A_j or B_m is the identity are read or
+    // written directly by the fold.
+    std::vector<ThinQ> tq[8];
+    std::vector<ThinD> td[8];
     std::vector<FoldTerm> fold;
-    std::vector<SumDesc> dsum;
-    std::vector<std::pair<int, GemmDesc>> qprod, dprod;  // (term, product) before splitting
+    struct QPlan { int term, lg; ThinQ d; int S; };
+    std::vector<QPlan> qplan;
+    int qctas_one = 0;
     for (int ti = 0; ti < F->T; ++ti) {
         const Term& t = F->terms[ti];
-        const int nj = 1 << t.j, nm = 1 << t.m;
         FoldTerm f{};
         f.j = t.j;
         f.m = t.m;
         f.off = t.off;
-        Operand Lq = op_f64(F->lnq_full, nm, 0);  // Lq_t(yh, yl)
         if (t.left && t.idB) {
             f.kind = 1;       // Q_t = U_t
             f.idB_left = 1;   // M_t = Lq_t
         } else if (!t.left && t.idA) {
             f.kind = 2;        // Q_t = V_t
             f.idA_right = 1;   // N_t = Lq_t
-        } else if (t.left) {
-            // Q_t = U_t B_m: U_t(yh, x_lo) = U^T[x_lo][off + yh]; B_m(x_lo, yl)
-            qprod.push_back({ti, make_desc(op_f64(F->UL + t.off, KL, 1),
-                                           op_u16(H->B.rows + bundle_offset(t.m), H->B.stride, 0), nullptr, nm, 1,
-                                           nj, nm, H2)});
-            // M_t = Lq_t B_m^T -> RB rows [off, off + 2^j)
-            dprod.push_back({ti, make_desc(Lq, op_u16(H->B.rows + bundle_offset(t.m), H->B.stride, 1),
-                                           F->RB + (int64_t)t.off * H2, H2, 1, nj, H2, nm)});
         } else {
-            // Q_t = A_j^T V_t: A_j^T(yh, x_hi) = A_j[x_hi][yh]; V_t(x_hi, yl) = V[x_hi][off + yl]
-            qprod.push_back({ti, make_desc(op_u16(H->A.rows + bundle_offset(t.j), H->A.stride, 1),
-                                           op_f64(F->VR + t.off, KR, 0), nullptr, nm, 1, nj, nm, H1)});
-            // N_t = A_j Lq_t -> LA columns [KL + off, + 2^m) of the rows x_hi < H1h
-            dprod.push_back({ti, make_desc(op_u16(H->A.rows + bundle_offset(t.j), H->A.stride, 0), Lq,
-                                           F->LA + KL + t.off, Kp, 1, H1, nm, nj)});
+            ThinQ q{};
+            ThinD d{};
+            if (t.left) {
+                // Q_t[yh][yl] = sum_{x_lo} U^T[x_lo][off + yh] B_m[x_lo][yl]
+                q.small = F->UL + t.off;
+                q.small_stride = KL;
+                q.small_u16 = 0;
+                q.wide = H->B.rows + bundle_offset(t.m);
+                q.wide_stride = H->B.stride;
+                q.wide_u16 = 1;
+                q.SMALL = 1 << t.j;
+                q.WIDE = 1 << t.m;
+                q.s1 = H2;
+                q.out_trans = 0;
+                // M_t[yh][x_lo] = sum_yl B_m[x_lo][yl] Lq[yh][yl] -> RB[off + yh][x_lo]
+                d.wide = H->B.rows + bundle_offset(t.m);
+                d.wide_stride = H->B.stride;
+                d.SMALL = 1 << t.j;
+                d.WIDE = 1 << t.m;
+                d.rows = H2;
+                d.lq_trans = 0;
+                d.out = F->RB + (int64_t)t.off * H2;
+                d.out_s = 1;
+                d.out_i = H2;
+            } else {
+                // Q_t[yh][yl] = sum_{x_hi} A_j[x_hi][yh] V[x_hi][off + yl]
+                q.small = F->VR + t.off;
+                q.small_stride = KR;
+                q.small_u16 = 0;
+                q.wide = H->A.rows + bundle_offset(t.j);
+                q.wide_stride = H->A.stride;
+                q.wide_u16 = 1;
+                q.SMALL = 1 << t.m;
+                q.WIDE = 1 << t.j;
+                q.s1 = H1;
+                q.out_trans = 1;
+                // N_t[x_hi][yl] = sum_yh A_j[x_hi][yh] Lq[yh][yl] -> LA[x_hi][KL + off + yl]
+                d.wide = H->A.rows + bundle_offset(t.j);
+                d.wide_stride = H->A.stride;
+                d.SMALL = 1 << t.m;
+                d.WIDE = 1 << t.j;
+                d.rows = H1;
+                d.lq_trans = 1;
+                d.out = F->LA + KL + t.off;
+                d.out_s = Kp;
+                d.out_i = 1;
+            }
+            int lg = 0;
+            while ((1 << lg) < q.SMALL) ++lg;
+            if (lg > 6) return fail(BDC_ERR_UNSUPPORTED, "factored engine: term with more than 64 small outputs");
+            qplan.push_back({ti, lg, q, 1});
+            qctas_one += (q.WIDE + 255) / 256;
+            td[lg].push_back(d);
         }
         fold.push_back(f);
     }
+    // one split count for every q-side product: about 8 CTAs per SM, >= 64 rows a slice
+    int QS = 1;
+    while (qctas_one > 0 && QS < 64 && qctas_one * QS * 2 <= 8 * H->num_sms && std::min(H1, H2) / (QS * 2) >= 64)
+        QS *= 2;
     int64_t qelems = 0;
-    for (auto& pq : qprod) qelems += (int64_t)split_of(pq.second.K) * ny;
-    int64_t delems = 0;
-    for (auto& pd : dprod) {
-        const int S = split_of(pd.second.K);
-        if (S > 1) delems += (int64_t)S * pd.second.M * pd.second.N;
-    }
+    for (auto& qp : qplan) qelems += (int64_t)QS * ny;
     BDC_CUDA_TRY(al(&F->qparts, (size_t)std::max<int64_t>(qelems, 1)));
     BDC_CUDA_TRY(al(&F->qsum, (size_t)F->T * ny));
-    BDC_CUDA_TRY(al(&F->dparts, (size_t)std::max<int64_t>(delems, 1)));
     BDC_CUDA_TRY(cudaMemsetAsync(F->qparts, 0, sizeof(double) * std::max<int64_t>(qelems, 1), H->stream));
     int64_t qo = 0;
-    for (auto& pq : qprod) {
-        GemmDesc d = pq.second;
-        const int S = split_of(d.K);
-        d.C = F->qparts + qo;
-        fold[pq.first].qoff = qo;
-        fold[pq.first].qs = S;
-        split_k(qs[small_cfg(d.M, d.N)], d, S, ny);
-        qo += (int64_t)S * ny;
-    }
-    int64_t dpo = 0, dbegin = 0;
-    for (auto& pd : dprod) {
-        GemmDesc d = pd.second;
-        const int S = split_of(d.K);
-        if (S == 1) {
-            ds[small_cfg(d.M, d.N)].push_back(d);
-            continue;
+    for (auto& qp : qplan) {
+        fold[qp.term].qoff = qo;
+        fold[qp.term].qs = QS;
+        const int S = qp.d.s1;
+        for (int sp = 0; sp < QS; ++sp) {
+            ThinQ q = qp.d;
+            q.s0 = (int)((int64_t)S * sp / QS);
+            q.s1 = (int)((int64_t)S * (sp + 1) / QS);
+            q.out = F->qparts + qo + (int64_t)sp * ny;
+            tq[qp.lg].push_back(q);
         }
-        SumDesc sd{};
-        sd.part = F->dparts + dpo;
-        sd.dst = d.C;
-        sd.ldc_m = d.ldc_m;
-        sd.ldc_n = d.ldc_n;
-        sd.S = S;
-        sd.M = d.M;
-        sd.N = d.N;
-        sd.begin = dbegin;
-        dsum.push_back(sd);
-        // slices are dense [S][M][N]
-        d.C = F->dparts + dpo;
-        d.ldc_m = d.N;
-        d.ldc_n = 1;
-        split_k(ds[small_cfg(d.M, d.N)], d, S, (int64_t)d.M * d.N);
-        dpo += (int64_t)S * d.M * d.N;
-        dbegin += (int64_t)d.M * d.N;
+        qo += (int64_t)QS * ny;
     }
-    F->n_dsum = (int)dsum.size();
-    F->dsum_elems = dbegin;
-    if (!dsum.empty()) {
-        BDC_CUDA_TRY(cudaMalloc(&F->d_dsum, sizeof(SumDesc) * dsum.size()));
-        BDC_CUDA_TRY(cudaMemcpy(F->d_dsum, dsum.data(), sizeof(SumDesc) * dsum.size(), cudaMemcpyHostToDevice));
-    }
-    for (int c = 0; c < CFG_COUNT; ++c) {
-        if (!qs[c].empty()) {
-            F->qsmall.emplace_back();
-            BDC_CUDA_TRY(make_launch(F->qsmall.back(), qs[c], c));
+    for (int lg = 0; lg < 8; ++lg) {
+        if (!tq[lg].empty()) {
+            BDC_CUDA_TRY(cudaMalloc(&F->d_thinq[lg], sizeof(ThinQ) * tq[lg].size()));
+            BDC_CUDA_TRY(cudaMemcpy(F->d_thinq[lg], tq[lg].data(), sizeof(ThinQ) * tq[lg].size(), cudaMemcpyHostToDevice));
+            F->n_thinq[lg] = (int)tq[lg].size();
         }
-        if (!ds[c].empty()) {
-            F->dsmall.emplace_back();
-            BDC_CUDA_TRY(make_launch(F->dsmall.back(), ds[c], c));
+        if (!td[lg].empty()) {
+            int cta = 0;
+            for (auto& d : td[lg]) {
+                d.cta_begin = cta;
+                cta += (d.rows + kThinDRows - 1) / kThinDRows;
+            }
+            BDC_CUDA_TRY(cudaMalloc(&F->d_thind[lg], sizeof(ThinD) * td[lg].size()));
+            BDC_CUDA_TRY(cudaMemcpy(F->d_thind[lg], td[lg].data(), sizeof(ThinD) * td[lg].size(), cudaMemcpyHostToDevice));
+            F->n_thind[lg] = (int)td[lg].size();
+            F->ctas_thind[lg] = cta;
         }
     }
+    BDC_CUDA_TRY(set_thin_smem(ny));
+    for (int lg = 0; lg < 8; ++lg) {
+        BDC_CUDA_TRY(cudaStreamCreateWithFlags(&F->side[lg], cudaStreamNonBlocking));
+        BDC_CUDA_TRY(cudaEventCreateWithFlags(&F->ev_join[lg], cudaEventDisableTiming));
+    }
+    BDC_CUDA_TRY(cudaEventCreateWithFlags(&F->ev_fork, cudaEventDisableTiming));
     {
         BDC_CUDA_TRY(cudaMalloc(&F->d_fold, sizeof(FoldTerm) * fold.size()));
         BDC_CUDA_TRY(cudaMemcpy(F->d_fold, fold.data(), sizeof(FoldTerm) * fold.size(), cudaMemcpyHostToDevice));
@@ -968,7 +1180,7 @@ bdc_status factored_init(bdc_handle* H) {
             Launch T;
             BDC_CUDA_TRY(make_launch(T, {d}, c));
             const float ms = time_ms(H, [&] { launch_ba(T, ep, H->stream, H->d_st); });
-            cudaFree(T.d);
+            free_launch(T);
             if (ms < best) {
                 best = ms;
                 best_cfg = c;
@@ -982,8 +1194,9 @@ bdc_status factored_init(bdc_handle* H) {
         BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
         BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
     }
-    F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + (int)F->qsmall.size() + 2 +
-                           (int)F->dsmall.size() + (F->n_dsum > 0) + 1 + 1;
+    int nthin = 0;
+    for (int lg = 0; lg < 8; ++lg) nthin += (F->n_thinq[lg] > 0) + (F->n_thind[lg] > 0);
+    F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + nthin + 2 + 1 + 1;
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
 }
@@ -992,12 +1205,17 @@ void factored_free(bdc_handle* H) {
     FactoredState* F = H->fac;
     if (!F) return;
     for (double* p : {F->Pw, F->Lt, F->hx, F->LA, F->RB, F->UL, F->VR, F->ulpart, F->vrpart, F->qparts,
-                      F->qsum, F->dparts, F->lnq_full, F->epart})
+                      F->qsum, F->lnq_full, F->epart})
         cudaFree(p);
-    cudaFree(F->d_dsum);
-    for (Launch* L : {&F->ul, &F->vr, &F->g}) cudaFree(L->d);
-    for (auto& L : F->qsmall) cudaFree(L.d);
-    for (auto& L : F->dsmall) cudaFree(L.d);
+    for (int lg = 0; lg < 8; ++lg) {
+        cudaFree(F->d_thinq[lg]);
+        cudaFree(F->d_thind[lg]);
+        if (F->side[lg]) cudaStreamDestroy(F->side[lg]);
+        if (F->ev_join[lg]) cudaEventDestroy(F->ev_join[lg]);
+    }
+    if (F->ev_fork) cudaEventDestroy(F->ev_fork);
+    if (F->graph) cudaGraphExecDestroy(F->graph);
+    for (Launch* L : {&F->ul, &F->vr, &F->g}) free_launch(*L);
     cudaFree(F->d_fold);
     delete F;
     H->fac = nullptr;
@@ -1035,8 +1253,16 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             break;
         }
         case ST_QSMALL:
-            for (auto& L : F->qsmall)
-                if ((e = launch_store(L, s, H->d_st)) != cudaSuccess) return e;
+            // fork: each size class on its own branch, joined before the fold
+            if ((e = cudaEventRecord(F->ev_fork, s)) != cudaSuccess) return e;
+            for (int lg = 0; lg < 8; ++lg) {
+                if (!F->n_thinq[lg]) continue;
+                if ((e = cudaStreamWaitEvent(F->side[lg], F->ev_fork, 0)) != cudaSuccess) return e;
+                if ((e = launch_thin_q(lg, F->d_thinq[lg], F->n_thinq[lg], 1 << H->k, F->side[lg], H->d_st)) != cudaSuccess)
+                    return e;
+                if ((e = cudaEventRecord(F->ev_join[lg], F->side[lg])) != cudaSuccess) return e;
+                if ((e = cudaStreamWaitEvent(s, F->ev_join[lg], 0)) != cudaSuccess) return e;
+            }
             break;
         case ST_FOLD: {
             const int ny = 1 << H->k;
@@ -1048,12 +1274,15 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             break;
         }
         case ST_DSMALL:
-            for (auto& L : F->dsmall)
-                if ((e = launch_store(L, s, H->d_st)) != cudaSuccess) return e;
-            if (F->n_dsum > 0) {
-                int64_t b = (F->dsum_elems + 255) / 256;
-                if (b > H->num_sms * 8) b = H->num_sms * 8;
-                k_dsum<<<(int)b, 256, 0, s>>>(F->d_dsum, F->n_dsum, F->dsum_elems, H->d_st);
+            if ((e = cudaEventRecord(F->ev_fork, s)) != cudaSuccess) return e;
+            for (int lg = 0; lg < 8; ++lg) {
+                if (!F->n_thind[lg]) continue;
+                if ((e = cudaStreamWaitEvent(F->side[lg], F->ev_fork, 0)) != cudaSuccess) return e;
+                if ((e = launch_thin_d(lg, F->d_thind[lg], F->n_thind[lg], F->ctas_thind[lg], 1 << H->k, F->lnq_full,
+                                       F->side[lg], H->d_st)) != cudaSuccess)
+                    return e;
+                if ((e = cudaEventRecord(F->ev_join[lg], F->side[lg])) != cudaSuccess) return e;
+                if ((e = cudaStreamWaitEvent(s, F->ev_join[lg], 0)) != cudaSuccess) return e;
             }
             break;
         case ST_G:
@@ -1111,7 +1340,36 @@ static void fill_stats(bdc_handle* H, long long it0, bdc_stats* stats) {
     stats->converged = H->h_st->done;
 }
 
+// kGraphIters iterations captured once (per threshold a) on the handle's own
+// stream and replayed on whatever stream the handle queues on; the device
+// done / error flags make iterations past convergence no-ops
+constexpr int kGraphIters = 8;
+
+static bdc_status ensure_graph(bdc_handle* H, double a) {
+    FactoredState* F = H->fac;
+    if (F->graph && F->graph_a == a) return BDC_OK;
+    if (F->graph) {
+        cudaGraphExecDestroy(F->graph);
+        F->graph = nullptr;
+    }
+    cudaStream_t keep = H->stream;
+    H->stream = H->own_stream;
+    BDC_CUDA_TRY(cudaStreamSynchronize(keep));
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(H->own_stream, cudaStreamCaptureModeThreadLocal);
+    for (int i = 0; i < kGraphIters && e == cudaSuccess; ++i) e = enqueue_iteration(H, a);
+    cudaError_t e2 = cudaStreamEndCapture(H->own_stream, &g);
+    H->stream = keep;
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&F->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    BDC_CUDA_TRY(e);
+    F->graph_a = a;
+    return BDC_OK;
+}
+
 bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats) {
+    FactoredState* F = H->fac;
     BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), H->stream));
     const long long it0 = H->h_st->iter;
     long long target = it0 + max_iters;
@@ -1121,7 +1379,14 @@ bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stat
         const int64_t remaining = target - done_iters;
         if (remaining <= 0) break;
         const int64_t c = chunk < remaining ? chunk : remaining;
-        for (int64_t i = 0; i < c; ++i) BDC_CUDA_TRY(enqueue_iteration(H, a));
+        // whole graphs for the bulk of the chunk, single iterations for the rest
+        const int64_t ng = (c >= kGraphIters) ? c / kGraphIters : 0;
+        if (ng > 0) {
+            bdc_status rc = ensure_graph(H, a);
+            if (rc != BDC_OK) return rc;
+        }
+        for (int64_t i = 0; i < ng; ++i) BDC_CUDA_TRY(cudaGraphLaunch(F->graph, H->stream));
+        for (int64_t i = ng * kGraphIters; i < c; ++i) BDC_CUDA_TRY(enqueue_iteration(H, a));
         BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
         BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
         if (H->h_st->error == kErrShift) {
@@ -1133,7 +1398,7 @@ bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stat
             return fail(BDC_ERR_NUMERIC, "factored engine: device error %d", H->h_st->error);
         }
         if (H->h_st->done) break;
-        if (chunk < 64) chunk *= 2;
+        if (chunk < 256) chunk *= 2;
     }
     fill_stats(H, it0, stats);
     return BDC_OK;

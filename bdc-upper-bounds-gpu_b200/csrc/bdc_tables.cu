@@ -51,19 +51,19 @@ cudaError_t launch_gen_cache(int n, int k, uint32_t* out, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
-// bundle row v: entry e < 2^{mmax+1} - 1 is cache_{h,m}[v][w] with
-// m = floor(log2(e + 1)), w = e - (2^m - 1); the padding entry is 0.
+// bundle row v: entry e in [1, 2^{mmax+1}) is cache_{h,m}[v][w] with
+// m = floor(log2 e), w = e - 2^m; entry 0 is unused (0).
 __global__ void k_gen_bundle(int h, int mmax, int stride, uint16_t* __restrict__ rows) {
     const uint64_t total = (uint64_t)stride << h;
-    const int used = (1 << (mmax + 1)) - 1;
+    const int used = 1 << (mmax + 1);
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v = (uint32_t)(i / stride);
         const int e = (int)(i % stride);
         uint16_t val = 0;
-        if (e < used) {
-            const int m = 31 - __clz(e + 1);
-            const uint32_t w = (uint32_t)(e - ((1 << m) - 1));
+        if (e >= 1 && e < used) {
+            const int m = 31 - __clz(e);
+            const uint32_t w = (uint32_t)(e - (1 << m));
             val = (uint16_t)dp_count(v, h, w, m);
         }
         rows[i] = val;
@@ -85,15 +85,15 @@ struct CachePtrs { const uint32_t* p[kMaxHalf + 1]; };
 __global__ void k_build_bundle(int h, int mmax, int stride, CachePtrs caches,
                                uint16_t* __restrict__ rows, int* overflow) {
     const uint64_t total = (uint64_t)stride << h;
-    const int used = (1 << (mmax + 1)) - 1;
+    const int used = 1 << (mmax + 1);
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v = (uint32_t)(i / stride);
         const int e = (int)(i % stride);
         uint32_t val = 0;
-        if (e < used) {
-            const int m = 31 - __clz(e + 1);
-            const uint32_t w = (uint32_t)(e - ((1 << m) - 1));
+        if (e >= 1 && e < used) {
+            const int m = 31 - __clz(e);
+            const uint32_t w = (uint32_t)(e - (1 << m));
             val = caches.p[m][((uint64_t)v << m) | w];
         }
         if (val > 0xFFFFu) { atomicExch(overflow, 1); val = 0xFFFFu; }
