@@ -40,6 +40,7 @@ EXPORTED_SYMBOLS = [
     "bdc_log_w", "bdc_divergence", "bdc_rate", "bdc_max_deviation", "bdc_counts",
     "bdc_generate_cache", "bdc_read_cache_file", "bdc_write_cache_file", "bdc_read_dist_file",
     "bdc_write_dist_file", "bdc_work", "bdc_profile", "bdc_set_stream", "bdc_peak_probe",
+    "bdc_max_deviation_noalloc",
 ]
 
 
@@ -119,6 +120,8 @@ def library() -> ctypes.CDLL:
     L.bdc_work.argtypes = [h, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int)]
     L.bdc_profile.argtypes = [h, ctypes.c_int, ctypes.POINTER(Profile)]
     L.bdc_set_stream.argtypes = [h, ctypes.c_void_p]
+    L.bdc_max_deviation_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                            ctypes.c_void_p]
     L.bdc_peak_probe.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                  ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTED_SYMBOLS:
@@ -317,6 +320,17 @@ def generate_cache(n: int, k: int, device: int = 0) -> np.ndarray:
     out = np.empty(1 << (n + k), dtype=np.uint32)
     _check(library().bdc_generate_cache(n, k, device, out.ctypes.data_as(_u32p)), "bdc_generate_cache")
     return out
+
+
+def max_deviation_noalloc(p_ptr: int, p_before_ptr: int, num_reps: int, mx_ptr: int, stream: int = 0) -> None:
+    """Allocation-free max_i log2 p - log2 p_before over caller-owned device
+    arrays (raw device pointers), result written to the device double at
+    mx_ptr.  For callers whose device memory all comes from their own pool:
+    the library allocates nothing here and uses one fixed scratch array per
+    device instead (num_reps <= 2^27; overlapping calls on the GPU race)."""
+    _check(library().bdc_max_deviation_noalloc(ctypes.c_void_p(p_ptr), ctypes.c_void_p(p_before_ptr),
+                                               int(num_reps), ctypes.c_void_p(mx_ptr), ctypes.c_void_p(stream)),
+           "bdc_max_deviation_noalloc")
 
 
 def peak_probe(kind: str, device: int = 0, ms: float = 50.0) -> float:

@@ -17,6 +17,7 @@
 #include <cfloat>
 
 #include "bdc_common.cuh"
+#include "bdc_engine.cuh"
 #include "bdc_kernels.cuh"
 
 namespace bdc {
@@ -255,3 +256,80 @@ cudaError_t launch_max_dev(const double* p, const double* pb, int64_t R, double*
 }
 
 }  // namespace bdc
+
+// ===================================================================
+// Allocation-free max deviation.
+//
+// For callers that cannot allocate device memory: code that owns every byte
+// of its GPU memory through its own pool or arena (so a cudaMalloc behind its
+// back would break its accounting or fail outright), code running where the
+// allocator must not be called, and plugins that are handed buffers by a
+// host application.  They pass their own device buffers for the inputs and
+// for the one-double result; the block partials of the reduction live in a
+// fixed array in the library's device memory instead of a buffer the library
+// allocates.
+//
+// Limits and sharing:
+//   * num_reps <= kNoAllocMaxReps (2^27 = 134,217,728 representatives, i.e.
+//     every n <= 28); larger inputs return BDC_ERR_ARG.
+//   * The array (kNoAllocSlots doubles, 128 KB) exists once per device that
+//     loads the library and stays resident until the process exits.
+//   * Every call on a device uses the same array.  Each call writes every
+//     slot it later reads, so nothing has to start at zero and a call never
+//     sees a previous call's values; but two calls whose kernels overlap on
+//     the GPU (e.g. issued on different streams without ordering) race on
+//     the array and may return wrong results.  Order such calls.
+//   * The first call on each device looks up the array's device address
+//     (cudaGetSymbolAddress, with that device current) and caches it; make
+//     that first call before any stream capture is in progress on the
+//     calling thread.
+namespace bdc {
+
+constexpr int kNoAllocSlots = 16384;
+constexpr int kNoAllocTile = 8192;  // representatives reduced per block
+constexpr int64_t kNoAllocMaxReps = (int64_t)kNoAllocSlots * kNoAllocTile;
+
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocSlots];
+
+// block b reduces representatives [b * kNoAllocTile, (b + 1) * kNoAllocTile)
+__global__ void __launch_bounds__(kUpdThreads)
+k_maxdev_tile(const double* __restrict__ p, const double* __restrict__ pb, int64_t R, double* __restrict__ part) {
+    const int64_t i0 = (int64_t)blockIdx.x * kNoAllocTile;
+    const int64_t i1 = (i0 + kNoAllocTile < R) ? i0 + kNoAllocTile : R;
+    double m = -DBL_MAX;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) m = OpMax()(m, log2(p[i]) - log2(pb[i]));
+    m = block_reduce(m, OpMax(), -DBL_MAX);
+    if (threadIdx.x == 0) part[blockIdx.x] = m;
+}
+
+static double* g_noalloc_addr[64];
+static bool g_noalloc_ready[64];
+
+}  // namespace bdc
+
+extern "C" bdc_status bdc_max_deviation_noalloc(const double* p_dev, const double* p_before_dev,
+                                                int64_t num_reps, double* mx_dev, void* cuda_stream) {
+    using namespace bdc;
+    if (!p_dev || !p_before_dev || !mx_dev || num_reps < 1)
+        return fail(BDC_ERR_ARG, "bdc_max_deviation_noalloc: NULL pointer or num_reps < 1");
+    if (num_reps > kNoAllocMaxReps)
+        return fail(BDC_ERR_ARG,
+                    "bdc_max_deviation_noalloc: num_reps %lld exceeds the fixed scratch limit of %lld "
+                    "(%d slots of %d); use bdc_max_deviation",
+                    (long long)num_reps, (long long)kNoAllocMaxReps, kNoAllocSlots, kNoAllocTile);
+    int dev = 0;
+    BDC_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(BDC_ERR_ARG, "bdc_max_deviation_noalloc: device %d out of range", dev);
+    if (!g_noalloc_ready[dev]) {
+        void* addr = nullptr;
+        BDC_CUDA_TRY(cudaGetSymbolAddress(&addr, g_noalloc_partials));
+        g_noalloc_addr[dev] = (double*)addr;
+        g_noalloc_ready[dev] = true;
+    }
+    cudaStream_t s = (cudaStream_t)cuda_stream;
+    const int blocks = (int)((num_reps + kNoAllocTile - 1) / kNoAllocTile);
+    k_maxdev_tile<<<blocks, kUpdThreads, 0, s>>>(p_dev, p_before_dev, num_reps, g_noalloc_addr[dev]);
+    k_fold_max<<<1, kUpdThreads, 0, s>>>(g_noalloc_addr[dev], blocks, mx_dev);
+    BDC_CUDA_TRY(cudaGetLastError());
+    return BDC_OK;
+}

@@ -159,6 +159,19 @@ bdc_status bdc_set_stream(bdc_handle_t h, void* cuda_stream);
  * operation).  Used as the measured denominator of roofline fractions. */
 bdc_status bdc_peak_probe(int device, int kind, double ms, double* ops_per_s);
 
+/* Allocation-free variant of bdc_max_deviation (no counterpart in the
+ * reference): max_i log2 p[i] - log2 p_before[i] over device arrays the
+ * caller owns, written to the device double *mx_dev, queued on cuda_stream
+ * (NULL: the legacy default stream).  For callers that cannot allocate
+ * device memory (their own pool or arena owns it all, or an allocator call
+ * is not allowed where they run): no handle, no cudaMalloc/cudaFree.  The
+ * reduction's block partials live in one fixed 128 KB array per device,
+ * shared by every call: num_reps <= 2^27 (else BDC_ERR_ARG), calls whose
+ * kernels overlap on the GPU race, and the first call on a device (which
+ * looks up the array's address) should come before any stream capture. */
+bdc_status bdc_max_deviation_noalloc(const double* p_dev, const double* p_before_dev, int64_t num_reps,
+                                     double* mx_dev, void* cuda_stream);
+
 /* ------------------------------------------------------- cache generator
  * The table cache_{n,k} of generate_bit_transition_cache.cpp:46-77, computed on
  * the device: out holds 2^{n+k} uint32, index (x << k) | y.  n + k <= 34. */
