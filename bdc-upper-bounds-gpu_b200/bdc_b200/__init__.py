@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = [
     "bdc_log_w", "bdc_divergence", "bdc_rate", "bdc_max_deviation", "bdc_counts",
     "bdc_generate_cache", "bdc_read_cache_file", "bdc_write_cache_file", "bdc_read_dist_file",
     "bdc_write_dist_file", "bdc_work", "bdc_profile", "bdc_set_stream", "bdc_peak_probe",
-    "bdc_max_deviation_noalloc",
+    "bdc_max_deviation_noalloc", "bdc_accelerate", "bdc_mi_forward", "bdc_mi_backward",
 ]
 
 
@@ -67,6 +67,7 @@ class Profile(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("iters", ctypes.c_int64), ("total_iters", ctypes.c_int64), ("mx", ctypes.c_double),
                 ("upper_bound", ctypes.c_double), ("rate", ctypes.c_double), ("lse", ctypes.c_double),
+                ("best_upper_bound", ctypes.c_double), ("best_rate", ctypes.c_double),
                 ("converged", ctypes.c_int)]
 
     def as_dict(self) -> dict:
@@ -105,6 +106,9 @@ def library() -> ctypes.CDLL:
     L.bdc_get_p_device.argtypes = [h, ctypes.c_void_p, ctypes.c_int64]
     L.bdc_iterate.argtypes = [h, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats)]
     L.bdc_baa_iteration.argtypes = [h, _f64p, _f64p, ctypes.c_int64]
+    L.bdc_accelerate.argtypes = [h, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats)]
+    L.bdc_mi_forward.argtypes = [h, _f64p, ctypes.c_int64, _f64p]
+    L.bdc_mi_backward.argtypes = [h, _f64p, ctypes.c_int64]
     L.bdc_log_q.argtypes = [h, _f64p, ctypes.c_int64]
     L.bdc_log_w.argtypes = [h, _f64p, _f64p, ctypes.c_int64]
     L.bdc_divergence.argtypes = [h, _f64p, _f64p, ctypes.c_int64]
@@ -239,6 +243,31 @@ class Engine:
         st = Stats()
         _check(library().bdc_iterate(self._h, int(max_iters), float(a), ctypes.byref(st)), "bdc_iterate")
         return st.as_dict()
+
+    def accelerate(self, max_evals: int, gap_bits: float = 0.0) -> dict:
+        """Accelerated BA on the device (factored engine): runs until the
+        certified gap best_upper_bound - best_rate < gap_bits or max_evals
+        BA map evaluations."""
+        st = Stats()
+        _check(library().bdc_accelerate(self._h, int(max_evals), float(gap_bits), ctypes.byref(st)),
+               "bdc_accelerate")
+        return st.as_dict()
+
+    def mi_forward(self, p=None) -> float:
+        """I(p;W) in nats; p (per representative) becomes the current iterate."""
+        r = ctypes.c_double()
+        if p is None:
+            _check(library().bdc_mi_forward(self._h, None, self.R, ctypes.byref(r)), "bdc_mi_forward")
+        else:
+            p, pp = _f64(p)
+            _check(library().bdc_mi_forward(self._h, pp, len(p), ctypes.byref(r)), "bdc_mi_forward")
+        return r.value
+
+    def mi_backward(self) -> np.ndarray:
+        """dI/dp per representative (nats) at the current iterate."""
+        out = np.empty(self.R, dtype=np.float64)
+        _check(library().bdc_mi_backward(self._h, out.ctypes.data_as(_f64p), self.R), "bdc_mi_backward")
+        return out
 
     def baa_iteration(self, p) -> np.ndarray:
         p, pp = _f64(p)

@@ -179,6 +179,40 @@ bdc_status bdc_iterate(bdc_handle_t H, int64_t max_iters, double a, bdc_stats* s
     return engine_iterate(H, max_iters, a, stats);
 }
 
+bdc_status bdc_accelerate(bdc_handle_t H, int64_t max_evals, double gap_bits, bdc_stats* stats) {
+    if (!H) return fail(BDC_ERR_ARG, "bdc_accelerate: NULL handle");
+    if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_accelerate: no distribution set");
+    if (H->engine != BDC_ENGINE_FACTORED)
+        return fail(BDC_ERR_UNSUPPORTED, "bdc_accelerate: needs the factored engine (k < n)");
+    if (max_evals < 0) return fail(BDC_ERR_ARG, "bdc_accelerate: max_evals < 0");
+    cudaSetDevice(H->device);
+    return factored_accelerate(H, max_evals, gap_bits, stats);
+}
+
+bdc_status bdc_mi_forward(bdc_handle_t H, const double* p, int64_t R, double* I_nats) {
+    if (!H || !I_nats) return fail(BDC_ERR_ARG, "bdc_mi_forward: NULL argument");
+    if (p) {
+        bdc_status rc = bdc_set_p(H, p, R);
+        if (rc != BDC_OK) return rc;
+    }
+    return bdc_rate(H, I_nats);
+}
+
+bdc_status bdc_mi_backward(bdc_handle_t H, double* grad, int64_t R) {
+    if (!H || !grad) return fail(BDC_ERR_ARG, "bdc_mi_backward: NULL argument");
+    if (R != H->R) return fail(BDC_ERR_ARG, "bdc_mi_backward: %lld slots for %lld representatives", (long long)R, (long long)H->R);
+    if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_mi_backward: no distribution set");
+    cudaSetDevice(H->device);
+    bdc_status rc = engine_log_q(H);
+    if (rc != BDC_OK) return rc;
+    rc = engine_divergence(H);
+    if (rc != BDC_OK) return rc;
+    BDC_CUDA_TRY(launch_mi_grad(H->n, H->d_reps, H->R, H->d_d, H->d_logw, H->stream));
+    BDC_CUDA_TRY(cudaMemcpyAsync(grad, H->d_logw, sizeof(double) * R, cudaMemcpyDeviceToHost, H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    return BDC_OK;
+}
+
 bdc_status bdc_baa_iteration(bdc_handle_t H, const double* p_in, double* p_out, int64_t R) {
     if (!H || !p_in || !p_out) return fail(BDC_ERR_ARG, "bdc_baa_iteration: NULL argument");
     bdc_status rc = bdc_set_p(H, p_in, R);

@@ -138,11 +138,17 @@ struct DevState {
     double rate;         // sum |O| p D of the iterate the D pass used (nats)
     double lnp_max;      // max_x ln p of the current iterate
     double lse;          // ln sum |O| p e^D of the last D pass (nats)
+    double best_ub;      // min over evaluated iterates of max_x D(x) (nats): still a bound
+    double best_rate;    // max over evaluated iterates of I(p;W) (nats): a lower bound
+    double ub_theta1;    // accelerated loop: bound at the middle point of a cycle
+    double sq_alpha;     // accelerated loop: extrapolation step of the current cycle
+    double sq_max;       // accelerated loop: max of the extrapolated log iterate
     long long iter;      // iterations done since the last reset
     int cur;             // which of the two p buffers holds the current iterate
     int done;            // set when mx < a: later iterations do nothing
     int zero_p;          // the current iterate has a zero entry
     int error;           // device-detected error code (0 = none)
+    int restore;         // accelerated loop: the extrapolated point was rejected
     unsigned int ticket[4];  // last-block counters of the grid reductions
 };
 

@@ -5,7 +5,9 @@
 // (backend/main_BAA.cu:46-50): representatives are compacted on the device,
 // the two half-table bundles are built (from cache files or by the device
 // generator), and the entropy term h(x) = sum_y W ln W is computed once.
+#include <cfloat>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "bdc_engine.cuh"
@@ -252,8 +254,11 @@ void engine_free(bdc_handle* H) {
 }
 
 static bdc_status reset_state(bdc_handle* H) {
-    BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
     memset(H->h_st, 0, sizeof(DevState));
+    H->h_st->best_ub = DBL_MAX;
+    H->h_st->best_rate = -DBL_MAX;
+    BDC_CUDA_TRY(cudaMemcpyAsync(H->d_st, H->h_st, sizeof(DevState), cudaMemcpyHostToDevice, H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
 }
 
@@ -398,6 +403,8 @@ bdc_status engine_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats*
         stats->upper_bound = H->h_st->max_d / ln2;
         stats->rate = H->h_st->rate / ln2;
         stats->lse = H->h_st->lse / ln2;
+        stats->best_upper_bound = H->h_st->best_ub / ln2;
+        stats->best_rate = H->h_st->best_rate / ln2;
         stats->converged = H->h_st->done;
     }
     return BDC_OK;

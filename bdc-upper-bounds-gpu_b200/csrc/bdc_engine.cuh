@@ -76,5 +76,6 @@ bdc_status factored_load_p(bdc_handle* H);                 // d_p[0] -> dense st
 bdc_status factored_store_p(bdc_handle* H, double* p_out);  // dense state -> p per rep
 bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats);
 bdc_status factored_profile(bdc_handle* H, int iters, bdc_profile_t* out);
+bdc_status factored_accelerate(bdc_handle* H, int64_t max_evals, double gap_bits, bdc_stats* stats);
 
 }  // namespace bdc

@@ -136,6 +136,11 @@ struct FactoredState {
     // a captured chunk of kGraphIters iterations for the threshold graph_a
     cudaGraphExec_t graph = nullptr;
     double graph_a = 0.0;
+    // accelerated loop: snapshots of the normalised log iterate and its graph
+    double* snap0 = nullptr;
+    double* snap1 = nullptr;
+    double* snap2 = nullptr;
+    cudaGraphExec_t cycle = nullptr;
 };
 
 namespace bdc {
@@ -653,6 +658,8 @@ k_fac_finalize(const double* __restrict__ part, int nb, double a, DevState* st) 
     const double mx = st->zero_p ? INFINITY : (mD - st->shift - lnz) / ln2;
     st->max_d = mD;
     st->rate = sR;
+    st->best_ub = fmin(st->best_ub, mD);
+    st->best_rate = fmax(st->best_rate, sR);
     st->lse = st->shift + lnz;
     st->mx = mx;
     st->max_logw = mL + st->shift;
@@ -698,6 +705,8 @@ __global__ void k_fac_rescale_finish(const double* part, int nb, double a, DevSt
     const double lnz = log(sE);
     const double ln2 = 0.69314718055994530942;
     const double mx = st->zero_p ? INFINITY : (st->max_d - shift_eff - lnz) / ln2;
+    st->best_ub = fmin(st->best_ub, st->max_d);
+    st->best_rate = fmax(st->best_rate, st->rate);
     st->lse = shift_eff + lnz;
     st->mx = mx;
     st->max_logw = shift_eff;
@@ -1215,6 +1224,10 @@ void factored_free(bdc_handle* H) {
     }
     if (F->ev_fork) cudaEventDestroy(F->ev_fork);
     if (F->graph) cudaGraphExecDestroy(F->graph);
+    if (F->cycle) cudaGraphExecDestroy(F->cycle);
+    cudaFree(F->snap0);
+    cudaFree(F->snap1);
+    cudaFree(F->snap2);
     for (Launch* L : {&F->ul, &F->vr, &F->g}) free_launch(*L);
     cudaFree(F->d_fold);
     delete F;
@@ -1337,6 +1350,8 @@ static void fill_stats(bdc_handle* H, long long it0, bdc_stats* stats) {
     stats->upper_bound = H->h_st->max_d / ln2;
     stats->rate = H->h_st->rate / ln2;
     stats->lse = H->h_st->lse / ln2;
+    stats->best_upper_bound = H->h_st->best_ub / ln2;
+    stats->best_rate = H->h_st->best_rate / ln2;
     stats->converged = H->h_st->done;
 }
 
@@ -1401,6 +1416,256 @@ bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stat
         if (chunk < 256) chunk *= 2;
     }
     fill_stats(H, it0, stats);
+    return BDC_OK;
+}
+
+// ------------------------------------------------------ accelerated loop
+// One cycle (squared extrapolation of the BA map F in ln p):
+//   S0 = ln p; F; S1 = ln p; F (ub1 = bound at S1); S2 = ln p;
+//   alpha = clamp(-|r| / |v|, -64, -1), r = S1 - S0, v = S2 - 2 S1 + S0
+//   ln p' = S0 - 2 alpha r + alpha^2 v; F at p' (bound u');
+//   keep F(p') unless u' > ub1, else go back to S2.
+// Norms are weighted by the orbit sizes (the full-space Euclidean norm).
+constexpr double kSqAlphaMin = -64.0;
+
+__device__ __forceinline__ bool sq_gated(const DevState* st) { return st->error != 0; }
+
+__global__ void __launch_bounds__(256) k_sq_save(const uint32_t* __restrict__ reps, int64_t R,
+                                                 const double* __restrict__ Lt, double* __restrict__ dst,
+                                                 const DevState* st) {
+    if (sq_gated(st)) return;
+    const double lnz = st->log_z;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t x = reps[i];
+        dst[x] = Lt[x] - lnz;
+    }
+}
+
+__global__ void k_sq_mark(DevState* st) {
+    if (sq_gated(st)) return;
+    st->ub_theta1 = st->max_d;
+}
+
+__device__ __forceinline__ double block_sum256(double v) {
+    __shared__ double red[256];
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int t = 128; t > 0; t >>= 1) {
+        if (threadIdx.x < t) red[threadIdx.x] += red[threadIdx.x + t];
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ double block_max256(double v) {
+    __shared__ double red[256];
+    red[threadIdx.x] = v;
+    __syncthreads();
+    for (int t = 128; t > 0; t >>= 1) {
+        if (threadIdx.x < t) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + t]);
+        __syncthreads();
+    }
+    const double r = red[0];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(256) k_sq_norms(const uint32_t* __restrict__ reps, int64_t R, int n,
+                                                  const double* __restrict__ S0, const double* __restrict__ S1,
+                                                  const double* __restrict__ Lt, double* __restrict__ part,
+                                                  const DevState* st) {
+    if (sq_gated(st)) return;
+    const double lnz = st->log_z;
+    double rr = 0.0, vv = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t x = reps[i];
+        const double o = (double)orbit_size(x, n);
+        const double s0 = S0[x], s1 = S1[x], s2 = Lt[x] - lnz;
+        const double r = s1 - s0, v = s2 - 2.0 * s1 + s0;
+        rr = fma(o * r, r, rr);
+        vv = fma(o * v, v, vv);
+    }
+    rr = block_sum256(rr);
+    vv = block_sum256(vv);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = rr;
+        part[2 * blockIdx.x + 1] = vv;
+    }
+}
+
+__global__ void k_sq_alpha(const double* __restrict__ part, int nb, DevState* st) {
+    if (sq_gated(st) || threadIdx.x != 0) return;
+    double rr = 0.0, vv = 0.0;
+    for (int b = 0; b < nb; ++b) {
+        rr += part[2 * b];
+        vv += part[2 * b + 1];
+    }
+    double a = (vv > 0.0) ? -sqrt(rr / vv) : -1.0;
+    if (!(a <= -1.0)) a = -1.0;  // also catches NaN
+    if (a < kSqAlphaMin) a = kSqAlphaMin;
+    st->sq_alpha = a;
+}
+
+// S2 = current ln p; Lt = S0 - 2 a (S1 - S0) + a^2 (S2 - 2 S1 + S0); block max
+__global__ void __launch_bounds__(256) k_sq_extrap(const uint32_t* __restrict__ reps, int64_t R,
+                                                   const double* __restrict__ S0, const double* __restrict__ S1,
+                                                   double* __restrict__ S2, double* __restrict__ Lt,
+                                                   double* __restrict__ part, const DevState* st) {
+    if (sq_gated(st)) return;
+    const double a = st->sq_alpha, lnz = st->log_z;
+    double mx = -DBL_MAX;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t x = reps[i];
+        const double s0 = S0[x], s1 = S1[x], s2 = Lt[x] - lnz;
+        S2[x] = s2;
+        const double t = s0 - 2.0 * a * (s1 - s0) + a * a * (s2 - 2.0 * s1 + s0);
+        Lt[x] = t;
+        mx = fmax(mx, t);
+    }
+    mx = block_max256(mx);
+    if (threadIdx.x == 0) part[blockIdx.x] = mx;
+}
+
+__global__ void k_sq_max(const double* __restrict__ part, int nb, DevState* st) {
+    if (sq_gated(st) || threadIdx.x != 0) return;
+    double m = -DBL_MAX;
+    for (int b = 0; b < nb; ++b) m = fmax(m, part[b]);
+    st->sq_max = m;
+}
+
+// Lt -= max, Pw = |O| exp(Lt); block sums of |O| exp(Lt).  With restore set
+// the source is S2 instead (the extrapolated point was rejected).
+__global__ void __launch_bounds__(256) k_sq_pw(const uint32_t* __restrict__ reps, int64_t R, int n,
+                                               const double* __restrict__ S2, double* __restrict__ Lt,
+                                               double* __restrict__ Pw, double* __restrict__ part, int from_s2,
+                                               const DevState* st) {
+    if (sq_gated(st)) return;
+    if (from_s2 && !st->restore) return;
+    const double m = from_s2 ? 0.0 : st->sq_max;
+    double sum = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t x = reps[i];
+        const double l = (from_s2 ? S2[x] : Lt[x]) - m;
+        const double o = (double)orbit_size(x, n);
+        const double e = exp(l);
+        Lt[x] = l;
+        Pw[x] = o * e;
+        sum = fma(o, e, sum);
+    }
+    sum = block_sum256(sum);
+    if (threadIdx.x == 0) part[blockIdx.x] = sum;
+}
+
+// ln Z of the new point and the next exp shift (max ln p + the last bound)
+__global__ void k_sq_setz(const double* __restrict__ part, int nb, int from_s2, DevState* st) {
+    if (sq_gated(st) || threadIdx.x != 0) return;
+    if (from_s2 && !st->restore) return;
+    double s = 0.0;
+    for (int b = 0; b < nb; ++b) s += part[b];
+    const double lnz = log(s);
+    st->log_z = lnz;
+    st->shift = -lnz + (from_s2 ? st->ub_theta1 : st->max_d);
+    if (from_s2) st->restore = 0;
+}
+
+__global__ void k_sq_guard(DevState* st) {
+    if (sq_gated(st)) return;
+    st->restore = !(st->max_d <= st->ub_theta1);
+}
+
+static cudaError_t enqueue_cycle(bdc_handle* H) {
+    FactoredState* F = H->fac;
+    cudaStream_t s = H->stream;
+    const int nb = H->nb_upd;
+    const int64_t R = H->R;
+    cudaError_t e;
+    k_sq_save<<<nb, 256, 0, s>>>(H->d_reps, R, F->Lt, F->snap0, H->d_st);
+    if ((e = enqueue_iteration(H, -INFINITY)) != cudaSuccess) return e;
+    k_sq_save<<<nb, 256, 0, s>>>(H->d_reps, R, F->Lt, F->snap1, H->d_st);
+    if ((e = enqueue_iteration(H, -INFINITY)) != cudaSuccess) return e;
+    k_sq_mark<<<1, 1, 0, s>>>(H->d_st);
+    k_sq_norms<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap0, F->snap1, F->Lt, F->epart, H->d_st);
+    k_sq_alpha<<<1, 32, 0, s>>>(F->epart, nb, H->d_st);
+    k_sq_extrap<<<nb, 256, 0, s>>>(H->d_reps, R, F->snap0, F->snap1, F->snap2, F->Lt, F->epart, H->d_st);
+    k_sq_max<<<1, 32, 0, s>>>(F->epart, nb, H->d_st);
+    k_sq_pw<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap2, F->Lt, F->Pw, F->epart, 0, H->d_st);
+    k_sq_setz<<<1, 32, 0, s>>>(F->epart, nb, 0, H->d_st);
+    if ((e = enqueue_iteration(H, -INFINITY)) != cudaSuccess) return e;
+    k_sq_guard<<<1, 1, 0, s>>>(H->d_st);
+    k_sq_pw<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap2, F->Lt, F->Pw, F->epart, 1, H->d_st);
+    k_sq_setz<<<1, 32, 0, s>>>(F->epart, nb, 1, H->d_st);
+    return cudaGetLastError();
+}
+
+static bdc_status ensure_cycle_graph(bdc_handle* H) {
+    FactoredState* F = H->fac;
+    if (F->cycle) return BDC_OK;
+    const size_t NX = (size_t)1 << (H->n - 1);
+    if (!F->snap0) {
+        BDC_CUDA_TRY(cudaMalloc(&F->snap0, sizeof(double) * NX));
+        BDC_CUDA_TRY(cudaMalloc(&F->snap1, sizeof(double) * NX));
+        BDC_CUDA_TRY(cudaMalloc(&F->snap2, sizeof(double) * NX));
+        H->bytes += 3 * sizeof(double) * NX;
+    }
+    cudaStream_t keep = H->stream;
+    H->stream = H->own_stream;
+    BDC_CUDA_TRY(cudaStreamSynchronize(keep));
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(H->own_stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = enqueue_cycle(H);
+    cudaError_t e2 = cudaStreamEndCapture(H->own_stream, &g);
+    H->stream = keep;
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&F->cycle, g, 0);
+    if (g) cudaGraphDestroy(g);
+    BDC_CUDA_TRY(e);
+    return BDC_OK;
+}
+
+bdc_status factored_accelerate(bdc_handle* H, int64_t max_evals, double gap_bits, bdc_stats* stats) {
+    FactoredState* F = H->fac;
+    const double ln2 = 0.69314718055994530942;
+    BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), H->stream));
+    BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    const long long it0 = H->h_st->iter;
+    // a plain step first when the iterate still carries the caller's exact zeros
+    if (H->h_st->iter == 0 && max_evals > 0) {
+        bdc_status rc = factored_iterate(H, 1, -INFINITY, nullptr);
+        if (rc != BDC_OK) return rc;
+    }
+    bdc_status rc = ensure_cycle_graph(H);
+    if (rc != BDC_OK) return rc;
+    int64_t chunk = 1;
+    bool converged = false;
+    for (int guard = 0; guard < 1000000; ++guard) {
+        const double gap = (H->h_st->best_ub - H->h_st->best_rate) / ln2;
+        if (gap < gap_bits) {
+            converged = true;
+            break;
+        }
+        const int64_t remaining = max_evals - (H->h_st->iter - it0);
+        if (remaining < 3) break;
+        const int64_t c = std::min<int64_t>(chunk, remaining / 3);
+        for (int64_t i = 0; i < c; ++i) BDC_CUDA_TRY(cudaGraphLaunch(F->cycle, H->stream));
+        BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
+        BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+        if (H->h_st->error == kErrShift) {
+            // an exp shift went out of range inside a cycle: finish that
+            // evaluation by re-scaling and start the next cycle from there
+            rc = rescale(H, -INFINITY);
+            if (rc != BDC_OK) return rc;
+            BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
+            BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+        } else if (H->h_st->error) {
+            return fail(BDC_ERR_NUMERIC, "accelerated loop: device error %d", H->h_st->error);
+        }
+        if (chunk < 64) chunk *= 2;
+    }
+    fill_stats(H, it0, stats);
+    if (stats) stats->converged = converged;
     return BDC_OK;
 }
 

@@ -55,6 +55,8 @@ struct UpdateLaunch {
 cudaError_t launch_update(const UpdateLaunch& U);
 cudaError_t launch_logw(int n, const uint32_t* reps, int64_t R, const double* p, const double* d,
                         double* logw, cudaStream_t stream);
+cudaError_t launch_mi_grad(int n, const uint32_t* reps, int64_t R, const double* d, double* grad,
+                           cudaStream_t stream);
 cudaError_t launch_rate(int n, const uint32_t* reps, int64_t R, const double* p, const double* d,
                         double* part, int nblocks, double* out, cudaStream_t stream);
 cudaError_t launch_max_dev(const double* p, const double* pb, int64_t R, double* part, int nblocks,

@@ -117,6 +117,8 @@ k_upd_logw(int n, const uint32_t* __restrict__ reps, int64_t R, const double* __
         st->max_logw = r0;
         st->max_d = r1;
         st->rate = r2;
+        st->best_ub = fmin(st->best_ub, r1);
+        st->best_rate = fmax(st->best_rate, r2);
         st->zero_p = (r3 != 0.0);
         st->shift = r0;
         st->ticket[0] = 0;
@@ -228,6 +230,24 @@ __global__ void __launch_bounds__(kUpdThreads)
 k_fold_max(const double* __restrict__ part, int nb, double* out) {
     const double s = fold_partials(part, nb, OpMax(), -DBL_MAX);
     if (threadIdx.x == 0) *out = s;
+}
+
+// adjoint of I(p;W) = sum_x p(x) D(x) over the representative parametrisation:
+// dI/dp_rep = |O(rep)| (D(rep) - 1) -- the q-dependence of D cancels because
+// sum_y W(y|x) = 1 (backend/BAA.cu:413-425 computes the same D)
+__global__ void k_mi_grad(int n, const uint32_t* __restrict__ reps, int64_t R, const double* __restrict__ d,
+                          double* __restrict__ grad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
+        grad[i] = (double)orbit_size(reps[i], n) * (d[i] - 1.0);
+}
+
+cudaError_t launch_mi_grad(int n, const uint32_t* reps, int64_t R, const double* d, double* grad,
+                           cudaStream_t stream) {
+    int64_t b = (R + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    if (b < 1) b = 1;
+    k_mi_grad<<<(int)b, 256, 0, stream>>>(n, reps, R, d, grad);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_rate(int n, const uint32_t* reps, int64_t R, const double* p, const double* d,

@@ -63,7 +63,12 @@ typedef struct {
     double upper_bound;       /* max_x D(x) of the last iteration's D pass (bits): C <= this */
     double rate;              /* sum_x p(x) D(x) of that iterate (bits) = I(p;W) */
     double lse;               /* log2 sum_x p(x) 2^{D(x)} of that iterate (bits) */
-    int converged;            /* 1 when the last mx < a (the loop of main_BAA.cu:73 ends) */
+    double best_upper_bound;  /* min of max_x D(x) over every iterate evaluated since the
+                                 distribution was set (bits): C <= this */
+    double best_rate;         /* max of I(p;W) over those iterates (bits): this <= C */
+    int converged;            /* bdc_iterate: 1 when the last mx < a (the loop of
+                                 main_BAA.cu:73 ends); bdc_accelerate: 1 when
+                                 best_upper_bound - best_rate < gap */
 } bdc_stats;
 
 typedef struct bdc_handle* bdc_handle_t;
@@ -97,6 +102,26 @@ bdc_status bdc_get_p_device(bdc_handle_t h, double* p_dev, int64_t num_reps);
  * BAA.cu:590-639 and compute_max_deviation, BAA.cu:916-946): runs iterations
  * until mx < a or max_iters iterations, all on the device.  stats may be NULL. */
 bdc_status bdc_iterate(bdc_handle_t h, int64_t max_iters, double a, bdc_stats* stats);
+
+/* Accelerated BA (no counterpart in the reference): the BA map is the
+ * exponentiated-gradient step ln p' = ln p + dI/dp + const with the adjoint
+ * gradient dI/dp(x) = D(x) - 1; this loop extrapolates that map in ln p
+ * (squared extrapolation: two steps, a step length alpha fitted to them and
+ * clamped to [-64, -1], one stabilising step, and a fallback to the plain
+ * second step when the bound at the extrapolated point is worse).  Every
+ * evaluated iterate gives a valid bound, so best_upper_bound stays an upper
+ * bound on C.  Runs until best_upper_bound - best_rate < gap_bits or
+ * max_evals BA map evaluations.  Factored engine only. */
+bdc_status bdc_accelerate(bdc_handle_t h, int64_t max_evals, double gap_bits, bdc_stats* stats);
+
+/* The mutual-information functional and its adjoint (no counterpart in the
+ * reference).  Forward: I(p;W) in nats for p (host, one entry per
+ * representative, not necessarily normalised; NULL: the current iterate),
+ * which becomes the current iterate.  Backward: grad[i] = dI/dp_i in nats for
+ * the current iterate, where p_i moves the probability of every string of
+ * orbit i together: grad[i] = |O_i| (D(x_i) - 1). */
+bdc_status bdc_mi_forward(bdc_handle_t h, const double* p, int64_t num_reps, double* I_nats);
+bdc_status bdc_mi_backward(bdc_handle_t h, double* grad, int64_t num_reps);
 
 /* One reference-shaped iteration with host vectors: p_in -> p_out, like
  * baa_iteration (BAA.cu:590-639, decl. BAA.cuh:295); p_out may equal p_in. */
