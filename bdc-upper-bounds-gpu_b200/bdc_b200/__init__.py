@@ -41,6 +41,7 @@ EXPORTED_SYMBOLS = [
     "bdc_generate_cache", "bdc_read_cache_file", "bdc_write_cache_file", "bdc_read_dist_file",
     "bdc_write_dist_file", "bdc_work", "bdc_profile", "bdc_set_stream", "bdc_peak_probe",
     "bdc_max_deviation_noalloc", "bdc_accelerate", "bdc_mi_forward", "bdc_mi_backward",
+    "bdc_batch_create", "bdc_batch_iterate", "bdc_batch_destroy", "bdc_batch_set_stream",
 ]
 
 
@@ -107,6 +108,10 @@ def library() -> ctypes.CDLL:
     L.bdc_iterate.argtypes = [h, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats)]
     L.bdc_baa_iteration.argtypes = [h, _f64p, _f64p, ctypes.c_int64]
     L.bdc_accelerate.argtypes = [h, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats)]
+    L.bdc_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.bdc_batch_iterate.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats)]
+    L.bdc_batch_destroy.argtypes = [ctypes.c_void_p]
+    L.bdc_batch_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.bdc_mi_forward.argtypes = [h, _f64p, ctypes.c_int64, _f64p]
     L.bdc_mi_backward.argtypes = [h, _f64p, ctypes.c_int64]
     L.bdc_log_q.argtypes = [h, _f64p, ctypes.c_int64]
@@ -341,6 +346,44 @@ class Engine:
         out = np.empty(len(xs), dtype=np.uint32)
         _check(library().bdc_counts(self._h, px, py, len(xs), out.ctypes.data_as(_u32p)), "bdc_counts")
         return out
+
+
+class Batch:
+    """Several engines (any mix of (n,k) and starting distributions) iterated
+    together from one captured CUDA graph, one branch per engine."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        arr = (ctypes.c_void_p * len(self.engines))(*[E._h.value for E in self.engines])
+        b = ctypes.c_void_p()
+        _check(library().bdc_batch_create(arr, len(self.engines), ctypes.byref(b)), "bdc_batch_create")
+        self._b = b
+
+    def iterate(self, max_iters: int, a: float = float("-inf")) -> list:
+        st = (Stats * len(self.engines))()
+        _check(library().bdc_batch_iterate(self._b, int(max_iters), float(a), st), "bdc_batch_iterate")
+        return [s.as_dict() for s in st]
+
+    def set_stream(self, stream: int | None) -> None:
+        """Queue the batch's work on a cudaStream_t given as an integer handle."""
+        _check(library().bdc_batch_set_stream(self._b, ctypes.c_void_p(stream or 0)), "bdc_batch_set_stream")
+
+    def close(self) -> None:
+        if getattr(self, "_b", None):
+            library().bdc_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 # ------------------------------------------------------------ file formats

@@ -380,6 +380,11 @@ bdc_status engine_profile(bdc_handle* H, int iters, bdc_profile_t* out) {
     return BDC_OK;
 }
 
+cudaError_t engine_enqueue_iteration(bdc_handle* H, double a) {
+    if (H->engine == BDC_ENGINE_FACTORED) return factored_enqueue_iteration(H, a);
+    return enqueue_count_iteration(H, a);
+}
+
 bdc_status engine_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats) {
     if (H->engine == BDC_ENGINE_FACTORED) return factored_iterate(H, max_iters, a, stats);
     BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), H->stream));

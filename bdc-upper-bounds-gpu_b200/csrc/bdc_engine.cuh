@@ -66,6 +66,7 @@ bdc_status engine_divergence(bdc_handle* H);  // D from H->d_lnq into H->d_d
 CountLaunch count_launch(const bdc_handle* H);
 UpdateLaunch update_launch(const bdc_handle* H, double a);
 bdc_status engine_profile(bdc_handle* H, int iters, bdc_profile_t* out);
+cudaError_t engine_enqueue_iteration(bdc_handle* H, double a);  // one iteration, gated by done
 int count_group_size(int k);
 
 // factored engine (bdc_factored.cu)
@@ -77,5 +78,9 @@ bdc_status factored_store_p(bdc_handle* H, double* p_out);  // dense state -> p 
 bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats);
 bdc_status factored_profile(bdc_handle* H, int iters, bdc_profile_t* out);
 bdc_status factored_accelerate(bdc_handle* H, int64_t max_evals, double gap_bits, bdc_stats* stats);
+cudaError_t factored_enqueue_iteration(bdc_handle* H, double a);
+// finishes an iteration that stopped on an exp-shift overflow (on H->stream);
+// any other device error is returned as BDC_ERR_NUMERIC
+bdc_status factored_recover(bdc_handle* H, double a);
 
 }  // namespace bdc

@@ -59,9 +59,9 @@ struct Term {
 };
 
 // tile configurations of the FP64 tensor-core products (BM x BN, warps WM x WN)
-enum MmaConfig { CFG_128x128 = 0, CFG_128x64, CFG_64x128, CFG_64x64, CFG_128x16, CFG_16x128, CFG_COUNT };
-static const int kCfgBM[CFG_COUNT] = {128, 128, 64, 64, 128, 16};
-static const int kCfgBN[CFG_COUNT] = {128, 64, 128, 64, 16, 128};
+enum MmaConfig { CFG_128x128 = 0, CFG_128x64, CFG_64x128, CFG_64x64, CFG_128x16, CFG_16x128, CFG_128x32, CFG_COUNT };
+static const int kCfgBM[CFG_COUNT] = {128, 128, 64, 64, 128, 16, 128};
+static const int kCfgBN[CFG_COUNT] = {128, 64, 128, 64, 16, 128, 32};
 
 struct Launch {
     GemmDesc* d = nullptr;   // device descriptors
@@ -110,6 +110,8 @@ struct FactoredState {
     double* Pw = nullptr;     // [2^{n-1}]  |O(x)| e(x) at representatives, 0 elsewhere
     double* Lt = nullptr;     // [2^{n-1}]  ln e(x) (p = e / Z)
     double* hx = nullptr;     // [2^{n-1}]  h(x) at representatives
+    uint16_t* Bp = nullptr;   // low-half tables, row c = table row rev(c) (dense column order)
+    std::vector<int> colmax;  // per dense column: largest x_hi of a representative, -1 if none
     double* LA = nullptr;     // [H1h][Kp]  = [AL | NR]
     double* RB = nullptr;     // [Kp][H2]  = [ML ; BR^T]
     double* UL = nullptr;     // [H2][KL]  (U^T)
@@ -124,6 +126,10 @@ struct FactoredState {
     int n_thinq[8] = {};
     bdc::ThinD* d_thind[8] = {};
     int n_thind[8] = {}, ctas_thind[8] = {};
+    // the same products on the FP64 tensor-core path, used for the size
+    // classes where the tuner found them faster
+    bdc::Launch mq[8], md[8];
+    bool use_mq[8] = {}, use_md[8] = {};
     double* lnq_full = nullptr;  // [2^k]
     double* epart = nullptr;  // [ctas][8]
     int ctas_g = 0;
@@ -146,6 +152,16 @@ struct FactoredState {
 namespace bdc {
 
 __device__ __forceinline__ bool gated(const DevState* st) { return st && (st->done || st->error); }
+
+// Dense layout of the iterate: row x_hi, column rev(x_lo) (the low half
+// bit-reversed).  A representative x satisfies x <= rev(x) and x <=
+// rev(comp(x)), so x_hi is at most a bound that rises and then falls along
+// the columns; whole tiles of the dense matrices then hold no
+// representative and are skipped.  The map is its own inverse.
+__host__ __device__ __forceinline__ uint32_t fac_pos(uint32_t x, int n2) {
+    const uint32_t m = low_mask(n2);
+    return (x & ~m) | reverse_bits(x & m, n2);
+}
 
 
 // ------------------------------------------------ products: plain store
@@ -185,13 +201,13 @@ __global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ 
 // are updated; block partials [max D, sum |O| e, max (logW - shift),
 // sum |O| p D, input-zero flag] go to ep.part[blockIdx.x * 8 + 0..4].
 template <int BM, int BN, int WM, int WN>
-__global__ void __launch_bounds__(256) k_mma_ba(const GemmDesc* __restrict__ descs, BaEpilogue ep,
-                                                const DevState* st) {
+__global__ void __launch_bounds__(256) k_mma_ba(const GemmDesc* __restrict__ descs, const int* __restrict__ tiles,
+                                                BaEpilogue ep, const DevState* st) {
     using C = MmaCfg<BM, BN, WM, WN>;
     if (gated(st)) return;
     extern __shared__ __align__(16) double smem[];
     const GemmDesc& d = descs[0];
-    const int t = blockIdx.x;
+    const int t = tiles[blockIdx.x];  // the tiles that hold representatives
     const int m0 = (t / d.tiles_n) * BM, n0 = (t % d.tiles_n) * BN;
     double acc[C::MT][C::NT][2];
     mma_mainloop<BM, BN, WM, WN>(d, m0, n0, smem, acc);
@@ -212,22 +228,23 @@ __global__ void __launch_bounds__(256) k_mma_ba(const GemmDesc* __restrict__ des
             for (int h = 0; h < 2; ++h) {
                 const int n = n0 + wn0 + j * 8 + 2 * tq + h;
                 if (n >= d.N) continue;
-                const uint32_t x = ((uint32_t)m << ep.n2) | (uint32_t)n;
+                const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
+                const uint32_t x = fac_pos(xd, ep.n2);
                 if (!is_rep(x, ep.n)) continue;
                 const double o = (double)orbit_size(x, ep.n);
-                const double D = __ldg(ep.hx + x) - acc[i][j][h] * ep.inv_c;
+                const double D = __ldg(ep.hx + xd) - acc[i][j][h] * ep.inv_c;
                 // an entry that is exactly 0 in the caller's distribution (Lt
                 // holds NaN) takes ln p = 0, as the reference's apply_log_kernel
                 // leaves ln 0 at 0 (backend/BAA.cu:573-580); later iterates keep
                 // exact logarithms
-                const double pw = ep.Pw[x];
-                const double lt = ep.Lt[x];
+                const double pw = ep.Pw[xd];
+                const double lt = ep.Lt[xd];
                 const bool zero_in = (lt != lt);
                 const double lnp = zero_in ? 0.0 : lt - lnz;
                 const double lw = lnp + D - shift;
                 const double e = exp(lw);
-                ep.Lt[x] = lw;
-                ep.Pw[x] = o * e;
+                ep.Lt[xd] = lw;
+                ep.Pw[xd] = o * e;
                 mD = fmax(mD, D);
                 mL = fmax(mL, lw);
                 sE = fma(o, e, sE);
@@ -276,6 +293,7 @@ __global__ void __launch_bounds__(256) k_mma_ba(const GemmDesc* __restrict__ des
 #define BDC_CFG_ARGS_64x64 64, 64, 2, 4
 #define BDC_CFG_ARGS_128x16 128, 16, 8, 1
 #define BDC_CFG_ARGS_16x128 16, 128, 1, 8
+#define BDC_CFG_ARGS_128x32 128, 32, 4, 2
 
 static int cfg_smem(int cfg) {
     switch (cfg) {
@@ -285,6 +303,7 @@ static int cfg_smem(int cfg) {
         case CFG_64x64: return mma_smem_bytes<BDC_CFG_ARGS_64x64>();
         case CFG_128x16: return mma_smem_bytes<BDC_CFG_ARGS_128x16>();
         case CFG_16x128: return mma_smem_bytes<BDC_CFG_ARGS_16x128>();
+        case CFG_128x32: return mma_smem_bytes<BDC_CFG_ARGS_128x32>();
     }
     return 0;
 }
@@ -304,6 +323,7 @@ static cudaError_t set_smem_attrs() {
     SET_(k_mma_store, BDC_CFG_ARGS_64x64)
     SET_(k_mma_store, BDC_CFG_ARGS_128x16)
     SET_(k_mma_store, BDC_CFG_ARGS_16x128)
+    SET_(k_mma_store, BDC_CFG_ARGS_128x32)
     SET_(k_mma_ba, BDC_CFG_ARGS_128x128)
     SET_(k_mma_ba, BDC_CFG_ARGS_128x64)
     SET_(k_mma_ba, BDC_CFG_ARGS_64x128)
@@ -322,6 +342,7 @@ static cudaError_t launch_store(const Launch& L, cudaStream_t s, const DevState*
         case CFG_64x64: k_mma_store<BDC_CFG_ARGS_64x64><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
         case CFG_128x16: k_mma_store<BDC_CFG_ARGS_128x16><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
         case CFG_16x128: k_mma_store<BDC_CFG_ARGS_16x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
+        case CFG_128x32: k_mma_store<BDC_CFG_ARGS_128x32><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -330,9 +351,9 @@ static cudaError_t launch_store(const Launch& L, cudaStream_t s, const DevState*
 static cudaError_t launch_ba(const Launch& L, const BaEpilogue& ep, cudaStream_t s, const DevState* st) {
     const int sm = cfg_smem(L.cfg);
     switch (L.cfg) {
-        case CFG_128x128: k_mma_ba<BDC_CFG_ARGS_128x128><<<L.tiles, 256, sm, s>>>(L.d, ep, st); break;
-        case CFG_128x64: k_mma_ba<BDC_CFG_ARGS_128x64><<<L.tiles, 256, sm, s>>>(L.d, ep, st); break;
-        case CFG_64x128: k_mma_ba<BDC_CFG_ARGS_64x128><<<L.tiles, 256, sm, s>>>(L.d, ep, st); break;
+        case CFG_128x128: k_mma_ba<BDC_CFG_ARGS_128x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st); break;
+        case CFG_128x64: k_mma_ba<BDC_CFG_ARGS_128x64><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st); break;
+        case CFG_64x128: k_mma_ba<BDC_CFG_ARGS_64x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -572,7 +593,7 @@ __device__ __forceinline__ double term_value(const FoldTerm& f, const double* qs
                                              uint32_t y) {
     if (f.kind == 0) return qsum[(size_t)t * ny + y];
     const uint32_t yh = y >> f.m, yl = y & ((1u << f.m) - 1u);
-    if (f.kind == 1) return ULt[(size_t)yl * KL + f.off + yh];  // Q_t = U_t
+    if (f.kind == 1) return ULt[(size_t)reverse_bits(yl, f.m) * KL + f.off + yh];  // Q_t = U_t (rows: rev x_lo)
     return yh < (uint32_t)H1h ? VR[(size_t)yh * KR + f.off + yl] : 0.0;  // Q_t = V_t
 }
 
@@ -605,7 +626,7 @@ __global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double
         for (int t = 0; t < T; ++t) {
             const FoldTerm& f = terms[t];
             const uint32_t yh = (uint32_t)y >> f.m, yl = (uint32_t)y & ((1u << f.m) - 1u);
-            if (f.idB_left) RB[(size_t)(f.off + yh) * H2 + yl] = lq;  // M_t = Lq_t
+            if (f.idB_left) RB[(size_t)(f.off + yh) * H2 + reverse_bits(yl, f.m)] = lq;  // M_t = Lq_t
             if (f.idA_right && yh < (uint32_t)H1h) LA[(size_t)yh * Kp + KL + f.off + yl] = lq;  // N_t = Lq_t
         }
     }
@@ -678,12 +699,12 @@ k_fac_rescale(const uint32_t* __restrict__ reps, int64_t R, int n, double* Lt, d
     const double s = st->max_logw;  // max of Lt after the failed epilogue
     double sum = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i];
-        const double l = Lt[x] - s;
+        const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
+        const double l = Lt[xd] - s;
         const double o = (double)orbit_size(x, n);
-        Lt[x] = l;
+        Lt[xd] = l;
         const double e = exp(l);
-        Pw[x] = o * e;
+        Pw[xd] = o * e;
         sum = fma(o, e, sum);
     }
     __shared__ double red[256];
@@ -725,12 +746,12 @@ k_fac_load(const uint32_t* __restrict__ reps, int64_t R, int n, const double* __
     double mx = -DBL_MAX;
     int zero = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i];
+        const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
         const double v = p[i];
-        Pw[x] = (double)orbit_size(x, n) * v;
+        Pw[xd] = (double)orbit_size(x, n) * v;
         // ln 0 = 0 (backend/BAA.cu:573-580): marked with NaN for the epilogue
         const double l = (v != 0.0) ? log(v) : 0.0;
-        Lt[x] = (v != 0.0) ? l : __longlong_as_double(0x7ff8000000000000ll);
+        Lt[xd] = (v != 0.0) ? l : __longlong_as_double(0x7ff8000000000000ll);
         mx = fmax(mx, l);
         if (v == 0.0) zero = 1;
     }
@@ -770,15 +791,15 @@ __global__ void k_fac_store(const uint32_t* __restrict__ reps, int64_t R, int n,
     const double inv_z = exp(-st->log_z);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t x = reps[i];
-        p[i] = Pw[x] * inv_z / (double)orbit_size(x, n);
+        p[i] = Pw[fac_pos(x, n >> 1)] * inv_z / (double)orbit_size(x, n);
     }
 }
 
 // scatter h per representative into the dense layout
-__global__ void k_scatter(const uint32_t* __restrict__ reps, int64_t R, const double* __restrict__ v,
+__global__ void k_scatter(const uint32_t* __restrict__ reps, int64_t R, int n, const double* __restrict__ v,
                           double* __restrict__ dense) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
-        dense[reps[i]] = v[i];
+        dense[fac_pos(reps[i], n >> 1)] = v[i];
 }
 
 // constant parts of LA (AL columns) and RB (BR^T rows) from the bundles
@@ -800,6 +821,16 @@ __global__ void k_fill_tables(int H1, int H2, int Kp, const uint16_t* __restrict
             const int64_t xl = f % H2;
             RB[(int64_t)(KL + c) * H2 + xl] = (double)blo[xl * strideB + colmap[KL + c]];
         }
+    }
+}
+
+// the low-half tables in dense-column order: row c = table row rev(c)
+__global__ void k_permute_rows(const uint16_t* __restrict__ src, int64_t stride, int rows, int n2,
+                               uint16_t* __restrict__ dst) {
+    const int64_t total = (int64_t)rows * stride;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = e / stride, w = e % stride;
+        dst[e] = src[(int64_t)reverse_bits((uint32_t)c, n2) * stride + w];
     }
 }
 
@@ -901,17 +932,45 @@ static float time_ms(bdc_handle* H, F&& launch) {
     return (cudaGetLastError() == cudaSuccess) ? ms / 3.f : 1e30f;
 }
 
-// chooses tile shape and split of one of the thin products by timing them
-static bdc_status tune_thin(bdc_handle* H, Launch& L, const GemmDesc& base, int64_t cstride, int max_split,
-                            int kmin, const char* what, int* split_out) {
+// G with only the tiles that hold representatives (colmax: per dense column
+// the largest row of a representative); CTA i runs tile map[i]
+static cudaError_t make_tile_launch(Launch& L, GemmDesc d, int cfg, const std::vector<int>& colmax) {
+    free_launch(L);
+    L.cfg = cfg;
+    L.n = 1;
+    const int BM = kCfgBM[cfg], BN = kCfgBN[cfg];
+    d.tiles_m = (d.M + BM - 1) / BM;
+    d.tiles_n = (d.N + BN - 1) / BN;
+    d.tile_begin = 0;
+    std::vector<int> ids;
+    for (int tm = 0; tm < d.tiles_m; ++tm)
+        for (int tn = 0; tn < d.tiles_n; ++tn) {
+            int mx = -1;
+            for (int c = tn * BN; c < std::min(d.N, (tn + 1) * BN); ++c) mx = std::max(mx, colmax[c]);
+            if (mx >= tm * BM) ids.push_back(tm * d.tiles_n + tn);
+        }
+    L.tiles = (int)ids.size();
+    if (ids.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&L.d, sizeof(GemmDesc));
+    if (e == cudaSuccess) e = cudaMemcpy(L.d, &d, sizeof(GemmDesc), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&L.map, sizeof(int) * ids.size());
+    if (e == cudaSuccess) e = cudaMemcpy(L.map, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice);
+    return e;
+}
+
+// chooses tile shape and split of one of the wide q-side products by timing
+// them; gen(cfg, S) lists the descriptors of a candidate (S: the split of
+// the longest contraction, kfull its length)
+template <typename Gen>
+static bdc_status tune_thin(bdc_handle* H, Launch& L, Gen&& gen, int kfull, int max_split, int kmin,
+                            const char* what, int* split_out) {
     const int cfgs[4] = {CFG_128x128, CFG_128x64, CFG_64x128, CFG_64x64};
     float best = 1e30f;
     int best_cfg = CFG_64x64, best_s = 1;
     for (int ci = 0; ci < 4; ++ci) {
         for (int S = 1; S <= max_split; S *= 2) {
-            if (base.K / S < kmin) break;
-            std::vector<GemmDesc> v;
-            split_k(v, base, S, cstride);
+            if (kfull / S < kmin) break;
+            std::vector<GemmDesc> v = gen(cfgs[ci], S);
             Launch T;
             BDC_CUDA_TRY(make_launch(T, v, cfgs[ci]));
             if (T.tiles > 64 * H->num_sms) {
@@ -927,13 +986,71 @@ static bdc_status tune_thin(bdc_handle* H, Launch& L, const GemmDesc& base, int6
             }
         }
     }
-    std::vector<GemmDesc> v;
-    split_k(v, base, best_s, cstride);
-    BDC_CUDA_TRY(make_launch(L, v, best_cfg));
+    BDC_CUDA_TRY(make_launch(L, gen(best_cfg, best_s), best_cfg));
     *split_out = best_s;
     if (H->verbose)
         printf("bdc: tuned %s: tile %dx%d, split %d, %.1f us\n", what, kCfgBM[best_cfg], kCfgBN[best_cfg], best_s,
                best * 1e3f);
+    return BDC_OK;
+}
+
+// A thin q-side product as a matrix product on the tensor-core path, in the
+// orientation whose long side (the wide index w) is M:
+//   C(w, i) = sum_s wide(s)[w] small(s)[i] over s in [s0, s1)
+static GemmDesc thin_q_desc(const ThinQ& q) {
+    Operand A, B;
+    A.ptr = q.wide;
+    A.ld = q.wide_stride;
+    A.kind = q.wide_u16 ? OP_U16 : OP_F64;
+    A.trans = 1;
+    B.ptr = q.small;
+    B.ld = q.small_stride;
+    B.kind = q.small_u16 ? OP_U16 : OP_F64;
+    B.trans = 0;
+    GemmDesc d = make_desc(k_offset(A, true, q.s0), k_offset(B, false, q.s0), q.out, q.out_trans ? q.SMALL : 1,
+                           q.out_trans ? 1 : q.WIDE, q.WIDE, q.SMALL, q.s1 - q.s0);
+    return d;
+}
+
+// A thin D-side product: C(s, i) = sum_w wide(s)[w] Lq'[w][i]
+static GemmDesc thin_d_desc(const ThinD& t, const double* lnq_full) {
+    Operand A, B;
+    A.ptr = t.wide;
+    A.ld = t.wide_stride;
+    A.kind = OP_U16;
+    A.trans = 0;
+    B.ptr = lnq_full;
+    B.kind = OP_F64;
+    B.trans = t.lq_trans ? 0 : 1;
+    B.ld = t.lq_trans ? t.SMALL : t.WIDE;
+    return make_desc(A, B, t.out, t.out_s, t.out_i, t.rows, t.SMALL, t.WIDE);
+}
+
+// times the CUDA-core kernel of one size class against the tensor-core
+// launch in a few tile shapes and keeps the fastest
+static bdc_status tune_class(bdc_handle* H, const std::vector<GemmDesc>& descs, Launch& L, bool& use_mma,
+                             float core_ms, const char* what, int lg) {
+    const int cfgs[5] = {CFG_128x16, CFG_128x32, CFG_64x64, CFG_128x64, CFG_64x128};
+    float best = core_ms;
+    int best_cfg = -1;
+    for (int c : cfgs) {
+        Launch T;
+        BDC_CUDA_TRY(make_launch(T, descs, c));
+        const float ms = time_ms(H, [&] { launch_store(T, H->stream, nullptr); });
+        free_launch(T);
+        if (ms < best) {
+            best = ms;
+            best_cfg = c;
+        }
+    }
+    use_mma = best_cfg >= 0;
+    if (use_mma) BDC_CUDA_TRY(make_launch(L, descs, best_cfg));
+    if (H->verbose)
+        printf("bdc: tuned %s, %d outputs per term: %s %.1f us (CUDA cores %.1f us)\n", what, 1 << lg,
+               use_mma ? (best_cfg == CFG_128x16 ? "mma 128x16" : best_cfg == CFG_128x32 ? "mma 128x32"
+                          : best_cfg == CFG_64x64 ? "mma 64x64" : best_cfg == CFG_128x64 ? "mma 128x64" : "mma 64x128")
+                       : "CUDA cores",
+               best * 1e3f, core_ms * 1e3f);
     return BDC_OK;
 }
 
@@ -1000,6 +1117,26 @@ bdc_status factored_init(bdc_handle* H) {
     BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
     BDC_CUDA_TRY(cudaMemsetAsync(F->lnq_full, 0, sizeof(double) * ny, H->stream));
 
+    // low-half tables in dense-column order, and the largest row of a
+    // representative in each dense column (for skipping empty tiles)
+    {
+        const size_t cnt = (size_t)H2 * H->B.stride;
+        BDC_CUDA_TRY(cudaMalloc(&F->Bp, cnt * sizeof(uint16_t) + 16));
+        H->bytes += cnt * sizeof(uint16_t);
+        k_permute_rows<<<H->num_sms * 8, 256, 0, H->stream>>>(H->B.rows, H->B.stride, H2, s.n2, F->Bp);
+        BDC_CUDA_TRY(cudaGetLastError());
+        std::vector<uint32_t> hr((size_t)H->R);
+        BDC_CUDA_TRY(cudaMemcpyAsync(hr.data(), H->d_reps, sizeof(uint32_t) * hr.size(), cudaMemcpyDeviceToHost,
+                                     H->stream));
+        BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+        F->colmax.assign(H2, -1);
+        for (uint32_t x : hr) {
+            const uint32_t xd = fac_pos(x, s.n2);
+            const int c = (int)(xd & low_mask(s.n2)), xh = (int)(xd >> s.n2);
+            if (xh > F->colmax[c]) F->colmax[c] = xh;
+        }
+    }
+
     // constant table columns of LA (AL) and rows of RB (BR^T); a left term's
     // A_j or a right term's B_m is never the identity
     {
@@ -1011,27 +1148,63 @@ bdc_status factored_init(bdc_handle* H) {
         int* d_cm = nullptr;
         BDC_CUDA_TRY(cudaMalloc(&d_cm, sizeof(int) * colmap.size()));
         BDC_CUDA_TRY(cudaMemcpy(d_cm, colmap.data(), sizeof(int) * colmap.size(), cudaMemcpyHostToDevice));
-        k_fill_tables<<<H->num_sms * 8, 256, 0, H->stream>>>(H1, H2, Kp, H->A.rows, H->A.stride, H->B.rows,
+        k_fill_tables<<<H->num_sms * 8, 256, 0, H->stream>>>(H1, H2, Kp, H->A.rows, H->A.stride, F->Bp,
                                                             H->B.stride, d_cm, KL, KR, F->LA, F->RB);
         BDC_CUDA_TRY(cudaGetLastError());
         BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
         cudaFree(d_cm);
     }
-    k_scatter<<<H->num_sms * 8, 256, 0, H->stream>>>(H->d_reps, H->R, H->d_h, F->hx);
+    k_scatter<<<H->num_sms * 8, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, H->d_h, F->hx);
     BDC_CUDA_TRY(cudaGetLastError());
 
     // ---- the two thin products: U^T (H2 x KL) = (AL^T Pw)^T, V (H1h x KR) = Pw BR
+    // Only the rows x_hi <= colmax[c] of a dense column c hold
+    // representatives: U^T contracts each block of columns over those rows
+    // only, V each block of rows over the columns that reach it.  The split
+    // of a block is proportional to its contraction; split slices that no
+    // block writes stay zero.
     if (KL > 0) {
-        // A(m = c, kk = x_hi) = LA[x_hi * Kp + c]; B(kk = x_hi, n = x_lo) = Pw; C(c, x_lo) -> U^T[x_lo][c]
-        GemmDesc d = make_desc(op_f64(F->LA, Kp, 1), op_f64(F->Pw, H2, 0), F->ulpart, 1, KL, KL, H2, H1);
-        bdc_status rc = tune_thin(H, F->ul, d, (int64_t)H2 * KL, max_split, 16, "U = AL^T Pw", &F->S1);
+        // A(m = c, kk = x_hi) = LA[x_hi * Kp + c]; B(kk = x_hi, n = col) = Pw; C(c, col) -> U^T[col][c]
+        auto gen = [&](int cfg, int S) {
+            std::vector<GemmDesc> v;
+            const int BN = kCfgBN[cfg];
+            for (int n0 = 0; n0 < H2; n0 += BN) {
+                const int nb = std::min(BN, H2 - n0);
+                int kb = 0;
+                for (int c = n0; c < n0 + nb; ++c) kb = std::max(kb, F->colmax[c] + 1);
+                if (kb == 0) continue;
+                GemmDesc d = make_desc(op_f64(F->LA, Kp, 1), op_f64(F->Pw + n0, H2, 0), F->ulpart + (int64_t)n0 * KL,
+                                       1, KL, KL, nb, kb);
+                split_k(v, d, std::max(1, (int)(((int64_t)S * kb + H1 - 1) / H1)), (int64_t)H2 * KL);
+            }
+            return v;
+        };
+        bdc_status rc = tune_thin(H, F->ul, gen, H1, max_split, 16, "U = AL^T Pw", &F->S1);
         if (rc != BDC_OK) return rc;
     }
     if (KR > 0) {
-        // A(m = x_hi, kk = x_lo) = Pw; B(kk = x_lo, n = c) = RB[(KL + c) * H2 + x_lo]
-        GemmDesc d = make_desc(op_f64(F->Pw, H2, 0), op_f64(F->RB + (int64_t)KL * H2, H2, 1), F->vrpart, KR, 1,
-                               H1, KR, H2);
-        bdc_status rc = tune_thin(H, F->vr, d, (int64_t)H1 * KR, max_split, 16, "V = Pw BR", &F->S2);
+        // A(m = x_hi, kk = col) = Pw; B(kk = col, n = c) = RB[(KL + c) * H2 + col]
+        auto gen = [&](int cfg, int S) {
+            std::vector<GemmDesc> v;
+            const int BM = kCfgBM[cfg];
+            for (int m0 = 0; m0 < H1; m0 += BM) {
+                const int mb = std::min(BM, H1 - m0);
+                int clo = H2, chi = -1;
+                for (int c = 0; c < H2; ++c)
+                    if (F->colmax[c] >= m0) {
+                        clo = std::min(clo, c);
+                        chi = c;
+                    }
+                if (chi < 0) continue;
+                const int kb = chi + 1 - clo;
+                const Operand A = k_offset(op_f64(F->Pw + (int64_t)m0 * H2, H2, 0), true, clo);
+                const Operand B = k_offset(op_f64(F->RB + (int64_t)KL * H2, H2, 1), false, clo);
+                GemmDesc d = make_desc(A, B, F->vrpart + (int64_t)m0 * KR, KR, 1, mb, KR, kb);
+                split_k(v, d, std::max(1, (int)(((int64_t)S * kb + H2 - 1) / H2)), (int64_t)H1 * KR);
+            }
+            return v;
+        };
+        bdc_status rc = tune_thin(H, F->vr, gen, H2, max_split, 16, "V = Pw BR", &F->S2);
         if (rc != BDC_OK) return rc;
     }
 
@@ -1066,7 +1239,7 @@ bdc_status factored_init(bdc_handle* H) {
                 q.small = F->UL + t.off;
                 q.small_stride = KL;
                 q.small_u16 = 0;
-                q.wide = H->B.rows + bundle_offset(t.m);
+                q.wide = F->Bp + bundle_offset(t.m);
                 q.wide_stride = H->B.stride;
                 q.wide_u16 = 1;
                 q.SMALL = 1 << t.j;
@@ -1074,7 +1247,7 @@ bdc_status factored_init(bdc_handle* H) {
                 q.s1 = H2;
                 q.out_trans = 0;
                 // M_t[yh][x_lo] = sum_yl B_m[x_lo][yl] Lq[yh][yl] -> RB[off + yh][x_lo]
-                d.wide = H->B.rows + bundle_offset(t.m);
+                d.wide = F->Bp + bundle_offset(t.m);
                 d.wide_stride = H->B.stride;
                 d.SMALL = 1 << t.j;
                 d.WIDE = 1 << t.m;
@@ -1158,6 +1331,24 @@ bdc_status factored_init(bdc_handle* H) {
     }
     BDC_CUDA_TRY(set_thin_smem(ny));
     for (int lg = 0; lg < 8; ++lg) {
+        if (F->n_thinq[lg]) {
+            std::vector<GemmDesc> v;
+            for (auto& q : tq[lg]) v.push_back(thin_q_desc(q));
+            const float core = time_ms(H, [&] { launch_thin_q(lg, F->d_thinq[lg], F->n_thinq[lg], ny, H->stream, nullptr); });
+            bdc_status rc = tune_class(H, v, F->mq[lg], F->use_mq[lg], core, "q-side term products", lg);
+            if (rc != BDC_OK) return rc;
+        }
+        if (F->n_thind[lg]) {
+            std::vector<GemmDesc> v;
+            for (auto& d : td[lg]) v.push_back(thin_d_desc(d, F->lnq_full));
+            const float core = time_ms(H, [&] {
+                launch_thin_d(lg, F->d_thind[lg], F->n_thind[lg], F->ctas_thind[lg], ny, F->lnq_full, H->stream, nullptr);
+            });
+            bdc_status rc = tune_class(H, v, F->md[lg], F->use_md[lg], core, "D-side term products", lg);
+            if (rc != BDC_OK) return rc;
+        }
+    }
+    for (int lg = 0; lg < 8; ++lg) {
         BDC_CUDA_TRY(cudaStreamCreateWithFlags(&F->side[lg], cudaStreamNonBlocking));
         BDC_CUDA_TRY(cudaEventCreateWithFlags(&F->ev_join[lg], cudaEventDisableTiming));
     }
@@ -1187,7 +1378,7 @@ bdc_status factored_init(bdc_handle* H) {
         ep.part = F->epart;
         for (int c : cfgs) {
             Launch T;
-            BDC_CUDA_TRY(make_launch(T, {d}, c));
+            BDC_CUDA_TRY(make_tile_launch(T, d, c, F->colmax));
             const float ms = time_ms(H, [&] { launch_ba(T, ep, H->stream, H->d_st); });
             free_launch(T);
             if (ms < best) {
@@ -1195,13 +1386,19 @@ bdc_status factored_init(bdc_handle* H) {
                 best_cfg = c;
             }
         }
-        BDC_CUDA_TRY(make_launch(F->g, {d}, best_cfg));
+        BDC_CUDA_TRY(make_tile_launch(F->g, d, best_cfg, F->colmax));
         F->ctas_g = F->g.tiles;
         if (H->verbose)
-            printf("bdc: tuned G: tile %dx%d, %.1f us\n", kCfgBM[best_cfg], kCfgBN[best_cfg], best * 1e3f);
+            printf("bdc: tuned G: tile %dx%d, %d of %d tiles hold representatives, %.1f us\n", kCfgBM[best_cfg],
+                   kCfgBN[best_cfg], F->g.tiles,
+                   ((H1 + kCfgBM[best_cfg] - 1) / kCfgBM[best_cfg]) * ((H2 + kCfgBN[best_cfg] - 1) / kCfgBN[best_cfg]),
+                   best * 1e3f);
         BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
         BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
         BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
+        // split slices that the chosen launches never write must read zero
+        BDC_CUDA_TRY(cudaMemsetAsync(F->ulpart, 0, sizeof(double) * max_split * H2 * KLa, H->stream));
+        BDC_CUDA_TRY(cudaMemsetAsync(F->vrpart, 0, sizeof(double) * max_split * H1 * KRa, H->stream));
     }
     int nthin = 0;
     for (int lg = 0; lg < 8; ++lg) nthin += (F->n_thinq[lg] > 0) + (F->n_thind[lg] > 0);
@@ -1216,6 +1413,7 @@ void factored_free(bdc_handle* H) {
     for (double* p : {F->Pw, F->Lt, F->hx, F->LA, F->RB, F->UL, F->VR, F->ulpart, F->vrpart, F->qparts,
                       F->qsum, F->lnq_full, F->epart})
         cudaFree(p);
+    cudaFree(F->Bp);
     for (int lg = 0; lg < 8; ++lg) {
         cudaFree(F->d_thinq[lg]);
         cudaFree(F->d_thind[lg]);
@@ -1229,6 +1427,10 @@ void factored_free(bdc_handle* H) {
     cudaFree(F->snap1);
     cudaFree(F->snap2);
     for (Launch* L : {&F->ul, &F->vr, &F->g}) free_launch(*L);
+    for (int lg = 0; lg < 8; ++lg) {
+        free_launch(F->mq[lg]);
+        free_launch(F->md[lg]);
+    }
     cudaFree(F->d_fold);
     delete F;
     H->fac = nullptr;
@@ -1271,8 +1473,9 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             for (int lg = 0; lg < 8; ++lg) {
                 if (!F->n_thinq[lg]) continue;
                 if ((e = cudaStreamWaitEvent(F->side[lg], F->ev_fork, 0)) != cudaSuccess) return e;
-                if ((e = launch_thin_q(lg, F->d_thinq[lg], F->n_thinq[lg], 1 << H->k, F->side[lg], H->d_st)) != cudaSuccess)
-                    return e;
+                e = F->use_mq[lg] ? launch_store(F->mq[lg], F->side[lg], H->d_st)
+                                  : launch_thin_q(lg, F->d_thinq[lg], F->n_thinq[lg], 1 << H->k, F->side[lg], H->d_st);
+                if (e != cudaSuccess) return e;
                 if ((e = cudaEventRecord(F->ev_join[lg], F->side[lg])) != cudaSuccess) return e;
                 if ((e = cudaStreamWaitEvent(s, F->ev_join[lg], 0)) != cudaSuccess) return e;
             }
@@ -1291,9 +1494,10 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             for (int lg = 0; lg < 8; ++lg) {
                 if (!F->n_thind[lg]) continue;
                 if ((e = cudaStreamWaitEvent(F->side[lg], F->ev_fork, 0)) != cudaSuccess) return e;
-                if ((e = launch_thin_d(lg, F->d_thind[lg], F->n_thind[lg], F->ctas_thind[lg], 1 << H->k, F->lnq_full,
-                                       F->side[lg], H->d_st)) != cudaSuccess)
-                    return e;
+                e = F->use_md[lg] ? launch_store(F->md[lg], F->side[lg], H->d_st)
+                                  : launch_thin_d(lg, F->d_thind[lg], F->n_thind[lg], F->ctas_thind[lg], 1 << H->k,
+                                                  F->lnq_full, F->side[lg], H->d_st);
+                if (e != cudaSuccess) return e;
                 if ((e = cudaEventRecord(F->ev_join[lg], F->side[lg])) != cudaSuccess) return e;
                 if ((e = cudaStreamWaitEvent(s, F->ev_join[lg], 0)) != cudaSuccess) return e;
             }
@@ -1315,6 +1519,8 @@ static cudaError_t enqueue_iteration(bdc_handle* H, double a) {
     return cudaSuccess;
 }
 
+cudaError_t factored_enqueue_iteration(bdc_handle* H, double a) { return enqueue_iteration(H, a); }
+
 bdc_status factored_load_p(bdc_handle* H) {
     FactoredState* F = H->fac;
     const int64_t NX = (int64_t)1 << (H->n - 1);  // representatives have x < 2^{n-1}
@@ -1331,6 +1537,12 @@ bdc_status factored_store_p(bdc_handle* H, double* p_out) {
     k_fac_store<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Pw, p_out, H->d_st);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
+}
+
+static bdc_status rescale(bdc_handle* H, double a);
+bdc_status factored_recover(bdc_handle* H, double a) {
+    if (H->h_st->error != kErrShift) return fail(BDC_ERR_NUMERIC, "factored engine: device error %d", H->h_st->error);
+    return rescale(H, a);
 }
 
 static bdc_status rescale(bdc_handle* H, double a) {
@@ -1430,14 +1642,14 @@ constexpr double kSqAlphaMin = -64.0;
 
 __device__ __forceinline__ bool sq_gated(const DevState* st) { return st->error != 0; }
 
-__global__ void __launch_bounds__(256) k_sq_save(const uint32_t* __restrict__ reps, int64_t R,
+__global__ void __launch_bounds__(256) k_sq_save(const uint32_t* __restrict__ reps, int64_t R, int n,
                                                  const double* __restrict__ Lt, double* __restrict__ dst,
                                                  const DevState* st) {
     if (sq_gated(st)) return;
     const double lnz = st->log_z;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i];
-        dst[x] = Lt[x] - lnz;
+        const uint32_t xd = fac_pos(reps[i], n >> 1);
+        dst[xd] = Lt[xd] - lnz;
     }
 }
 
@@ -1480,9 +1692,9 @@ __global__ void __launch_bounds__(256) k_sq_norms(const uint32_t* __restrict__ r
     const double lnz = st->log_z;
     double rr = 0.0, vv = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i];
+        const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
         const double o = (double)orbit_size(x, n);
-        const double s0 = S0[x], s1 = S1[x], s2 = Lt[x] - lnz;
+        const double s0 = S0[xd], s1 = S1[xd], s2 = Lt[xd] - lnz;
         const double r = s1 - s0, v = s2 - 2.0 * s1 + s0;
         rr = fma(o * r, r, rr);
         vv = fma(o * v, v, vv);
@@ -1509,7 +1721,7 @@ __global__ void k_sq_alpha(const double* __restrict__ part, int nb, DevState* st
 }
 
 // S2 = current ln p; Lt = S0 - 2 a (S1 - S0) + a^2 (S2 - 2 S1 + S0); block max
-__global__ void __launch_bounds__(256) k_sq_extrap(const uint32_t* __restrict__ reps, int64_t R,
+__global__ void __launch_bounds__(256) k_sq_extrap(const uint32_t* __restrict__ reps, int64_t R, int n,
                                                    const double* __restrict__ S0, const double* __restrict__ S1,
                                                    double* __restrict__ S2, double* __restrict__ Lt,
                                                    double* __restrict__ part, const DevState* st) {
@@ -1517,11 +1729,11 @@ __global__ void __launch_bounds__(256) k_sq_extrap(const uint32_t* __restrict__ 
     const double a = st->sq_alpha, lnz = st->log_z;
     double mx = -DBL_MAX;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i];
-        const double s0 = S0[x], s1 = S1[x], s2 = Lt[x] - lnz;
-        S2[x] = s2;
+        const uint32_t xd = fac_pos(reps[i], n >> 1);
+        const double s0 = S0[xd], s1 = S1[xd], s2 = Lt[xd] - lnz;
+        S2[xd] = s2;
         const double t = s0 - 2.0 * a * (s1 - s0) + a * a * (s2 - 2.0 * s1 + s0);
-        Lt[x] = t;
+        Lt[xd] = t;
         mx = fmax(mx, t);
     }
     mx = block_max256(mx);
@@ -1546,12 +1758,12 @@ __global__ void __launch_bounds__(256) k_sq_pw(const uint32_t* __restrict__ reps
     const double m = from_s2 ? 0.0 : st->sq_max;
     double sum = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i];
-        const double l = (from_s2 ? S2[x] : Lt[x]) - m;
+        const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
+        const double l = (from_s2 ? S2[xd] : Lt[xd]) - m;
         const double o = (double)orbit_size(x, n);
         const double e = exp(l);
-        Lt[x] = l;
-        Pw[x] = o * e;
+        Lt[xd] = l;
+        Pw[xd] = o * e;
         sum = fma(o, e, sum);
     }
     sum = block_sum256(sum);
@@ -1581,14 +1793,14 @@ static cudaError_t enqueue_cycle(bdc_handle* H) {
     const int nb = H->nb_upd;
     const int64_t R = H->R;
     cudaError_t e;
-    k_sq_save<<<nb, 256, 0, s>>>(H->d_reps, R, F->Lt, F->snap0, H->d_st);
+    k_sq_save<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->Lt, F->snap0, H->d_st);
     if ((e = enqueue_iteration(H, -INFINITY)) != cudaSuccess) return e;
-    k_sq_save<<<nb, 256, 0, s>>>(H->d_reps, R, F->Lt, F->snap1, H->d_st);
+    k_sq_save<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->Lt, F->snap1, H->d_st);
     if ((e = enqueue_iteration(H, -INFINITY)) != cudaSuccess) return e;
     k_sq_mark<<<1, 1, 0, s>>>(H->d_st);
     k_sq_norms<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap0, F->snap1, F->Lt, F->epart, H->d_st);
     k_sq_alpha<<<1, 32, 0, s>>>(F->epart, nb, H->d_st);
-    k_sq_extrap<<<nb, 256, 0, s>>>(H->d_reps, R, F->snap0, F->snap1, F->snap2, F->Lt, F->epart, H->d_st);
+    k_sq_extrap<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap0, F->snap1, F->snap2, F->Lt, F->epart, H->d_st);
     k_sq_max<<<1, 32, 0, s>>>(F->epart, nb, H->d_st);
     k_sq_pw<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap2, F->Lt, F->Pw, F->epart, 0, H->d_st);
     k_sq_setz<<<1, 32, 0, s>>>(F->epart, nb, 0, H->d_st);

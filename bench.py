@@ -97,6 +97,22 @@ class ClockSampler:
                 if any(r[3].replace(".", "").isdigit() for r in rows) else None}
 
 
+def profile_traffic(kernel: str, n: int, k: int):
+    """DRAM bytes per launch of `kernel` at (n, k) from the committed ncu
+    summaries (profiles/*.md lines "traffic <kernel> <n> <k> <bytes>"), or None."""
+    d = os.path.join(REPO, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for f in sorted(os.listdir(d)):
+        if not f.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(d, f)):
+            w = line.strip().strip("`").split()
+            if len(w) == 5 and w[0] == "traffic" and w[1] == kernel and w[2] == str(n) and w[3] == str(k):
+                return float(w[4])
+    return None
+
+
 # --------------------------------------------------------------- CPU legs
 def cpu_ba_iteration_rate(n: int, k: int, sample: int, threads: int | None = None) -> dict:
     """The CPU oracle's q pass + D pass on `sample` evenly spaced
@@ -195,7 +211,9 @@ def ours_arm(args) -> None:
     pairs, S = E.work()
 
     # warm-up, then K iterations timed with events on the stream the engine uses
-    E.iterate(args.warmup, float("-inf"))
+    # warm-up (at least 16 iterations, so that the captured iteration graph
+    # exists before timing)
+    E.iterate(max(args.warmup, 16), float("-inf"))
     prof = E.profile(2)
     launches_per_iter = prof["launches"]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -247,14 +265,19 @@ def ours_arm(args) -> None:
                                        f"{prof['work_main']:.4e} multiply-adds",
                     "peak_source": "bdc_peak_probe int32 IMAD chain, measured in this run"}
     else:
+        # the G stage: one k_mma_ba launch (FP64 mma.sync tiles, the BA update
+        # fused in the epilogue); ms_main is its CUDA-event time per iteration
         achieved = prof["work_main"] / (prof["ms_main"] / 1e3)
-        roofline = {"bound": "fp64 FMA pipe (CUDA cores; sm_100 tensor cores have no FP64)",
-                    "kernel": "k_gemm_tile<128,128,8,4,2,1> (G = LA*RB fused with the BA update)",
-                    "achieved": achieved / 1e12, "peak": 2 * dfma / 1e12, "unit": "TFLOP/s",
-                    "frac": achieved / (2 * dfma), "traffic": None,
-                    "work_per_launch": f"2*H1*H2*K = {prof['work_main']:.4e} flops "
-                                       f"(H1=H2={1 << ((args.n + 1) // 2)}, K = sum of the term widths)",
-                    "peak_source": "bdc_peak_probe FP64 FMA chain, measured in this run (2 flops per FMA)"}
+        dmma = bdc_b200.peak_probe("dmma", local)
+        roofline = {"bound": "tensor",
+                    "kernel": "k_mma_ba (G = [A_L | N_R] [M_L ; B_R^T] on FP64 mma.sync, BA update in the epilogue)",
+                    "achieved": achieved / 1e12, "peak": 2 * dmma / 1e12, "unit": "TFLOP/s",
+                    "frac": achieved / (2 * dmma), "traffic": profile_traffic("k_mma_ba", args.n, args.k),
+                    "work_per_launch": f"2*H1h*H2*K = {prof['work_main']:.4e} flops "
+                                       f"(H1h = {1 << ((args.n + 1) // 2 - 1)}, H2 = {1 << (args.n // 2)}, "
+                                       f"K = sum of the split-term widths)",
+                    "peak_source": "bdc_peak_probe FP64 mma.sync m8n8k4 chains on all SMs, measured in this "
+                                   "run (2 flops per multiply-add); MEASURED_PEAKS.json holds no FP64 figure"}
     upd_bytes = R * 72
     roofline_update = None if E.engine != "count" else {"bound": "hbm", "achieved": upd_bytes / (prof["ms_update"] / 1e3) / 1e9,
                        "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
@@ -279,7 +302,8 @@ def ours_arm(args) -> None:
         "gpu_launches": launches_per_iter * args.steps,
         "profile_ms": {k2: prof[k2] for k2 in ("ms_q", "ms_fold", "ms_d", "ms_update", "ms_iter", "ms_main")},
         "roofline": roofline, "roofline_update": roofline_update,
-        "peaks_measured": {"int32_madd_tops": imad / 1e12, "fp64_fma_tflops": 2 * dfma / 1e12},
+        "peaks_measured": {"int32_madd_tops": imad / 1e12, "fp64_fma_tflops": 2 * dfma / 1e12,
+                           "hbm_gbs": peaks.get("hbm_gbs"), "hbm_source": peak_src},
         "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
         "bound_bits": st["upper_bound"], "rate_bits": st["rate"],
     }
@@ -288,6 +312,142 @@ def ours_arm(args) -> None:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def time_to_bound(args) -> dict:
+    """Time-to-bound at (n, k) from the uniform start.  The converged bound C*
+    comes from the accelerated loop run to a certified gap best_ub - best_rate
+    < 1e-12 bits (C lies in that bracket, so C* is the plain BA's limit to
+    within 1e-12); then plain BA and the accelerated loop each run from the
+    uniform start, in chunks timed with CUDA events, until their best upper
+    bound is within 1e-9 bits of C*."""
+    import torch
+
+    import bdc_b200
+
+    tol = 1e-9
+    E = bdc_b200.Engine(args.n, args.k, engine="factored")
+    stream = torch.cuda.current_stream()
+    E.set_stream(stream.cuda_stream)
+    E.set_uniform()
+    E.accelerate(48, 0.0)  # warm-up: builds the iteration and cycle graphs
+    E.set_uniform()
+    E.iterate(16, float("-inf"))
+    E.set_uniform()
+    ref = E.accelerate(args.ttb_max, 1e-12)
+    C = ref["best_upper_bound"]
+    out = {"C_star_bits": C, "C_star_gap_bits": ref["best_upper_bound"] - ref["best_rate"],
+           "C_star_evals": ref["iters"], "tolerance_bits": tol}
+    for name in ("plain", "accelerated"):
+        E.set_uniform()
+        evals, ms = 0, 0.0
+        chunk = 64
+        reached = False
+        st = None
+        while evals < args.ttb_max:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = E.iterate(chunk, float("-inf")) if name == "plain" else E.accelerate(chunk, 0.0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            evals += st["iters"]
+            if st["best_upper_bound"] - C < tol:
+                reached = True
+                break
+            chunk = min(chunk * 2, 2048)
+        out[name] = {"reached": reached, "evals": evals, "seconds": ms / 1e3,
+                     "bound_bits": st["best_upper_bound"], "gap_to_C_star_bits": st["best_upper_bound"] - C}
+    if out["plain"]["reached"] and out["accelerated"]["reached"]:
+        out["speedup"] = out["plain"]["seconds"] / out["accelerated"]["seconds"]
+    E.close()
+    return out
+
+
+BATCH_MIX = [(16, 8), (18, 6), (20, 10), (22, 11), (24, 8), (24, 12)]
+
+
+def batched(args) -> dict | None:
+    """The batched form: the six (n,k) instances of BATCH_MIX x 8 seeds of a
+    Dirichlet(0.5) start (48 BA instances), iterated together from one
+    captured CUDA graph, against the same engines iterated one after the
+    other.  Both legs run the same number of BA iterations per instance with
+    no stopping threshold; the figure is instance-iterations per second.
+    Under torchrun the instances are spread over the ranks (replicas, no
+    data-path collective) and the time is the max over ranks."""
+    import torch
+
+    import bdc_b200
+    from bdc_b200 import dist as bdist
+    from bdc_b200 import replicas
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    tdist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+    seeds = range(8)
+    mix = [(n, k, s) for n, k in BATCH_MIX for s in seeds]
+    mine = replicas.partition([(n, k) for n, k, _ in mix], world)[rank]
+    engines = []
+    for i in mine:
+        n, k, s = mix[i]
+        E = bdc_b200.Engine(n, k, engine="factored", device=local)
+        E.set_p(bdist.dirichlet_start(n, 0.5, s))
+        engines.append(E)
+    stream = torch.cuda.current_stream()
+    iters = max(args.steps, 8)
+    B = bdc_b200.Batch(engines)
+    B.set_stream(stream.cuda_stream)
+    B.iterate(16, float("-inf"))  # warm-up: captures the batch graph
+    for E in engines:
+        E.set_stream(stream.cuda_stream)
+        E.iterate(16, float("-inf"))  # warm-up: each engine's own graph
+    torch.cuda.synchronize()
+
+    def max_over_ranks(v: float) -> float:
+        if tdist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn) -> float:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if tdist is not None:
+            tdist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3)
+
+    t_batch = timed(lambda: B.iterate(iters, float("-inf")))
+    t_seq = timed(lambda: [E.iterate(iters, float("-inf")) for E in engines])
+    per_nk = {}
+    if world == 1:
+        for i, (n, k) in enumerate(BATCH_MIX):
+            E = engines[i * len(seeds)]
+            per_nk[f"{n}_{k}"] = iters / timed(lambda: E.iterate(iters, float("-inf")))
+    total = len(mix) * iters
+    out = {"instances": len(mix), "n_gpus": world, "iters_per_instance": iters,
+           "batched_instance_iters_per_s": total / t_batch,
+           "sequential_instance_iters_per_s": total / t_seq,
+           "batch_speedup": t_seq / t_batch,
+           "single_engine_iters_per_s": per_nk}
+    B.close()
+    for E in engines:
+        E.close()
+    if tdist is not None:
+        tdist.destroy_process_group()
+    return out if rank == 0 else None
 
 
 def kernels_only(args) -> None:
@@ -313,12 +473,19 @@ def main() -> None:
     ap.add_argument("--engine", default="auto")
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", choices=["bench", "kernels"], default="bench")
+    ap.add_argument("--mode", choices=["bench", "kernels", "ttb", "batch"], default="bench")
+    ap.add_argument("--ttb-max", type=int, default=400000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.mode == "kernels":
         kernels_only(args)
+    elif args.mode == "ttb":
+        print(json.dumps({"time_to_bound": time_to_bound(args), "n": args.n, "k": args.k}), flush=True)
+    elif args.mode == "batch":
+        res = batched(args)
+        if res is not None:
+            print(json.dumps({"batched": res}), flush=True)
     elif args.impl == "reference":
         reference_arm(args)
     else:

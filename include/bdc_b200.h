@@ -123,6 +123,21 @@ bdc_status bdc_accelerate(bdc_handle_t h, int64_t max_evals, double gap_bits, bd
 bdc_status bdc_mi_forward(bdc_handle_t h, const double* p, int64_t num_reps, double* I_nats);
 bdc_status bdc_mi_backward(bdc_handle_t h, double* grad, int64_t num_reps);
 
+/* Batches (no counterpart in the reference, which runs one (n,k) per
+ * process): many handles -- different (n,k) and starting distributions --
+ * iterated together from one captured CUDA graph with one branch per handle.
+ * bdc_batch_iterate runs the BA loop of every handle until each one's mx < a
+ * (it then idles) or max_iters; stats (may be NULL) receives one entry per
+ * handle, in the order given.  The handles stay owned by the caller and must
+ * outlive the batch; they must all be on one device. */
+typedef struct bdc_batch* bdc_batch_t;
+bdc_status bdc_batch_create(bdc_handle_t* handles, int count, bdc_batch_t* out);
+bdc_status bdc_batch_iterate(bdc_batch_t batch, int64_t max_iters, double a, bdc_stats* stats);
+bdc_status bdc_batch_destroy(bdc_batch_t batch);
+/* Queue the batch's work on a caller's cudaStream_t (NULL: the batch's own
+ * stream); bdc_batch_iterate still returns only when that work is done. */
+bdc_status bdc_batch_set_stream(bdc_batch_t batch, void* stream);
+
 /* One reference-shaped iteration with host vectors: p_in -> p_out, like
  * baa_iteration (BAA.cu:590-639, decl. BAA.cuh:295); p_out may equal p_in. */
 bdc_status bdc_baa_iteration(bdc_handle_t h, const double* p_in, double* p_out, int64_t num_reps);
