@@ -41,7 +41,7 @@ EXPORTED_SYMBOLS = [
     "bdc_generate_cache", "bdc_read_cache_file", "bdc_write_cache_file", "bdc_read_dist_file",
     "bdc_write_dist_file", "bdc_work", "bdc_profile", "bdc_set_stream", "bdc_peak_probe",
     "bdc_max_deviation_noalloc", "bdc_accelerate", "bdc_mi_forward", "bdc_mi_backward",
-    "bdc_batch_create", "bdc_batch_iterate", "bdc_batch_destroy", "bdc_batch_set_stream",
+    "bdc_batch_create", "bdc_batch_iterate", "bdc_batch_destroy", "bdc_batch_set_stream", "bdc_solve",
 ]
 
 
@@ -108,6 +108,7 @@ def library() -> ctypes.CDLL:
     L.bdc_iterate.argtypes = [h, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats)]
     L.bdc_baa_iteration.argtypes = [h, _f64p, _f64p, ctypes.c_int64]
     L.bdc_accelerate.argtypes = [h, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats)]
+    L.bdc_solve.argtypes = [h, ctypes.c_double, ctypes.c_int64, ctypes.POINTER(Stats)]
     L.bdc_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
     L.bdc_batch_iterate.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats)]
     L.bdc_batch_destroy.argtypes = [ctypes.c_void_p]
@@ -256,6 +257,14 @@ class Engine:
         st = Stats()
         _check(library().bdc_accelerate(self._h, int(max_evals), float(gap_bits), ctypes.byref(st)),
                "bdc_accelerate")
+        return st.as_dict()
+
+    def solve(self, gap_bits: float = 1e-9, max_evals: int = 100000) -> dict:
+        """Certified bracket best_rate <= C <= best_upper_bound (bits) by
+        accelerated BA, a restricted solve on the inputs that carry mass and a
+        full-space check; the iterate becomes the final point."""
+        st = Stats()
+        _check(library().bdc_solve(self._h, float(gap_bits), int(max_evals), ctypes.byref(st)), "bdc_solve")
         return st.as_dict()
 
     def mi_forward(self, p=None) -> float:

@@ -262,12 +262,12 @@ static bdc_status reset_state(bdc_handle* H) {
     return BDC_OK;
 }
 
-bdc_status engine_after_set_p(bdc_handle* H) {
+bdc_status engine_after_set_p(bdc_handle* H, int strict_zero) {
     bdc_status rc = reset_state(H);
     if (rc != BDC_OK) return rc;
     H->p_set = true;
     if (H->engine == BDC_ENGINE_FACTORED) {
-        rc = factored_load_p(H);
+        rc = factored_load_p(H, strict_zero);
         if (rc != BDC_OK) return rc;
     }
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));

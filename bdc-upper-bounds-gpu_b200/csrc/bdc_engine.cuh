@@ -57,7 +57,7 @@ bdc_status fail(bdc_status st, const char* fmt, ...) __attribute__((format(print
 int select_engine(int requested, int n, int k);
 bdc_status engine_init(bdc_handle* H);
 void engine_free(bdc_handle* H);
-bdc_status engine_after_set_p(bdc_handle* H);
+bdc_status engine_after_set_p(bdc_handle* H, int strict_zero = 0);
 bdc_status engine_current_p(bdc_handle* H, const double** p);
 bdc_status engine_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats);
 bdc_status engine_log_q(bdc_handle* H);       // ln q of the current p into H->d_lnq
@@ -73,7 +73,9 @@ int count_group_size(int k);
 bool factored_supports(int n, int k);
 bdc_status factored_init(bdc_handle* H);
 void factored_free(bdc_handle* H);
-bdc_status factored_load_p(bdc_handle* H);                 // d_p[0] -> dense state
+// d_p[0] -> dense state; strict_zero: a zero entry stays zero (ln p = -inf)
+// instead of the reference's ln 0 = 0
+bdc_status factored_load_p(bdc_handle* H, int strict_zero = 0);
 bdc_status factored_store_p(bdc_handle* H, double* p_out);  // dense state -> p per rep
 bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats);
 bdc_status factored_profile(bdc_handle* H, int iters, bdc_profile_t* out);
@@ -82,5 +84,8 @@ cudaError_t factored_enqueue_iteration(bdc_handle* H, double a);
 // finishes an iteration that stopped on an exp-shift overflow (on H->stream);
 // any other device error is returned as BDC_ERR_NUMERIC
 bdc_status factored_recover(bdc_handle* H, double a);
+bdc_status factored_map(bdc_handle* H, const double* p_in, double* p_out, double* D_out);
+cudaError_t dgemm_nt(const double* A, int lda, const double* B, int ldb, double* C, int ldc, int M, int N, int K,
+                     double alpha, int accumulate, cudaStream_t s);
 
 }  // namespace bdc

@@ -111,6 +111,8 @@ struct FactoredState {
     double* Lt = nullptr;     // [2^{n-1}]  ln e(x) (p = e / Z)
     double* hx = nullptr;     // [2^{n-1}]  h(x) at representatives
     uint16_t* Bp = nullptr;   // low-half tables, row c = table row rev(c) (dense column order)
+    double* Ddense = nullptr; // [2^{n-1}] D(x) of a map with D output (allocated on first use)
+    double* dout = nullptr;   // where the G epilogue writes D (nullptr: nowhere)
     std::vector<int> colmax;  // per dense column: largest x_hi of a representative, -1 if none
     double* LA = nullptr;     // [H1h][Kp]  = [AL | NR]
     double* RB = nullptr;     // [Kp][H2]  = [ML ; BR^T]
@@ -233,6 +235,7 @@ __global__ void __launch_bounds__(256) k_mma_ba(const GemmDesc* __restrict__ des
                 if (!is_rep(x, ep.n)) continue;
                 const double o = (double)orbit_size(x, ep.n);
                 const double D = __ldg(ep.hx + xd) - acc[i][j][h] * ep.inv_c;
+                if (ep.Dout) ep.Dout[xd] = D;
                 // an entry that is exactly 0 in the caller's distribution (Lt
                 // holds NaN) takes ln p = 0, as the reference's apply_log_kernel
                 // leaves ln 0 at 0 (backend/BAA.cu:573-580); later iterates keep
@@ -742,13 +745,19 @@ __global__ void k_fac_rescale_finish(const double* part, int nb, double a, DevSt
 // p -> (Pw, Lt) at representatives; block max of ln p for the first shift
 __global__ void __launch_bounds__(256)
 k_fac_load(const uint32_t* __restrict__ reps, int64_t R, int n, const double* __restrict__ p,
-           double* Pw, double* Lt, double* part, DevState* st) {
+           double* Pw, double* Lt, double* part, int strict_zero, DevState* st) {
     double mx = -DBL_MAX;
     int zero = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
         const double v = p[i];
         Pw[xd] = (double)orbit_size(x, n) * v;
+        if (strict_zero) {
+            // p = 0 stays 0 (ln p = -inf): the map of the BA update itself
+            Lt[xd] = (v > 0.0) ? log(v) : -INFINITY;
+            if (v > 0.0) mx = fmax(mx, log(v));
+            continue;
+        }
         // ln 0 = 0 (backend/BAA.cu:573-580): marked with NaN for the epilogue
         const double l = (v != 0.0) ? log(v) : 0.0;
         Lt[xd] = (v != 0.0) ? l : __longlong_as_double(0x7ff8000000000000ll);
@@ -1052,6 +1061,29 @@ static bdc_status tune_class(bdc_handle* H, const std::vector<GemmDesc>& descs, 
                        : "CUDA cores",
                best * 1e3f, core_ms * 1e3f);
     return BDC_OK;
+}
+
+// C (M x N, row stride ldc) = alpha A B^T (+ C when accumulate) for row-major
+// A (M x K, stride lda) and B (N x K, stride ldb) on the FP64 tensor-core
+// path; a helper for small dense work outside the iteration (the certified
+// solver's Newton systems)
+cudaError_t dgemm_nt(const double* A, int lda, const double* B, int ldb, double* C, int ldc, int M, int N, int K,
+                     double alpha, int accumulate, cudaStream_t s) {
+    static bool attrs = false;
+    if (!attrs) {
+        cudaError_t e = set_smem_attrs();
+        if (e != cudaSuccess) return e;
+        attrs = true;
+    }
+    GemmDesc d = make_desc(op_f64(A, lda, 0), op_f64(B, ldb, 1), C, ldc, 1, M, N, K);
+    d.alpha = alpha;
+    d.accumulate = accumulate;
+    Launch L;
+    cudaError_t e = make_launch(L, {d}, CFG_64x64);
+    if (e == cudaSuccess) e = launch_store(L, s, nullptr);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    free_launch(L);
+    return e;
 }
 
 bool factored_supports(int n, int k) {
@@ -1414,6 +1446,7 @@ void factored_free(bdc_handle* H) {
                       F->qsum, F->lnq_full, F->epart})
         cudaFree(p);
     cudaFree(F->Bp);
+    cudaFree(F->Ddense);
     for (int lg = 0; lg < 8; ++lg) {
         cudaFree(F->d_thinq[lg]);
         cudaFree(F->d_thind[lg]);
@@ -1447,6 +1480,7 @@ static BaEpilogue make_epilogue(bdc_handle* H) {
     ep.inv_c = H->inv_c;
     ep.part = F->epart;
     ep.st = H->d_st;
+    ep.Dout = F->dout;
     return ep;
 }
 
@@ -1521,12 +1555,13 @@ static cudaError_t enqueue_iteration(bdc_handle* H, double a) {
 
 cudaError_t factored_enqueue_iteration(bdc_handle* H, double a) { return enqueue_iteration(H, a); }
 
-bdc_status factored_load_p(bdc_handle* H) {
+bdc_status factored_load_p(bdc_handle* H, int strict_zero) {
     FactoredState* F = H->fac;
     const int64_t NX = (int64_t)1 << (H->n - 1);  // representatives have x < 2^{n-1}
     BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
     const int nb = H->nb_upd;
-    k_fac_load<<<nb, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, H->d_p[0], F->Pw, F->Lt, F->epart, H->d_st);
+    k_fac_load<<<nb, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, H->d_p[0], F->Pw, F->Lt, F->epart, strict_zero,
+                                          H->d_st);
     k_fac_load_finish<<<1, 32, 0, H->stream>>>(F->epart, nb, H->k, H->d_st);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
@@ -1539,7 +1574,52 @@ bdc_status factored_store_p(bdc_handle* H, double* p_out) {
     return BDC_OK;
 }
 
+__global__ void k_gather_dense(const uint32_t* __restrict__ reps, int64_t R, int n, const double* __restrict__ dense,
+                               double* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = dense[fac_pos(reps[i], n >> 1)];
+}
+
 static bdc_status rescale(bdc_handle* H, double a);
+
+// One BA map on device vectors: p_in (per representative, sum |O| p = 1; a
+// zero entry stays zero) -> p_out.  The bound max_x D(x) and the rate I(p;W)
+// of p_in (nats) are left in H->h_st->max_d / rate; with D_out set, D(x) of
+// p_in per representative.  Leaves the handle's iterate at p_out.
+bdc_status factored_map(bdc_handle* H, const double* p_in, double* p_out, double* D_out) {
+    FactoredState* F = H->fac;
+    const int64_t NX = (int64_t)1 << (H->n - 1);
+    if (D_out && !F->Ddense) {
+        BDC_CUDA_TRY(cudaMalloc(&F->Ddense, sizeof(double) * NX));
+        H->bytes += sizeof(double) * NX;
+    }
+    BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), H->stream));
+    BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
+    const int nb = H->nb_upd;
+    k_fac_load<<<nb, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, p_in, F->Pw, F->Lt, F->epart, 1, H->d_st);
+    k_fac_load_finish<<<1, 32, 0, H->stream>>>(F->epart, nb, H->k, H->d_st);
+    BDC_CUDA_TRY(cudaGetLastError());
+    F->dout = D_out ? F->Ddense : nullptr;
+    cudaError_t e = enqueue_iteration(H, -INFINITY);
+    F->dout = nullptr;
+    BDC_CUDA_TRY(e);
+    BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    if (H->h_st->error) {
+        bdc_status rc = factored_recover(H, -INFINITY);
+        if (rc != BDC_OK) return rc;
+    }
+    if (D_out) {
+        k_gather_dense<<<H->num_sms * 8, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Ddense, D_out);
+        BDC_CUDA_TRY(cudaGetLastError());
+    }
+    k_fac_store<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Pw, p_out, H->d_st);
+    BDC_CUDA_TRY(cudaGetLastError());
+    BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    return BDC_OK;
+}
+
 bdc_status factored_recover(bdc_handle* H, double a) {
     if (H->h_st->error != kErrShift) return fail(BDC_ERR_NUMERIC, "factored engine: device error %d", H->h_st->error);
     return rescale(H, a);

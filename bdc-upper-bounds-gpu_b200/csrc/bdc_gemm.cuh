@@ -50,6 +50,7 @@ struct BaEpilogue {
     double inv_c;
     double* part;                // per-CTA partials [ctas][4]
     const DevState* st;
+    double* Dout;                // optional: D(x) at every representative (dense layout)
 };
 
 }  // namespace bdc

@@ -1,0 +1,1087 @@
+// bdc_solve.cu -- a certified solver for C_{n,k} on the factored engine.
+//
+// For every input distribution p the Blahut-Arimoto bracket
+//     I(p;W) <= C <= max_x D(W(.|x) || q_p)
+// holds (the right side is the bound the reference prints as its stopping
+// statistic, backend/BAA.cu:413-425 and 820-913), so a solver may move p by
+// any rule as long as each reported number is evaluated exactly at the point
+// it belongs to.  No counterpart in the reference, which runs plain BA until
+// max_x log2 p'/p < a (backend/main_BAA.cu:73).  Three phases:
+//
+//  1. Anderson-accelerated BA on the whole input space: the last m
+//     differences of the BA map F are mixed in p (orbit-weighted least
+//     squares), negative entries are clipped to 0, and a mixed point is kept
+//     only when the rate at it is at least the rate of the plain step.
+//  2. Support: the inputs with positive mass or with D(x) near the bound form
+//     a set S.  BA restricted to S runs with the same acceleration on rows
+//     N(x, .) of S held in device memory (exact integers in FP32).
+//  3. Certification: one full evaluation at p_S gives D(x) for every x, the
+//     bound and the rate.  Inputs outside S whose D(x) exceeds the rate join
+//     S and phase 2 repeats; otherwise the bracket is final.
+//
+// Slowly vanishing inputs (D(x) just below C) make plain BA converge
+// sublinearly; removing them in phase 2 leaves a problem that converges fast,
+// and phase 3 proves that nothing outside S could carry mass.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "bdc_engine.cuh"
+
+namespace bdc {
+
+constexpr int kAAMax = 10;  // history of the Anderson mixing
+
+// ------------------------------------------------------------ vector kernels
+// out = sum_i w_i u_i v_i over blocks (w = orbit sizes, 2 or 4)
+__device__ __forceinline__ double block_reduce_sum(double v, double* sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += sh[w];
+    return r;  // valid in thread 0
+}
+
+// f = g - x; with have_last: dF = f - f_last, dG = g - g_last into the ring
+// slot; then f_last = f, g_last = g
+__global__ void k_aa_push(int64_t L, const double* __restrict__ x, const double* __restrict__ g,
+                          double* __restrict__ f_last, double* __restrict__ g_last, double* __restrict__ dF,
+                          double* __restrict__ dG, int have_last) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x) {
+        const double gi = g[i], fi = gi - x[i];
+        if (have_last) {
+            dF[i] = fi - f_last[i];
+            dG[i] = gi - g_last[i];
+        }
+        f_last[i] = fi;
+        g_last[i] = gi;
+    }
+}
+
+struct AAPtrs {
+    const double* dF[kAAMax];
+    const double* dG[kAAMax];
+    double gamma[kAAMax];
+    int m;
+};
+
+// partial sums of w dF_a . dF_new and w dF_a . f_last for the m active slots
+__global__ void __launch_bounds__(256) k_aa_dots(int64_t L, const uint8_t* __restrict__ wts, AAPtrs P,
+                                                 const double* __restrict__ dF_new, const double* __restrict__ f,
+                                                 double* __restrict__ part) {
+    __shared__ double sh[8];
+    double a1[kAAMax], a2[kAAMax];
+    for (int a = 0; a < kAAMax; ++a) a1[a] = a2[a] = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x) {
+        const double w = (double)wts[i];
+        const double dn = w * dF_new[i], fn = w * f[i];
+#pragma unroll
+        for (int a = 0; a < kAAMax; ++a)
+            if (a < P.m) {
+                const double d = P.dF[a][i];
+                a1[a] = fma(d, dn, a1[a]);
+                a2[a] = fma(d, fn, a2[a]);
+            }
+    }
+    for (int a = 0; a < P.m; ++a) {
+        const double r1 = block_reduce_sum(a1[a], sh);
+        const double r2 = block_reduce_sum(a2[a], sh);
+        if (threadIdx.x == 0) {
+            part[(size_t)blockIdx.x * 2 * kAAMax + a] = r1;
+            part[(size_t)blockIdx.x * 2 * kAAMax + kAAMax + a] = r2;
+        }
+    }
+}
+
+__global__ void k_aa_dots_finish(const double* __restrict__ part, int nb, int m, double* __restrict__ out) {
+    const int a = threadIdx.x;
+    if (a >= 2 * kAAMax) return;
+    if ((a % kAAMax) >= m) return;
+    double s = 0.0;
+    for (int b = 0; b < nb; ++b) s += part[(size_t)b * 2 * kAAMax + a];
+    out[a] = s;
+}
+
+// x = g_last - sum_a gamma_a dG_a, clipped at 0; partial sums of w x
+__global__ void __launch_bounds__(256) k_aa_mix(int64_t L, const uint8_t* __restrict__ wts, AAPtrs P,
+                                                const double* __restrict__ g_last, double* __restrict__ x,
+                                                double* __restrict__ part) {
+    __shared__ double sh[8];
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x) {
+        double v = g_last[i];
+#pragma unroll
+        for (int a = 0; a < kAAMax; ++a)
+            if (a < P.m) v -= P.gamma[a] * P.dG[a][i];
+        v = v > 0.0 ? v : 0.0;
+        x[i] = v;
+        s = fma((double)wts[i], v, s);
+    }
+    const double r = block_reduce_sum(s, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+// x /= sum of the partials (every block re-adds them: nb is small)
+__global__ void k_scale_by_sum(int64_t L, double* __restrict__ x, const double* __restrict__ part, int nb) {
+    __shared__ double inv;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int b = 0; b < nb; ++b) s += part[b];
+        inv = s > 0.0 ? 1.0 / s : 0.0;
+    }
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] *= inv;
+}
+
+// ------------------------------------------------------------- support set
+// appends i to idx (capacity cap) when it is not yet in S and either carries
+// mass (p > pmin) or has D(x) > dmin; in_s marks members
+__global__ void k_select(int64_t R, const double* __restrict__ p, const double* __restrict__ D, double pmin,
+                         double dmin, uint8_t* __restrict__ in_s, int* __restrict__ count, uint32_t* __restrict__ idx,
+                         int cap) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
+        if (in_s[i]) continue;
+        if ((p && p[i] > pmin) || D[i] > dmin) {
+            const int slot = atomicAdd(count, 1);
+            if (slot < cap) idx[slot] = (uint32_t)i;
+        }
+    }
+}
+
+__global__ void k_max_vec(int64_t L, const double* __restrict__ v, double* __restrict__ part) {
+    __shared__ double sh[8];
+    double m = -DBL_MAX;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, v[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, sh[w]);
+        part[blockIdx.x] = fmax(m, sh[0]);
+    }
+}
+
+// N(x_s, y) for the members of S, as FP32 (exact: N <= C(n,k) < 2^24 for n <= 26)
+__global__ void k_rows(Split sp, HalfTables A, HalfTables B, const uint32_t* __restrict__ reps,
+                       const uint32_t* __restrict__ idx, int S, float* __restrict__ rows) {
+    const int ny = 1 << sp.k;
+    const int64_t tot = (int64_t)S * ny;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int s = (int)(e / ny), y = (int)(e % ny);
+        rows[e] = (float)split_count(sp, A, B, reps[idx[s]], (uint32_t)y);
+    }
+}
+
+__global__ void k_gather_u8(int S, const uint32_t* __restrict__ idx, const uint32_t* __restrict__ reps, int n,
+                            uint8_t* __restrict__ w) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x)
+        w[s] = (uint8_t)orbit_size(reps[idx[s]], n);
+}
+
+__global__ void k_gather_f64(int S, const uint32_t* __restrict__ idx, const double* __restrict__ src,
+                             double* __restrict__ dst) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) dst[s] = src[idx[s]];
+}
+
+__global__ void k_scatter_f64(int S, const uint32_t* __restrict__ idx, const double* __restrict__ src,
+                              double* __restrict__ dst) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) dst[idx[s]] = src[s];
+}
+
+__global__ void k_orbit_weights(int64_t R, const uint32_t* __restrict__ reps, int n, uint8_t* __restrict__ w) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
+        w[i] = (uint8_t)orbit_size(reps[i], n);
+}
+
+// ---------------------------------------------------- the restricted BA map
+// acc_part[c][y] = sum_{s in chunk c} |O_s| p_s N(x_s, y)
+constexpr int kRsChunk = 64;
+
+__global__ void __launch_bounds__(256) k_rs_acc(int S, int ny, const float* __restrict__ rows,
+                                                const uint8_t* __restrict__ w, const double* __restrict__ p,
+                                                double* __restrict__ part) {
+    const int y = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (y >= ny) return;
+    const int s0 = c * kRsChunk, s1 = min(S, s0 + kRsChunk);
+    double a = 0.0;
+    for (int s = s0; s < s1; ++s) a = fma((double)w[s] * p[s], (double)rows[(int64_t)s * ny + y], a);
+    part[(int64_t)c * ny + y] = a;
+}
+
+// ln q(y) over all y: q(y) = (1/(4C)) sum over the group {id, rev, comp,
+// rev comp} of acc(g y), acc = sum of the chunk partials; ln 0 = 0
+__global__ void k_rs_sum(int ny, int nc, const double* __restrict__ part, double* __restrict__ acc) {
+    const int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= ny) return;
+    double a = 0.0;
+    for (int c = 0; c < nc; ++c) a += part[(int64_t)c * ny + y];
+    acc[y] = a;
+}
+
+__global__ void k_rs_lnq(int k, double inv_c, const double* __restrict__ acc, double* __restrict__ lnq) {
+    const int ny = 1 << k;
+    const int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= ny) return;
+    const uint32_t r = reverse_bits((uint32_t)y, k), c = complement_bits((uint32_t)y, k), rc = reverse_bits(c, k);
+    const double q = 0.25 * inv_c * (acc[y] + acc[r] + acc[c] + acc[rc]);
+    lnq[y] = q > 0.0 ? log(q) : 0.0;
+}
+
+// D_s = h_s - (1/C) sum_y N(x_s, y) ln q(y): one warp per member; block
+// partials [max D, sum |O| p D]
+__global__ void __launch_bounds__(256) k_rs_div(int S, int ny, const float* __restrict__ rows,
+                                                const double* __restrict__ lnq, const double* __restrict__ h,
+                                                const uint8_t* __restrict__ w, const double* __restrict__ p,
+                                                double inv_c, double* __restrict__ D, double* __restrict__ part) {
+    __shared__ double smax[8], ssum[8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int s = blockIdx.x * 8 + warp;
+    double d = -DBL_MAX, r = 0.0;
+    if (s < S) {
+        const float* row = rows + (int64_t)s * ny;
+        double a = 0.0;
+        for (int y = lane; y < ny; y += 32) a = fma((double)row[y], lnq[y], a);
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+        d = h[s] - a * inv_c;
+        r = (double)w[s] * p[s] * d;
+        if (lane == 0) D[s] = d;
+    }
+    if (lane == 0) {
+        smax[warp] = d;
+        ssum[warp] = r;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = smax[0], t = ssum[0];
+        for (int i = 1; i < 8; ++i) {
+            m = fmax(m, smax[i]);
+            t += ssum[i];
+        }
+        part[2 * blockIdx.x] = m;
+        part[2 * blockIdx.x + 1] = t;
+    }
+}
+
+// p'_s = p_s e^{D_s - max D} / Z (one block: S is small); out[0] = max D,
+// out[1] = rate of p (nats)
+__global__ void __launch_bounds__(1024) k_rs_update(int S, const double* __restrict__ part, int nb,
+                                                    const double* __restrict__ D, const uint8_t* __restrict__ w,
+                                                    const double* __restrict__ p, double* __restrict__ pn,
+                                                    double* __restrict__ out) {
+    __shared__ double sh[32];
+    __shared__ double mD, Zs;
+    if (threadIdx.x == 0) {
+        double m = -DBL_MAX, r = 0.0;
+        for (int b = 0; b < nb; ++b) {
+            m = fmax(m, part[2 * b]);
+            r += part[2 * b + 1];
+        }
+        mD = m;
+        out[0] = m;
+        out[1] = r;
+    }
+    __syncthreads();
+    double z = 0.0;
+    for (int s = threadIdx.x; s < S; s += blockDim.x) {
+        const double v = p[s] * exp(D[s] - mD);
+        pn[s] = v;
+        z = fma((double)w[s], v, z);
+    }
+    for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xFFFFFFFFu, z, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = z;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += sh[i];
+        Zs = t;
+    }
+    __syncthreads();
+    const double inv = 1.0 / Zs;
+    for (int s = threadIdx.x; s < S; s += blockDim.x) pn[s] *= inv;
+}
+
+// ------------------------------------------------- Newton on the support
+// The support equations D_s(p) = c (s in F), sum_s |O_s| p_s = 1.  With
+// q(y) = (1/4C) sum_g acc(g y) invariant under the group G = {id, rev, comp,
+// rev comp}, dD_s/dp_t = -(|O_t| / C^2) M_st where M = Nbar diag(1/q) Nbar^T
+// and Nbar_s(y) = (1/4) sum_g N(x_s, g y) (symmetric positive semidefinite).
+// Rows of Nbar / sqrt(q) for the members F of S:
+__global__ void k_nt_rows(int nF, int k, const int* __restrict__ F, const float* __restrict__ rows,
+                          const double* __restrict__ acc, double inv_c, double* __restrict__ out) {
+    const int ny = 1 << k;
+    const int64_t tot = (int64_t)nF * ny;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int f = (int)(e / ny);
+        const uint32_t y = (uint32_t)(e % ny);
+        const uint32_t r = reverse_bits(y, k), c = complement_bits(y, k), rc = reverse_bits(c, k);
+        const float* row = rows + (int64_t)F[f] * ny;
+        const double nb = 0.25 * ((double)row[y] + (double)row[r] + (double)row[c] + (double)row[rc]);
+        const double q = 0.25 * inv_c * (acc[y] + acc[r] + acc[c] + acc[rc]);
+        out[e] = q > 0.0 ? nb / sqrt(q) : 0.0;
+    }
+}
+
+// one panel [j0, j1) of a right-looking Cholesky of the lower triangle of M
+// (row-major, stride ld), one CTA; the trailing block is updated afterwards
+// by a matrix product.  bad[0] is set when a pivot is not positive.
+__global__ void __launch_bounds__(1024) k_chol_panel(double* __restrict__ M, int n, int ld, int j0, int j1,
+                                                     int* __restrict__ bad) {
+    __shared__ double piv;
+    for (int c = j0; c < j1; ++c) {
+        if (threadIdx.x == 0) {
+            const double d = M[(int64_t)c * ld + c];
+            if (!(d > 0.0)) bad[0] = 1;
+            piv = d > 0.0 ? sqrt(d) : 1.0;
+            M[(int64_t)c * ld + c] = piv;
+        }
+        __syncthreads();
+        for (int i = c + 1 + threadIdx.x; i < n; i += blockDim.x) M[(int64_t)i * ld + c] /= piv;
+        __syncthreads();
+        const int w = j1 - c - 1;  // panel columns right of c
+        if (w > 0) {
+            const int64_t tot = (int64_t)(n - c - 1) * w;
+            for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+                const int i = c + 1 + (int)(e / w), cc = c + 1 + (int)(e % w);
+                if (cc <= i) M[(int64_t)i * ld + cc] -= M[(int64_t)i * ld + c] * M[(int64_t)cc * ld + c];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// With M = L L^T: z1 = M^-1 D_F, z2 = M^-1 1, c = sum z1 / sum z2,
+// u = z1 - c z2, d_t = C^2 u_t / |O_t|, pn = p_F + d.  out = [c, number of
+// pn <= 0, max |d|, max p_F].  One CTA; b1, b2 are scratch of length n.
+__global__ void __launch_bounds__(1024) k_newton_solve(const double* __restrict__ L, int n, int ld,
+                                                       const double* __restrict__ Dv, const int* __restrict__ F,
+                                                       const uint8_t* __restrict__ w, const double* __restrict__ p,
+                                                       double C2, double* __restrict__ b1, double* __restrict__ b2,
+                                                       double* __restrict__ pn, double* __restrict__ out) {
+    __shared__ double sh[32], sh2[32];
+    __shared__ double y1, y2;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        b1[i] = Dv[F[i]];
+        b2[i] = 1.0;
+    }
+    __syncthreads();
+    for (int i = 0; i < n; ++i) {  // forward: L y = b
+        if (threadIdx.x == 0) {
+            const double d = L[(int64_t)i * ld + i];
+            y1 = b1[i] / d;
+            y2 = b2[i] / d;
+            b1[i] = y1;
+            b2[i] = y2;
+        }
+        __syncthreads();
+        for (int t = i + 1 + threadIdx.x; t < n; t += blockDim.x) {
+            const double l = L[(int64_t)t * ld + i];
+            b1[t] -= l * y1;
+            b2[t] -= l * y2;
+        }
+        __syncthreads();
+    }
+    for (int i = n - 1; i >= 0; --i) {  // back: L^T x = y
+        if (threadIdx.x == 0) {
+            const double d = L[(int64_t)i * ld + i];
+            y1 = b1[i] / d;
+            y2 = b2[i] / d;
+            b1[i] = y1;
+            b2[i] = y2;
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < i; t += blockDim.x) {
+            const double l = L[(int64_t)i * ld + t];
+            b1[t] -= l * y1;
+            b2[t] -= l * y2;
+        }
+        __syncthreads();
+    }
+    double s1 = 0.0, s2 = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        s1 += b1[i];
+        s2 += b2[i];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s1 += __shfl_xor_sync(0xFFFFFFFFu, s1, o);
+        s2 += __shfl_xor_sync(0xFFFFFFFFu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sh[threadIdx.x >> 5] = s1;
+        sh2[threadIdx.x >> 5] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            a += sh[i];
+            b += sh2[i];
+        }
+        y1 = a / b;
+    }
+    __syncthreads();
+    const double c = y1;
+    double neg = 0.0, md = 0.0, mp = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int s = F[i];
+        const double d = C2 * (b1[i] - c * b2[i]) / (double)w[s];
+        const double v = p[s] + d;
+        pn[i] = v;
+        if (!(v > 0.0)) neg += 1.0;
+        md = fmax(md, fabs(d));
+        mp = fmax(mp, p[s]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        neg += __shfl_xor_sync(0xFFFFFFFFu, neg, o);
+        md = fmax(md, __shfl_xor_sync(0xFFFFFFFFu, md, o));
+        mp = fmax(mp, __shfl_xor_sync(0xFFFFFFFFu, mp, o));
+    }
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+        sh[threadIdx.x >> 5] = neg;
+        sh2[threadIdx.x >> 5] = md;
+        b1[threadIdx.x >> 5] = mp;  // b1 is no longer needed
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0, m = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            a += sh[i];
+            b = fmax(b, sh2[i]);
+            m = fmax(m, b1[i]);
+        }
+        out[0] = c;
+        out[1] = a;
+        out[2] = b;
+        out[3] = m;
+    }
+}
+
+// p_S <- 0 outside F, pn on F, then sum |O| p = 1 (one CTA)
+__global__ void __launch_bounds__(1024) k_newton_apply(int S, int nF, const int* __restrict__ F,
+                                                       const double* __restrict__ pn, const uint8_t* __restrict__ w,
+                                                       double* __restrict__ p, int keep_outside) {
+    __shared__ double sh[32];
+    __shared__ double tot;
+    if (!keep_outside)
+        for (int s = threadIdx.x; s < S; s += blockDim.x) p[s] = 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nF; i += blockDim.x) p[F[i]] = pn[i] > 0.0 ? pn[i] : 0.0;
+    __syncthreads();
+    double z = 0.0;
+    for (int s = threadIdx.x; s < S; s += blockDim.x) z = fma((double)w[s], p[s], z);
+    for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xFFFFFFFFu, z, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = z;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += sh[i];
+        tot = t;
+    }
+    __syncthreads();
+    const double inv = 1.0 / tot;
+    for (int s = threadIdx.x; s < S; s += blockDim.x) p[s] *= inv;
+}
+
+// ------------------------------------------------------------ host side
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() { cudaFree(p); }
+    template <typename T>
+    T* get() const { return (T*)p; }
+};
+
+static cudaError_t dalloc(DevBuf& b, size_t bytes) {
+    cudaFree(b.p);
+    b.p = nullptr;
+    return cudaMalloc(&b.p, bytes > 0 ? bytes : 16);
+}
+
+// Anderson mixing on vectors of length L with orbit weights w; the Gram
+// matrix of the stored differences lives on the host (m <= kAAMax numbers a
+// row), the vectors on the device.
+struct Anderson {
+    int64_t L = 0;
+    int m = 0, count = 0, head = 0, nb = 0;
+    DevBuf f_last, g_last, part, dots;
+    DevBuf dF[kAAMax], dG[kAAMax];
+    int slot[kAAMax];              // ring order: slot[0] oldest
+    double A[kAAMax][kAAMax];      // w dF_a . dF_b for ring positions a, b
+    double b[kAAMax];              // w dF_a . f_last
+    bool have_last = false;
+
+    cudaError_t init(int64_t len, int mem, int sms) {
+        L = len;
+        m = mem;
+        nb = (int)std::min<int64_t>(sms * 4, (L + 255) / 256);
+        nb = std::max(nb, 1);
+        cudaError_t e = dalloc(f_last, sizeof(double) * L);
+        if (e == cudaSuccess) e = dalloc(g_last, sizeof(double) * L);
+        if (e == cudaSuccess) e = dalloc(part, sizeof(double) * nb * 2 * kAAMax);
+        if (e == cudaSuccess) e = dalloc(dots, sizeof(double) * 2 * kAAMax);
+        for (int i = 0; i < m && e == cudaSuccess; ++i) {
+            e = dalloc(dF[i], sizeof(double) * L);
+            if (e == cudaSuccess) e = dalloc(dG[i], sizeof(double) * L);
+        }
+        clear();
+        return e;
+    }
+    void clear() {
+        count = 0;
+        head = 0;
+        have_last = false;
+    }
+    AAPtrs ptrs() const {
+        AAPtrs P{};
+        P.m = count;
+        for (int a = 0; a < count; ++a) {
+            P.dF[a] = dF[slot[a]].get<double>();
+            P.dG[a] = dG[slot[a]].get<double>();
+        }
+        return P;
+    }
+    // records the pair (x, g = F(x)); updates the Gram rows on the host
+    bdc_status push(const double* x, const double* g, const uint8_t* w, cudaStream_t s) {
+        if (!have_last) {
+            k_aa_push<<<nb, 256, 0, s>>>(L, x, g, f_last.get<double>(), g_last.get<double>(), nullptr, nullptr, 0);
+            BDC_CUDA_TRY(cudaGetLastError());
+            have_last = true;
+            return BDC_OK;
+        }
+        // the new difference goes to the next free slot (dropping the oldest)
+        int sl;
+        if (count < m) {
+            sl = count;
+            slot[count++] = sl;
+        } else {
+            sl = slot[0];
+            for (int a = 1; a < m; ++a) slot[a - 1] = slot[a];
+            slot[m - 1] = sl;
+            for (int a = 1; a < m; ++a)
+                for (int c = 1; c < m; ++c) A[a - 1][c - 1] = A[a][c];
+        }
+        k_aa_push<<<nb, 256, 0, s>>>(L, x, g, f_last.get<double>(), g_last.get<double>(), dF[sl].get<double>(),
+                                     dG[sl].get<double>(), 1);
+        BDC_CUDA_TRY(cudaGetLastError());
+        AAPtrs P = ptrs();
+        k_aa_dots<<<nb, 256, 0, s>>>(L, w, P, dF[sl].get<double>(), f_last.get<double>(), part.get<double>());
+        k_aa_dots_finish<<<1, 32, 0, s>>>(part.get<double>(), nb, count, dots.get<double>());
+        BDC_CUDA_TRY(cudaGetLastError());
+        double hd[2 * kAAMax];
+        BDC_CUDA_TRY(cudaMemcpyAsync(hd, dots.get<double>(), sizeof(hd), cudaMemcpyDeviceToHost, s));
+        BDC_CUDA_TRY(cudaStreamSynchronize(s));
+        const int nw = count - 1;  // ring position of the new difference
+        for (int a = 0; a < count; ++a) {
+            A[nw][a] = A[a][nw] = hd[a];
+            b[a] = hd[kAAMax + a];
+        }
+        return BDC_OK;
+    }
+    // least-squares weights: (A + lambda I) gamma = b, by Cholesky with a
+    // small ridge; false when the system is degenerate
+    bool solve(double* gamma) const {
+        const int c = count;
+        if (c < 1) return false;
+        double M[kAAMax][kAAMax];
+        double tr = 0.0;
+        for (int a = 0; a < c; ++a) tr += A[a][a];
+        if (!(tr > 0.0) || !std::isfinite(tr)) return false;
+        const double lam = 1e-12 * tr / c;
+        for (int a = 0; a < c; ++a)
+            for (int d = 0; d < c; ++d) M[a][d] = A[a][d] + (a == d ? lam : 0.0);
+        for (int j = 0; j < c; ++j) {
+            double dsum = M[j][j];
+            for (int t = 0; t < j; ++t) dsum -= M[j][t] * M[j][t];
+            if (!(dsum > 0.0)) return false;
+            M[j][j] = std::sqrt(dsum);
+            for (int i = j + 1; i < c; ++i) {
+                double v = M[i][j];
+                for (int t = 0; t < j; ++t) v -= M[i][t] * M[j][t];
+                M[i][j] = v / M[j][j];
+            }
+        }
+        double y[kAAMax];
+        for (int i = 0; i < c; ++i) {
+            double v = b[i];
+            for (int t = 0; t < i; ++t) v -= M[i][t] * y[t];
+            y[i] = v / M[i][i];
+        }
+        for (int i = c - 1; i >= 0; --i) {
+            double v = y[i];
+            for (int t = i + 1; t < c; ++t) v -= M[t][i] * gamma[t];
+            gamma[i] = v / M[i][i];
+        }
+        for (int i = 0; i < c; ++i)
+            if (!std::isfinite(gamma[i])) return false;
+        return true;
+    }
+    // x = g_last - sum gamma dG, clipped and normalised (sum w x = 1)
+    bdc_status mix(const double* gamma, const uint8_t* w, double* x, cudaStream_t s) {
+        AAPtrs P = ptrs();
+        for (int a = 0; a < P.m; ++a) P.gamma[a] = gamma[a];
+        k_aa_mix<<<nb, 256, 0, s>>>(L, w, P, g_last.get<double>(), x, part.get<double>());
+        k_scale_by_sum<<<nb, 256, 0, s>>>(L, x, part.get<double>(), nb);
+        BDC_CUDA_TRY(cudaGetLastError());
+        return BDC_OK;
+    }
+};
+
+struct Bracket {
+    double ub = DBL_MAX, rate = -DBL_MAX;
+    void add(double u, double r) {
+        if (std::isfinite(u)) ub = std::min(ub, u);
+        if (std::isfinite(r)) rate = std::max(rate, r);
+    }
+    double gap_bits() const { return (ub - rate) / 0.69314718055994530942; }
+};
+
+// The restricted problem on S: rows, weights, h, and its BA map
+struct Restricted {
+    int S = 0, ny = 0, nc = 0, nbd = 0;
+    DevBuf idx, rows, w, h, part, acc, lnq, D, dpart, out;
+
+    bdc_status build(bdc_handle* H, const std::vector<uint32_t>& members) {
+        S = (int)members.size();
+        ny = 1 << H->k;
+        nc = (S + kRsChunk - 1) / kRsChunk;
+        nbd = (S + 7) / 8;
+        BDC_CUDA_TRY(dalloc(idx, sizeof(uint32_t) * S));
+        BDC_CUDA_TRY(dalloc(rows, sizeof(float) * (size_t)S * ny));
+        BDC_CUDA_TRY(dalloc(w, S));
+        BDC_CUDA_TRY(dalloc(h, sizeof(double) * S));
+        BDC_CUDA_TRY(dalloc(part, sizeof(double) * (size_t)nc * ny));
+        BDC_CUDA_TRY(dalloc(acc, sizeof(double) * ny));
+        BDC_CUDA_TRY(dalloc(lnq, sizeof(double) * ny));
+        BDC_CUDA_TRY(dalloc(D, sizeof(double) * S));
+        BDC_CUDA_TRY(dalloc(dpart, sizeof(double) * 2 * nbd));
+        BDC_CUDA_TRY(dalloc(out, sizeof(double) * 2));
+        BDC_CUDA_TRY(cudaMemcpyAsync(idx.p, members.data(), sizeof(uint32_t) * S, cudaMemcpyHostToDevice, H->stream));
+        const int g = std::max(1, std::min(H->num_sms * 8, (int)(((int64_t)S * ny + 255) / 256)));
+        k_rows<<<g, 256, 0, H->stream>>>(H->s, H->A, H->B, H->d_reps, idx.get<uint32_t>(), S, rows.get<float>());
+        k_gather_u8<<<(S + 255) / 256, 256, 0, H->stream>>>(S, idx.get<uint32_t>(), H->d_reps, H->n, w.get<uint8_t>());
+        k_gather_f64<<<(S + 255) / 256, 256, 0, H->stream>>>(S, idx.get<uint32_t>(), H->d_h, h.get<double>());
+        BDC_CUDA_TRY(cudaGetLastError());
+        return BDC_OK;
+    }
+    // p -> pn; ub / rate (nats) of p
+    bdc_status map(bdc_handle* H, const double* p, double* pn, double* ub, double* rate) {
+        cudaStream_t s = H->stream;
+        k_rs_acc<<<dim3((ny + 255) / 256, nc), 256, 0, s>>>(S, ny, rows.get<float>(), w.get<uint8_t>(), p,
+                                                            part.get<double>());
+        k_rs_sum<<<(ny + 255) / 256, 256, 0, s>>>(ny, nc, part.get<double>(), acc.get<double>());
+        k_rs_lnq<<<(ny + 255) / 256, 256, 0, s>>>(H->k, H->inv_c, acc.get<double>(), lnq.get<double>());
+        k_rs_div<<<nbd, 256, 0, s>>>(S, ny, rows.get<float>(), lnq.get<double>(), h.get<double>(), w.get<uint8_t>(),
+                                     p, H->inv_c, D.get<double>(), dpart.get<double>());
+        k_rs_update<<<1, 1024, 0, s>>>(S, dpart.get<double>(), nbd, D.get<double>(), w.get<uint8_t>(), p, pn,
+                                       out.get<double>());
+        BDC_CUDA_TRY(cudaGetLastError());
+        double o[2];
+        BDC_CUDA_TRY(cudaMemcpyAsync(o, out.p, sizeof(o), cudaMemcpyDeviceToHost, s));
+        BDC_CUDA_TRY(cudaStreamSynchronize(s));
+        *ub = o[0];
+        *rate = o[1];
+        return BDC_OK;
+    }
+};
+
+__global__ void __launch_bounds__(1024) k_ridge(double* __restrict__ M, int n, int ld, double rel) {
+    __shared__ double sh[32];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, M[(int64_t)i * ld + i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+    __syncthreads();
+    double mm = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) mm = fmax(mm, sh[i]);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) M[(int64_t)i * ld + i] += rel * mm;
+}
+
+// Active-set Newton on the support equations of the restricted problem,
+// started from p (device, |S|): F = members with D_s within `margin` of the
+// rate; each step solves the linearised equations on F (Cholesky of M on
+// the device), members that the step would make non-positive leave F, and
+// members outside F whose D_s exceeds the rate join it.  *ok = false when
+// the factorisation breaks down (p is then left at a valid point).
+static bdc_status newton_polish(bdc_handle* H, Restricted& rs, double* p, double* scratch, double margin, Bracket& rb,
+                                bool* ok) {
+    cudaStream_t s = H->stream;
+    const int S = rs.S, ny = rs.ny;
+    *ok = true;
+    if (S > 8192) {
+        *ok = false;
+        return BDC_OK;
+    }
+    DevBuf dF, Bq, M, b1, b2, pn, out, bad;
+    BDC_CUDA_TRY(dalloc(dF, sizeof(int) * S));
+    BDC_CUDA_TRY(dalloc(Bq, sizeof(double) * (size_t)S * ny));
+    BDC_CUDA_TRY(dalloc(M, sizeof(double) * (size_t)S * S));
+    BDC_CUDA_TRY(dalloc(b1, sizeof(double) * std::max(S, 64)));
+    BDC_CUDA_TRY(dalloc(b2, sizeof(double) * S));
+    BDC_CUDA_TRY(dalloc(pn, sizeof(double) * S));
+    BDC_CUDA_TRY(dalloc(out, sizeof(double) * 4));
+    BDC_CUDA_TRY(dalloc(bad, sizeof(int)));
+    std::vector<double> hD(S), hp(S);
+    auto fetch = [&]() -> bdc_status {
+        BDC_CUDA_TRY(cudaMemcpyAsync(hD.data(), rs.D.p, sizeof(double) * S, cudaMemcpyDeviceToHost, s));
+        BDC_CUDA_TRY(cudaMemcpyAsync(hp.data(), p, sizeof(double) * S, cudaMemcpyDeviceToHost, s));
+        BDC_CUDA_TRY(cudaStreamSynchronize(s));
+        return BDC_OK;
+    };
+    // sets p to vals on F, 0 elsewhere, normalised
+    auto apply = [&](const std::vector<int>& F, const double* vals_dev) -> bdc_status {
+        BDC_CUDA_TRY(cudaMemcpyAsync(dF.p, F.data(), sizeof(int) * F.size(), cudaMemcpyHostToDevice, s));
+        k_newton_apply<<<1, 1024, 0, s>>>(S, (int)F.size(), dF.get<int>(), vals_dev, rs.w.get<uint8_t>(), p, 0);
+        BDC_CUDA_TRY(cudaGetLastError());
+        return BDC_OK;
+    };
+    double ub, c;
+    bdc_status rc = rs.map(H, p, scratch, &ub, &c);
+    if (rc != BDC_OK) return rc;
+    rb.add(ub, c);
+    rc = fetch();
+    if (rc != BDC_OK) return rc;
+    std::vector<int> F;
+    for (int i = 0; i < S; ++i)
+        if (hD[i] > c - margin) F.push_back(i);
+    const double C2 = H->C * H->C;
+    for (int outer = 0; outer < 10; ++outer) {
+        for (int inner = 0; inner < 40 && !F.empty(); ++inner) {
+            const int nF = (int)F.size();
+            BDC_CUDA_TRY(cudaMemcpyAsync(dF.p, F.data(), sizeof(int) * nF, cudaMemcpyHostToDevice, s));
+            const int g = std::max(1, std::min(H->num_sms * 8, (int)(((int64_t)nF * ny + 255) / 256)));
+            k_nt_rows<<<g, 256, 0, s>>>(nF, H->k, dF.get<int>(), rs.rows.get<float>(), rs.acc.get<double>(), H->inv_c,
+                                        Bq.get<double>());
+            BDC_CUDA_TRY(cudaGetLastError());
+            BDC_CUDA_TRY(dgemm_nt(Bq.get<double>(), ny, Bq.get<double>(), ny, M.get<double>(), nF, nF, nF, ny, 1.0, 0, s));
+            k_ridge<<<1, 1024, 0, s>>>(M.get<double>(), nF, nF, 1e-15);
+            BDC_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+            for (int j0 = 0; j0 < nF; j0 += 32) {
+                const int j1 = std::min(nF, j0 + 32);
+                k_chol_panel<<<1, 1024, 0, s>>>(M.get<double>(), nF, nF, j0, j1, bad.get<int>());
+                BDC_CUDA_TRY(cudaGetLastError());
+                if (j1 < nF)
+                    BDC_CUDA_TRY(dgemm_nt(M.get<double>() + (int64_t)j1 * nF + j0, nF, M.get<double>() + (int64_t)j1 * nF + j0,
+                                          nF, M.get<double>() + (int64_t)j1 * nF + j1, nF, nF - j1, nF - j1, j1 - j0, -1.0,
+                                          1, s));
+            }
+            int hbad = 0;
+            BDC_CUDA_TRY(cudaMemcpyAsync(&hbad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            BDC_CUDA_TRY(cudaStreamSynchronize(s));
+            if (hbad) {
+                *ok = false;
+                return BDC_OK;
+            }
+            k_newton_solve<<<1, 1024, 0, s>>>(M.get<double>(), nF, nF, rs.D.get<double>(), dF.get<int>(),
+                                              rs.w.get<uint8_t>(), p, C2, b1.get<double>(), b2.get<double>(),
+                                              pn.get<double>(), out.get<double>());
+            BDC_CUDA_TRY(cudaGetLastError());
+            double ho[4];
+            BDC_CUDA_TRY(cudaMemcpyAsync(ho, out.p, sizeof(ho), cudaMemcpyDeviceToHost, s));
+            BDC_CUDA_TRY(cudaStreamSynchronize(s));
+            if (ho[1] > 0.0) {
+                // members that the step sends to zero or below leave F
+                std::vector<double> hpn(nF);
+                BDC_CUDA_TRY(cudaMemcpyAsync(hpn.data(), pn.p, sizeof(double) * nF, cudaMemcpyDeviceToHost, s));
+                BDC_CUDA_TRY(cudaStreamSynchronize(s));
+                std::vector<int> keep;
+                std::vector<double> kv;
+                for (int i = 0; i < nF; ++i)
+                    if (hpn[i] > 0.0) {
+                        keep.push_back(F[i]);
+                        kv.push_back(hp[F[i]]);
+                    }
+                F.swap(keep);
+                BDC_CUDA_TRY(cudaMemcpyAsync(pn.p, kv.data(), sizeof(double) * kv.size(), cudaMemcpyHostToDevice, s));
+                rc = apply(F, pn.get<double>());
+                if (rc != BDC_OK) return rc;
+            } else {
+                rc = apply(F, pn.get<double>());
+                if (rc != BDC_OK) return rc;
+            }
+            rc = rs.map(H, p, scratch, &ub, &c);
+            if (rc != BDC_OK) return rc;
+            rb.add(ub, c);
+            rc = fetch();
+            if (rc != BDC_OK) return rc;
+            if (ho[1] == 0.0 && (ub - c <= 1e-15 * std::fabs(c) || ho[2] <= 1e-16 * ho[3])) break;
+        }
+        // members outside F that beat the rate join it with a small mass
+        std::vector<int> add;
+        double mp = 0.0;
+        for (int i = 0; i < S; ++i) mp = std::max(mp, hp[i]);
+        std::vector<char> inF(S, 0);
+        for (int f : F) inF[f] = 1;
+        for (int i = 0; i < S; ++i)
+            if (!inF[i] && hD[i] > c + 1e-14 * std::fabs(c)) add.push_back(i);
+        if (add.empty()) break;
+        std::vector<int> F2 = F;
+        F2.insert(F2.end(), add.begin(), add.end());
+        std::sort(F2.begin(), F2.end());
+        std::vector<double> vals(F2.size());
+        for (size_t i = 0; i < F2.size(); ++i) vals[i] = inF[F2[i]] ? hp[F2[i]] : 1e-3 * mp;
+        F.swap(F2);
+        BDC_CUDA_TRY(cudaMemcpyAsync(pn.p, vals.data(), sizeof(double) * vals.size(), cudaMemcpyHostToDevice, s));
+        rc = apply(F, pn.get<double>());
+        if (rc != BDC_OK) return rc;
+        rc = rs.map(H, p, scratch, &ub, &c);
+        if (rc != BDC_OK) return rc;
+        rb.add(ub, c);
+        rc = fetch();
+        if (rc != BDC_OK) return rc;
+    }
+    return BDC_OK;
+}
+
+// Anderson-accelerated BA with the rate guard on an abstract map; stops when
+// the bracket of the evaluated points is below gap_bits or after max_evals
+// evaluations.  x holds the start and receives the last accepted point.
+template <typename Map>
+static bdc_status accelerated_ba(bdc_handle* H, Anderson& aa, const uint8_t* w, Map&& F, double* x, double* g,
+                                 double* xa, double* ga, int64_t L, double gap_bits, int64_t max_evals,
+                                 Bracket& br, int64_t* evals) {
+    cudaStream_t s = H->stream;
+    aa.clear();
+    int64_t ev = 0;
+    while (ev < max_evals) {
+        double u, r;
+        bdc_status rc = F(x, g, &u, &r);
+        if (rc != BDC_OK) return rc;
+        ++ev;
+        br.add(u, r);
+        if (br.gap_bits() < gap_bits) {
+            BDC_CUDA_TRY(cudaMemcpyAsync(x, g, sizeof(double) * L, cudaMemcpyDeviceToDevice, s));
+            break;
+        }
+        rc = aa.push(x, g, w, s);
+        if (rc != BDC_OK) return rc;
+        double gamma[kAAMax];
+        bool mixed = false;
+        if (aa.count >= 1 && aa.solve(gamma)) {
+            rc = aa.mix(gamma, w, xa, s);
+            if (rc != BDC_OK) return rc;
+            double ua, ra;
+            rc = F(xa, ga, &ua, &ra);
+            if (rc != BDC_OK) return rc;
+            ++ev;
+            br.add(ua, ra);
+            if (std::isfinite(ua) && ra >= r) {
+                BDC_CUDA_TRY(cudaMemcpyAsync(x, ga, sizeof(double) * L, cudaMemcpyDeviceToDevice, s));
+                mixed = true;
+            }
+        }
+        if (!mixed) {
+            if (aa.count >= 1) aa.clear();
+            BDC_CUDA_TRY(cudaMemcpyAsync(x, g, sizeof(double) * L, cudaMemcpyDeviceToDevice, s));
+        }
+        if (br.gap_bits() < gap_bits) break;
+    }
+    *evals += ev;
+    return BDC_OK;
+}
+
+}  // namespace bdc
+
+using namespace bdc;
+
+extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_evals, bdc_stats* stats) {
+    if (!H) return fail(BDC_ERR_ARG, "bdc_solve: NULL handle");
+    if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_solve: no distribution set");
+    if (H->engine != BDC_ENGINE_FACTORED) return fail(BDC_ERR_UNSUPPORTED, "bdc_solve: needs the factored engine (k < n)");
+    if (!(gap_bits > 0.0) || max_evals < 1) return fail(BDC_ERR_ARG, "bdc_solve: need gap_bits > 0 and max_evals >= 1");
+    if (H->n > 26) return fail(BDC_ERR_UNSUPPORTED, "bdc_solve: counts of n > 26 do not fit FP32 exactly");
+    cudaSetDevice(H->device);
+    cudaStream_t s = H->stream;
+    const int64_t R = H->R;
+    const int sms = H->num_sms;
+    const int nbR = (int)std::min<int64_t>(sms * 8, (R + 255) / 256);
+
+    // start: the handle's current iterate
+    const double* cur = nullptr;
+    bdc_status rc = engine_current_p(H, &cur);
+    if (rc != BDC_OK) return rc;
+    DevBuf x, g, xa, ga, D, wts, in_s, cnt, sel, mpart;
+    BDC_CUDA_TRY(dalloc(x, sizeof(double) * R));
+    BDC_CUDA_TRY(dalloc(g, sizeof(double) * R));
+    BDC_CUDA_TRY(dalloc(xa, sizeof(double) * R));
+    BDC_CUDA_TRY(dalloc(ga, sizeof(double) * R));
+    BDC_CUDA_TRY(dalloc(D, sizeof(double) * R));
+    BDC_CUDA_TRY(dalloc(wts, R));
+    BDC_CUDA_TRY(dalloc(in_s, R));
+    BDC_CUDA_TRY(dalloc(cnt, sizeof(int)));
+    BDC_CUDA_TRY(dalloc(mpart, sizeof(double) * nbR));
+    const int cap = (int)std::min<int64_t>(R, 1 << 20);
+    BDC_CUDA_TRY(dalloc(sel, sizeof(uint32_t) * cap));
+    BDC_CUDA_TRY(cudaMemcpyAsync(x.p, cur, sizeof(double) * R, cudaMemcpyDeviceToDevice, s));
+    k_orbit_weights<<<nbR, 256, 0, s>>>(R, H->d_reps, H->n, wts.get<uint8_t>());
+    BDC_CUDA_TRY(cudaMemsetAsync(in_s.p, 0, R, s));
+    BDC_CUDA_TRY(cudaGetLastError());
+
+    Bracket br;
+    int64_t evals = 0;
+    auto full_map = [&](const double* pin, double* pout, double* u, double* r) -> bdc_status {
+        bdc_status e = factored_map(H, pin, pout, nullptr);
+        *u = H->h_st->max_d;
+        *r = H->h_st->rate;
+        return e;
+    };
+    // ---- phase 1
+    const double switch_bits = std::max(gap_bits, 1e-4);
+    {
+        Anderson aa;
+        BDC_CUDA_TRY(aa.init(R, 8, sms));
+        rc = accelerated_ba(H, aa, wts.get<uint8_t>(), full_map, x.get<double>(), g.get<double>(), xa.get<double>(),
+                            ga.get<double>(), R, switch_bits, max_evals, br, &evals);
+        if (rc != BDC_OK) return rc;
+    }
+    if (H->verbose)
+        printf("bdc: solve phase 1: %lld full evaluations, gap %.3e bits\n", (long long)evals, br.gap_bits());
+
+    // ---- phases 2 and 3
+    std::vector<uint32_t> members;
+    bool certified = br.gap_bits() < gap_bits;
+    double cert_ub = br.ub, cert_rate = br.rate;
+    for (int round = 0; round < 32 && !certified && evals < max_evals; ++round) {
+        // full evaluation at x with D for every representative
+        rc = factored_map(H, x.get<double>(), g.get<double>(), D.get<double>());
+        if (rc != BDC_OK) return rc;
+        ++evals;
+        const double ub = H->h_st->max_d, rate = H->h_st->rate;
+        br.add(ub, rate);
+        cert_ub = ub;
+        cert_rate = rate;
+        if ((ub - rate) / 0.69314718055994530942 < gap_bits) {
+            certified = true;
+            break;
+        }
+        // candidates: mass above 1e-12 of the largest (first round only), or
+        // D(x) within max(10 gap, 1e-3 nats) of the bound (first round) / above
+        // the rate (later rounds: the inputs that violate optimality of p_S)
+        double pmax = 0.0;
+        if (round == 0) {
+            k_max_vec<<<nbR, 256, 0, s>>>(R, x.get<double>(), mpart.get<double>());
+            std::vector<double> hp(nbR);
+            BDC_CUDA_TRY(cudaMemcpyAsync(hp.data(), mpart.p, sizeof(double) * nbR, cudaMemcpyDeviceToHost, s));
+            BDC_CUDA_TRY(cudaStreamSynchronize(s));
+            for (double v : hp) pmax = std::max(pmax, v);
+        }
+        const double dmin = round == 0 ? ub - std::max(10.0 * (ub - rate), 1e-3) : rate + 1e-13 * std::fabs(rate);
+        BDC_CUDA_TRY(cudaMemsetAsync(cnt.p, 0, sizeof(int), s));
+        k_select<<<nbR, 256, 0, s>>>(R, round == 0 ? x.get<double>() : nullptr, D.get<double>(), 1e-12 * pmax, dmin,
+                                     in_s.get<uint8_t>(), cnt.get<int>(), sel.get<uint32_t>(), cap);
+        BDC_CUDA_TRY(cudaGetLastError());
+        int nnew = 0;
+        BDC_CUDA_TRY(cudaMemcpyAsync(&nnew, cnt.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        BDC_CUDA_TRY(cudaStreamSynchronize(s));
+        if (nnew == 0 && round > 0) {
+            certified = true;  // p_S is optimal: no input outside S beats the rate
+            break;
+        }
+        if (nnew > cap || (int64_t)members.size() + nnew > (1 << 18))
+            return fail(BDC_ERR_UNSUPPORTED, "bdc_solve: support candidates exceed %d", 1 << 18);
+        std::vector<uint32_t> add(nnew);
+        BDC_CUDA_TRY(cudaMemcpyAsync(add.data(), sel.p, sizeof(uint32_t) * nnew, cudaMemcpyDeviceToHost, s));
+        BDC_CUDA_TRY(cudaStreamSynchronize(s));
+        members.insert(members.end(), add.begin(), add.end());
+        std::sort(members.begin(), members.end());
+        members.erase(std::unique(members.begin(), members.end()), members.end());
+        {
+            std::vector<uint8_t> flags(R, 0);
+            for (uint32_t i : members) flags[i] = 1;
+            BDC_CUDA_TRY(cudaMemcpyAsync(in_s.p, flags.data(), R, cudaMemcpyHostToDevice, s));
+            BDC_CUDA_TRY(cudaStreamSynchronize(s));
+        }
+        // restricted problem, started from x on S (new members get a small
+        // share of the largest entry so that they can grow)
+        Restricted rs;
+        rc = rs.build(H, members);
+        if (rc != BDC_OK) return rc;
+        const int Sn = rs.S;
+        DevBuf ps, pg, psa, pga;
+        BDC_CUDA_TRY(dalloc(ps, sizeof(double) * Sn));
+        BDC_CUDA_TRY(dalloc(pg, sizeof(double) * Sn));
+        BDC_CUDA_TRY(dalloc(psa, sizeof(double) * Sn));
+        BDC_CUDA_TRY(dalloc(pga, sizeof(double) * Sn));
+        {
+            std::vector<double> hx(Sn);
+            k_gather_f64<<<(Sn + 255) / 256, 256, 0, s>>>(Sn, rs.idx.get<uint32_t>(), x.get<double>(), ps.get<double>());
+            BDC_CUDA_TRY(cudaMemcpyAsync(hx.data(), ps.p, sizeof(double) * Sn, cudaMemcpyDeviceToHost, s));
+            std::vector<uint8_t> hw(Sn);
+            BDC_CUDA_TRY(cudaMemcpyAsync(hw.data(), rs.w.p, Sn, cudaMemcpyDeviceToHost, s));
+            BDC_CUDA_TRY(cudaStreamSynchronize(s));
+            double mx = 0.0;
+            for (double v : hx) mx = std::max(mx, v);
+            double z = 0.0;
+            for (int i = 0; i < Sn; ++i) {
+                if (!(hx[i] > 1e-6 * mx)) hx[i] = 1e-6 * mx;
+                z += hw[i] * hx[i];
+            }
+            for (double& v : hx) v /= z;
+            BDC_CUDA_TRY(cudaMemcpyAsync(ps.p, hx.data(), sizeof(double) * Sn, cudaMemcpyHostToDevice, s));
+        }
+        Anderson aa;
+        BDC_CUDA_TRY(aa.init(Sn, kAAMax, sms));
+        Bracket rb;
+        int64_t revals = 0;
+        auto rmap = [&](const double* pin, double* pout, double* u, double* r) -> bdc_status {
+            return rs.map(H, pin, pout, u, r);
+        };
+        // accelerated restricted BA to a moderate gap, then Newton on the
+        // support to the precision of FP64; BA again if the Newton systems
+        // break down
+        const double target = std::min(gap_bits * 1e-2, 1e-11);
+        rc = accelerated_ba(H, aa, rs.w.get<uint8_t>(), rmap, ps.get<double>(), pg.get<double>(), psa.get<double>(),
+                            pga.get<double>(), Sn, std::max(target, 1e-7), 400000, rb, &revals);
+        if (rc != BDC_OK) return rc;
+        bool newton_ok = false;
+        if (rb.gap_bits() >= target) {
+            Bracket nb;
+            rc = newton_polish(H, rs, ps.get<double>(), pg.get<double>(),
+                               std::max(1e-5, 100.0 * rb.gap_bits() * 0.69314718055994530942), nb, &newton_ok);
+            if (rc != BDC_OK) return rc;
+            if (newton_ok) rb = nb;
+            if (H->verbose)
+                printf("bdc: solve round %d: Newton on the support %s, restricted gap %.3e bits\n", round,
+                       newton_ok ? "done" : "failed", nb.gap_bits());
+            if (!newton_ok || rb.gap_bits() >= target) {
+                aa.clear();
+                rc = accelerated_ba(H, aa, rs.w.get<uint8_t>(), rmap, ps.get<double>(), pg.get<double>(),
+                                    psa.get<double>(), pga.get<double>(), Sn, target, 400000, rb, &revals);
+                if (rc != BDC_OK) return rc;
+            }
+        }
+        if (H->verbose)
+            printf("bdc: solve round %d: |S| = %d, %lld restricted evaluations, restricted gap %.3e bits\n", round, Sn,
+                   (long long)revals, rb.gap_bits());
+        // expand p_S into the full space
+        BDC_CUDA_TRY(cudaMemsetAsync(x.p, 0, sizeof(double) * R, s));
+        k_scatter_f64<<<(Sn + 255) / 256, 256, 0, s>>>(Sn, rs.idx.get<uint32_t>(), ps.get<double>(), x.get<double>());
+        BDC_CUDA_TRY(cudaGetLastError());
+    }
+    // leave the handle at the final point; its zero entries stay zero under
+    // later BA iterations
+    BDC_CUDA_TRY(cudaMemcpyAsync(H->d_p[0], x.p, sizeof(double) * R, cudaMemcpyDeviceToDevice, s));
+    rc = engine_after_set_p(H, 1);
+    if (rc != BDC_OK) return rc;
+    if (stats) {
+        const double ln2 = 0.69314718055994530942;
+        stats->iters = evals;
+        stats->total_iters = evals;
+        stats->mx = br.gap_bits();
+        stats->upper_bound = cert_ub / ln2;
+        stats->rate = cert_rate / ln2;
+        stats->lse = NAN;
+        stats->best_upper_bound = br.ub / ln2;
+        stats->best_rate = br.rate / ln2;
+        stats->converged = br.gap_bits() < gap_bits;
+    }
+    (void)certified;
+    return BDC_OK;
+}

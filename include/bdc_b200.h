@@ -123,6 +123,19 @@ bdc_status bdc_accelerate(bdc_handle_t h, int64_t max_evals, double gap_bits, bd
 bdc_status bdc_mi_forward(bdc_handle_t h, const double* p, int64_t num_reps, double* I_nats);
 bdc_status bdc_mi_backward(bdc_handle_t h, double* grad, int64_t num_reps);
 
+/* Certified solver (no counterpart in the reference, which runs plain BA
+ * until max_x log2 p'/p < a, backend/main_BAA.cu:73).  Anderson-accelerated
+ * BA on all inputs, then BA restricted to the inputs that can carry mass,
+ * then a full evaluation that proves no other input can (and widens the set
+ * if one could).  Every reported number is evaluated exactly at its point:
+ * best_rate = I(p;W) <= C <= best_upper_bound = max_x D(x).  Runs until the
+ * bracket is below gap_bits or max_evals full-space BA evaluations; the
+ * handle's iterate becomes the final point (entries that are zero there stay
+ * zero under later iterations).  stats->iters = full-space evaluations,
+ * stats->mx = the bracket in bits, converged = bracket < gap_bits.  Factored
+ * engine, n <= 26. */
+bdc_status bdc_solve(bdc_handle_t h, double gap_bits, int64_t max_evals, bdc_stats* stats);
+
 /* Batches (no counterpart in the reference, which runs one (n,k) per
  * process): many handles -- different (n,k) and starting distributions --
  * iterated together from one captured CUDA graph with one branch per handle.
