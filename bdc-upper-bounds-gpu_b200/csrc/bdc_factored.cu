@@ -29,6 +29,8 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <map>
+#include <string>
 #include <vector>
 
 #include "bdc_engine.cuh"
@@ -101,6 +103,19 @@ struct ThinD {
     int cta_begin;
 };
 
+// D side, fused over all terms: one entry per CTA, rows [row0, row0 + the
+// CTA's row count) of one term; IT outputs x RT rows per thread, LPR lanes
+// splitting the contraction
+struct ThinDF {
+    const uint16_t* wide;
+    int64_t wide_stride;
+    int SMALL, WIDE, rows, row0;
+    int lq_trans;
+    double* out;
+    int64_t out_s, out_i;
+    int IT, LPR;
+};
+
 }  // namespace bdc
 
 struct FactoredState {
@@ -132,6 +147,12 @@ struct FactoredState {
     // classes where the tuner found them faster
     bdc::Launch mq[8], md[8];
     bool use_mq[8] = {}, use_md[8] = {};
+    // all per-term products of a side in one launch (used when faster)
+    bdc::ThinQ* d_qf = nullptr;
+    int n_qf = 0;
+    bdc::ThinDF* d_df[4] = {};  // by log2 IT
+    int n_df[4] = {};
+    bool use_qf = false, use_df = false;
     double* lnq_full = nullptr;  // [2^k]
     double* epart = nullptr;  // [ctas][8]
     int ctas_g = 0;
@@ -154,6 +175,9 @@ struct FactoredState {
 namespace bdc {
 
 __device__ __forceinline__ bool gated(const DevState* st) { return st && (st->done || st->error); }
+
+enum Stage { ST_QBIG = 0, ST_QSMALL, ST_FOLD, ST_DSMALL, ST_G, ST_FIN, ST_COUNT };
+static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a);
 
 // Dense layout of the iterate: row x_hi, column rev(x_lo) (the low half
 // bit-reversed).  A representative x satisfies x <= rev(x) and x <=
@@ -202,9 +226,9 @@ __global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ 
 // rows are x_hi, columns x_lo, x = (x_hi << n2) | x_lo; only representatives
 // are updated; block partials [max D, sum |O| e, max (logW - shift),
 // sum |O| p D, input-zero flag] go to ep.part[blockIdx.x * 8 + 0..4].
-template <int BM, int BN, int WM, int WN>
-__global__ void __launch_bounds__(256) k_mma_ba(const GemmDesc* __restrict__ descs, const int* __restrict__ tiles,
-                                                BaEpilogue ep, const DevState* st) {
+template <int BM, int BN, int WM, int WN, bool WITH_D>
+__global__ void __launch_bounds__(256, 2) k_mma_ba(const GemmDesc* __restrict__ descs, const int* __restrict__ tiles,
+                                                   BaEpilogue ep, const DevState* st) {
     using C = MmaCfg<BM, BN, WM, WN>;
     if (gated(st)) return;
     extern __shared__ __align__(16) double smem[];
@@ -235,7 +259,7 @@ __global__ void __launch_bounds__(256) k_mma_ba(const GemmDesc* __restrict__ des
                 if (!is_rep(x, ep.n)) continue;
                 const double o = (double)orbit_size(x, ep.n);
                 const double D = __ldg(ep.hx + xd) - acc[i][j][h] * ep.inv_c;
-                if (ep.Dout) ep.Dout[xd] = D;
+                if (WITH_D) ep.Dout[xd] = D;
                 // an entry that is exactly 0 in the caller's distribution (Lt
                 // holds NaN) takes ln p = 0, as the reference's apply_log_kernel
                 // leaves ln 0 at 0 (backend/BAA.cu:573-580); later iterates keep
@@ -327,9 +351,19 @@ static cudaError_t set_smem_attrs() {
     SET_(k_mma_store, BDC_CFG_ARGS_128x16)
     SET_(k_mma_store, BDC_CFG_ARGS_16x128)
     SET_(k_mma_store, BDC_CFG_ARGS_128x32)
-    SET_(k_mma_ba, BDC_CFG_ARGS_128x128)
-    SET_(k_mma_ba, BDC_CFG_ARGS_128x64)
-    SET_(k_mma_ba, BDC_CFG_ARGS_64x128)
+#define SET_BA_(ARGS, WD)                                                                          \
+    {                                                                                              \
+        cudaError_t e = cudaFuncSetAttribute(k_mma_ba<ARGS, WD>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                             mma_smem_bytes<ARGS>());                              \
+        if (e != cudaSuccess) return e;                                                            \
+    }
+    SET_BA_(BDC_CFG_ARGS_128x128, false)
+    SET_BA_(BDC_CFG_ARGS_128x64, false)
+    SET_BA_(BDC_CFG_ARGS_64x128, false)
+    SET_BA_(BDC_CFG_ARGS_128x128, true)
+    SET_BA_(BDC_CFG_ARGS_128x64, true)
+    SET_BA_(BDC_CFG_ARGS_64x128, true)
+#undef SET_BA_
 #undef SET_
     done = true;
     return cudaSuccess;
@@ -353,10 +387,20 @@ static cudaError_t launch_store(const Launch& L, cudaStream_t s, const DevState*
 
 static cudaError_t launch_ba(const Launch& L, const BaEpilogue& ep, cudaStream_t s, const DevState* st) {
     const int sm = cfg_smem(L.cfg);
+    const bool wd = ep.Dout != nullptr;
     switch (L.cfg) {
-        case CFG_128x128: k_mma_ba<BDC_CFG_ARGS_128x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st); break;
-        case CFG_128x64: k_mma_ba<BDC_CFG_ARGS_128x64><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st); break;
-        case CFG_64x128: k_mma_ba<BDC_CFG_ARGS_64x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st); break;
+        case CFG_128x128:
+            if (wd) k_mma_ba<BDC_CFG_ARGS_128x128, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
+            else k_mma_ba<BDC_CFG_ARGS_128x128, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
+            break;
+        case CFG_128x64:
+            if (wd) k_mma_ba<BDC_CFG_ARGS_128x64, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
+            else k_mma_ba<BDC_CFG_ARGS_128x64, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
+            break;
+        case CFG_64x128:
+            if (wd) k_mma_ba<BDC_CFG_ARGS_64x128, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
+            else k_mma_ba<BDC_CFG_ARGS_64x128, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
+            break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -533,6 +577,162 @@ static cudaError_t launch_thin_d(int lg, const ThinD* d, int n, int ctas, int ny
         case 4: k_thin_d<16><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
         case 5: k_thin_d<32><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
         case 6: k_thin_d<64><<<ctas, 64, sm, s>>>(d, n, lnq_full, st); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+// q side, every term and slice in one launch: CTA = one ThinQ entry (a term
+// and a slice [s0, s1) of its contraction), 2^k / 16 threads, each owning IT
+// (1 or 2) small indices x 16 / IT consecutive wide indices, the latter read
+// as 16-byte pieces of the table row; 16 FP64 FMAs per row and thread.
+__device__ __forceinline__ void unpack8(const uint4 p, double* v) {
+    v[0] = (double)(p.x & 0xFFFFu);
+    v[1] = (double)(p.x >> 16);
+    v[2] = (double)(p.y & 0xFFFFu);
+    v[3] = (double)(p.y >> 16);
+    v[4] = (double)(p.z & 0xFFFFu);
+    v[5] = (double)(p.z >> 16);
+    v[6] = (double)(p.w & 0xFFFFu);
+    v[7] = (double)(p.w >> 16);
+}
+
+__global__ void __launch_bounds__(1024) k_qthin(const ThinQ* __restrict__ descs, const DevState* st) {
+    if (gated(st)) return;
+    const ThinQ& q = descs[blockIdx.x];
+    const int IT = q.SMALL >= 2 ? 2 : 1;
+    const int WT = 16 / IT;
+    const int nwb = q.WIDE / WT;
+    const int wb = threadIdx.x % nwb, ib = threadIdx.x / nwb;
+    const int i0 = ib * IT, w0 = wb * WT;
+    if (i0 >= q.SMALL) return;
+    const uint16_t* wide = (const uint16_t*)q.wide + w0;
+    const double* small = (const double*)q.small + i0;
+    double acc[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+    double v[16];
+    if (IT == 2) {
+#pragma unroll 4
+        for (int s = q.s0; s < q.s1; ++s) {
+            const uint4 pk = __ldg(reinterpret_cast<const uint4*>(wide + (int64_t)s * q.wide_stride));
+            const double* sr = small + (int64_t)s * q.small_stride;
+            const double a0 = __ldg(sr), a1 = __ldg(sr + 1);
+            unpack8(pk, v);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                acc[u] = fma(a0, v[u], acc[u]);
+                acc[8 + u] = fma(a1, v[u], acc[8 + u]);
+            }
+        }
+    } else {
+#pragma unroll 2
+        for (int s = q.s0; s < q.s1; ++s) {
+            const uint4* wr = reinterpret_cast<const uint4*>(wide + (int64_t)s * q.wide_stride);
+            const uint4 p0 = __ldg(wr), p1 = __ldg(wr + 1);
+            const double a0 = __ldg(small + (int64_t)s * q.small_stride);
+            unpack8(p0, v);
+            unpack8(p1, v + 8);
+#pragma unroll
+            for (int u = 0; u < 16; ++u) acc[u] = fma(a0, v[u], acc[u]);
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        const int i = i0 + (IT == 2 ? e / 8 : 0), w = w0 + (IT == 2 ? e % 8 : e);
+        if (q.out_trans) q.out[(int64_t)w * q.SMALL + i] = acc[e];
+        else q.out[(int64_t)i * q.WIDE + w] = acc[e];
+    }
+}
+
+// D side, every term in one launch: CTA = one ThinDF entry.  Lq' of the term
+// is staged in shared memory in chunks of 8 contraction indices padded by
+// one double (so that lanes 8 indices apart fall on different banks); each
+// thread accumulates RT rows x IT outputs over its lane's share of the
+// contraction, reading 8 table entries per row at a time, and the LPR lanes
+// of a row group add their partial sums by shuffles.
+constexpr int kDfRT = 4;
+
+template <int IT>
+__global__ void __launch_bounds__(256) k_dthin(const ThinDF* __restrict__ descs, const double* __restrict__ lnq_full,
+                                               const DevState* st) {
+    if (gated(st)) return;
+    extern __shared__ double lq[];
+    const ThinDF& t = descs[blockIdx.x];
+    const int SMALL = t.SMALL, WIDE = t.WIDE;
+    const int cs = 8 * SMALL + 1;  // padded chunk of 8 contraction indices
+    for (int e = threadIdx.x; e < SMALL * WIDE; e += blockDim.x) {
+        const int w = e / SMALL, i = e % SMALL;
+        lq[(w >> 3) * cs + (w & 7) * SMALL + i] = t.lq_trans ? lnq_full[w * SMALL + i] : lnq_full[i * WIDE + w];
+    }
+    __syncthreads();
+    const int LPR = t.LPR;
+    const int lane = threadIdx.x % LPR, rest = threadIdx.x / LPR;
+    const int ng = SMALL / IT;
+    const int ig = rest % ng, rg = rest / ng;
+    const int r0 = t.row0 + rg * kDfRT;
+    const int i0 = ig * IT;
+    double acc[kDfRT][IT];
+#pragma unroll
+    for (int r = 0; r < kDfRT; ++r)
+#pragma unroll
+        for (int i = 0; i < IT; ++i) acc[r][i] = 0.0;
+    const uint16_t* rowp[kDfRT];
+#pragma unroll
+    for (int r = 0; r < kDfRT; ++r) rowp[r] = t.wide + (int64_t)min(r0 + r, t.rows - 1) * t.wide_stride;
+    for (int w8 = lane * 8; w8 < WIDE; w8 += LPR * 8) {
+        uint32_t pk[kDfRT][4];
+#pragma unroll
+        for (int r = 0; r < kDfRT; ++r) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4*>(rowp[r] + w8));
+            pk[r][0] = q.x;
+            pk[r][1] = q.y;
+            pk[r][2] = q.z;
+            pk[r][3] = q.w;
+        }
+        const double* lc = lq + (w8 >> 3) * cs + i0;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            double v[kDfRT];
+#pragma unroll
+            for (int r = 0; r < kDfRT; ++r) v[r] = (double)((pk[r][u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+#pragma unroll
+            for (int i = 0; i < IT; ++i) {
+                const double l = lc[u * SMALL + i];
+#pragma unroll
+                for (int r = 0; r < kDfRT; ++r) acc[r][i] = fma(v[r], l, acc[r][i]);
+            }
+        }
+    }
+    for (int o = LPR >> 1; o > 0; o >>= 1)
+#pragma unroll
+        for (int r = 0; r < kDfRT; ++r)
+#pragma unroll
+            for (int i = 0; i < IT; ++i) acc[r][i] += __shfl_xor_sync(0xFFFFFFFFu, acc[r][i], o);
+    if (lane != 0) return;
+#pragma unroll
+    for (int r = 0; r < kDfRT; ++r) {
+        if (r0 + r >= t.rows) break;
+#pragma unroll
+        for (int i = 0; i < IT; ++i) t.out[(int64_t)(r0 + r) * t.out_s + (int64_t)(i0 + i) * t.out_i] = acc[r][i];
+    }
+}
+
+static cudaError_t launch_qthin(const ThinQ* d, int n, int k, cudaStream_t s, const DevState* st) {
+    k_qthin<<<n, (1 << k) / 16, 0, s>>>(d, st);
+    return cudaGetLastError();
+}
+
+static int dthin_smem(int k) { return (int)sizeof(double) * ((1 << k) + (1 << k) / 8 + 8); }
+
+static cudaError_t launch_dthin(const ThinDF* d, int n, int it, int k, const double* lnq_full, cudaStream_t s,
+                                const DevState* st) {
+    const int sm = dthin_smem(k);
+    switch (it) {
+        case 1: k_dthin<1><<<n, 256, sm, s>>>(d, lnq_full, st); break;
+        case 2: k_dthin<2><<<n, 256, sm, s>>>(d, lnq_full, st); break;
+        case 4: k_dthin<4><<<n, 256, sm, s>>>(d, lnq_full, st); break;
+        case 8: k_dthin<8><<<n, 256, sm, s>>>(d, lnq_full, st); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -926,19 +1126,24 @@ static cudaError_t make_launch(Launch& L, std::vector<GemmDesc> v, int cfg) {
 
 template <typename F>
 static float time_ms(bdc_handle* H, F&& launch) {
+    // the best of three rounds of three launches, after a warm-up launch
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    launch();  // warm-up
-    cudaEventRecord(a, H->stream);
-    for (int r = 0; r < 3; ++r) launch();
-    cudaEventRecord(b, H->stream);
-    cudaEventSynchronize(b);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, a, b);
+    launch();
+    float best = 1e30f;
+    for (int round = 0; round < 3; ++round) {
+        cudaEventRecord(a, H->stream);
+        for (int r = 0; r < 3; ++r) launch();
+        cudaEventRecord(b, H->stream);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        best = std::min(best, ms / 3.f);
+    }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    return (cudaGetLastError() == cudaSuccess) ? ms / 3.f : 1e30f;
+    return (cudaGetLastError() == cudaSuccess) ? best : 1e30f;
 }
 
 // G with only the tiles that hold representatives (colmax: per dense column
@@ -967,16 +1172,63 @@ static cudaError_t make_tile_launch(Launch& L, GemmDesc d, int cfg, const std::v
     return e;
 }
 
+// Tuning choices pinned in a text file named by the environment variable
+// BDC_TUNE_FILE (lines "n k key a b"): a choice found there is used without
+// timing, new choices are appended, so that repeated runs (a profiler's, for
+// instance) execute the same kernels.
+struct TuneFile {
+    std::string path;
+    std::map<std::string, std::pair<int, int>> m;
+    std::vector<std::string> fresh;
+    int n = 0, k = 0;
+    void load(int n_, int k_) {
+        n = n_;
+        k = k_;
+        const char* e = getenv("BDC_TUNE_FILE");
+        if (!e || !*e) return;
+        path = e;
+        FILE* f = fopen(path.c_str(), "r");
+        if (!f) return;
+        int a, b, nn, kk;
+        char key[64];
+        while (fscanf(f, "%d %d %63s %d %d", &nn, &kk, key, &a, &b) == 5)
+            if (nn == n && kk == k) m[key] = {a, b};
+        fclose(f);
+    }
+    bool get(const char* key, int* a, int* b) const {
+        auto it = m.find(key);
+        if (it == m.end()) return false;
+        *a = it->second.first;
+        *b = it->second.second;
+        return true;
+    }
+    void put(const char* key, int a, int b) {
+        if (path.empty()) return;
+        m[key] = {a, b};
+        char line[128];
+        snprintf(line, sizeof(line), "%d %d %s %d %d\n", n, k, key, a, b);
+        fresh.push_back(line);
+    }
+    void save() const {
+        if (path.empty() || fresh.empty()) return;
+        FILE* f = fopen(path.c_str(), "a");
+        if (!f) return;
+        for (auto& l : fresh) fputs(l.c_str(), f);
+        fclose(f);
+    }
+};
+
 // chooses tile shape and split of one of the wide q-side products by timing
 // them; gen(cfg, S) lists the descriptors of a candidate (S: the split of
 // the longest contraction, kfull its length)
 template <typename Gen>
-static bdc_status tune_thin(bdc_handle* H, Launch& L, Gen&& gen, int kfull, int max_split, int kmin,
-                            const char* what, int* split_out) {
+static bdc_status tune_thin(bdc_handle* H, TuneFile& tf, const char* key, Launch& L, Gen&& gen, int kfull,
+                            int max_split, int kmin, const char* what, int* split_out) {
     const int cfgs[4] = {CFG_128x128, CFG_128x64, CFG_64x128, CFG_64x64};
     float best = 1e30f;
     int best_cfg = CFG_64x64, best_s = 1;
-    for (int ci = 0; ci < 4; ++ci) {
+    const bool pinned = tf.get(key, &best_cfg, &best_s);
+    for (int ci = 0; ci < 4 && !pinned; ++ci) {
         for (int S = 1; S <= max_split; S *= 2) {
             if (kfull / S < kmin) break;
             std::vector<GemmDesc> v = gen(cfgs[ci], S);
@@ -995,6 +1247,7 @@ static bdc_status tune_thin(bdc_handle* H, Launch& L, Gen&& gen, int kfull, int 
             }
         }
     }
+    if (!pinned) tf.put(key, best_cfg, best_s);
     BDC_CUDA_TRY(make_launch(L, gen(best_cfg, best_s), best_cfg));
     *split_out = best_s;
     if (H->verbose)
@@ -1037,12 +1290,16 @@ static GemmDesc thin_d_desc(const ThinD& t, const double* lnq_full) {
 
 // times the CUDA-core kernel of one size class against the tensor-core
 // launch in a few tile shapes and keeps the fastest
-static bdc_status tune_class(bdc_handle* H, const std::vector<GemmDesc>& descs, Launch& L, bool& use_mma,
-                             float core_ms, const char* what, int lg) {
+template <typename Core>
+static bdc_status tune_class(bdc_handle* H, TuneFile& tf, const char* key, const std::vector<GemmDesc>& descs,
+                             Launch& L, bool& use_mma, Core&& core_launch, const char* what, int lg) {
     const int cfgs[5] = {CFG_128x16, CFG_128x32, CFG_64x64, CFG_128x64, CFG_64x128};
+    int best_cfg = -1, unused = 0;
+    const bool pinned = tf.get(key, &best_cfg, &unused);
+    const float core_ms = pinned ? 0.f : time_ms(H, core_launch);
     float best = core_ms;
-    int best_cfg = -1;
     for (int c : cfgs) {
+        if (pinned) break;
         Launch T;
         BDC_CUDA_TRY(make_launch(T, descs, c));
         const float ms = time_ms(H, [&] { launch_store(T, H->stream, nullptr); });
@@ -1052,6 +1309,7 @@ static bdc_status tune_class(bdc_handle* H, const std::vector<GemmDesc>& descs, 
             best_cfg = c;
         }
     }
+    if (!pinned) tf.put(key, best_cfg, 0);
     use_mma = best_cfg >= 0;
     if (use_mma) BDC_CUDA_TRY(make_launch(L, descs, best_cfg));
     if (H->verbose)
@@ -1096,6 +1354,8 @@ bdc_status factored_init(bdc_handle* H) {
     BDC_CUDA_TRY(set_smem_attrs());
     FactoredState* F = new FactoredState();
     H->fac = F;
+    TuneFile tf;
+    tf.load(H->n, H->k);
     const Split& s = H->s;
     F->H1 = 1 << s.n1;
     F->H2 = 1 << s.n2;
@@ -1211,7 +1471,7 @@ bdc_status factored_init(bdc_handle* H) {
             }
             return v;
         };
-        bdc_status rc = tune_thin(H, F->ul, gen, H1, max_split, 16, "U = AL^T Pw", &F->S1);
+        bdc_status rc = tune_thin(H, tf, "ul", F->ul, gen, H1, max_split, 16, "U = AL^T Pw", &F->S1);
         if (rc != BDC_OK) return rc;
     }
     if (KR > 0) {
@@ -1236,7 +1496,7 @@ bdc_status factored_init(bdc_handle* H) {
             }
             return v;
         };
-        bdc_status rc = tune_thin(H, F->vr, gen, H2, max_split, 16, "V = Pw BR", &F->S2);
+        bdc_status rc = tune_thin(H, tf, "vr", F->vr, gen, H2, max_split, 16, "V = Pw BR", &F->S2);
         if (rc != BDC_OK) return rc;
     }
 
@@ -1366,17 +1626,26 @@ bdc_status factored_init(bdc_handle* H) {
         if (F->n_thinq[lg]) {
             std::vector<GemmDesc> v;
             for (auto& q : tq[lg]) v.push_back(thin_q_desc(q));
-            const float core = time_ms(H, [&] { launch_thin_q(lg, F->d_thinq[lg], F->n_thinq[lg], ny, H->stream, nullptr); });
-            bdc_status rc = tune_class(H, v, F->mq[lg], F->use_mq[lg], core, "q-side term products", lg);
+            char key[16];
+            snprintf(key, sizeof(key), "q%d", lg);
+            bdc_status rc = tune_class(
+                H, tf, key, v, F->mq[lg], F->use_mq[lg],
+                [&] { launch_thin_q(lg, F->d_thinq[lg], F->n_thinq[lg], ny, H->stream, nullptr); },
+                "q-side term products", lg);
             if (rc != BDC_OK) return rc;
         }
         if (F->n_thind[lg]) {
             std::vector<GemmDesc> v;
             for (auto& d : td[lg]) v.push_back(thin_d_desc(d, F->lnq_full));
-            const float core = time_ms(H, [&] {
-                launch_thin_d(lg, F->d_thind[lg], F->n_thind[lg], F->ctas_thind[lg], ny, F->lnq_full, H->stream, nullptr);
-            });
-            bdc_status rc = tune_class(H, v, F->md[lg], F->use_md[lg], core, "D-side term products", lg);
+            char key[16];
+            snprintf(key, sizeof(key), "d%d", lg);
+            bdc_status rc = tune_class(
+                H, tf, key, v, F->md[lg], F->use_md[lg],
+                [&] {
+                    launch_thin_d(lg, F->d_thind[lg], F->n_thind[lg], F->ctas_thind[lg], ny, F->lnq_full, H->stream,
+                                  nullptr);
+                },
+                "D-side term products", lg);
             if (rc != BDC_OK) return rc;
         }
     }
@@ -1390,10 +1659,105 @@ bdc_status factored_init(bdc_handle* H) {
         BDC_CUDA_TRY(cudaMemcpy(F->d_fold, fold.data(), sizeof(FoldTerm) * fold.size(), cudaMemcpyHostToDevice));
     }
 
+    // ---- the per-term products of each side fused into one launch (per
+    // side, and per output-tile width on the D side), used where the tuner
+    // times them faster than the per-class launches.  They need 16-byte
+    // aligned table rows of >= 16 entries and 2^k / 16 >= 32 threads.
+    {
+        bool qok = k >= 9 && k <= 14, dok = k >= 9 && k <= 14;
+        std::vector<ThinQ> all_q;
+        for (int lg = 0; lg < 8; ++lg)
+            for (auto& q : tq[lg]) {
+                const int IT = q.SMALL >= 2 ? 2 : 1;
+                const int WT = 16 / IT;
+                if (q.WIDE % WT != 0 || (q.WIDE / WT) * (q.SMALL / IT) != ny / 16 ||
+                    ((uintptr_t)q.wide & 15) != 0 || (q.wide_stride % 8) != 0 || q.wide_u16 != 1 || q.small_u16 != 0)
+                    qok = false;
+                all_q.push_back(q);
+            }
+        std::vector<ThinDF> all_d[4];
+        for (int lg = 0; lg < 8; ++lg)
+            for (auto& d : td[lg]) {
+                if (d.WIDE < 8 || ((uintptr_t)d.wide & 15) != 0 || (d.wide_stride % 8) != 0) dok = false;
+                ThinDF f{};
+                f.wide = d.wide;
+                f.wide_stride = d.wide_stride;
+                f.SMALL = d.SMALL;
+                f.WIDE = d.WIDE;
+                f.rows = d.rows;
+                f.lq_trans = d.lq_trans;
+                f.out = d.out;
+                f.out_s = d.out_s;
+                f.out_i = d.out_i;
+                f.IT = std::min(d.SMALL, 8);
+                f.LPR = std::max(1, std::min(32, d.WIDE / 64));
+                const int ng = d.SMALL / f.IT;
+                if (f.LPR * ng > 256) dok = false;
+                const int rows_per_cta = (256 / (f.LPR * ng)) * kDfRT;
+                int cl = 0;
+                while ((1 << cl) < f.IT) ++cl;
+                for (int r0 = 0; r0 < d.rows; r0 += rows_per_cta) {
+                    f.row0 = r0;
+                    all_d[cl].push_back(f);
+                }
+            }
+        int pinned_q = -1, pinned_d = -1, unused = 0;
+        tf.get("qf", &pinned_q, &unused);
+        tf.get("df", &pinned_d, &unused);
+        BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
+        if (qok && !all_q.empty()) {
+            BDC_CUDA_TRY(cudaMalloc(&F->d_qf, sizeof(ThinQ) * all_q.size()));
+            BDC_CUDA_TRY(cudaMemcpy(F->d_qf, all_q.data(), sizeof(ThinQ) * all_q.size(), cudaMemcpyHostToDevice));
+            F->n_qf = (int)all_q.size();
+            if (pinned_q >= 0) {
+                F->use_qf = pinned_q != 0;
+            } else {
+                const float tc = time_ms(H, [&] { enqueue_stage(H, ST_QSMALL, -INFINITY); });
+                const float tfu = time_ms(H, [&] { launch_qthin(F->d_qf, F->n_qf, k, H->stream, nullptr); });
+                F->use_qf = tfu < tc;
+                tf.put("qf", F->use_qf ? 1 : 0, 0);
+                if (H->verbose)
+                    printf("bdc: tuned q-side term products: %s (one launch %.1f us, per class %.1f us)\n",
+                           F->use_qf ? "one launch" : "per class", tfu * 1e3f, tc * 1e3f);
+            }
+        }
+        if (dok) {
+            const int sm = dthin_smem(k);
+            if (sm > 48 * 1024) {
+                BDC_CUDA_TRY(cudaFuncSetAttribute(k_dthin<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+                BDC_CUDA_TRY(cudaFuncSetAttribute(k_dthin<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+                BDC_CUDA_TRY(cudaFuncSetAttribute(k_dthin<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+                BDC_CUDA_TRY(cudaFuncSetAttribute(k_dthin<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+            }
+            for (int cl = 0; cl < 4; ++cl) {
+                if (all_d[cl].empty()) continue;
+                BDC_CUDA_TRY(cudaMalloc(&F->d_df[cl], sizeof(ThinDF) * all_d[cl].size()));
+                BDC_CUDA_TRY(cudaMemcpy(F->d_df[cl], all_d[cl].data(), sizeof(ThinDF) * all_d[cl].size(),
+                                        cudaMemcpyHostToDevice));
+                F->n_df[cl] = (int)all_d[cl].size();
+            }
+            if (pinned_d >= 0) {
+                F->use_df = pinned_d != 0;
+            } else {
+                F->use_df = false;
+                const float tc = time_ms(H, [&] { enqueue_stage(H, ST_DSMALL, -INFINITY); });
+                F->use_df = true;
+                const float tfu = time_ms(H, [&] { enqueue_stage(H, ST_DSMALL, -INFINITY); });
+                F->use_df = tfu < tc;
+                tf.put("df", F->use_df ? 1 : 0, 0);
+                if (H->verbose)
+                    printf("bdc: tuned D-side term products: %s (fused %.1f us, per class %.1f us)\n",
+                           F->use_df ? "fused" : "per class", tfu * 1e3f, tc * 1e3f);
+            }
+        }
+    }
+
     // ---- G = LA RB with the BA epilogue; the tile shape is tuned on the
     // zero state (set_p re-initialises everything it touches)
     {
-        const int cfgs[3] = {CFG_128x128, CFG_128x64, CFG_64x128};
+        // (128x128 tiles do not fit the two-CTAs-per-SM register budget of the
+        // fused epilogue)
+        const int cfgs[2] = {CFG_128x64, CFG_64x128};
         int ctas_max = 0;
         for (int c : cfgs) ctas_max = std::max(ctas_max, ((H1 + kCfgBM[c] - 1) / kCfgBM[c]) * ((H2 + kCfgBN[c] - 1) / kCfgBN[c]));
         BDC_CUDA_TRY(al(&F->epart, (size_t)std::max(ctas_max, H->nb_upd) * 8));
@@ -1408,7 +1772,10 @@ bdc_status factored_init(bdc_handle* H) {
         ep.Pw = F->Pw;
         ep.inv_c = H->inv_c;
         ep.part = F->epart;
+        int unused = 0;
+        const bool pinned = tf.get("g", &best_cfg, &unused);
         for (int c : cfgs) {
+            if (pinned) break;
             Launch T;
             BDC_CUDA_TRY(make_tile_launch(T, d, c, F->colmax));
             const float ms = time_ms(H, [&] { launch_ba(T, ep, H->stream, H->d_st); });
@@ -1418,13 +1785,15 @@ bdc_status factored_init(bdc_handle* H) {
                 best_cfg = c;
             }
         }
+        if (!pinned) tf.put("g", best_cfg, 0);
+        tf.save();
         BDC_CUDA_TRY(make_tile_launch(F->g, d, best_cfg, F->colmax));
         F->ctas_g = F->g.tiles;
         if (H->verbose)
-            printf("bdc: tuned G: tile %dx%d, %d of %d tiles hold representatives, %.1f us\n", kCfgBM[best_cfg],
+            printf("bdc: tuned G: tile %dx%d, %d of %d tiles hold representatives, %.1f us%s\n", kCfgBM[best_cfg],
                    kCfgBN[best_cfg], F->g.tiles,
                    ((H1 + kCfgBM[best_cfg] - 1) / kCfgBM[best_cfg]) * ((H2 + kCfgBN[best_cfg] - 1) / kCfgBN[best_cfg]),
-                   best * 1e3f);
+                   pinned ? 0.f : best * 1e3f, pinned ? " (pinned)" : "");
         BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
         BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
         BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
@@ -1447,6 +1816,8 @@ void factored_free(bdc_handle* H) {
         cudaFree(p);
     cudaFree(F->Bp);
     cudaFree(F->Ddense);
+    cudaFree(F->d_qf);
+    for (auto* d : F->d_df) cudaFree(d);
     for (int lg = 0; lg < 8; ++lg) {
         cudaFree(F->d_thinq[lg]);
         cudaFree(F->d_thind[lg]);
@@ -1484,8 +1855,7 @@ static BaEpilogue make_epilogue(bdc_handle* H) {
     return ep;
 }
 
-// the stages of one iteration, each gated by DevState::done / error
-enum Stage { ST_QBIG = 0, ST_QSMALL, ST_FOLD, ST_DSMALL, ST_G, ST_FIN, ST_COUNT };
+// the stages of one iteration (enum Stage), each gated by DevState::done / error
 
 static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
     FactoredState* F = H->fac;
@@ -1502,6 +1872,7 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             break;
         }
         case ST_QSMALL:
+            if (F->use_qf) return launch_qthin(F->d_qf, F->n_qf, H->k, s, H->d_st);
             // fork: each size class on its own branch, joined before the fold
             if ((e = cudaEventRecord(F->ev_fork, s)) != cudaSuccess) return e;
             for (int lg = 0; lg < 8; ++lg) {
@@ -1525,6 +1896,18 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
         }
         case ST_DSMALL:
             if ((e = cudaEventRecord(F->ev_fork, s)) != cudaSuccess) return e;
+            if (F->use_df) {
+                // one launch per output-tile width, each on its own branch
+                for (int cl = 0; cl < 4; ++cl) {
+                    if (!F->n_df[cl]) continue;
+                    if ((e = cudaStreamWaitEvent(F->side[cl], F->ev_fork, 0)) != cudaSuccess) return e;
+                    e = launch_dthin(F->d_df[cl], F->n_df[cl], 1 << cl, H->k, F->lnq_full, F->side[cl], H->d_st);
+                    if (e != cudaSuccess) return e;
+                    if ((e = cudaEventRecord(F->ev_join[cl], F->side[cl])) != cudaSuccess) return e;
+                    if ((e = cudaStreamWaitEvent(s, F->ev_join[cl], 0)) != cudaSuccess) return e;
+                }
+                break;
+            }
             for (int lg = 0; lg < 8; ++lg) {
                 if (!F->n_thind[lg]) continue;
                 if ((e = cudaStreamWaitEvent(F->side[lg], F->ev_fork, 0)) != cudaSuccess) return e;

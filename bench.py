@@ -285,6 +285,10 @@ def ours_arm(args) -> None:
                        "traffic": None, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_src})",
                        "work_per_launch": "72 bytes per representative over the three update kernels"}
 
+    ttb = None
+    if world == 1 and not args.no_ttb and E.engine == "factored":
+        ttb = time_to_bound(args, E)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_ba_iteration_rate(args.n, args.k, max(args.cpu_sample, 50000))
@@ -304,7 +308,7 @@ def ours_arm(args) -> None:
         "roofline": roofline, "roofline_update": roofline_update,
         "peaks_measured": {"int32_madd_tops": imad / 1e12, "fp64_fma_tflops": 2 * dfma / 1e12,
                            "hbm_gbs": peaks.get("hbm_gbs"), "hbm_source": peak_src},
-        "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks,
+        "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "time_to_bound": ttb,
         "bound_bits": st["upper_bound"], "rate_bits": st["rate"],
     }
     E.close()
@@ -314,53 +318,71 @@ def ours_arm(args) -> None:
         print(json.dumps(line), flush=True)
 
 
-def time_to_bound(args) -> dict:
-    """Time-to-bound at (n, k) from the uniform start.  The converged bound C*
-    comes from the accelerated loop run to a certified gap best_ub - best_rate
-    < 1e-12 bits (C lies in that bracket, so C* is the plain BA's limit to
-    within 1e-12); then plain BA and the accelerated loop each run from the
-    uniform start, in chunks timed with CUDA events, until their best upper
-    bound is within 1e-9 bits of C*."""
+def time_to_bound(args, E=None) -> dict:
+    """Time-to-bound at (n, k) from the uniform start, tolerance 1e-9 bits.
+
+    The certified solver (bdc_solve) returns a bracket rate <= C <= bound,
+    both evaluated at its final point; its time is the CUDA-event time of the
+    call.  Plain BA and the squared-extrapolation loop then run from the
+    uniform start in chunks, each for at most `budget` seconds of device
+    time; a run has reached the bound when its best upper bound is within
+    1e-9 bits of C, i.e. best_ub - certified rate < 1e-9 (C >= that rate)."""
     import torch
 
     import bdc_b200
 
     tol = 1e-9
-    E = bdc_b200.Engine(args.n, args.k, engine="factored")
+    own = E is None
+    if own:
+        E = bdc_b200.Engine(args.n, args.k, engine="factored")
     stream = torch.cuda.current_stream()
     E.set_stream(stream.cuda_stream)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1) / 1e3
+
+    # warm-up: the iteration graph, the accelerated cycle graph and one solve
     E.set_uniform()
-    E.accelerate(48, 0.0)  # warm-up: builds the iteration and cycle graphs
+    E.accelerate(48, 0.0)
     E.set_uniform()
     E.iterate(16, float("-inf"))
     E.set_uniform()
-    ref = E.accelerate(args.ttb_max, 1e-12)
-    C = ref["best_upper_bound"]
-    out = {"C_star_bits": C, "C_star_gap_bits": ref["best_upper_bound"] - ref["best_rate"],
-           "C_star_evals": ref["iters"], "tolerance_bits": tol}
-    for name in ("plain", "accelerated"):
+    E.solve(1e-6, 20000)
+    E.set_uniform()
+    st, sec = timed(lambda: E.solve(tol, 200000))
+    lo, hi = st["best_rate"], st["best_upper_bound"]
+    out = {"tolerance_bits": tol, "C_bracket_bits": [lo, hi],
+           "certified": {"seconds": sec, "full_evaluations": st["iters"], "gap_bits": hi - lo,
+                         "reached": bool(hi - lo < tol)}}
+    for name in ("plain", "accelerated_squarem"):
         E.set_uniform()
-        evals, ms = 0, 0.0
+        evals, total = 0, 0.0
         chunk = 64
         reached = False
-        st = None
-        while evals < args.ttb_max:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            st = E.iterate(chunk, float("-inf")) if name == "plain" else E.accelerate(chunk, 0.0)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ms += e0.elapsed_time(e1)
+        best = None
+        while total < args.ttb_budget:
+            st, sec = timed(lambda: E.iterate(chunk, float("-inf")) if name == "plain" else E.accelerate(chunk, 0.0))
+            total += sec
             evals += st["iters"]
-            if st["best_upper_bound"] - C < tol:
+            best = st["best_upper_bound"]
+            if best - lo < tol:
                 reached = True
                 break
-            chunk = min(chunk * 2, 2048)
-        out[name] = {"reached": reached, "evals": evals, "seconds": ms / 1e3,
-                     "bound_bits": st["best_upper_bound"], "gap_to_C_star_bits": st["best_upper_bound"] - C}
-    if out["plain"]["reached"] and out["accelerated"]["reached"]:
-        out["speedup"] = out["plain"]["seconds"] / out["accelerated"]["seconds"]
-    E.close()
+            chunk = min(chunk * 2, 4096)
+        out[name] = {"budget_s": args.ttb_budget, "seconds": total, "evaluations": evals, "reached": reached,
+                     "bound_minus_C_bits_at_most": best - lo}
+    if out["plain"]["reached"]:
+        out["speedup_vs_plain"] = out["plain"]["seconds"] / out["certified"]["seconds"]
+    else:
+        out["speedup_vs_plain_at_least"] = out["plain"]["seconds"] / out["certified"]["seconds"]
+    if own:
+        E.close()
     return out
 
 
@@ -474,7 +496,9 @@ def main() -> None:
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mode", choices=["bench", "kernels", "ttb", "batch"], default="bench")
-    ap.add_argument("--ttb-max", type=int, default=400000)
+    ap.add_argument("--ttb-budget", type=float, default=15.0,
+                    help="device seconds for each of the plain and squarem legs of time-to-bound")
+    ap.add_argument("--no-ttb", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -48,6 +48,7 @@ CONFIGS = [
     ("n13k7_dirichlet1_s1", 13, 7, 6, ("dirichlet", 1.0, 1)),
     ("n16k8_dirichlet1_s0", 16, 8, 4, ("dirichlet", 1.0, 0)),
     ("n20k10_dirichlet1_s0", 20, 10, 3, ("dirichlet", 1.0, 0)),
+    ("n24k12_uniform", 24, 12, 2, ("uniform",)),
 ]
 
 
@@ -109,7 +110,7 @@ def cmd_ba(out_dir: str, names: list[str] | None) -> None:
     os.makedirs(out_dir, exist_ok=True)
     with tempfile.TemporaryDirectory() as td:
         os.makedirs(os.path.join(td, "transition_counts"))
-        max_half = max((c[1] + 1) // 2 for c in CONFIGS)
+        max_half = max((c[1] + 1) // 2 for c in CONFIGS if not names or c[0] in names)
         subprocess.run([gen, str(max_half)], cwd=td, check=True)
         for name, n, k, iters, spec in CONFIGS:
             if names and name not in names:
