@@ -69,6 +69,7 @@ struct Launch {
     GemmDesc* d = nullptr;   // device descriptors
     int* map = nullptr;      // CTA -> descriptor index
     int n = 0, tiles = 0, cfg = CFG_64x64;
+    int layout = -1;         // -1: register-staged mainloop; else the cp.async one (see k_mma_store)
 };
 
 // q side thin product of one term over a slice [s0, s1) of its contraction:
@@ -138,6 +139,7 @@ struct FactoredState {
     int S1 = 1, S2 = 1;
     double* qparts = nullptr; // split slices of the small q products (FoldTerm::qoff)
     double* qsum = nullptr;   // [T][2^k]  qparts summed over the splits
+    double* qacc = nullptr;   // [2^k]     sum over the terms
     // thin per-term products, grouped by the small size (index log2 SMALL)
     bdc::ThinQ* d_thinq[8] = {};
     int n_thinq[8] = {};
@@ -191,7 +193,10 @@ __host__ __device__ __forceinline__ uint32_t fac_pos(uint32_t x, int n2) {
 
 
 // ------------------------------------------------ products: plain store
-template <int BM, int BN, int WM, int WN>
+// LAYOUT < 0: register-staged mainloop (any operand kind); otherwise the
+// cp.async mainloop with A k-major when bit 0 is set and B k-major when bit 1
+// is set (FP64 operands only)
+template <int BM, int BN, int WM, int WN, int LAYOUT>
 __global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ descs, const int* __restrict__ map,
                                                    const DevState* st) {
     using C = MmaCfg<BM, BN, WM, WN>;
@@ -201,7 +206,8 @@ __global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ 
     const int t = blockIdx.x - d.tile_begin;
     const int m0 = (t / d.tiles_n) * BM, n0 = (t % d.tiles_n) * BN;
     double acc[C::MT][C::NT][2];
-    mma_mainloop<BM, BN, WM, WN>(d, m0, n0, smem, acc);
+    if constexpr (LAYOUT < 0) mma_mainloop<BM, BN, WM, WN>(d, m0, n0, smem, acc);
+    else mma_mainloop_cp<BM, BN, WM, WN, (LAYOUT & 1) != 0, (LAYOUT & 2) != 0, 3>(d, m0, n0, smem, acc);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, tq = lane & 3;
     const int wm0 = (warp / WN) * (8 * C::MT), wn0 = (warp % WN) * (8 * C::NT);
@@ -226,7 +232,7 @@ __global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ 
 // rows are x_hi, columns x_lo, x = (x_hi << n2) | x_lo; only representatives
 // are updated; block partials [max D, sum |O| e, max (logW - shift),
 // sum |O| p D, input-zero flag] go to ep.part[blockIdx.x * 8 + 0..4].
-template <int BM, int BN, int WM, int WN, bool WITH_D>
+template <int BM, int BN, int WM, int WN, bool WITH_D, bool CP>
 __global__ void __launch_bounds__(256, 2) k_mma_ba(const GemmDesc* __restrict__ descs, const int* __restrict__ tiles,
                                                    BaEpilogue ep, const DevState* st) {
     using C = MmaCfg<BM, BN, WM, WN>;
@@ -236,7 +242,8 @@ __global__ void __launch_bounds__(256, 2) k_mma_ba(const GemmDesc* __restrict__ 
     const int t = tiles[blockIdx.x];  // the tiles that hold representatives
     const int m0 = (t / d.tiles_n) * BM, n0 = (t % d.tiles_n) * BN;
     double acc[C::MT][C::NT][2];
-    mma_mainloop<BM, BN, WM, WN>(d, m0, n0, smem, acc);
+    if constexpr (CP) mma_mainloop_cp<BM, BN, WM, WN, false, true, 3>(d, m0, n0, smem, acc);
+    else mma_mainloop<BM, BN, WM, WN>(d, m0, n0, smem, acc);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, tq = lane & 3;
     const int wm0 = (warp / WN) * (8 * C::MT), wn0 = (warp % WN) * (8 * C::NT);
@@ -322,87 +329,115 @@ __global__ void __launch_bounds__(256, 2) k_mma_ba(const GemmDesc* __restrict__ 
 #define BDC_CFG_ARGS_16x128 16, 128, 1, 8
 #define BDC_CFG_ARGS_128x32 128, 32, 4, 2
 
-static int cfg_smem(int cfg) {
+static int cfg_smem(int cfg, int layout = -1) {
+#define CASE_(C, ARGS)                                                                          \
+    case C:                                                                                     \
+        switch (layout) {                                                                       \
+            case 0: return mma_cp_smem_bytes<ARGS, false, false, 3>();                          \
+            case 1: return mma_cp_smem_bytes<ARGS, true, false, 3>();                           \
+            case 2: return mma_cp_smem_bytes<ARGS, false, true, 3>();                           \
+            case 3: return mma_cp_smem_bytes<ARGS, true, true, 3>();                            \
+            default: return mma_smem_bytes<ARGS>();                                             \
+        }
     switch (cfg) {
-        case CFG_128x128: return mma_smem_bytes<BDC_CFG_ARGS_128x128>();
-        case CFG_128x64: return mma_smem_bytes<BDC_CFG_ARGS_128x64>();
-        case CFG_64x128: return mma_smem_bytes<BDC_CFG_ARGS_64x128>();
-        case CFG_64x64: return mma_smem_bytes<BDC_CFG_ARGS_64x64>();
-        case CFG_128x16: return mma_smem_bytes<BDC_CFG_ARGS_128x16>();
-        case CFG_16x128: return mma_smem_bytes<BDC_CFG_ARGS_16x128>();
-        case CFG_128x32: return mma_smem_bytes<BDC_CFG_ARGS_128x32>();
+        CASE_(CFG_128x128, BDC_CFG_ARGS_128x128)
+        CASE_(CFG_128x64, BDC_CFG_ARGS_128x64)
+        CASE_(CFG_64x128, BDC_CFG_ARGS_64x128)
+        CASE_(CFG_64x64, BDC_CFG_ARGS_64x64)
+        CASE_(CFG_128x16, BDC_CFG_ARGS_128x16)
+        CASE_(CFG_16x128, BDC_CFG_ARGS_16x128)
+        CASE_(CFG_128x32, BDC_CFG_ARGS_128x32)
     }
+#undef CASE_
     return 0;
+}
+
+// the cp.async mainloop is instantiated for the layouts the products use:
+// 3 (U: both k-major), 0 (V and the solver's A B^T: both contraction-major)
+static bool cp_instantiated(int cfg, int layout) {
+    const bool big = cfg == CFG_128x128 || cfg == CFG_128x64 || cfg == CFG_64x128 || cfg == CFG_64x64;
+    return big && (layout == 0 || layout == 3);
 }
 
 static cudaError_t set_smem_attrs() {
     static bool done = false;
     if (done) return cudaSuccess;
-#define SET_(NAME, ARGS)                                                                       \
-    {                                                                                          \
-        cudaError_t e = cudaFuncSetAttribute(NAME<ARGS>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                             mma_smem_bytes<ARGS>());                          \
-        if (e != cudaSuccess) return e;                                                        \
+#define SET_K(KERNEL, BYTES)                                                                     \
+    {                                                                                            \
+        cudaError_t e = cudaFuncSetAttribute(KERNEL, cudaFuncAttributeMaxDynamicSharedMemorySize, BYTES); \
+        if (e != cudaSuccess) return e;                                                          \
     }
-    SET_(k_mma_store, BDC_CFG_ARGS_128x128)
-    SET_(k_mma_store, BDC_CFG_ARGS_128x64)
-    SET_(k_mma_store, BDC_CFG_ARGS_64x128)
-    SET_(k_mma_store, BDC_CFG_ARGS_64x64)
-    SET_(k_mma_store, BDC_CFG_ARGS_128x16)
-    SET_(k_mma_store, BDC_CFG_ARGS_16x128)
-    SET_(k_mma_store, BDC_CFG_ARGS_128x32)
-#define SET_BA_(ARGS, WD)                                                                          \
-    {                                                                                              \
-        cudaError_t e = cudaFuncSetAttribute(k_mma_ba<ARGS, WD>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                             mma_smem_bytes<ARGS>());                              \
-        if (e != cudaSuccess) return e;                                                            \
-    }
-    SET_BA_(BDC_CFG_ARGS_128x128, false)
-    SET_BA_(BDC_CFG_ARGS_128x64, false)
-    SET_BA_(BDC_CFG_ARGS_64x128, false)
-    SET_BA_(BDC_CFG_ARGS_128x128, true)
-    SET_BA_(BDC_CFG_ARGS_128x64, true)
-    SET_BA_(BDC_CFG_ARGS_64x128, true)
-#undef SET_BA_
-#undef SET_
+#define SET_STORE(ARGS)                                                                          \
+    SET_K((k_mma_store<ARGS, -1>), (mma_smem_bytes<ARGS>()))
+#define SET_STORE_CP(ARGS)                                                                       \
+    SET_K((k_mma_store<ARGS, 0>), (mma_cp_smem_bytes<ARGS, false, false, 3>()))                 \
+    SET_K((k_mma_store<ARGS, 3>), (mma_cp_smem_bytes<ARGS, true, true, 3>()))
+#define SET_BA(ARGS)                                                                             \
+    SET_K((k_mma_ba<ARGS, false, false>), (mma_smem_bytes<ARGS>()))                              \
+    SET_K((k_mma_ba<ARGS, true, false>), (mma_smem_bytes<ARGS>()))                               \
+    SET_K((k_mma_ba<ARGS, false, true>), (mma_cp_smem_bytes<ARGS, false, true, 3>()))            \
+    SET_K((k_mma_ba<ARGS, true, true>), (mma_cp_smem_bytes<ARGS, false, true, 3>()))
+    SET_STORE(BDC_CFG_ARGS_128x128)
+    SET_STORE(BDC_CFG_ARGS_128x64)
+    SET_STORE(BDC_CFG_ARGS_64x128)
+    SET_STORE(BDC_CFG_ARGS_64x64)
+    SET_STORE(BDC_CFG_ARGS_128x16)
+    SET_STORE(BDC_CFG_ARGS_16x128)
+    SET_STORE(BDC_CFG_ARGS_128x32)
+    SET_STORE_CP(BDC_CFG_ARGS_128x128)
+    SET_STORE_CP(BDC_CFG_ARGS_128x64)
+    SET_STORE_CP(BDC_CFG_ARGS_64x128)
+    SET_STORE_CP(BDC_CFG_ARGS_64x64)
+    SET_BA(BDC_CFG_ARGS_128x128)
+    SET_BA(BDC_CFG_ARGS_128x64)
+    SET_BA(BDC_CFG_ARGS_64x128)
+#undef SET_BA
+#undef SET_STORE_CP
+#undef SET_STORE
+#undef SET_K
     done = true;
     return cudaSuccess;
 }
 
 static cudaError_t launch_store(const Launch& L, cudaStream_t s, const DevState* st) {
     if (L.n == 0 || L.tiles == 0) return cudaSuccess;
-    const int sm = cfg_smem(L.cfg);
+    const int lay = cp_instantiated(L.cfg, L.layout) ? L.layout : -1;
+    const int sm = cfg_smem(L.cfg, lay);
+#define GO_(ARGS)                                                                                          \
+    if (lay == 0) k_mma_store<ARGS, 0><<<L.tiles, 256, sm, s>>>(L.d, L.map, st);                           \
+    else if (lay == 3) k_mma_store<ARGS, 3><<<L.tiles, 256, sm, s>>>(L.d, L.map, st);                      \
+    else k_mma_store<ARGS, -1><<<L.tiles, 256, sm, s>>>(L.d, L.map, st);
     switch (L.cfg) {
-        case CFG_128x128: k_mma_store<BDC_CFG_ARGS_128x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
-        case CFG_128x64: k_mma_store<BDC_CFG_ARGS_128x64><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
-        case CFG_64x128: k_mma_store<BDC_CFG_ARGS_64x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
-        case CFG_64x64: k_mma_store<BDC_CFG_ARGS_64x64><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
-        case CFG_128x16: k_mma_store<BDC_CFG_ARGS_128x16><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
-        case CFG_16x128: k_mma_store<BDC_CFG_ARGS_16x128><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
-        case CFG_128x32: k_mma_store<BDC_CFG_ARGS_128x32><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
+        case CFG_128x128: GO_(BDC_CFG_ARGS_128x128) break;
+        case CFG_128x64: GO_(BDC_CFG_ARGS_128x64) break;
+        case CFG_64x128: GO_(BDC_CFG_ARGS_64x128) break;
+        case CFG_64x64: GO_(BDC_CFG_ARGS_64x64) break;
+        case CFG_128x16: k_mma_store<BDC_CFG_ARGS_128x16, -1><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
+        case CFG_16x128: k_mma_store<BDC_CFG_ARGS_16x128, -1><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
+        case CFG_128x32: k_mma_store<BDC_CFG_ARGS_128x32, -1><<<L.tiles, 256, sm, s>>>(L.d, L.map, st); break;
         default: return cudaErrorInvalidValue;
     }
+#undef GO_
     return cudaGetLastError();
 }
 
+// G: A = [A_L | N_R] contiguous along the contraction, B = [M_L ; B_R^T]
+// contiguous along the output columns: the cp.async mainloop with layout 2
 static cudaError_t launch_ba(const Launch& L, const BaEpilogue& ep, cudaStream_t s, const DevState* st) {
-    const int sm = cfg_smem(L.cfg);
-    const bool wd = ep.Dout != nullptr;
+    const bool wd = ep.Dout != nullptr, cp = L.layout == 2;
+    const int sm = cfg_smem(L.cfg, cp ? 2 : -1);
+#define GO_(ARGS)                                                                                  \
+    if (wd && cp) k_mma_ba<ARGS, true, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);         \
+    else if (wd) k_mma_ba<ARGS, true, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);         \
+    else if (cp) k_mma_ba<ARGS, false, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);         \
+    else k_mma_ba<ARGS, false, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
     switch (L.cfg) {
-        case CFG_128x128:
-            if (wd) k_mma_ba<BDC_CFG_ARGS_128x128, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
-            else k_mma_ba<BDC_CFG_ARGS_128x128, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
-            break;
-        case CFG_128x64:
-            if (wd) k_mma_ba<BDC_CFG_ARGS_128x64, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
-            else k_mma_ba<BDC_CFG_ARGS_128x64, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
-            break;
-        case CFG_64x128:
-            if (wd) k_mma_ba<BDC_CFG_ARGS_64x128, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
-            else k_mma_ba<BDC_CFG_ARGS_64x128, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
-            break;
+        case CFG_128x128: GO_(BDC_CFG_ARGS_128x128) break;
+        case CFG_128x64: GO_(BDC_CFG_ARGS_128x64) break;
+        case CFG_64x128: GO_(BDC_CFG_ARGS_64x128) break;
         default: return cudaErrorInvalidValue;
     }
+#undef GO_
     return cudaGetLastError();
 }
 
@@ -612,29 +647,69 @@ __global__ void __launch_bounds__(1024) k_qthin(const ThinQ* __restrict__ descs,
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0.0;
     double v[16];
+    // four table rows in flight per thread: their loads are issued before
+    // any of them is used
+    constexpr int U = 4;
+    int s = q.s0;
     if (IT == 2) {
-#pragma unroll 4
-        for (int s = q.s0; s < q.s1; ++s) {
+        for (; s + U <= q.s1; s += U) {
+            uint4 pk[U];
+            double a0[U], a1[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                pk[u] = __ldg(reinterpret_cast<const uint4*>(wide + (int64_t)(s + u) * q.wide_stride));
+                const double* sr = small + (int64_t)(s + u) * q.small_stride;
+                a0[u] = __ldg(sr);
+                a1[u] = __ldg(sr + 1);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                unpack8(pk[u], v);
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    acc[e] = fma(a0[u], v[e], acc[e]);
+                    acc[8 + e] = fma(a1[u], v[e], acc[8 + e]);
+                }
+            }
+        }
+        for (; s < q.s1; ++s) {
             const uint4 pk = __ldg(reinterpret_cast<const uint4*>(wide + (int64_t)s * q.wide_stride));
             const double* sr = small + (int64_t)s * q.small_stride;
             const double a0 = __ldg(sr), a1 = __ldg(sr + 1);
             unpack8(pk, v);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                acc[u] = fma(a0, v[u], acc[u]);
-                acc[8 + u] = fma(a1, v[u], acc[8 + u]);
+            for (int e = 0; e < 8; ++e) {
+                acc[e] = fma(a0, v[e], acc[e]);
+                acc[8 + e] = fma(a1, v[e], acc[8 + e]);
             }
         }
     } else {
-#pragma unroll 2
-        for (int s = q.s0; s < q.s1; ++s) {
+        for (; s + U <= q.s1; s += U) {
+            uint4 p0[U], p1[U];
+            double a0[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint4* wr = reinterpret_cast<const uint4*>(wide + (int64_t)(s + u) * q.wide_stride);
+                p0[u] = __ldg(wr);
+                p1[u] = __ldg(wr + 1);
+                a0[u] = __ldg(small + (int64_t)(s + u) * q.small_stride);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                unpack8(p0[u], v);
+                unpack8(p1[u], v + 8);
+#pragma unroll
+                for (int e = 0; e < 16; ++e) acc[e] = fma(a0[u], v[e], acc[e]);
+            }
+        }
+        for (; s < q.s1; ++s) {
             const uint4* wr = reinterpret_cast<const uint4*>(wide + (int64_t)s * q.wide_stride);
             const uint4 p0 = __ldg(wr), p1 = __ldg(wr + 1);
             const double a0 = __ldg(small + (int64_t)s * q.small_stride);
             unpack8(p0, v);
             unpack8(p1, v + 8);
 #pragma unroll
-            for (int u = 0; u < 16; ++u) acc[u] = fma(a0, v[u], acc[u]);
+            for (int e = 0; e < 16; ++e) acc[e] = fma(a0, v[e], acc[e]);
         }
     }
 #pragma unroll
@@ -800,38 +875,55 @@ __device__ __forceinline__ double term_value(const FoldTerm& f, const double* qs
     return yh < (uint32_t)H1h ? VR[(size_t)yh * KR + f.off + yl] : 0.0;  // Q_t = V_t
 }
 
-// phase 2: q(rep r) = sum_{y in O(r)} sum_t Q_t[y] / (|O(r)| C Z); ln q with
-// the reference's 0 for q == 0 (backend/BAA.cu:573-580), expanded to every
-// y, and copied into RB / LA where a D-side product is the identity.
-__global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ qsum,
-                         const double* __restrict__ ULt, int KL, const double* __restrict__ VR, int KR, int H1h,
-                         int k, double inv_c, double* __restrict__ lnq_full, double* __restrict__ lnq,
-                         double* __restrict__ RB, int H2, double* __restrict__ LA, int Kp, const DevState* st) {
+// phase 2: acc[y] = sum_t Q_t[y] (one thread per y)
+__global__ void k_fold_acc(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ qsum,
+                           const double* __restrict__ ULt, int KL, const double* __restrict__ VR, int KR, int H1h,
+                           int k, double* __restrict__ acc, const DevState* st) {
     if (gated(st)) return;
     const int ny = 1 << k;
+    const int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= ny) return;
+    double a = 0.0;
+    for (int t = 0; t < T; ++t) a += term_value(terms[t], qsum, t, ny, ULt, KL, VR, KR, H1h, (uint32_t)y);
+    acc[y] = a;
+}
+
+// phase 3: q(rep r) = sum_{y in O(r)} acc[y] / (|O(r)| C Z); ln q with the
+// reference's 0 for q == 0 (backend/BAA.cu:573-580), expanded to every y,
+// and copied into RB / LA where a D-side product is the identity.
+__global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ accv, int k,
+                         double inv_c, double* __restrict__ lnq_full, double* __restrict__ lnq, double* __restrict__ RB,
+                         int H2, double* __restrict__ LA, int Kp, int KL, int H1h, const DevState* st) {
+    if (gated(st)) return;
+    const int ny = 1 << k;
+    const int y = blockIdx.x * blockDim.x + threadIdx.x;
+    if (y >= ny) return;
     const double inv_z = exp(-st->log_z);
-    for (int y = blockIdx.x * blockDim.x + threadIdx.x; y < ny; y += gridDim.x * blockDim.x) {
-        const uint32_t r = orbit_rep((uint32_t)y, k);
-        const uint32_t rv = reverse_bits(r, k), cv = complement_bits(r, k), rcv = reverse_bits(cv, k);
-        uint32_t mem[4];
-        int nm = 0;
-        mem[nm++] = r;
-        if (rv != r) mem[nm++] = rv;
-        if (cv != r && cv != rv) mem[nm++] = cv;
-        if (rcv != r && rcv != rv && rcv != cv) mem[nm++] = rcv;
-        double acc = 0.0;
-        for (int e = 0; e < nm; ++e)
-            for (int t = 0; t < T; ++t) acc += term_value(terms[t], qsum, t, ny, ULt, KL, VR, KR, H1h, mem[e]);
-        const double q = acc * inv_c * inv_z / (double)nm;
-        const double lq = (q != 0.0) ? log(q) : 0.0;
-        lnq_full[y] = lq;
-        if ((uint32_t)y == r) lnq[y] = lq;  // representatives are < 2^{k-1}
-        for (int t = 0; t < T; ++t) {
-            const FoldTerm& f = terms[t];
-            const uint32_t yh = (uint32_t)y >> f.m, yl = (uint32_t)y & ((1u << f.m) - 1u);
-            if (f.idB_left) RB[(size_t)(f.off + yh) * H2 + reverse_bits(yl, f.m)] = lq;  // M_t = Lq_t
-            if (f.idA_right && yh < (uint32_t)H1h) LA[(size_t)yh * Kp + KL + f.off + yl] = lq;  // N_t = Lq_t
-        }
+    const uint32_t r = orbit_rep((uint32_t)y, k);
+    const uint32_t rv = reverse_bits(r, k), cv = complement_bits(r, k), rcv = reverse_bits(cv, k);
+    double acc = accv[r];
+    int nm = 1;
+    if (rv != r) {
+        acc += accv[rv];
+        ++nm;
+    }
+    if (cv != r && cv != rv) {
+        acc += accv[cv];
+        ++nm;
+    }
+    if (rcv != r && rcv != rv && rcv != cv) {
+        acc += accv[rcv];
+        ++nm;
+    }
+    const double q = acc * inv_c * inv_z / (double)nm;
+    const double lq = (q != 0.0) ? log(q) : 0.0;
+    lnq_full[y] = lq;
+    if ((uint32_t)y == r) lnq[y] = lq;  // representatives are < 2^{k-1}
+    for (int t = 0; t < T; ++t) {
+        const FoldTerm& f = terms[t];
+        const uint32_t yh = (uint32_t)y >> f.m, yl = (uint32_t)y & ((1u << f.m) - 1u);
+        if (f.idB_left) RB[(size_t)(f.off + yh) * H2 + reverse_bits(yl, f.m)] = lq;  // M_t = Lq_t
+        if (f.idA_right && yh < (uint32_t)H1h) LA[(size_t)yh * Kp + KL + f.off + yl] = lq;  // N_t = Lq_t
     }
 }
 
@@ -1077,10 +1169,12 @@ static Operand k_offset(Operand o, bool is_a, int64_t k0) {
     return o;
 }
 
-// S products over consecutive slices of the contraction, output s at C + s * cstride
+// S products over consecutive slices of the contraction, output s at C + s * cstride;
+// slice boundaries are multiples of 16 (whole k-slices, aligned operands)
 static void split_k(std::vector<GemmDesc>& out, const GemmDesc& d, int S, int64_t cstride) {
     for (int s = 0; s < S; ++s) {
-        const int64_t k0 = (int64_t)d.K * s / S, k1 = (int64_t)d.K * (s + 1) / S;
+        const int64_t k0 = ((int64_t)d.K * s / S) & ~(int64_t)15;
+        const int64_t k1 = (s + 1 == S) ? d.K : (((int64_t)d.K * (s + 1) / S) & ~(int64_t)15);
         GemmDesc e = d;
         e.A = k_offset(d.A, true, k0);
         e.B = k_offset(d.B, false, k0);
@@ -1108,9 +1202,26 @@ static void free_launch(Launch& L) {
     L.map = nullptr;
 }
 
+// the cp.async layout of a list of products, or -1 when a product does not
+// qualify (an operand that is not FP64, an odd leading dimension or a base
+// that is not 16-byte aligned) or the layouts differ
+static int cp_layout(const std::vector<GemmDesc>& v) {
+    int lay = -2;
+    for (const auto& d : v) {
+        if (d.A.kind != OP_F64 || d.B.kind != OP_F64) return -1;
+        if ((d.A.ld & 1) || (d.B.ld & 1)) return -1;
+        if (((uintptr_t)d.A.ptr & 15) || ((uintptr_t)d.B.ptr & 15)) return -1;
+        const int l = (d.A.trans ? 1 : 0) | (d.B.trans ? 0 : 2);
+        if (lay == -2) lay = l;
+        else if (lay != l) return -1;
+    }
+    return lay < 0 ? -1 : lay;
+}
+
 static cudaError_t make_launch(Launch& L, std::vector<GemmDesc> v, int cfg) {
     free_launch(L);
     L.cfg = cfg;
+    L.layout = cp_layout(v);
     L.n = (int)v.size();
     L.tiles = assign_tiles(v, cfg);
     if (v.empty()) return cudaSuccess;
@@ -1151,6 +1262,7 @@ static float time_ms(bdc_handle* H, F&& launch) {
 static cudaError_t make_tile_launch(Launch& L, GemmDesc d, int cfg, const std::vector<int>& colmax) {
     free_launch(L);
     L.cfg = cfg;
+    L.layout = cp_layout({d});
     L.n = 1;
     const int BM = kCfgBM[cfg], BN = kCfgBN[cfg];
     d.tiles_m = (d.M + BM - 1) / BM;
@@ -1465,6 +1577,7 @@ bdc_status factored_init(bdc_handle* H) {
                 int kb = 0;
                 for (int c = n0; c < n0 + nb; ++c) kb = std::max(kb, F->colmax[c] + 1);
                 if (kb == 0) continue;
+                kb = std::min(H1, (kb + 15) & ~15);  // rows past the last representative are zero
                 GemmDesc d = make_desc(op_f64(F->LA, Kp, 1), op_f64(F->Pw + n0, H2, 0), F->ulpart + (int64_t)n0 * KL,
                                        1, KL, KL, nb, kb);
                 split_k(v, d, std::max(1, (int)(((int64_t)S * kb + H1 - 1) / H1)), (int64_t)H2 * KL);
@@ -1488,7 +1601,9 @@ bdc_status factored_init(bdc_handle* H) {
                         chi = c;
                     }
                 if (chi < 0) continue;
-                const int kb = chi + 1 - clo;
+                // whole k-slices; the columns added at either end are zero in these rows
+                clo &= ~15;
+                const int kb = std::min(H2, (chi + 1 + 15) & ~15) - clo;
                 const Operand A = k_offset(op_f64(F->Pw + (int64_t)m0 * H2, H2, 0), true, clo);
                 const Operand B = k_offset(op_f64(F->RB + (int64_t)KL * H2, H2, 1), false, clo);
                 GemmDesc d = make_desc(A, B, F->vrpart + (int64_t)m0 * KR, KR, 1, mb, KR, kb);
@@ -1588,6 +1703,7 @@ bdc_status factored_init(bdc_handle* H) {
     for (auto& qp : qplan) qelems += (int64_t)QS * ny;
     BDC_CUDA_TRY(al(&F->qparts, (size_t)std::max<int64_t>(qelems, 1)));
     BDC_CUDA_TRY(al(&F->qsum, (size_t)F->T * ny));
+    BDC_CUDA_TRY(al(&F->qacc, (size_t)ny));
     BDC_CUDA_TRY(cudaMemsetAsync(F->qparts, 0, sizeof(double) * std::max<int64_t>(qelems, 1), H->stream));
     int64_t qo = 0;
     for (auto& qp : qplan) {
@@ -1801,9 +1917,18 @@ bdc_status factored_init(bdc_handle* H) {
         BDC_CUDA_TRY(cudaMemsetAsync(F->ulpart, 0, sizeof(double) * max_split * H2 * KLa, H->stream));
         BDC_CUDA_TRY(cudaMemsetAsync(F->vrpart, 0, sizeof(double) * max_split * H1 * KRa, H->stream));
     }
-    int nthin = 0;
-    for (int lg = 0; lg < 8; ++lg) nthin += (F->n_thinq[lg] > 0) + (F->n_thind[lg] > 0);
-    F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + nthin + 2 + 1 + 1;
+    int nq = 0, nd = 0;
+    for (int lg = 0; lg < 8; ++lg) {
+        nq += F->n_thinq[lg] > 0;
+        nd += F->n_thind[lg] > 0;
+    }
+    if (F->use_qf) nq = 1;
+    if (F->use_df) {
+        nd = 0;
+        for (int cl = 0; cl < 4; ++cl) nd += F->n_df[cl] > 0;
+    }
+    // U, V, the split sums; q-side terms; three fold kernels; D-side terms; G; finalize
+    F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + nq + 3 + nd + 1 + 1;
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
 }
@@ -1812,7 +1937,7 @@ void factored_free(bdc_handle* H) {
     FactoredState* F = H->fac;
     if (!F) return;
     for (double* p : {F->Pw, F->Lt, F->hx, F->LA, F->RB, F->UL, F->VR, F->ulpart, F->vrpart, F->qparts,
-                      F->qsum, F->lnq_full, F->epart})
+                      F->qsum, F->qacc, F->lnq_full, F->epart})
         cudaFree(p);
     cudaFree(F->Bp);
     cudaFree(F->Ddense);
@@ -1889,9 +2014,10 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             const int ny = 1 << H->k;
             const int nqs = (F->T * ny + 255) / 256;
             k_qsum<<<nqs < 4096 ? nqs : 4096, 256, 0, s>>>(F->d_fold, F->T, F->qparts, H->k, F->qsum, H->d_st);
-            k_fold_q<<<(ny + 63) / 64, 64, 0, s>>>(F->d_fold, F->T, F->qsum, F->UL, F->KL, F->VR, F->KR, F->H1h, H->k,
-                                                  H->inv_c, F->lnq_full, H->d_lnq, F->RB, F->H2, F->LA, F->Kp,
-                                                  H->d_st);
+            k_fold_acc<<<(ny + 127) / 128, 128, 0, s>>>(F->d_fold, F->T, F->qsum, F->UL, F->KL, F->VR, F->KR,
+                                                         F->H1h, H->k, F->qacc, H->d_st);
+            k_fold_q<<<(ny + 127) / 128, 128, 0, s>>>(F->d_fold, F->T, F->qacc, H->k, H->inv_c, F->lnq_full,
+                                                       H->d_lnq, F->RB, F->H2, F->LA, F->Kp, F->KL, F->H1h, H->d_st);
             break;
         }
         case ST_DSMALL:

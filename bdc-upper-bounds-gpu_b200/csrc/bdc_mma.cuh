@@ -148,3 +148,137 @@ constexpr int mma_smem_bytes() {
 }
 
 }  // namespace bdc
+
+namespace bdc {
+
+// ---------------------------------------------------------------------------
+// Multi-stage variant for FP64 operands: tiles move global -> shared memory by
+// cp.async (16-byte pieces, zero-filled past the operand's edge), STAGES deep,
+// so that several k-slices are in flight without staging registers.  Each
+// operand keeps its global orientation in shared memory:
+//   AK: A k-major [BK][BM+4] (A contiguous along m) or m-major [BM][BK+4]
+//   BKM: B k-major [BK][BN+4] (B contiguous along n) or n-major [BN][BK+4]
+// Requirements (checked by the host): both operands FP64, 16-byte aligned
+// bases, even leading dimensions and even contraction offsets.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <int BM, int BN, bool AK, bool BKM>
+struct CpCfg {
+    static constexpr int BK = 16;
+    static constexpr int PK = BK + 4;
+    static constexpr int A_ELEMS = AK ? BK * (BM + 4) : BM * PK;
+    static constexpr int B_ELEMS = BKM ? BK * (BN + 4) : BN * PK;
+    static constexpr int STAGE = A_ELEMS + B_ELEMS;
+};
+
+template <int BM, int BN, int WM, int WN, bool AK, bool BKM, int STAGES>
+constexpr int mma_cp_smem_bytes() {
+    return (int)sizeof(double) * STAGES * CpCfg<BM, BN, AK, BKM>::STAGE;
+}
+
+// one k-slice [k0, k0 + 16) of A and B into one stage
+template <int BM, int BN, bool AK, bool BKM>
+__device__ __forceinline__ void cp_stage(const GemmDesc& d, int m0, int n0, int k0, double* As, double* Bs) {
+    using C = CpCfg<BM, BN, AK, BKM>;
+    const double* A = (const double*)d.A.ptr;
+    const double* B = (const double*)d.B.ptr;
+    const int64_t lda = d.A.ld, ldb = d.B.ld;
+    const int M = d.M, N = d.N, K = d.K;
+    if (AK) {  // BK rows of BM doubles, pieces of two along m
+        constexpr int PIECES = C::BK * BM / 2;
+        for (int e = threadIdx.x; e < PIECES; e += 256) {
+            const int kk = e / (BM / 2), mm = (e % (BM / 2)) * 2;
+            const int k = k0 + kk, m = m0 + mm;
+            const int bytes = (k < K) ? (m + 1 < M ? 16 : (m < M ? 8 : 0)) : 0;
+            cp_async16(As + kk * (BM + 4) + mm, bytes ? A + (int64_t)k * lda + m : A, bytes);
+        }
+    } else {  // BM rows of BK doubles, pieces of two along k
+        constexpr int PIECES = BM * C::BK / 2;
+        for (int e = threadIdx.x; e < PIECES; e += 256) {
+            const int mm = e / (C::BK / 2), kk = (e % (C::BK / 2)) * 2;
+            const int k = k0 + kk, m = m0 + mm;
+            const int bytes = (m < M) ? (k + 1 < K ? 16 : (k < K ? 8 : 0)) : 0;
+            cp_async16(As + mm * C::PK + kk, bytes ? A + (int64_t)m * lda + k : A, bytes);
+        }
+    }
+    if (BKM) {
+        constexpr int PIECES = C::BK * BN / 2;
+        for (int e = threadIdx.x; e < PIECES; e += 256) {
+            const int kk = e / (BN / 2), nn = (e % (BN / 2)) * 2;
+            const int k = k0 + kk, n = n0 + nn;
+            const int bytes = (k < K) ? (n + 1 < N ? 16 : (n < N ? 8 : 0)) : 0;
+            cp_async16(Bs + kk * (BN + 4) + nn, bytes ? B + (int64_t)k * ldb + n : B, bytes);
+        }
+    } else {
+        constexpr int PIECES = BN * C::BK / 2;
+        for (int e = threadIdx.x; e < PIECES; e += 256) {
+            const int nn = e / (C::BK / 2), kk = (e % (C::BK / 2)) * 2;
+            const int k = k0 + kk, n = n0 + nn;
+            const int bytes = (n < N) ? (k + 1 < K ? 16 : (k < K ? 8 : 0)) : 0;
+            cp_async16(Bs + nn * C::PK + kk, bytes ? B + (int64_t)n * ldb + k : B, bytes);
+        }
+    }
+}
+
+template <int BM, int BN, int WM, int WN, bool AK, bool BKM, int STAGES>
+__device__ __forceinline__ void mma_mainloop_cp(const GemmDesc& d, int m0, int n0, double* smem,
+                                                double (&acc)[MmaCfg<BM, BN, WM, WN>::MT][MmaCfg<BM, BN, WM, WN>::NT][2]) {
+    using M_ = MmaCfg<BM, BN, WM, WN>;
+    using C = CpCfg<BM, BN, AK, BKM>;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm0 = (warp / WN) * (8 * M_::MT), wn0 = (warp % WN) * (8 * M_::NT);
+#pragma unroll
+    for (int i = 0; i < M_::MT; ++i)
+#pragma unroll
+        for (int j = 0; j < M_::NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    const int nk = (d.K + C::BK - 1) / C::BK;
+#pragma unroll
+    for (int st = 0; st < STAGES - 1; ++st) {
+        if (st < nk) cp_stage<BM, BN, AK, BKM>(d, m0, n0, st * C::BK, smem + st * C::STAGE, smem + st * C::STAGE + C::A_ELEMS);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();
+        {
+            const int nx = kt + STAGES - 1;
+            if (nx < nk) {
+                double* s = smem + (nx % STAGES) * C::STAGE;
+                cp_stage<BM, BN, AK, BKM>(d, m0, n0, nx * C::BK, s, s + C::A_ELEMS);
+            }
+            cp_async_commit();
+        }
+        const double* as = smem + (kt % STAGES) * C::STAGE;
+        const double* bs = as + C::A_ELEMS;
+#pragma unroll
+        for (int kq = 0; kq < C::BK / 4; ++kq) {
+            double a[M_::MT], b[M_::NT];
+            const int kr = kq * 4 + t;
+#pragma unroll
+            for (int i = 0; i < M_::MT; ++i) {
+                const int m = wm0 + i * 8 + g;
+                a[i] = AK ? as[kr * (BM + 4) + m] : as[m * C::PK + kr];
+            }
+#pragma unroll
+            for (int j = 0; j < M_::NT; ++j) {
+                const int n = wn0 + j * 8 + g;
+                b[j] = BKM ? bs[kr * (BN + 4) + n] : bs[n * C::PK + kr];
+            }
+#pragma unroll
+            for (int i = 0; i < M_::MT; ++i)
+#pragma unroll
+                for (int j = 0; j < M_::NT; ++j) mma_f64(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+}
+
+}  // namespace bdc
