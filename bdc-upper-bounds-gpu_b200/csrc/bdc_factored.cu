@@ -647,9 +647,9 @@ __global__ void __launch_bounds__(1024) k_qthin(const ThinQ* __restrict__ descs,
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0.0;
     double v[16];
-    // four table rows in flight per thread: their loads are issued before
+    // several table rows in flight per thread: their loads are issued before
     // any of them is used
-    constexpr int U = 4;
+    constexpr int U = 8;
     int s = q.s0;
     if (IT == 2) {
         for (; s + U <= q.s1; s += U) {
@@ -1806,7 +1806,7 @@ bdc_status factored_init(bdc_handle* H) {
                 f.out_s = d.out_s;
                 f.out_i = d.out_i;
                 f.IT = std::min(d.SMALL, 8);
-                f.LPR = std::max(1, std::min(32, d.WIDE / 64));
+                f.LPR = std::max(1, std::min(32, d.WIDE / 32));
                 const int ng = d.SMALL / f.IT;
                 if (f.LPR * ng > 256) dok = false;
                 const int rows_per_cta = (256 / (f.LPR * ng)) * kDfRT;
@@ -2505,7 +2505,8 @@ bdc_status factored_profile(bdc_handle* H, int iters, bdc_profile_t* out) {
     out->ms_update = acc[ST_FIN] / iters;
     out->ms_iter = tot / iters;
     out->ms_main = acc[ST_G] / iters;
-    out->work_main = 2.0 * (double)F->H1h * (double)F->H2 * (double)(F->KL + F->KR);
+    // algorithmic work of G: one K-long dot product per representative
+    out->work_main = 2.0 * (double)H->R * (double)(F->KL + F->KR);
     out->launches = F->launches_per_iter;
     out->iters = iters;
     return BDC_OK;

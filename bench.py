@@ -273,9 +273,9 @@ def ours_arm(args) -> None:
                     "kernel": "k_mma_ba (G = [A_L | N_R] [M_L ; B_R^T] on FP64 mma.sync, BA update in the epilogue)",
                     "achieved": achieved / 1e12, "peak": 2 * dmma / 1e12, "unit": "TFLOP/s",
                     "frac": achieved / (2 * dmma), "traffic": profile_traffic("k_mma_ba", args.n, args.k),
-                    "work_per_launch": f"2*H1h*H2*K = {prof['work_main']:.4e} flops "
-                                       f"(H1h = {1 << ((args.n + 1) // 2 - 1)}, H2 = {1 << (args.n // 2)}, "
-                                       f"K = sum of the split-term widths)",
+                    "work_per_launch": f"2*R*K = {prof['work_main']:.4e} flops: one K-long dot product per "
+                                       f"representative (R = {R}, K = sum of the split-term widths); the "
+                                       f"launch executes the tiles that hold representatives, 1.07x that",
                     "peak_source": "bdc_peak_probe FP64 mma.sync m8n8k4 chains on all SMs, measured in this "
                                    "run (2 flops per multiply-add); MEASURED_PEAKS.json holds no FP64 figure"}
     upd_bytes = R * 72
