@@ -151,7 +151,7 @@ struct FactoredState {
     bool use_mq[8] = {}, use_md[8] = {};
     // all per-term products of a side in one launch (used when faster)
     bdc::ThinQ* d_qf = nullptr;
-    int n_qf = 0;
+    int n_qf = 0, qf_stage = 0;
     bdc::ThinDF* d_df[4] = {};  // by log2 IT
     int n_df[4] = {};
     bool use_qf = false, use_df = false;
@@ -632,86 +632,92 @@ __device__ __forceinline__ void unpack8(const uint4 p, double* v) {
     v[7] = (double)(p.w >> 16);
 }
 
-__global__ void __launch_bounds__(1024) k_qthin(const ThinQ* __restrict__ descs, const DevState* st) {
+// The slice's rows stream through shared memory with cp.async, kQtRows rows a
+// stage and kQtStages stages in flight (the table rows are 16-byte pieces,
+// the small rows 8-byte ones since their stride is odd), so that the CTA keeps
+// tens of kilobytes of loads outstanding without holding them in registers.
+constexpr int kQtRows = 8;
+constexpr int kQtStages = 3;
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+
+__global__ void __launch_bounds__(256) k_qthin(const ThinQ* __restrict__ descs, int stage_bytes, const DevState* st) {
     if (gated(st)) return;
+    extern __shared__ __align__(16) uint8_t qsm[];
     const ThinQ& q = descs[blockIdx.x];
     const int IT = q.SMALL >= 2 ? 2 : 1;
     const int WT = 16 / IT;
     const int nwb = q.WIDE / WT;
-    const int wb = threadIdx.x % nwb, ib = threadIdx.x / nwb;
+    const int tid = threadIdx.x;
+    const int wb = tid % nwb, ib = tid / nwb;
     const int i0 = ib * IT, w0 = wb * WT;
-    if (i0 >= q.SMALL) return;
-    const uint16_t* wide = (const uint16_t*)q.wide + w0;
-    const double* small = (const double*)q.small + i0;
+    const uint16_t* wide = (const uint16_t*)q.wide;
+    const double* small = (const double*)q.small;
+    const int wpieces = q.WIDE / 8;              // 16-byte pieces per table row
+    const int wbytes = q.WIDE * 2, sbytes = q.SMALL * 8;
+    const int rows = q.s1 - q.s0;
+    const int nst = (rows + kQtRows - 1) / kQtRows;
+    auto issue = [&](int stg) {
+        uint8_t* base = qsm + (stg % kQtStages) * stage_bytes;
+        const int r0 = q.s0 + stg * kQtRows;
+        const int nr = min(kQtRows, q.s1 - r0);
+        for (int e = tid; e < nr * wpieces; e += blockDim.x) {
+            const int r = e / wpieces, c = e % wpieces;
+            cp_async16(base + r * wbytes + c * 16, wide + (int64_t)(r0 + r) * q.wide_stride + c * 8, 16);
+        }
+        uint8_t* sb = base + kQtRows * wbytes;
+        for (int e = tid; e < nr * q.SMALL; e += blockDim.x) {
+            const int r = e / q.SMALL, c = e % q.SMALL;
+            cp_async8(sb + r * sbytes + c * 8, small + (int64_t)(r0 + r) * q.small_stride + c);
+        }
+    };
     double acc[16];
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+#pragma unroll
+    for (int p = 0; p < kQtStages - 1; ++p) {
+        if (p < nst) issue(p);
+        cp_async_commit();
+    }
     double v[16];
-    // several table rows in flight per thread: their loads are issued before
-    // any of them is used
-    constexpr int U = 8;
-    int s = q.s0;
-    if (IT == 2) {
-        for (; s + U <= q.s1; s += U) {
-            uint4 pk[U];
-            double a0[U], a1[U];
+    for (int stg = 0; stg < nst; ++stg) {
+        cp_async_wait<kQtStages - 2>();
+        __syncthreads();
+        if (stg + kQtStages - 1 < nst) issue(stg + kQtStages - 1);
+        cp_async_commit();
+        const uint8_t* base = qsm + (stg % kQtStages) * stage_bytes;
+        const double* sb = reinterpret_cast<const double*>(base + kQtRows * wbytes);
+        const int nr = min(kQtRows, q.s1 - (q.s0 + stg * kQtRows));
+        if (i0 < q.SMALL) {
+            if (IT == 2) {
+                for (int r = 0; r < nr; ++r) {
+                    const uint4 pk = *reinterpret_cast<const uint4*>(base + r * wbytes + w0 * 2);
+                    const double a0 = sb[r * q.SMALL + i0], a1 = sb[r * q.SMALL + i0 + 1];
+                    unpack8(pk, v);
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                pk[u] = __ldg(reinterpret_cast<const uint4*>(wide + (int64_t)(s + u) * q.wide_stride));
-                const double* sr = small + (int64_t)(s + u) * q.small_stride;
-                a0[u] = __ldg(sr);
-                a1[u] = __ldg(sr + 1);
-            }
+                    for (int e = 0; e < 8; ++e) {
+                        acc[e] = fma(a0, v[e], acc[e]);
+                        acc[8 + e] = fma(a1, v[e], acc[8 + e]);
+                    }
+                }
+            } else {
+                for (int r = 0; r < nr; ++r) {
+                    const uint4* wr = reinterpret_cast<const uint4*>(base + r * wbytes + w0 * 2);
+                    const uint4 p0 = wr[0], p1 = wr[1];
+                    const double a0 = sb[r * q.SMALL + i0];
+                    unpack8(p0, v);
+                    unpack8(p1, v + 8);
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                unpack8(pk[u], v);
-#pragma unroll
-                for (int e = 0; e < 8; ++e) {
-                    acc[e] = fma(a0[u], v[e], acc[e]);
-                    acc[8 + e] = fma(a1[u], v[e], acc[8 + e]);
+                    for (int e = 0; e < 16; ++e) acc[e] = fma(a0, v[e], acc[e]);
                 }
             }
         }
-        for (; s < q.s1; ++s) {
-            const uint4 pk = __ldg(reinterpret_cast<const uint4*>(wide + (int64_t)s * q.wide_stride));
-            const double* sr = small + (int64_t)s * q.small_stride;
-            const double a0 = __ldg(sr), a1 = __ldg(sr + 1);
-            unpack8(pk, v);
-#pragma unroll
-            for (int e = 0; e < 8; ++e) {
-                acc[e] = fma(a0, v[e], acc[e]);
-                acc[8 + e] = fma(a1, v[e], acc[8 + e]);
-            }
-        }
-    } else {
-        for (; s + U <= q.s1; s += U) {
-            uint4 p0[U], p1[U];
-            double a0[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint4* wr = reinterpret_cast<const uint4*>(wide + (int64_t)(s + u) * q.wide_stride);
-                p0[u] = __ldg(wr);
-                p1[u] = __ldg(wr + 1);
-                a0[u] = __ldg(small + (int64_t)(s + u) * q.small_stride);
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                unpack8(p0[u], v);
-                unpack8(p1[u], v + 8);
-#pragma unroll
-                for (int e = 0; e < 16; ++e) acc[e] = fma(a0[u], v[e], acc[e]);
-            }
-        }
-        for (; s < q.s1; ++s) {
-            const uint4* wr = reinterpret_cast<const uint4*>(wide + (int64_t)s * q.wide_stride);
-            const uint4 p0 = __ldg(wr), p1 = __ldg(wr + 1);
-            const double a0 = __ldg(small + (int64_t)s * q.small_stride);
-            unpack8(p0, v);
-            unpack8(p1, v + 8);
-#pragma unroll
-            for (int e = 0; e < 16; ++e) acc[e] = fma(a0, v[e], acc[e]);
-        }
     }
+    cp_async_wait<0>();
+    if (i0 >= q.SMALL) return;
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
         const int i = i0 + (IT == 2 ? e / 8 : 0), w = w0 + (IT == 2 ? e % 8 : e);
@@ -755,27 +761,38 @@ __global__ void __launch_bounds__(256) k_dthin(const ThinDF* __restrict__ descs,
     const uint16_t* rowp[kDfRT];
 #pragma unroll
     for (int r = 0; r < kDfRT; ++r) rowp[r] = t.wide + (int64_t)min(r0 + r, t.rows - 1) * t.wide_stride;
-    for (int w8 = lane * 8; w8 < WIDE; w8 += LPR * 8) {
-        uint32_t pk[kDfRT][4];
+    // two chunks of 8 contraction indices per step: both chunks' table loads
+    // are issued before either is used
+    const int step = LPR * 8;
+    for (int w8 = lane * 8; w8 < WIDE; w8 += 2 * step) {
+        const bool two = w8 + step < WIDE;
+        uint32_t pk[2][kDfRT][4];
 #pragma unroll
-        for (int r = 0; r < kDfRT; ++r) {
-            const uint4 q = __ldg(reinterpret_cast<const uint4*>(rowp[r] + w8));
-            pk[r][0] = q.x;
-            pk[r][1] = q.y;
-            pk[r][2] = q.z;
-            pk[r][3] = q.w;
-        }
-        const double* lc = lq + (w8 >> 3) * cs + i0;
+        for (int c = 0; c < 2; ++c)
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            double v[kDfRT];
+            for (int r = 0; r < kDfRT; ++r) {
+                const uint4 q = (c == 0 || two) ? __ldg(reinterpret_cast<const uint4*>(rowp[r] + w8 + c * step))
+                                                : make_uint4(0u, 0u, 0u, 0u);
+                pk[c][r][0] = q.x;
+                pk[c][r][1] = q.y;
+                pk[c][r][2] = q.z;
+                pk[c][r][3] = q.w;
+            }
 #pragma unroll
-            for (int r = 0; r < kDfRT; ++r) v[r] = (double)((pk[r][u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+        for (int c = 0; c < 2; ++c) {
+            if (c == 1 && !two) break;
+            const double* lc = lq + ((w8 + c * step) >> 3) * cs + i0;
 #pragma unroll
-            for (int i = 0; i < IT; ++i) {
-                const double l = lc[u * SMALL + i];
+            for (int u = 0; u < 8; ++u) {
+                double v[kDfRT];
 #pragma unroll
-                for (int r = 0; r < kDfRT; ++r) acc[r][i] = fma(v[r], l, acc[r][i]);
+                for (int r = 0; r < kDfRT; ++r) v[r] = (double)((pk[c][r][u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+#pragma unroll
+                for (int i = 0; i < IT; ++i) {
+                    const double l = lc[u * SMALL + i];
+#pragma unroll
+                    for (int r = 0; r < kDfRT; ++r) acc[r][i] = fma(v[r], l, acc[r][i]);
+                }
             }
         }
     }
@@ -793,8 +810,15 @@ __global__ void __launch_bounds__(256) k_dthin(const ThinDF* __restrict__ descs,
     }
 }
 
-static cudaError_t launch_qthin(const ThinQ* d, int n, int k, cudaStream_t s, const DevState* st) {
-    k_qthin<<<n, (1 << k) / 16, 0, s>>>(d, st);
+// shared memory of k_qthin: the largest term's stage (table rows + small rows)
+static int qthin_stage_bytes(const std::vector<ThinQ>& v) {
+    int m = 0;
+    for (const auto& q : v) m = std::max(m, kQtRows * (q.WIDE * 2 + q.SMALL * 8));
+    return (m + 15) & ~15;
+}
+
+static cudaError_t launch_qthin(const ThinQ* d, int n, int stage_bytes, cudaStream_t s, const DevState* st) {
+    k_qthin<<<n, 256, stage_bytes * kQtStages, s>>>(d, stage_bytes, st);
     return cudaGetLastError();
 }
 
@@ -1333,9 +1357,9 @@ struct TuneFile {
 // chooses tile shape and split of one of the wide q-side products by timing
 // them; gen(cfg, S) lists the descriptors of a candidate (S: the split of
 // the longest contraction, kfull its length)
-template <typename Gen>
-static bdc_status tune_thin(bdc_handle* H, TuneFile& tf, const char* key, Launch& L, Gen&& gen, int kfull,
-                            int max_split, int kmin, const char* what, int* split_out) {
+template <typename Gen, typename Post>
+static bdc_status tune_thin(bdc_handle* H, TuneFile& tf, const char* key, Launch& L, Gen&& gen, Post&& post,
+                            int kfull, int max_split, int kmin, const char* what, int* split_out) {
     const int cfgs[4] = {CFG_128x128, CFG_128x64, CFG_64x128, CFG_64x64};
     float best = 1e30f;
     int best_cfg = CFG_64x64, best_s = 1;
@@ -1350,7 +1374,11 @@ static bdc_status tune_thin(bdc_handle* H, TuneFile& tf, const char* key, Launch
                 free_launch(T);
                 continue;
             }
-            const float ms = time_ms(H, [&] { launch_store(T, H->stream, nullptr); });
+            // the product and the sum of its S split slices
+            const float ms = time_ms(H, [&] {
+                launch_store(T, H->stream, nullptr);
+                post(S);
+            });
             free_launch(T);
             if (ms < best) {
                 best = ms;
@@ -1584,7 +1612,11 @@ bdc_status factored_init(bdc_handle* H) {
             }
             return v;
         };
-        bdc_status rc = tune_thin(H, tf, "ul", F->ul, gen, H1, max_split, 16, "U = AL^T Pw", &F->S1);
+        auto post = [&](int S) {
+            k_sum_parts<<<H->num_sms * 4, 256, 0, H->stream>>>(F->ulpart, S, (int64_t)KL * H2, F->UL, F->vrpart, 1, 0,
+                                                               F->VR, nullptr);
+        };
+        bdc_status rc = tune_thin(H, tf, "ul", F->ul, gen, post, H1, max_split, 16, "U = AL^T Pw", &F->S1);
         if (rc != BDC_OK) return rc;
     }
     if (KR > 0) {
@@ -1611,7 +1643,11 @@ bdc_status factored_init(bdc_handle* H) {
             }
             return v;
         };
-        bdc_status rc = tune_thin(H, tf, "vr", F->vr, gen, H2, max_split, 16, "V = Pw BR", &F->S2);
+        auto post = [&](int S) {
+            k_sum_parts<<<H->num_sms * 4, 256, 0, H->stream>>>(F->ulpart, 1, 0, F->UL, F->vrpart, S,
+                                                               (int64_t)H1 * KR, F->VR, nullptr);
+        };
+        bdc_status rc = tune_thin(H, tf, "vr", F->vr, gen, post, H2, max_split, 16, "V = Pw BR", &F->S2);
         if (rc != BDC_OK) return rc;
     }
 
@@ -1780,7 +1816,9 @@ bdc_status factored_init(bdc_handle* H) {
     // times them faster than the per-class launches.  They need 16-byte
     // aligned table rows of >= 16 entries and 2^k / 16 >= 32 threads.
     {
-        bool qok = k >= 9 && k <= 14, dok = k >= 9 && k <= 14;
+        // (the q kernel runs 256 threads, one per 16 outputs at k = 12 and
+        // fewer busy ones below)
+        bool qok = k >= 9 && k <= 12, dok = k >= 9 && k <= 14;
         std::vector<ThinQ> all_q;
         for (int lg = 0; lg < 8; ++lg)
             for (auto& q : tq[lg]) {
@@ -1822,6 +1860,9 @@ bdc_status factored_init(bdc_handle* H) {
         tf.get("df", &pinned_d, &unused);
         BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
         if (qok && !all_q.empty()) {
+            F->qf_stage = qthin_stage_bytes(all_q);
+            BDC_CUDA_TRY(cudaFuncSetAttribute(k_qthin, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              F->qf_stage * kQtStages));
             BDC_CUDA_TRY(cudaMalloc(&F->d_qf, sizeof(ThinQ) * all_q.size()));
             BDC_CUDA_TRY(cudaMemcpy(F->d_qf, all_q.data(), sizeof(ThinQ) * all_q.size(), cudaMemcpyHostToDevice));
             F->n_qf = (int)all_q.size();
@@ -1829,7 +1870,7 @@ bdc_status factored_init(bdc_handle* H) {
                 F->use_qf = pinned_q != 0;
             } else {
                 const float tc = time_ms(H, [&] { enqueue_stage(H, ST_QSMALL, -INFINITY); });
-                const float tfu = time_ms(H, [&] { launch_qthin(F->d_qf, F->n_qf, k, H->stream, nullptr); });
+                const float tfu = time_ms(H, [&] { launch_qthin(F->d_qf, F->n_qf, F->qf_stage, H->stream, nullptr); });
                 F->use_qf = tfu < tc;
                 tf.put("qf", F->use_qf ? 1 : 0, 0);
                 if (H->verbose)
@@ -1997,7 +2038,7 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             break;
         }
         case ST_QSMALL:
-            if (F->use_qf) return launch_qthin(F->d_qf, F->n_qf, H->k, s, H->d_st);
+            if (F->use_qf) return launch_qthin(F->d_qf, F->n_qf, F->qf_stage, s, H->d_st);
             // fork: each size class on its own branch, joined before the fold
             if ((e = cudaEventRecord(F->ev_fork, s)) != cudaSuccess) return e;
             for (int lg = 0; lg < 8; ++lg) {
