@@ -189,11 +189,34 @@ bdc_status bdc_accelerate(bdc_handle_t H, int64_t max_evals, double gap_bits, bd
     return factored_accelerate(H, max_evals, gap_bits, stats);
 }
 
+// The factored engine evaluates I(p;W) and D(x) with one BA map (the G
+// product's epilogue yields both); the map advances the dense iterate, which
+// is then reloaded from p so that the handle still holds p.
+static bdc_status factored_eval(bdc_handle_t H, bool with_d) {
+    const double* cur = nullptr;
+    bdc_status rc = engine_current_p(H, &cur);  // p in d_p[0]
+    if (rc != BDC_OK) return rc;
+    rc = factored_map(H, H->d_p[0], H->d_p[1], with_d ? H->d_d : nullptr);
+    if (rc != BDC_OK) return rc;
+    const double rate = H->h_st->rate;
+    rc = engine_after_set_p(H);
+    H->h_st->rate = rate;
+    return rc;
+}
+
 bdc_status bdc_mi_forward(bdc_handle_t H, const double* p, int64_t R, double* I_nats) {
     if (!H || !I_nats) return fail(BDC_ERR_ARG, "bdc_mi_forward: NULL argument");
     if (p) {
         bdc_status rc = bdc_set_p(H, p, R);
         if (rc != BDC_OK) return rc;
+    }
+    if (H->engine == BDC_ENGINE_FACTORED) {
+        if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_mi_forward: no distribution set");
+        cudaSetDevice(H->device);
+        bdc_status rc = factored_eval(H, false);
+        if (rc != BDC_OK) return rc;
+        *I_nats = H->h_st->rate;
+        return BDC_OK;
     }
     return bdc_rate(H, I_nats);
 }
@@ -203,9 +226,13 @@ bdc_status bdc_mi_backward(bdc_handle_t H, double* grad, int64_t R) {
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_mi_backward: %lld slots for %lld representatives", (long long)R, (long long)H->R);
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_mi_backward: no distribution set");
     cudaSetDevice(H->device);
-    bdc_status rc = engine_log_q(H);
-    if (rc != BDC_OK) return rc;
-    rc = engine_divergence(H);
+    bdc_status rc = BDC_OK;
+    if (H->engine == BDC_ENGINE_FACTORED) {
+        rc = factored_eval(H, true);
+    } else {
+        rc = engine_log_q(H);
+        if (rc == BDC_OK) rc = engine_divergence(H);
+    }
     if (rc != BDC_OK) return rc;
     BDC_CUDA_TRY(launch_mi_grad(H->n, H->d_reps, H->R, H->d_d, H->d_logw, H->stream));
     BDC_CUDA_TRY(cudaMemcpyAsync(grad, H->d_logw, sizeof(double) * R, cudaMemcpyDeviceToHost, H->stream));

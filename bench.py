@@ -472,6 +472,57 @@ def batched(args) -> dict | None:
     return out if rank == 0 else None
 
 
+def adjoint_check(args) -> dict:
+    """The adjoint at (n, k) (default 26/13): for each of `fd_seeds` Dirichlet(1)
+    starts, dI/dp from bdc_mi_backward against central differences of
+    bdc_mi_forward with h = 1e-7 on `fd_coords` seeded coordinates; the
+    iterate moves device to device (bdc_set_p_device), one coordinate at a
+    time.  Reports the largest error relative to max(1, |dI/dp|) and the time
+    of one forward and one backward evaluation."""
+    import torch
+
+    import bdc_b200
+    from bdc_b200 import dist as bdist
+
+    h = 1e-7
+    E = bdc_b200.Engine(args.n, args.k, engine="factored")
+    stream = torch.cuda.current_stream()
+    E.set_stream(stream.cuda_stream)
+    out = {"n": args.n, "k": args.k, "h": h, "coords_per_seed": args.fd_coords, "seeds": args.fd_seeds,
+           "max_rel_err": 0.0, "per_seed": []}
+    t_fwd, t_bwd = [], []
+    for seed in range(args.fd_seeds):
+        p = torch.from_numpy(bdist.dirichlet_start(args.n, 1.0, seed)).cuda()
+        E.set_p_device(p.data_ptr())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g = E.mi_backward()
+        t_bwd.append(time.perf_counter() - t0)
+        rng = np.random.default_rng(seed)
+        idx = rng.choice(E.R, args.fd_coords, replace=False)
+        worst = 0.0
+        for i in idx:
+            i = int(i)
+            v = float(p[i])
+            p[i] = v + h
+            E.set_p_device(p.data_ptr())
+            t0 = time.perf_counter()
+            ip = E.mi_forward(None)
+            t_fwd.append(time.perf_counter() - t0)
+            p[i] = v - h
+            E.set_p_device(p.data_ptr())
+            im = E.mi_forward(None)
+            p[i] = v
+            fd = (ip - im) / (2 * h)
+            worst = max(worst, abs(fd - g[i]) / max(1.0, abs(g[i])))
+        out["per_seed"].append(worst)
+        out["max_rel_err"] = max(out["max_rel_err"], worst)
+    out["forward_ms_median"] = 1e3 * float(np.median(t_fwd))
+    out["backward_ms_median"] = 1e3 * float(np.median(t_bwd))
+    E.close()
+    return out
+
+
 def kernels_only(args) -> None:
     """Engine set-up and `steps` iterations, nothing else: the command that
     the ncu captures under profiles/ run."""
@@ -495,10 +546,12 @@ def main() -> None:
     ap.add_argument("--engine", default="auto")
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", choices=["bench", "kernels", "ttb", "batch"], default="bench")
+    ap.add_argument("--mode", choices=["bench", "kernels", "ttb", "batch", "adjoint"], default="bench")
     ap.add_argument("--ttb-budget", type=float, default=15.0,
                     help="device seconds for each of the plain and squarem legs of time-to-bound")
     ap.add_argument("--no-ttb", action="store_true")
+    ap.add_argument("--fd-coords", type=int, default=1024)
+    ap.add_argument("--fd-seeds", type=int, default=16)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -506,6 +559,8 @@ def main() -> None:
         kernels_only(args)
     elif args.mode == "ttb":
         print(json.dumps({"time_to_bound": time_to_bound(args), "n": args.n, "k": args.k}), flush=True)
+    elif args.mode == "adjoint":
+        print(json.dumps({"adjoint": adjoint_check(args)}), flush=True)
     elif args.mode == "batch":
         res = batched(args)
         if res is not None:
