@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ 
 // are updated; block partials [max D, sum |O| e, max (logW - shift),
 // sum |O| p D, input-zero flag] go to ep.part[blockIdx.x * 8 + 0..4].
 template <int BM, int BN, int WM, int WN, bool WITH_D, bool CP>
-__global__ void __launch_bounds__(256, 2) k_mma_ba(const GemmDesc* __restrict__ descs, const int* __restrict__ tiles,
+__global__ void __launch_bounds__(256, (BM * BN <= 4096) ? 3 : 2) k_mma_ba(const GemmDesc* __restrict__ descs, const int* __restrict__ tiles,
                                                    BaEpilogue ep, const DevState* st) {
     using C = MmaCfg<BM, BN, WM, WN>;
     if (gated(st)) return;
@@ -391,6 +391,7 @@ static cudaError_t set_smem_attrs() {
     SET_BA(BDC_CFG_ARGS_128x128)
     SET_BA(BDC_CFG_ARGS_128x64)
     SET_BA(BDC_CFG_ARGS_64x128)
+    SET_BA(BDC_CFG_ARGS_64x64)
 #undef SET_BA
 #undef SET_STORE_CP
 #undef SET_STORE
@@ -435,6 +436,7 @@ static cudaError_t launch_ba(const Launch& L, const BaEpilogue& ep, cudaStream_t
         case CFG_128x128: GO_(BDC_CFG_ARGS_128x128) break;
         case CFG_128x64: GO_(BDC_CFG_ARGS_128x64) break;
         case CFG_64x128: GO_(BDC_CFG_ARGS_64x128) break;
+        case CFG_64x64: GO_(BDC_CFG_ARGS_64x64) break;
         default: return cudaErrorInvalidValue;
     }
 #undef GO_
@@ -1914,7 +1916,7 @@ bdc_status factored_init(bdc_handle* H) {
     {
         // (128x128 tiles do not fit the two-CTAs-per-SM register budget of the
         // fused epilogue)
-        const int cfgs[2] = {CFG_128x64, CFG_64x128};
+        const int cfgs[3] = {CFG_128x64, CFG_64x128, CFG_64x64};
         int ctas_max = 0;
         for (int c : cfgs) ctas_max = std::max(ctas_max, ((H1 + kCfgBM[c] - 1) / kCfgBM[c]) * ((H2 + kCfgBN[c] - 1) / kCfgBN[c]));
         BDC_CUDA_TRY(al(&F->epart, (size_t)std::max(ctas_max, H->nb_upd) * 8));
