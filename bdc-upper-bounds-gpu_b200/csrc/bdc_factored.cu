@@ -2031,9 +2031,13 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
     cudaError_t e = cudaSuccess;
     switch (stage) {
         case ST_QBIG: {
-            e = launch_store(F->ul, s, H->d_st);
-            if (e == cudaSuccess) e = launch_store(F->vr, s, H->d_st);
-            if (e != cudaSuccess) return e;
+            // U and V are independent: V runs on a branch beside U
+            if ((e = cudaEventRecord(F->ev_fork, s)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(F->side[0], F->ev_fork, 0)) != cudaSuccess) return e;
+            if ((e = launch_store(F->vr, F->side[0], H->d_st)) != cudaSuccess) return e;
+            if ((e = cudaEventRecord(F->ev_join[0], F->side[0])) != cudaSuccess) return e;
+            if ((e = launch_store(F->ul, s, H->d_st)) != cudaSuccess) return e;
+            if ((e = cudaStreamWaitEvent(s, F->ev_join[0], 0)) != cudaSuccess) return e;
             const int64_t na = (int64_t)F->KL * F->H2, nb = (int64_t)F->H1h * F->KR;
             k_sum_parts<<<H->num_sms * 4, 256, 0, s>>>(F->ulpart, F->S1, F->KL > 0 ? na : 0, F->UL, F->vrpart,
                                                        F->S2, F->KR > 0 ? nb : 0, F->VR, H->d_st);
