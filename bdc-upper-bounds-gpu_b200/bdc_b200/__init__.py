@@ -529,12 +529,16 @@ def orbit_sizes(xs, n: int) -> np.ndarray:
     return np.where((xs == r) | (xs == rc), 2.0, 4.0)
 
 
+_REV8 = np.array([int(f"{i:08b}"[::-1], 2) for i in range(256)], dtype=np.uint64)
+
+
 def reverse_bits(xs, n: int) -> np.ndarray:
+    """Bit reversal of n-bit strings (n <= 32), a byte at a time."""
     xs = np.asarray(xs, dtype=np.uint64)
-    r = np.zeros_like(xs)
-    for i in range(n):
-        r |= ((xs >> np.uint64(i)) & np.uint64(1)) << np.uint64(n - 1 - i)
-    return r
+    b = np.uint64(0xFF)
+    r = ((_REV8[xs & b] << np.uint64(24)) | (_REV8[(xs >> np.uint64(8)) & b] << np.uint64(16))
+         | (_REV8[(xs >> np.uint64(16)) & b] << np.uint64(8)) | _REV8[(xs >> np.uint64(24)) & b])
+    return r >> np.uint64(32 - n) if n > 0 else np.zeros_like(xs)
 
 
 def canonical_reps(n: int) -> np.ndarray:

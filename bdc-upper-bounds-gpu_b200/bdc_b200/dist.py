@@ -47,14 +47,34 @@ def normalise(p_rep: np.ndarray, n: int, reps=None) -> np.ndarray:
     return p_rep / np.sum(orbit_sizes(reps, n) * p_rep)
 
 
+def orbit_mean_at_reps(g: np.ndarray, n: int, reps=None) -> np.ndarray:
+    """The same per-representative means as orbit_average, computed from the
+    representatives' own orbits (O(#reps) work instead of O(2^n) searches):
+    the distinct members of each orbit are added in ascending order, as
+    orbit_average's bincount adds them, so the results agree bit for bit."""
+    reps = (canonical_reps(n) if reps is None else reps).astype(np.uint64)
+    m = np.uint64((1 << n) - 1)
+    imgs = np.stack([reps, reverse_bits(reps, n), reps ^ m, reverse_bits(reps ^ m, n)], axis=1)
+    imgs.sort(axis=1)
+    g = np.asarray(g, dtype=np.float64)
+    s = g[imgs[:, 0]].copy()
+    cnt = np.ones(len(reps))
+    for j in range(1, 4):
+        new = imgs[:, j] != imgs[:, j - 1]
+        s += np.where(new, g[imgs[:, j]], 0.0)
+        cnt += new
+    return s / cnt
+
+
 def dirichlet_start(n: int, alpha: float, seed: int) -> np.ndarray:
     """Seeded Dirichlet(alpha) draw over all 2^n strings (normalised gamma
     variates from numpy's PCG64 generator), symmetrised by averaging over each
     orbit and stored per representative with sum |O| p = 1."""
     rng = np.random.default_rng(seed)
     g = rng.gamma(alpha, 1.0, size=1 << n)
-    p = orbit_average(g, n)
-    return normalise(p, n)
+    reps = canonical_reps(n)
+    p = orbit_mean_at_reps(g, n, reps)
+    return normalise(p, n, reps)
 
 
 def uniform_start(n: int) -> np.ndarray:
