@@ -555,9 +555,11 @@ def canonical_reps(n: int) -> np.ndarray:
 def compute_C_n_k(in_len: int, out_len: int, a: float = 0.005, read_from_file: bool = False,
                   save_iterations: int = 100, base: str = ".", engine: str = "auto",
                   cache_dir: str | None = "transition_counts", verbose: bool = True,
-                  max_iters: int | None = None) -> dict:
+                  max_iters: int | None = None, certified_gap: float | None = None) -> dict:
     """backend/main_BAA.cu:39-131: BA until mx < a, saving the distribution
-    every save_iterations and at the end; returns rate (bits) and mx."""
+    every save_iterations and at the end; returns rate (bits) and mx.  With
+    certified_gap (bits) the certified solver replaces the loop and the result
+    also holds the bracket lower_bits <= C <= upper_bits."""
     E = load_cache(in_len, out_len, cache_dir=os.path.join(base, cache_dir) if cache_dir else None,
                    engine=engine)
     path = dist_filename(in_len, out_len, base)
@@ -569,6 +571,17 @@ def compute_C_n_k(in_len: int, out_len: int, a: float = 0.005, read_from_file: b
         if verbose:
             print("Initializing uniform distribution")
         E.set_uniform()
+    if certified_gap is not None:
+        t0 = time.perf_counter()
+        st = E.solve(certified_gap, 1000000)
+        p = E.get_p()
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        write_dist_file(path, p)
+        if verbose:
+            print(f"Certified C_{{{in_len},{out_len}}} in [{st['best_rate']:.15f}, {st['best_upper_bound']:.15f}] bits")
+        return {"rate_bits": st["best_rate"], "lower_bits": st["best_rate"], "upper_bits": st["best_upper_bound"],
+                "converged": bool(st["converged"]), "iters": st["iters"], "p": p,
+                "loop_s": time.perf_counter() - t0}
     if verbose:
         print("Starting BAA iterations...")
     i = 0

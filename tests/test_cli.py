@@ -116,3 +116,22 @@ def test_main_baa_device_tables_and_errors(tmp_path, O):
     (d / "distributions").mkdir()
     r = subprocess.run([OUR_MAIN, str(n), str(k)], cwd=d, capture_output=True, text=True, timeout=300)
     assert r.returncode != 0
+
+
+def test_main_baa_certified_solver_mode(tmp_path, O):
+    # BDC_SOLVE=<gap>: the certified solver instead of the plain loop; the
+    # saved distribution carries the printed lower end of the bracket
+    n, k = 12, 6
+    d = tmp_path / "solve"
+    (d / "distributions").mkdir(parents=True)
+    env = dict(os.environ, BDC_TABLES="device", BDC_SOLVE="1e-9")
+    r = subprocess.run([OUR_MAIN, str(n), str(k)], cwd=d, env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    m = re.search(r"^Certified C_\{12,6\} in \[(\S+), (\S+)\] bits", r.stdout, re.M)
+    assert m, r.stdout
+    lo, hi = float(m.group(1)), float(m.group(2))
+    assert 0.0 <= hi - lo < 1e-9
+    p = _dist(d, n, k)
+    reps = O.canonicals(n)
+    lnq = O.log_q(n, k, p, reps)
+    assert abs(O.rate(n, k, lnq, p, reps) / np.log(2.0) - lo) < 1e-11

@@ -1,6 +1,8 @@
 """The certified solver: its bracket is evaluated exactly at the point it
 returns (checked with the oracle), it contains the plain BA's limit, and it
 is below the requested gap."""
+import os
+
 import numpy as np
 import pytest
 
@@ -69,3 +71,18 @@ def test_solve_errors(bdc):
         E.set_uniform()
         with pytest.raises(bdc.BDCError):
             E.solve(0.0, 100)
+
+
+def test_compute_c_n_k_plain_and_certified(bdc, O, tmp_path):
+    # the reference-shaped driver (backend/main_BAA.cu:39-131): the plain loop
+    # matches the oracle's; certified_gap gives a bracket holding its rate
+    n, k = 10, 5
+    plain = bdc.compute_C_n_k(n, k, a=1e-3, base=str(tmp_path), cache_dir=None, verbose=False)
+    reps = O.canonicals(n)
+    ref = O.run_ba(n, k, np.full(len(reps), 1.0 / (1 << n)), reps, 1e-3, 100000)
+    assert plain["iters"] == ref["iters"]
+    assert abs(plain["rate_bits"] - ref["rate_bits"]) < 1e-11
+    cert = bdc.compute_C_n_k(n, k, base=str(tmp_path), cache_dir=None, verbose=False, certified_gap=1e-9)
+    assert cert["converged"] and 0.0 <= cert["upper_bits"] - cert["lower_bits"] < 1e-9
+    assert cert["lower_bits"] >= plain["rate_bits"] - 1e-12   # BA's rate never exceeds C
+    assert os.path.exists(os.path.join(str(tmp_path), "distributions", f"dist_{n}_{k}.txt"))
