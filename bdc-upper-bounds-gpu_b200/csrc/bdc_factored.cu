@@ -901,17 +901,28 @@ __device__ __forceinline__ double term_value(const FoldTerm& f, const double* qs
     return yh < (uint32_t)H1h ? VR[(size_t)yh * KR + f.off + yl] : 0.0;  // Q_t = V_t
 }
 
-// phase 2: acc[y] = sum_t Q_t[y] (one thread per y)
-__global__ void k_fold_acc(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ qsum,
-                           const double* __restrict__ ULt, int KL, const double* __restrict__ VR, int KR, int H1h,
-                           int k, double* __restrict__ acc, const DevState* st) {
+// phase 2: acc[y] = sum_t Q_t[y]: CTA = 32 consecutive y, warp w reads the
+// terms w, w + 8, ... (coalesced along y), and the 8 partial sums are added
+// in a fixed order
+__global__ void __launch_bounds__(256) k_fold_acc(const FoldTerm* __restrict__ terms, int T,
+                                                  const double* __restrict__ qsum, const double* __restrict__ ULt,
+                                                  int KL, const double* __restrict__ VR, int KR, int H1h, int k,
+                                                  double* __restrict__ acc, const DevState* st) {
     if (gated(st)) return;
+    __shared__ double part[8][33];
     const int ny = 1 << k;
-    const int y = blockIdx.x * blockDim.x + threadIdx.x;
-    if (y >= ny) return;
+    const int yy = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int y = blockIdx.x * 32 + yy;
     double a = 0.0;
-    for (int t = 0; t < T; ++t) a += term_value(terms[t], qsum, t, ny, ULt, KL, VR, KR, H1h, (uint32_t)y);
-    acc[y] = a;
+    if (y < ny)
+        for (int t = w; t < T; t += 8) a += term_value(terms[t], qsum, t, ny, ULt, KL, VR, KR, H1h, (uint32_t)y);
+    part[w][yy] = a;
+    __syncthreads();
+    if (w == 0 && y < ny) {
+        double s = part[0][yy];
+        for (int j = 1; j < 8; ++j) s += part[j][yy];
+        acc[y] = s;
+    }
 }
 
 // phase 3: q(rep r) = sum_{y in O(r)} acc[y] / (|O(r)| C Z); ln q with the
@@ -2061,8 +2072,8 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             const int ny = 1 << H->k;
             const int nqs = (F->T * ny + 255) / 256;
             k_qsum<<<nqs < 4096 ? nqs : 4096, 256, 0, s>>>(F->d_fold, F->T, F->qparts, H->k, F->qsum, H->d_st);
-            k_fold_acc<<<(ny + 127) / 128, 128, 0, s>>>(F->d_fold, F->T, F->qsum, F->UL, F->KL, F->VR, F->KR,
-                                                         F->H1h, H->k, F->qacc, H->d_st);
+            k_fold_acc<<<(ny + 31) / 32, 256, 0, s>>>(F->d_fold, F->T, F->qsum, F->UL, F->KL, F->VR, F->KR,
+                                                       F->H1h, H->k, F->qacc, H->d_st);
             k_fold_q<<<(ny + 127) / 128, 128, 0, s>>>(F->d_fold, F->T, F->qacc, H->k, H->inv_c, F->lnq_full,
                                                        H->d_lnq, F->RB, F->H2, F->LA, F->Kp, F->KL, F->H1h, H->d_st);
             break;
