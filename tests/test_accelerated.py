@@ -1,5 +1,5 @@
-"""The adjoint of I(p;W) and the accelerated BA loop (north-star forms beyond
-the reference): the gradient against central finite differences and against
+"""The adjoint of I(p;W) and the accelerated BA loop (forms beyond the
+reference's plain loop): the gradient against central finite differences and against
 the oracle's D(x); the accelerated loop against plain BA."""
 import numpy as np
 import pytest
