@@ -24,6 +24,7 @@
 // and phase 3 proves that nothing outside S could carry mass.
 #include <algorithm>
 #include <cfloat>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -33,6 +34,9 @@
 namespace bdc {
 
 constexpr int kAAMax = 10;  // history of the Anderson mixing
+// the restricted problem runs accelerated BA to this bracket (bits), then
+// Newton on the support
+constexpr double kRestrictedSwitchBits = 1e-7;
 
 // ------------------------------------------------------------ vector kernels
 // out = sum_i w_i u_i v_i over blocks (w = orbit sizes, 2 or 4)
@@ -902,6 +906,8 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
     const int64_t R = H->R;
     const int sms = H->num_sms;
     const int nbR = (int)std::min<int64_t>(sms * 8, (R + 255) / 256);
+    const auto t_start = std::chrono::steady_clock::now();
+    auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count(); };
 
     // start: the handle's current iterate
     const double* cur = nullptr;
@@ -942,7 +948,8 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
         if (rc != BDC_OK) return rc;
     }
     if (H->verbose)
-        printf("bdc: solve phase 1: %lld full evaluations, gap %.3e bits\n", (long long)evals, br.gap_bits());
+        printf("bdc: solve phase 1: %lld full evaluations, gap %.3e bits (%.3f s)\n", (long long)evals, br.gap_bits(),
+               elapsed());
 
     // ---- phases 2 and 3
     std::vector<uint32_t> members;
@@ -1038,7 +1045,7 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
         // break down
         const double target = std::min(gap_bits * 1e-2, 1e-11);
         rc = accelerated_ba(H, aa, rs.w.get<uint8_t>(), rmap, ps.get<double>(), pg.get<double>(), psa.get<double>(),
-                            pga.get<double>(), Sn, std::max(target, 1e-7), 400000, rb, &revals);
+                            pga.get<double>(), Sn, std::max(target, kRestrictedSwitchBits), 400000, rb, &revals);
         if (rc != BDC_OK) return rc;
         bool newton_ok = false;
         if (rb.gap_bits() >= target) {
@@ -1048,8 +1055,8 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
             if (rc != BDC_OK) return rc;
             if (newton_ok) rb = nb;
             if (H->verbose)
-                printf("bdc: solve round %d: Newton on the support %s, restricted gap %.3e bits\n", round,
-                       newton_ok ? "done" : "failed", nb.gap_bits());
+                printf("bdc: solve round %d: Newton on the support %s, restricted gap %.3e bits (%.3f s)\n", round,
+                       newton_ok ? "done" : "failed", nb.gap_bits(), elapsed());
             if (!newton_ok || rb.gap_bits() >= target) {
                 aa.clear();
                 rc = accelerated_ba(H, aa, rs.w.get<uint8_t>(), rmap, ps.get<double>(), pg.get<double>(),
@@ -1058,8 +1065,8 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
             }
         }
         if (H->verbose)
-            printf("bdc: solve round %d: |S| = %d, %lld restricted evaluations, restricted gap %.3e bits\n", round, Sn,
-                   (long long)revals, rb.gap_bits());
+            printf("bdc: solve round %d: |S| = %d, %lld restricted evaluations, restricted gap %.3e bits (%.3f s)\n",
+                   round, Sn, (long long)revals, rb.gap_bits(), elapsed());
         // expand p_S into the full space
         BDC_CUDA_TRY(cudaMemsetAsync(x.p, 0, sizeof(double) * R, s));
         k_scatter_f64<<<(Sn + 255) / 256, 256, 0, s>>>(Sn, rs.idx.get<uint32_t>(), ps.get<double>(), x.get<double>());
