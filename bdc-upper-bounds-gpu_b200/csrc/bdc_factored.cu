@@ -2161,7 +2161,8 @@ bdc_status factored_map(bdc_handle* H, const double* p_in, double* p_out, double
         H->bytes += sizeof(double) * NX;
     }
     BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), H->stream));
-    BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
+    // (Pw is zero away from the representatives from set-up on: every kernel
+    // writes it only there, and the load below rewrites all of them)
     const int nb = H->nb_upd;
     k_fac_load<<<nb, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, p_in, F->Pw, F->Lt, F->epart, 1, H->d_st);
     k_fac_load_finish<<<1, 32, 0, H->stream>>>(F->epart, nb, H->k, H->d_st);
