@@ -29,7 +29,7 @@ LIB_PATH = os.path.join(PKG_DIR, "libbdc_b200.so")
 BDC_OK = 0
 STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_IO", 4: "ERR_NOMEM",
                 5: "ERR_STATE", 6: "ERR_UNSUPPORTED", 7: "ERR_NUMERIC"}
-ENGINES = {"auto": 0, "count": 1, "factored": 2}
+ENGINES = {"auto": 0, "count": 1, "factored": 2, "count-fp32c": 3}
 ENGINE_NAMES = {v: k for k, v in ENGINES.items()}
 
 # every symbol the C ABI exports (include/bdc_b200.h)
@@ -42,6 +42,7 @@ EXPORTED_SYMBOLS = [
     "bdc_write_dist_file", "bdc_work", "bdc_profile", "bdc_set_stream", "bdc_peak_probe",
     "bdc_max_deviation_noalloc", "bdc_accelerate", "bdc_mi_forward", "bdc_mi_backward",
     "bdc_batch_create", "bdc_batch_iterate", "bdc_batch_destroy", "bdc_batch_set_stream", "bdc_solve",
+    "bdc_bound_error",
 ]
 
 
@@ -172,9 +173,10 @@ def num_q_slots(k: int) -> int:
 class Engine:
     """One (n, k) BA problem resident on one GPU.
 
-    engine: "auto" (fastest available), "count" (split-identity count path) or
-    "factored" (Kronecker-factored passes).  cache_dir: directory of
-    cache_n_k files; None builds the half tables on the device.
+    engine: "auto" (fastest available), "count" (split-identity count path),
+    "factored" (Kronecker-factored passes) or "count-fp32c" (the count path
+    with its q and D sums in compensated FP32, n <= 26).  cache_dir:
+    directory of cache_n_k files; None builds the half tables on the device.
     """
 
     def __init__(self, n: int, k: int, engine: str = "auto", device: int = 0,
@@ -249,6 +251,14 @@ class Engine:
         st = Stats()
         _check(library().bdc_iterate(self._h, int(max_iters), float(a), ctypes.byref(st)), "bdc_iterate")
         return st.as_dict()
+
+    def bound_error(self) -> tuple[float, float]:
+        """(|upper_bound - FP64|, |rate - FP64|) in bits for the last
+        iteration: the compensated-FP32 engine's reported numbers against an
+        FP64 re-evaluation at the same iterate; (0, 0) for the FP64 engines."""
+        ub, rate = ctypes.c_double(), ctypes.c_double()
+        _check(library().bdc_bound_error(self._h, ctypes.byref(ub), ctypes.byref(rate)), "bdc_bound_error")
+        return ub.value, rate.value
 
     def accelerate(self, max_evals: int, gap_bits: float = 0.0) -> dict:
         """Accelerated BA on the device (factored engine): runs until the

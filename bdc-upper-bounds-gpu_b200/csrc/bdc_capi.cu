@@ -82,6 +82,10 @@ bdc_status bdc_create(int n, int k, const bdc_options* opts, bdc_handle_t* out) 
         delete H;
         return fail(BDC_ERR_UNSUPPORTED, "requested engine does not support n=%d k=%d", n, k);
     }
+    if (H->engine == BDC_ENGINE_COUNT_FP32C) {
+        H->engine = BDC_ENGINE_COUNT;
+        H->c32 = 1;
+    }
     bdc_status rc = engine_init(H);
     if (rc != BDC_OK) {
         engine_free(H);
@@ -105,7 +109,7 @@ bdc_status bdc_info(bdc_handle_t H, int* n, int* k, int64_t* num_reps, int* engi
     if (n) *n = H->n;
     if (k) *k = H->k;
     if (num_reps) *num_reps = H->R;
-    if (engine) *engine = H->engine;
+    if (engine) *engine = H->c32 ? BDC_ENGINE_COUNT_FP32C : H->engine;
     return BDC_OK;
 }
 
@@ -177,6 +181,13 @@ bdc_status bdc_iterate(bdc_handle_t H, int64_t max_iters, double a, bdc_stats* s
     if (max_iters < 0) return fail(BDC_ERR_ARG, "bdc_iterate: max_iters < 0");
     cudaSetDevice(H->device);
     return engine_iterate(H, max_iters, a, stats);
+}
+
+bdc_status bdc_bound_error(bdc_handle_t H, double* ub_err, double* rate_err) {
+    if (!H || !ub_err || !rate_err) return fail(BDC_ERR_ARG, "bdc_bound_error: NULL argument");
+    if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_bound_error: no distribution set");
+    cudaSetDevice(H->device);
+    return engine_bound_error(H, ub_err, rate_err);
 }
 
 bdc_status bdc_accelerate(bdc_handle_t H, int64_t max_evals, double gap_bits, bdc_stats* stats) {

@@ -122,10 +122,40 @@ __device__ __forceinline__ void tile_row(const Split& s, const HalfTables& A, co
     tile_row_impl<K, TB, BB>(s, ar, br, xh, xl, g, N, std::make_integer_sequence<int, K + 1>{});
 }
 
+// ------------------------------------------------------- compensated FP32
+// Sums of FP32 products carried as an unevaluated pair (hi, lo) of floats.
+// A double operand enters as its two-float split v = vh + vl (48 bits); a
+// count N < 2^24 is exact as a float.  The product's rounding error comes
+// from an FMA, the sum's from Knuth's two-sum, and both go into lo:
+//     pr = vh N;  err = fma(vh, N, -pr);  tail = fma(vl, N, err)
+//     s = hi + pr;  e = two-sum error;  hi = s;  lo += e + tail
+// The _rn intrinsics keep the compiler from contracting the additions into
+// FMAs, which would break the error terms.
+struct F32Pair {
+    float hi = 0.0f, lo = 0.0f;
+    __device__ __forceinline__ void add_prod(float vh, float vl, float nf) {
+        const float pr = __fmul_rn(vh, nf);
+        const float err = fmaf(vh, nf, -pr);
+        const float tail = fmaf(vl, nf, err);
+        const float s = __fadd_rn(hi, pr);
+        const float bv = __fsub_rn(s, hi);
+        const float e = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bv)), __fsub_rn(pr, bv));
+        hi = s;
+        lo = __fadd_rn(lo, __fadd_rn(e, tail));
+    }
+    __device__ __forceinline__ double value() const { return (double)hi + (double)lo; }
+};
+
+__device__ __forceinline__ void split_f32(double v, float& vh, float& vl) {
+    vh = __double2float_rn(v);
+    vl = __double2float_rn(v - (double)vh);
+}
+
 // ------------------------------------------------------------- q pass
 // acc[y] = sum over this CTA's x of |O(x)| p(x) N(x,y), written per CTA to
-// part[blockIdx.x][y]; k_qfold reduces over CTAs.
-template <int K, int TB, int BB>
+// part[blockIdx.x][y]; k_qfold reduces over CTAs.  C32: the per-thread sums
+// run in compensated FP32 (F32Pair) and leave the thread as doubles.
+template <int K, int TB, int BB, bool C32>
 __global__ void __launch_bounds__(256) k_qpass(Split s, HalfTables A, HalfTables B,
                                                const uint32_t* __restrict__ reps,
                                                const double* __restrict__ p_buf0,
@@ -150,15 +180,42 @@ __global__ void __launch_bounds__(256) k_qpass(Split s, HalfTables A, HalfTables
 #pragma unroll
         for (int b = 0; b < TL::NB; ++b) acc[t][b] = 0.0;
 
-    for (int64_t i = i0; i < i1; ++i) {
-        const uint32_t x = __ldg(reps + i);
-        const double w = (double)orbit_size(x, s.n) * __ldg(p + i);
-        uint32_t N[TL::T][TL::NB];
-        tile_row<K, TB, BB>(s, A, B, x, g, N);
+    if constexpr (C32) {
+        // runs of kRun x's in compensated FP32, each run's sums added to the
+        // FP64 totals: the run length bounds the growth of the lo words'
+        // own rounding (at most kRun^2 u^2 of the run's sum, u = 2^-24)
+        constexpr int kRun = 32;
+        for (int64_t r0 = i0; r0 < i1; r0 += kRun) {
+            const int64_t r1 = (r0 + kRun < i1) ? r0 + kRun : i1;
+            F32Pair acc32[TL::T][TL::NB];
+            for (int64_t i = r0; i < r1; ++i) {
+                const uint32_t x = __ldg(reps + i);
+                const double w = (double)orbit_size(x, s.n) * __ldg(p + i);
+                uint32_t N[TL::T][TL::NB];
+                tile_row<K, TB, BB>(s, A, B, x, g, N);
+                float wh, wl;
+                split_f32(w, wh, wl);
 #pragma unroll
-        for (int t = 0; t < TL::T; ++t)
+                for (int t = 0; t < TL::T; ++t)
 #pragma unroll
-            for (int b = 0; b < TL::NB; ++b) acc[t][b] = fma(w, (double)N[t][b], acc[t][b]);
+                    for (int b = 0; b < TL::NB; ++b) acc32[t][b].add_prod(wh, wl, (float)N[t][b]);
+            }
+#pragma unroll
+            for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+                for (int b = 0; b < TL::NB; ++b) acc[t][b] += acc32[t][b].value();
+        }
+    } else {
+        for (int64_t i = i0; i < i1; ++i) {
+            const uint32_t x = __ldg(reps + i);
+            const double w = (double)orbit_size(x, s.n) * __ldg(p + i);
+            uint32_t N[TL::T][TL::NB];
+            tile_row<K, TB, BB>(s, A, B, x, g, N);
+#pragma unroll
+            for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+                for (int b = 0; b < TL::NB; ++b) acc[t][b] = fma(w, (double)N[t][b], acc[t][b]);
+        }
     }
 
     // reduce the CTA's groups (same g => same y set) in shared memory
@@ -181,7 +238,9 @@ __global__ void __launch_bounds__(256) k_qpass(Split s, HalfTables A, HalfTables
 // ------------------------------------------------------------- D / h pass
 // MODE 0: D(x) = h(x) - (1/C) sum_y N(x,y) ln q(rep y)       -> out_d[i]
 // MODE 1: h(x) = (1/C) sum_y N ln N - ln C                    -> out_d[i]
-template <int K, int TB, int BB, int MODE>
+// C32 (MODE 0 only): each thread's share of sum_y N ln q runs in
+// compensated FP32 (F32Pair); the group reduction and h - v/C stay FP64.
+template <int K, int TB, int BB, int MODE, bool C32 = false>
 __global__ void __launch_bounds__(256) k_dpass(Split s, HalfTables A, HalfTables B,
                                                const uint32_t* __restrict__ reps, int64_t R,
                                                const double* __restrict__ lnq,
@@ -201,13 +260,17 @@ __global__ void __launch_bounds__(256) k_dpass(Split s, HalfTables A, HalfTables
     const int64_t i1 = (i0 + chunk < R) ? i0 + chunk : R;
     const int lane = threadIdx.x & 31;
 
+    static_assert(!C32 || MODE == 0, "compensated FP32 is for the D pass");
     double lq[TL::T][TL::NB];
+    float lqh[C32 ? TL::T : 1][C32 ? TL::NB : 1], lql[C32 ? TL::T : 1][C32 ? TL::NB : 1];
     if (MODE == 0) {
 #pragma unroll
         for (int t = 0; t < TL::T; ++t)
 #pragma unroll
-            for (int b = 0; b < TL::NB; ++b)
+            for (int b = 0; b < TL::NB; ++b) {
                 lq[t][b] = __ldg(lnq + orbit_rep(TL::y_of(g, t, b), K));
+                if constexpr (C32) split_f32(lq[t][b], lqh[t][b], lql[t][b]);
+            }
     }
 
     // per-warp partial sums of the group's x, folded every XC rows
@@ -227,20 +290,29 @@ __global__ void __launch_bounds__(256) k_dpass(Split s, HalfTables A, HalfTables
                 const uint32_t x = __ldg(reps + i);
                 uint32_t N[TL::T][TL::NB];
                 tile_row<K, TB, BB>(s, A, B, x, g, N);
+                if constexpr (C32) {
+                    F32Pair sv;
 #pragma unroll
-                for (int t = 0; t < TL::T; ++t)
+                    for (int t = 0; t < TL::T; ++t)
 #pragma unroll
-                    for (int b = 0; b < TL::NB; ++b) {
-                        if (MODE == 0) {
-                            v = fma((double)N[t][b], lq[t][b], v);
-                        } else {
-                            const uint32_t c = N[t][b];
-                            if (c) {
-                                v = fma((double)c, log((double)c), v);
-                                ++nz;
+                        for (int b = 0; b < TL::NB; ++b) sv.add_prod(lqh[t][b], lql[t][b], (float)N[t][b]);
+                    v = sv.value();
+                } else {
+#pragma unroll
+                    for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+                        for (int b = 0; b < TL::NB; ++b) {
+                            if (MODE == 0) {
+                                v = fma((double)N[t][b], lq[t][b], v);
+                            } else {
+                                const uint32_t c = N[t][b];
+                                if (c) {
+                                    v = fma((double)c, log((double)c), v);
+                                    ++nz;
+                                }
                             }
                         }
-                    }
+                }
             }
             if (TL::GROUP <= 32) {
                 // the group is a lane-aligned slice of one warp
@@ -352,7 +424,7 @@ static cudaError_t launch_qpass_k(const CountLaunch& L, const double* p0, const 
     constexpr int TB = TileChoice<K>::TB, BB = TileChoice<K>::BB;
     const int threads = cta_threads<K>();
     const size_t shm = sizeof(double) << K;
-    auto kern = k_qpass<K, TB, BB>;
+    auto kern = L.c32 ? k_qpass<K, TB, BB, true> : k_qpass<K, TB, BB, false>;
     if (shm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
         if (e != cudaSuccess) return e;
@@ -367,8 +439,9 @@ static cudaError_t launch_dpass_k(const CountLaunch& L, const double* lnq, const
                                   const DevState* st, int use_state) {
     constexpr int TB = TileChoice<K>::TB, BB = TileChoice<K>::BB;
     const int threads = cta_threads<K>();
-    k_dpass<K, TB, BB, MODE><<<L.grid, threads, 0, L.stream>>>(L.s, L.A, L.B, L.reps, L.R, lnq, h,
-                                                               inv_c, log_c, out, nnz, st, use_state);
+    auto kern = (MODE == 0 && L.c32) ? k_dpass<K, TB, BB, MODE, MODE == 0> : k_dpass<K, TB, BB, MODE, false>;
+    kern<<<L.grid, threads, 0, L.stream>>>(L.s, L.A, L.B, L.reps, L.R, lnq, h, inv_c, log_c, out, nnz, st,
+                                           use_state);
     return cudaGetLastError();
 }
 

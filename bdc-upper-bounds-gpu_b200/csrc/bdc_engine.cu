@@ -91,6 +91,9 @@ static bdc_status make_bundle(bdc_handle* H, int hlen, int mmax, uint16_t** rows
 int select_engine(int requested, int n, int k) {
     switch (requested) {
         case BDC_ENGINE_COUNT: return BDC_ENGINE_COUNT;
+        // FP32 holds the counts exactly only below 2^24: max N(x,y) <= C(n,k)
+        // and C(26,13) = 10,400,600 < 2^24 < C(27,13)
+        case BDC_ENGINE_COUNT_FP32C: return n <= 26 ? BDC_ENGINE_COUNT_FP32C : -1;
         case BDC_ENGINE_FACTORED: return factored_supports(n, k) ? BDC_ENGINE_FACTORED : -1;
         case BDC_ENGINE_AUTO: return factored_supports(n, k) ? BDC_ENGINE_FACTORED : BDC_ENGINE_COUNT;
         default: return -1;
@@ -106,6 +109,7 @@ CountLaunch count_launch(const bdc_handle* H) {
     L.R = H->R;
     L.grid = H->grid_count;
     L.stream = H->stream;
+    L.c32 = H->c32;
     return L;
 }
 
@@ -183,6 +187,10 @@ bdc_status engine_init(bdc_handle* H) {
     const size_t nq = (size_t)1 << (H->k >= 1 ? H->k - 1 : 0);
     BDC_CUDA_TRY(dalloc(H, &H->d_lnq, nq));
     BDC_CUDA_TRY(dalloc(H, &H->d_q, nq));
+    if (H->c32) {
+        BDC_CUDA_TRY(dalloc(H, &H->d_lnq64, nq));
+        BDC_CUDA_TRY(dalloc(H, &H->d_d64, (size_t)R));
+    }
     const int group = count_group_size(H->k);
     const int cta = count_cta_threads(H->k);
     const int gpc = cta / group > 0 ? cta / group : 1;
@@ -226,7 +234,7 @@ bdc_status engine_init(bdc_handle* H) {
     }
     if (H->verbose)
         printf("bdc: n=%d k=%d reps=%lld engine=%s tables=%s device bytes=%.1f MB\n", H->n, H->k,
-               (long long)R, H->engine == BDC_ENGINE_FACTORED ? "factored" : "count",
+               (long long)R, H->engine == BDC_ENGINE_FACTORED ? "factored" : (H->c32 ? "count-fp32c" : "count"),
                H->cache_dir.empty() ? "generated" : H->cache_dir.c_str(), H->bytes / 1048576.0);
     return BDC_OK;
 }
@@ -244,6 +252,8 @@ void engine_free(bdc_handle* H) {
     cudaFree(H->d_lnq);
     cudaFree(H->d_q);
     cudaFree(H->d_qpart);
+    cudaFree(H->d_lnq64);
+    cudaFree(H->d_d64);
     cudaFree(H->d_red);
     cudaFree(H->d_scalar);
     cudaFree(H->d_st);
@@ -377,6 +387,33 @@ bdc_status engine_profile(bdc_handle* H, int iters, bdc_profile_t* out) {
     out->work_main = (double)H->nonzero_pairs * (double)(H->s.jhi - H->s.jlo + 1);
     out->launches = 6;
     out->iters = iters;
+    return BDC_OK;
+}
+
+bdc_status engine_bound_error(bdc_handle* H, double* ub_err_bits, double* rate_err_bits) {
+    *ub_err_bits = 0.0;
+    *rate_err_bits = 0.0;
+    if (!H->c32) return BDC_OK;
+    BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    if (H->h_st->iter == 0) return fail(BDC_ERR_STATE, "bdc_bound_error: no iteration since the distribution was set");
+    // the update wrote p' into the other buffer and flipped cur, so the
+    // iterate the last D pass used is still in d_p[cur ^ 1]
+    const double* pt = H->d_p[(H->h_st->cur ^ 1) & 1];
+    CountLaunch L = count_launch(H);
+    L.c32 = 0;
+    BDC_CUDA_TRY(launch_qpass(L, pt, pt, H->d_qpart, H->d_st, 0));
+    BDC_CUDA_TRY(launch_qfold(H->d_qpart, H->grid_count, H->k, H->inv_c, H->d_lnq64, nullptr, H->d_st, 0, H->stream));
+    BDC_CUDA_TRY(launch_dpass(L, H->d_lnq64, H->d_h, H->inv_c, H->log_c, H->d_d64, H->d_st, 0));
+    BDC_CUDA_TRY(launch_vec_max(H->d_d64, H->R, H->d_red, H->nb_upd, H->d_scalar + 6, H->stream));
+    BDC_CUDA_TRY(launch_rate(H->n, H->d_reps, H->R, pt, H->d_d64, H->d_red + H->nb_upd, H->nb_upd, H->d_scalar + 7,
+                             H->stream));
+    double v[2];
+    BDC_CUDA_TRY(cudaMemcpyAsync(v, H->d_scalar + 6, sizeof(v), cudaMemcpyDeviceToHost, H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    const double ln2 = 0.69314718055994530942;
+    *ub_err_bits = fabs(H->h_st->max_d - v[0]) / ln2;
+    *rate_err_bits = fabs(H->h_st->rate - v[1]) / ln2;
     return BDC_OK;
 }
 

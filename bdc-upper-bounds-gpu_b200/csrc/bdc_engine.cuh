@@ -17,6 +17,7 @@ struct bdc_handle {
     // placement / options
     int device = 0;
     int engine = BDC_ENGINE_COUNT;
+    int c32 = 0;  // count engine with compensated-FP32 sums (BDC_ENGINE_COUNT_FP32C)
     int verbose = 0;
     int num_sms = 148;
     std::string cache_dir;
@@ -37,6 +38,9 @@ struct bdc_handle {
     double* d_lnq = nullptr;   // [2^{k-1}]
     double* d_q = nullptr;     // [2^{k-1}]
     double* d_qpart = nullptr; // [grid][2^k]
+    // FP64 re-evaluation of a compensated-FP32 handle's bound
+    double* d_lnq64 = nullptr; // [2^{k-1}]
+    double* d_d64 = nullptr;   // [R]
     // reductions / state
     double* d_red = nullptr;
     double* d_scalar = nullptr;
@@ -62,6 +66,9 @@ bdc_status engine_current_p(bdc_handle* H, const double** p);
 bdc_status engine_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats);
 bdc_status engine_log_q(bdc_handle* H);       // ln q of the current p into H->d_lnq
 bdc_status engine_divergence(bdc_handle* H);  // D from H->d_lnq into H->d_d
+// compensated-FP32 handles: the last bound and rate re-evaluated in FP64 at
+// the same iterate; the absolute differences in bits (0 for FP64 engines)
+bdc_status engine_bound_error(bdc_handle* H, double* ub_err_bits, double* rate_err_bits);
 
 CountLaunch count_launch(const bdc_handle* H);
 UpdateLaunch update_launch(const bdc_handle* H, double a);

@@ -13,6 +13,7 @@ struct CountLaunch {
     int64_t R;
     int grid;                 // CTAs of the q / D passes
     cudaStream_t stream;
+    int c32 = 0;              // q and D sums in compensated FP32 (counts must be < 2^24)
 };
 
 // ---- count path (bdc_count.cu)
@@ -59,6 +60,8 @@ cudaError_t launch_mi_grad(int n, const uint32_t* reps, int64_t R, const double*
                            cudaStream_t stream);
 cudaError_t launch_rate(int n, const uint32_t* reps, int64_t R, const double* p, const double* d,
                         double* part, int nblocks, double* out, cudaStream_t stream);
+cudaError_t launch_vec_max(const double* v, int64_t R, double* part, int nblocks, double* out,
+                           cudaStream_t stream);
 cudaError_t launch_max_dev(const double* p, const double* pb, int64_t R, double* part, int nblocks,
                            double* out, cudaStream_t stream);
 

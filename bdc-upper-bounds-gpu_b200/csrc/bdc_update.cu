@@ -268,6 +268,23 @@ k_maxdev_part(const double* __restrict__ p, const double* __restrict__ pb, int64
     if (threadIdx.x == 0) part[blockIdx.x] = m;
 }
 
+__global__ void __launch_bounds__(kUpdThreads)
+k_vmax_part(const double* __restrict__ v, int64_t R, double* __restrict__ part) {
+    double m = -DBL_MAX;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R;
+         i += (int64_t)gridDim.x * blockDim.x)
+        m = OpMax()(m, v[i]);
+    m = block_reduce(m, OpMax(), -DBL_MAX);
+    if (threadIdx.x == 0) part[blockIdx.x] = m;
+}
+
+cudaError_t launch_vec_max(const double* v, int64_t R, double* part, int nblocks, double* out,
+                           cudaStream_t stream) {
+    k_vmax_part<<<nblocks, kUpdThreads, 0, stream>>>(v, R, part);
+    k_fold_max<<<1, kUpdThreads, 0, stream>>>(part, nblocks, out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_max_dev(const double* p, const double* pb, int64_t R, double* part, int nblocks,
                            double* out, cudaStream_t stream) {
     k_maxdev_part<<<nblocks, kUpdThreads, 0, stream>>>(p, pb, R, part);

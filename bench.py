@@ -536,6 +536,53 @@ def adjoint_check(args) -> dict:
     return out
 
 
+def precision_check(args) -> dict:
+    """The precision form: the count path with FP64 sums against the same path
+    with compensated-FP32 sums (engine count-fp32c), at 20/10 from the
+    Dirichlet(1) seed-0 start and at 24/12 from the uniform start.  Per engine:
+    iterations/s over `steps` iterations (CUDA events on the engine's stream),
+    the q/D pass split, and for count-fp32c the last bound's and rate's
+    distance from an FP64 re-evaluation at the same iterate (bdc_bound_error)
+    and from the FP64 engine's own bound after the same iterations."""
+    import torch
+
+    import bdc_b200
+    from bdc_b200 import dist as bdist
+
+    stream = torch.cuda.current_stream()
+    out = []
+    for n, k, start in [(20, 10, ("dirichlet", 1.0, 0)), (24, 12, ("uniform",))]:
+        p0 = bdist.uniform_start(n) if start[0] == "uniform" else bdist.dirichlet_start(n, start[1], start[2])
+        iters = max(3, min(args.steps, 40 if n <= 20 else 10))
+        row = {"n": n, "k": k, "start": "-".join(map(str, start)), "iters": iters}
+        for engine in ("count", "count-fp32c"):
+            E = bdc_b200.Engine(n, k, engine=engine)
+            E.set_stream(stream.cuda_stream)
+            E.set_p(p0)
+            E.iterate(3, float("-inf"))
+            prof = E.profile(2)
+            E.set_p(p0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = E.iterate(iters, float("-inf"))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            leg = {"iters_per_s": iters / (e0.elapsed_time(e1) / 1e3), "ms_q": prof["ms_q"], "ms_d": prof["ms_d"],
+                   "upper_bound_bits": st["upper_bound"], "rate_bits": st["rate"]}
+            if engine == "count-fp32c":
+                ub_err, rate_err = E.bound_error()
+                leg["bound_err_vs_fp64_reeval_bits"] = ub_err
+                leg["rate_err_vs_fp64_reeval_bits"] = rate_err
+            row[engine] = leg
+            E.close()
+        row["fp32c_bound_minus_fp64_engine_bits"] = (row["count-fp32c"]["upper_bound_bits"]
+                                                     - row["count"]["upper_bound_bits"])
+        row["fp32c_speed_vs_fp64"] = row["count-fp32c"]["iters_per_s"] / row["count"]["iters_per_s"]
+        out.append(row)
+    return {"precision": out}
+
+
 def kernels_only(args) -> None:
     """Engine set-up and `steps` iterations, nothing else: the command that
     the ncu captures under profiles/ run."""
@@ -551,7 +598,7 @@ def kernels_only(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=24)
@@ -559,7 +606,7 @@ def main() -> None:
     ap.add_argument("--engine", default="auto")
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", choices=["bench", "kernels", "ttb", "batch", "adjoint"], default="bench")
+    ap.add_argument("--mode", choices=["bench", "kernels", "ttb", "batch", "adjoint", "precision"], default="bench")
     ap.add_argument("--ttb-budget", type=float, default=15.0,
                     help="device seconds for each of the plain and squarem legs of time-to-bound")
     ap.add_argument("--no-ttb", action="store_true")
@@ -574,6 +621,8 @@ def main() -> None:
         print(json.dumps({"time_to_bound": time_to_bound(args), "n": args.n, "k": args.k}), flush=True)
     elif args.mode == "adjoint":
         print(json.dumps({"adjoint": adjoint_check(args)}), flush=True)
+    elif args.mode == "precision":
+        print(json.dumps(precision_check(args)), flush=True)
     elif args.mode == "batch":
         res = batched(args)
         if res is not None:

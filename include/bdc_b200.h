@@ -44,7 +44,11 @@ typedef enum {
 typedef enum {
     BDC_ENGINE_AUTO = 0,      /* the fastest engine that supports (n,k) */
     BDC_ENGINE_COUNT = 1,     /* split-identity count path: q pass + D pass per iteration */
-    BDC_ENGINE_FACTORED = 2   /* Kronecker-factored passes (FP64 matrix products) */
+    BDC_ENGINE_FACTORED = 2,  /* Kronecker-factored passes (FP64 matrix products) */
+    BDC_ENGINE_COUNT_FP32C = 3 /* the count path with its q and D sums in compensated FP32
+                                  (two-float accumulators, exact FP32 counts: n <= 26);
+                                  FP64 for the q fold, the update and the bound's max.
+                                  Opt-in: slower than the FP64 engines on a B200 */
 } bdc_engine;
 
 typedef struct {
@@ -102,6 +106,13 @@ bdc_status bdc_get_p_device(bdc_handle_t h, double* p_dev, int64_t num_reps);
  * BAA.cu:590-639 and compute_max_deviation, BAA.cu:916-946): runs iterations
  * until mx < a or max_iters iterations, all on the device.  stats may be NULL. */
 bdc_status bdc_iterate(bdc_handle_t h, int64_t max_iters, double a, bdc_stats* stats);
+
+/* Error of the last reported bound (no counterpart in the reference): for a
+ * BDC_ENGINE_COUNT_FP32C handle, re-evaluates q and D in FP64 at the iterate
+ * the last bdc_iterate's D pass used and returns |upper_bound - FP64 value|
+ * and |rate - FP64 value| in bits; 0 and 0 for the FP64 engines.  Needs at
+ * least one iteration since the distribution was set (BDC_ERR_STATE). */
+bdc_status bdc_bound_error(bdc_handle_t h, double* upper_bound_err_bits, double* rate_err_bits);
 
 /* Accelerated BA (no counterpart in the reference): the BA map is the
  * exponentiated-gradient step ln p' = ln p + dI/dp + const with the adjoint

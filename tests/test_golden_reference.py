@@ -122,7 +122,7 @@ def test_oracle_matches_reference_ba(O, name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("engine", ["count", "factored"])
+@pytest.mark.parametrize("engine", ["count", "factored", "count-fp32c"])
 @pytest.mark.parametrize("name", NAMES)
 def test_engine_matches_reference_ba(bdc, O, name, engine):
     z = np.load(os.path.join(GOLDEN, "ref_ba", f"ref_ba_{name}.npz"))

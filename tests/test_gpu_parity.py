@@ -4,6 +4,8 @@ Counts are compared bit-exactly; ln q, ln p + D, D and p' within the
 tolerances below (FP64 sums in a different order than the reference's):
   TOL_REL = 1e-12 relative on q and p', TOL_ABS = 1e-12 absolute on ln q,
   logW and D (all O(1..20) in size).
+The compensated-FP32 engine (count-fp32c) is held to the same tolerances in
+the single-pass and iterate checks.
 """
 import hashlib
 import json
@@ -20,6 +22,7 @@ TOL_REL = 1e-12
 TOL_ABS = 1e-12
 
 ENGINES = ["count", "factored"]
+NUMERIC_ENGINES = ENGINES + ["count-fp32c"]
 
 
 def start(n, kind, O):
@@ -67,7 +70,7 @@ def test_reps_and_counts_bit_exact(bdc, O, engine, n, k):
         assert np.array_equal(got, want)
 
 
-@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("engine", NUMERIC_ENGINES)
 @pytest.mark.parametrize("n,k,kind", [(12, 6, "uniform"), (13, 5, "uniform"), (10, 4, "dirichlet"),
                                       (16, 8, "dirichlet"), (10, 5, "zeros"), (9, 9, "uniform"),
                                       (9, 1, "dirichlet"), (11, 10, "dirichlet"), (14, 3, "dirichlet")])
@@ -92,7 +95,7 @@ def test_single_passes_match_oracle(bdc, O, engine, n, k, kind):
         np.testing.assert_allclose(pn, pn_o, rtol=TOL_REL, atol=0)
 
 
-@pytest.mark.parametrize("engine", ENGINES)
+@pytest.mark.parametrize("engine", NUMERIC_ENGINES)
 @pytest.mark.parametrize("n,k,kind,iters", [(12, 6, "uniform", 25), (13, 7, "dirichlet", 10),
                                             (16, 8, "dirichlet", 5)])
 def test_iterates_track_oracle(bdc, O, engine, n, k, kind, iters):
