@@ -68,26 +68,54 @@ __device__ __forceinline__ void tile_term(const Split& s, const uint16_t* __rest
     constexpr int BT = (J >= TB) ? 1 : (1 << (TB - J));
     constexpr int BN = (M >= BB) ? NB : (1 << M);
     if (J < s.jlo || J > s.jhi) return;  // uniform across the grid
-    const bool idA = (J == s.n1);
-    const bool idB = (M == s.n2);
+    // y = (t << (K-TB)) + (g << BB) + b with disjoint bit fields, so y >> M and
+    // y & (2^M - 1) split into the same fields without carries: a per-thread
+    // part (from g) and a compile-time part (from t, b) that becomes the
+    // load's immediate offset.
+    constexpr uint32_t mlo = (1u << M) - 1u;
+    const uint32_t gA = (g << BB) >> M;
+    const uint32_t gB = (g << BB) & mlo;
+    // The identity halves (j = n1: A_j[xh][yh] = [xh == yh]; k-j = n2 likewise
+    // for B) are uniform branches, so the table terms carry no compare/select.
     uint32_t av[AT][AB], bv[BT][BN];
+    if (J == s.n1) {
 #pragma unroll
-    for (int ta = 0; ta < AT; ++ta)
+        for (int ta = 0; ta < AT; ++ta)
 #pragma unroll
-        for (int ba = 0; ba < AB; ++ba) {
-            const int t = (J >= TB) ? ta : (ta << (TB - J));
-            const int b = (M >= BB) ? 0 : (ba << M);
-            const uint32_t yh = Tile<K, TB, BB>::y_of(g, t, b) >> M;
-            av[ta][ba] = idA ? (uint32_t)(xh == yh) : (uint32_t)__ldg(ar + bundle_offset(J) + yh);
-        }
+            for (int ba = 0; ba < AB; ++ba) {
+                const uint32_t t = (J >= TB) ? ta : (ta << (TB - J));
+                const uint32_t b = (M >= BB) ? 0 : (ba << M);
+                av[ta][ba] = (uint32_t)(xh == gA + ((t << (K - TB)) >> M) + (b >> M));
+            }
+    } else {
+        const uint16_t* __restrict__ pa = ar + bundle_offset(J) + gA;
 #pragma unroll
-    for (int tb = 0; tb < BT; ++tb)
+        for (int ta = 0; ta < AT; ++ta)
 #pragma unroll
-        for (int bb = 0; bb < BN; ++bb) {
-            const int t = (J >= TB) ? 0 : tb;
-            const uint32_t yl = Tile<K, TB, BB>::y_of(g, t, bb) & low_mask(M);
-            bv[tb][bb] = idB ? (uint32_t)(xl == yl) : (uint32_t)__ldg(br + bundle_offset(M) + yl);
-        }
+            for (int ba = 0; ba < AB; ++ba) {
+                const uint32_t t = (J >= TB) ? ta : (ta << (TB - J));
+                const uint32_t b = (M >= BB) ? 0 : (ba << M);
+                av[ta][ba] = (uint32_t)__ldg(pa + (((t << (K - TB)) >> M) + (b >> M)));
+            }
+    }
+    if (M == s.n2) {
+#pragma unroll
+        for (int tb = 0; tb < BT; ++tb)
+#pragma unroll
+            for (int bb = 0; bb < BN; ++bb) {
+                const uint32_t t = (J >= TB) ? 0 : tb;
+                bv[tb][bb] = (uint32_t)(xl == gB + ((t << (K - TB)) & mlo) + ((uint32_t)bb & mlo));
+            }
+    } else {
+        const uint16_t* __restrict__ pb = br + bundle_offset(M) + gB;
+#pragma unroll
+        for (int tb = 0; tb < BT; ++tb)
+#pragma unroll
+            for (int bb = 0; bb < BN; ++bb) {
+                const uint32_t t = (J >= TB) ? 0 : tb;
+                bv[tb][bb] = (uint32_t)__ldg(pb + (((t << (K - TB)) & mlo) + ((uint32_t)bb & mlo)));
+            }
+    }
 #pragma unroll
     for (int t = 0; t < T; ++t)
 #pragma unroll
@@ -121,6 +149,18 @@ __device__ __forceinline__ void tile_row(const Split& s, const HalfTables& A, co
     const uint16_t* br = B.rows + (size_t)xl * B.stride;
     tile_row_impl<K, TB, BB>(s, ar, br, xh, xl, g, N, std::make_integer_sequence<int, K + 1>{});
 }
+
+// Residency of the two passes.  They wait on L1/L2 table loads, so
+// occupancy pays: tiles of 16 words per thread are compiled for 4 CTAs of 256
+// threads per SM (64 registers; 829 -> 918 iterations/s at 20/10, 10.7 ->
+// 13.5 at 24/12 over 2 CTAs) and launched with 4 CTAs per SM; larger tiles
+// keep their registers and 2 CTAs per SM in the grid.
+template <int TB, int BB>
+struct CountOcc {
+    static constexpr bool small = (1 << (TB + BB)) <= 16;
+    static constexpr int min_blocks = small ? 4 : 1;
+    static constexpr int grid_per_sm = small ? 4 : 2;
+};
 
 // ------------------------------------------------------- compensated FP32
 // Sums of FP32 products carried as an unevaluated pair (hi, lo) of floats.
@@ -156,7 +196,7 @@ __device__ __forceinline__ void split_f32(double v, float& vh, float& vl) {
 // part[blockIdx.x][y]; k_qfold reduces over CTAs.  C32: the per-thread sums
 // run in compensated FP32 (F32Pair) and leave the thread as doubles.
 template <int K, int TB, int BB, bool C32>
-__global__ void __launch_bounds__(256) k_qpass(Split s, HalfTables A, HalfTables B,
+__global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_qpass(Split s, HalfTables A, HalfTables B,
                                                const uint32_t* __restrict__ reps,
                                                const double* __restrict__ p_buf0,
                                                const double* __restrict__ p_buf1, int64_t R,
@@ -241,7 +281,7 @@ __global__ void __launch_bounds__(256) k_qpass(Split s, HalfTables A, HalfTables
 // C32 (MODE 0 only): each thread's share of sum_y N ln q runs in
 // compensated FP32 (F32Pair); the group reduction and h - v/C stay FP64.
 template <int K, int TB, int BB, int MODE, bool C32 = false>
-__global__ void __launch_bounds__(256) k_dpass(Split s, HalfTables A, HalfTables B,
+__global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_dpass(Split s, HalfTables A, HalfTables B,
                                                const uint32_t* __restrict__ reps, int64_t R,
                                                const double* __restrict__ lnq,
                                                const double* __restrict__ h,
@@ -453,6 +493,15 @@ int count_group_size(int k) {
         BDC_K_CASES(C_)
 #undef C_
         default: return 0;
+    }
+}
+
+int count_ctas_per_sm(int k) {
+    switch (k) {
+#define C_(K) case K: return CountOcc<TileChoice<K>::TB, TileChoice<K>::BB>::grid_per_sm;
+        BDC_K_CASES(C_)
+#undef C_
+        default: return 1;
     }
 }
 

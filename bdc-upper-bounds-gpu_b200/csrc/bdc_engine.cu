@@ -195,7 +195,7 @@ bdc_status engine_init(bdc_handle* H) {
     const int cta = count_cta_threads(H->k);
     const int gpc = cta / group > 0 ? cta / group : 1;
     int64_t grid = (R + gpc - 1) / gpc;
-    const int64_t gmax = (int64_t)H->num_sms * 2;
+    const int64_t gmax = (int64_t)H->num_sms * count_ctas_per_sm(H->k);
     if (grid > gmax) grid = gmax;
     if (grid < 1) grid = 1;
     H->grid_count = (int)grid;

@@ -18,6 +18,7 @@ struct CountLaunch {
 
 // ---- count path (bdc_count.cu)
 int count_cta_threads(int k);
+int count_ctas_per_sm(int k);  // CTAs per SM in the grid of the q / D passes
 cudaError_t launch_count_pairs(const Split& s, const HalfTables& A, const HalfTables& B,
                                const uint32_t* xs, const uint32_t* ys, int64_t npairs,
                                uint32_t* out, cudaStream_t stream);
