@@ -27,6 +27,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "bdc_engine.cuh"
@@ -35,7 +36,8 @@ namespace bdc {
 
 constexpr int kAAMax = 10;  // history of the Anderson mixing
 // the restricted problem runs accelerated BA to this bracket (bits), then
-// Newton on the support
+// Newton on the support (Newton from 1e-5 or 1e-6 bits stops short at 16/8 to
+// 26/13 and costs more than the BA steps it saves)
 constexpr double kRestrictedSwitchBits = 1e-7;
 
 // ------------------------------------------------------------ vector kernels
@@ -209,9 +211,39 @@ __global__ void k_orbit_weights(int64_t R, const uint32_t* __restrict__ reps, in
 // acc_part[c][y] = sum_{s in chunk c} |O_s| p_s N(x_s, y)
 constexpr int kRsChunk = 64;
 
+// Device state of the restricted problem's accelerated loop (rs_accelerated):
+// the Anderson Gram matrix by physical history slot, the mixing weights, the
+// bracket of all evaluated points and the flags that gate every kernel of a
+// captured step, so that a CUDA graph of several steps runs without the host.
+struct RsAAState {
+    double A[kAAMax][kAAMax];  // w dF_a . dF_b for physical slots a, b
+    double b[kAAMax];          // w dF_a . f_last, by physical slot
+    double gamma[kAAMax];      // mixing weights of this step, oldest difference first
+    double ub, rate;           // bracket over every evaluated point (nats)
+    double u, r, ua, ra;       // this step's plain and mixed evaluations (nats)
+    double target;             // stop once ub - rate < target (nats)
+    long long evals;
+    int npush;                 // differences pushed since the last clear
+    int have_last;             // f_last / g_last hold the previous pair
+    int solve_ok;              // this step has mixing weights
+    int stop_plain;            // the bracket reached the target at the plain point
+    int stop_mixed;            // ... at the mixed point
+    int fin;                   // finished: every later kernel returns at once
+};
+
+// gate 0: always run; 1: not finished; 2: and the plain point did not stop
+// the loop; 3: and this step has mixing weights
+__device__ __forceinline__ bool rs_skip(const RsAAState* st, int gate) {
+    if (!st || gate == 0) return false;
+    if (st->fin) return true;
+    if (gate >= 2 && st->stop_plain) return true;
+    return gate >= 3 && !st->solve_ok;
+}
+
 __global__ void __launch_bounds__(256) k_rs_acc(int S, int ny, const float* __restrict__ rows,
                                                 const uint8_t* __restrict__ w, const double* __restrict__ p,
-                                                double* __restrict__ part) {
+                                                double* __restrict__ part, const RsAAState* st, int gate) {
+    if (rs_skip(st, gate)) return;
     const int y = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = blockIdx.y;
     if (y >= ny) return;
@@ -221,22 +253,26 @@ __global__ void __launch_bounds__(256) k_rs_acc(int S, int ny, const float* __re
     part[(int64_t)c * ny + y] = a;
 }
 
-// ln q(y) over all y: q(y) = (1/(4C)) sum over the group {id, rev, comp,
-// rev comp} of acc(g y), acc = sum of the chunk partials; ln 0 = 0
-__global__ void k_rs_sum(int ny, int nc, const double* __restrict__ part, double* __restrict__ acc) {
-    const int y = blockIdx.x * blockDim.x + threadIdx.x;
-    if (y >= ny) return;
-    double a = 0.0;
-    for (int c = 0; c < nc; ++c) a += part[(int64_t)c * ny + y];
-    acc[y] = a;
-}
-
-__global__ void k_rs_lnq(int k, double inv_c, const double* __restrict__ acc, double* __restrict__ lnq) {
+// acc(y) = sum of the chunk partials; ln q(y) with q(y) = (1/(4C)) sum over
+// the group {id, rev, comp, rev comp} of acc(g y) (each thread adds the
+// partials of its y's four images itself); ln 0 = 0
+__global__ void k_rs_sum_lnq(int k, int nc, const double* __restrict__ part, double inv_c, double* __restrict__ acc,
+                             double* __restrict__ lnq, const RsAAState* st, int gate) {
+    if (rs_skip(st, gate)) return;
     const int ny = 1 << k;
     const int y = blockIdx.x * blockDim.x + threadIdx.x;
     if (y >= ny) return;
     const uint32_t r = reverse_bits((uint32_t)y, k), c = complement_bits((uint32_t)y, k), rc = reverse_bits(c, k);
-    const double q = 0.25 * inv_c * (acc[y] + acc[r] + acc[c] + acc[rc]);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    for (int ch = 0; ch < nc; ++ch) {
+        const double* pc = part + (int64_t)ch * ny;
+        a0 += pc[y];
+        a1 += pc[r];
+        a2 += pc[c];
+        a3 += pc[rc];
+    }
+    acc[y] = a0;
+    const double q = 0.25 * inv_c * (a0 + a1 + a2 + a3);
     lnq[y] = q > 0.0 ? log(q) : 0.0;
 }
 
@@ -245,7 +281,9 @@ __global__ void k_rs_lnq(int k, double inv_c, const double* __restrict__ acc, do
 __global__ void __launch_bounds__(256) k_rs_div(int S, int ny, const float* __restrict__ rows,
                                                 const double* __restrict__ lnq, const double* __restrict__ h,
                                                 const uint8_t* __restrict__ w, const double* __restrict__ p,
-                                                double inv_c, double* __restrict__ D, double* __restrict__ part) {
+                                                double inv_c, double* __restrict__ D, double* __restrict__ part,
+                                                const RsAAState* st, int gate) {
+    if (rs_skip(st, gate)) return;
     __shared__ double smax[8], ssum[8];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int s = blockIdx.x * 8 + warp;
@@ -276,11 +314,14 @@ __global__ void __launch_bounds__(256) k_rs_div(int S, int ny, const float* __re
 }
 
 // p'_s = p_s e^{D_s - max D} / Z (one block: S is small); out[0] = max D,
-// out[1] = rate of p (nats)
+// out[1] = rate of p (nats).  rec 1 / 2 records them in st as the step's
+// plain / mixed evaluation, adds them to the bracket and sets the stop flag
+// when the bracket is below the target.
 __global__ void __launch_bounds__(1024) k_rs_update(int S, const double* __restrict__ part, int nb,
                                                     const double* __restrict__ D, const uint8_t* __restrict__ w,
                                                     const double* __restrict__ p, double* __restrict__ pn,
-                                                    double* __restrict__ out) {
+                                                    double* __restrict__ out, RsAAState* st, int gate, int rec) {
+    if (rs_skip(st, gate)) return;
     __shared__ double sh[32];
     __shared__ double mD, Zs;
     if (threadIdx.x == 0) {
@@ -292,6 +333,22 @@ __global__ void __launch_bounds__(1024) k_rs_update(int S, const double* __restr
         mD = m;
         out[0] = m;
         out[1] = r;
+        if (rec) {
+            if (rec == 1) {
+                st->u = m;
+                st->r = r;
+            } else {
+                st->ua = m;
+                st->ra = r;
+            }
+            if (isfinite(m)) st->ub = fmin(st->ub, m);
+            if (isfinite(r)) st->rate = fmax(st->rate, r);
+            st->evals += 1;
+            if (st->ub - st->rate < st->target) {
+                if (rec == 1) st->stop_plain = 1;
+                else st->stop_mixed = 1;
+            }
+        }
     }
     __syncthreads();
     double z = 0.0;
@@ -675,18 +732,24 @@ struct Restricted {
         BDC_CUDA_TRY(cudaGetLastError());
         return BDC_OK;
     }
+    // queues p -> pn (four kernels, gated by st / gate, recorded by rec; see
+    // k_rs_update)
+    cudaError_t enqueue_map(bdc_handle* H, const double* p, double* pn, RsAAState* st, int gate, int rec) {
+        cudaStream_t s = H->stream;
+        k_rs_acc<<<dim3((ny + 255) / 256, nc), 256, 0, s>>>(S, ny, rows.get<float>(), w.get<uint8_t>(), p,
+                                                            part.get<double>(), st, gate);
+        k_rs_sum_lnq<<<(ny + 255) / 256, 256, 0, s>>>(H->k, nc, part.get<double>(), H->inv_c, acc.get<double>(),
+                                                      lnq.get<double>(), st, gate);
+        k_rs_div<<<nbd, 256, 0, s>>>(S, ny, rows.get<float>(), lnq.get<double>(), h.get<double>(), w.get<uint8_t>(),
+                                     p, H->inv_c, D.get<double>(), dpart.get<double>(), st, gate);
+        k_rs_update<<<1, 1024, 0, s>>>(S, dpart.get<double>(), nbd, D.get<double>(), w.get<uint8_t>(), p, pn,
+                                       out.get<double>(), st, gate, rec);
+        return cudaGetLastError();
+    }
     // p -> pn; ub / rate (nats) of p
     bdc_status map(bdc_handle* H, const double* p, double* pn, double* ub, double* rate) {
         cudaStream_t s = H->stream;
-        k_rs_acc<<<dim3((ny + 255) / 256, nc), 256, 0, s>>>(S, ny, rows.get<float>(), w.get<uint8_t>(), p,
-                                                            part.get<double>());
-        k_rs_sum<<<(ny + 255) / 256, 256, 0, s>>>(ny, nc, part.get<double>(), acc.get<double>());
-        k_rs_lnq<<<(ny + 255) / 256, 256, 0, s>>>(H->k, H->inv_c, acc.get<double>(), lnq.get<double>());
-        k_rs_div<<<nbd, 256, 0, s>>>(S, ny, rows.get<float>(), lnq.get<double>(), h.get<double>(), w.get<uint8_t>(),
-                                     p, H->inv_c, D.get<double>(), dpart.get<double>());
-        k_rs_update<<<1, 1024, 0, s>>>(S, dpart.get<double>(), nbd, D.get<double>(), w.get<uint8_t>(), p, pn,
-                                       out.get<double>());
-        BDC_CUDA_TRY(cudaGetLastError());
+        BDC_CUDA_TRY(enqueue_map(H, p, pn, nullptr, 0, 0));
         double o[2];
         BDC_CUDA_TRY(cudaMemcpyAsync(o, out.p, sizeof(o), cudaMemcpyDeviceToHost, s));
         BDC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -695,6 +758,295 @@ struct Restricted {
         return BDC_OK;
     }
 };
+
+// ------------------------------- the restricted loop, resident on the device
+// The same Anderson-accelerated BA with the rate guard as accelerated_ba, for
+// the restricted problem, with every decision taken on the device from
+// RsAAState: one step is the plain map, the push of the new differences with
+// their Gram products, the least-squares weights, the mixed point, its map and
+// the choice of the next iterate -- fourteen kernels, captured kRsGraphSteps
+// steps to a CUDA graph; the host reads the state once per graph.
+constexpr int kRsGraphSteps = 16;
+
+struct RsSlots {
+    double* dF[kAAMax];
+    double* dG[kAAMax];
+};
+
+// f = g - x.  After a previous pair: the differences dF = f - f_last and
+// dG = g - g_last go to physical slot sl = npush % m, with block partials of
+// w dF_a . dF_sl and w dF_a . f over the slots in use after the push; then
+// f_last = f, g_last = g.
+__global__ void __launch_bounds__(256) k_rs_push_dots(int L, int m, const uint8_t* __restrict__ wts,
+                                                      const double* __restrict__ x, const double* __restrict__ g,
+                                                      double* __restrict__ f_last, double* __restrict__ g_last,
+                                                      RsSlots P, double* __restrict__ part, const RsAAState* st) {
+    if (rs_skip(st, 2)) return;
+    __shared__ double sh[8];
+    const bool diff = st->have_last != 0;
+    const int sl = st->npush % m;
+    const int act = min(st->npush + 1, m);
+    double a1[kAAMax], a2[kAAMax];
+#pragma unroll
+    for (int a = 0; a < kAAMax; ++a) a1[a] = a2[a] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) {
+        const double gi = g[i], fi = gi - x[i];
+        if (diff) {
+            const double dn = fi - f_last[i];
+            P.dF[sl][i] = dn;
+            P.dG[sl][i] = gi - g_last[i];
+            const double w = (double)wts[i];
+#pragma unroll
+            for (int a = 0; a < kAAMax; ++a)
+                if (a < act) {
+                    const double d = (a == sl) ? dn : P.dF[a][i];
+                    a1[a] = fma(d, w * dn, a1[a]);
+                    a2[a] = fma(d, w * fi, a2[a]);
+                }
+        }
+        f_last[i] = fi;
+        g_last[i] = gi;
+    }
+    if (!diff) return;  // uniform
+    for (int a = 0; a < act; ++a) {
+        const double r1 = block_reduce_sum(a1[a], sh);
+        const double r2 = block_reduce_sum(a2[a], sh);
+        if (threadIdx.x == 0) {
+            part[(size_t)blockIdx.x * 2 * kAAMax + a] = r1;
+            part[(size_t)blockIdx.x * 2 * kAAMax + kAAMax + a] = r2;
+        }
+    }
+}
+
+// one thread: the new Gram row and right side from the partials, then the
+// weights gamma of (A + lambda I) gamma = b by Cholesky with the ridge
+// lambda = 1e-12 tr(A) / c over the c slots in use; solve_ok = 0 when the
+// system is degenerate or this was the first pair after a clear
+__global__ void k_rs_aa_solve(int m, int nb, const double* __restrict__ part, RsAAState* st) {
+    if (rs_skip(st, 2) || threadIdx.x != 0) return;
+    st->solve_ok = 0;
+    if (!st->have_last) {
+        st->have_last = 1;
+        return;
+    }
+    const int sl = st->npush % m;
+    const int c = min(st->npush + 1, m);
+    for (int a = 0; a < c; ++a) {
+        double r1 = 0.0, r2 = 0.0;
+        for (int bb = 0; bb < nb; ++bb) {
+            r1 += part[(size_t)bb * 2 * kAAMax + a];
+            r2 += part[(size_t)bb * 2 * kAAMax + kAAMax + a];
+        }
+        st->A[sl][a] = r1;
+        st->A[a][sl] = r1;
+        st->b[a] = r2;
+    }
+    st->npush += 1;
+    // the system in ring order, oldest difference first: position j holds
+    // physical slot (npush - c + j) % m.  Products and differences are
+    // rounded separately (no FMA contraction), as in the host-side solve of
+    // the full-space loop, so both loops take the same steps on equal data.
+    int ph[kAAMax];
+    for (int j = 0; j < c; ++j) ph[j] = (st->npush - c + j) % m;
+    double M[kAAMax][kAAMax], y[kAAMax], gam[kAAMax];
+    double tr = 0.0;
+    for (int a = 0; a < c; ++a) tr += st->A[ph[a]][ph[a]];
+    if (!(tr > 0.0) || !isfinite(tr)) return;
+    const double lam = 1e-12 * tr / c;
+    for (int a = 0; a < c; ++a)
+        for (int d = 0; d < c; ++d) M[a][d] = st->A[ph[a]][ph[d]] + (a == d ? lam : 0.0);
+    for (int j = 0; j < c; ++j) {
+        double dsum = M[j][j];
+        for (int t = 0; t < j; ++t) dsum = __dsub_rn(dsum, __dmul_rn(M[j][t], M[j][t]));
+        if (!(dsum > 0.0)) return;
+        M[j][j] = sqrt(dsum);
+        for (int i = j + 1; i < c; ++i) {
+            double v = M[i][j];
+            for (int t = 0; t < j; ++t) v = __dsub_rn(v, __dmul_rn(M[i][t], M[j][t]));
+            M[i][j] = v / M[j][j];
+        }
+    }
+    for (int i = 0; i < c; ++i) {
+        double v = st->b[ph[i]];
+        for (int t = 0; t < i; ++t) v = __dsub_rn(v, __dmul_rn(M[i][t], y[t]));
+        y[i] = v / M[i][i];
+    }
+    for (int i = c - 1; i >= 0; --i) {
+        double v = y[i];
+        for (int t = i + 1; t < c; ++t) v = __dsub_rn(v, __dmul_rn(M[t][i], gam[t]));
+        gam[i] = v / M[i][i];
+    }
+    for (int i = 0; i < c; ++i)
+        if (!isfinite(gam[i])) return;
+    for (int i = 0; i < c; ++i) st->gamma[i] = gam[i];  // ring order
+    st->solve_ok = 1;
+}
+
+// xa = g_last - sum_a gamma_a dG_a, clipped at 0; block partials of w xa
+__global__ void __launch_bounds__(256) k_rs_mix(int L, int m, const uint8_t* __restrict__ wts, RsSlots P,
+                                                const double* __restrict__ g_last, double* __restrict__ xa,
+                                                double* __restrict__ part, const RsAAState* st) {
+    if (rs_skip(st, 3)) return;
+    __shared__ double sh[8];
+    const int c = min(st->npush, m);
+    // ring order, oldest first (the order of gamma)
+    double gam[kAAMax];
+    const double* dg[kAAMax];
+#pragma unroll
+    for (int a = 0; a < kAAMax; ++a) {
+        gam[a] = (a < c) ? st->gamma[a] : 0.0;
+        dg[a] = P.dG[(a < c) ? (st->npush - c + a) % m : 0];
+    }
+    double sum = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) {
+        double v = g_last[i];
+#pragma unroll
+        for (int a = 0; a < kAAMax; ++a)
+            if (a < c) v -= gam[a] * dg[a][i];
+        v = v > 0.0 ? v : 0.0;
+        xa[i] = v;
+        sum = fma((double)wts[i], v, sum);
+    }
+    const double r = block_reduce_sum(sum, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = r;
+}
+
+__global__ void k_rs_scale(int L, double* __restrict__ xa, const double* __restrict__ part, int nb,
+                           const RsAAState* st) {
+    if (rs_skip(st, 3)) return;
+    __shared__ double inv;
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int bb = 0; bb < nb; ++bb) t += part[bb];
+        inv = t > 0.0 ? 1.0 / t : 0.0;
+    }
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) xa[i] *= inv;
+}
+
+// the rate guard: the mixed point is kept when it has weights, a finite
+// bound and a rate at least the plain step's
+__device__ __forceinline__ bool rs_mixed_kept(const RsAAState* st) {
+    return st->solve_ok && isfinite(st->ua) && st->ra >= st->r;
+}
+
+// next iterate: the mixed map's image when kept, else the plain image
+__global__ void k_rs_accept_copy(int L, double* __restrict__ x, const double* __restrict__ g,
+                                 const double* __restrict__ ga, const RsAAState* st) {
+    if (rs_skip(st, 1)) return;
+    const double* __restrict__ src = (!st->stop_plain && rs_mixed_kept(st)) ? ga : g;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) x[i] = src[i];
+}
+
+// a rejected mixed point clears the history (when it holds a difference);
+// a stop flag ends the loop
+__global__ void k_rs_accept_state(int m, RsAAState* st) {
+    if (rs_skip(st, 1) || threadIdx.x != 0) return;
+    if (st->stop_plain) {
+        st->fin = 1;
+        return;
+    }
+    if (!rs_mixed_kept(st) && min(st->npush, m) >= 1) {
+        st->npush = 0;
+        st->have_last = 0;
+    }
+    if (st->stop_mixed) st->fin = 1;
+    st->solve_ok = 0;
+}
+
+struct RsAA {
+    int L = 0, m = 0, nb = 0;
+    DevBuf f_last, g_last, part, mpart, st;
+    DevBuf dF[kAAMax], dG[kAAMax];
+
+    cudaError_t init(int len, int mem, int sms) {
+        L = len;
+        m = mem;
+        nb = std::max(1, std::min(sms * 4, (L + 255) / 256));
+        cudaError_t e = dalloc(f_last, sizeof(double) * L);
+        if (e == cudaSuccess) e = dalloc(g_last, sizeof(double) * L);
+        if (e == cudaSuccess) e = dalloc(part, sizeof(double) * nb * 2 * kAAMax);
+        if (e == cudaSuccess) e = dalloc(mpart, sizeof(double) * nb);
+        if (e == cudaSuccess) e = dalloc(st, sizeof(RsAAState));
+        for (int i = 0; i < m && e == cudaSuccess; ++i) {
+            e = dalloc(dF[i], sizeof(double) * L);
+            if (e == cudaSuccess) e = dalloc(dG[i], sizeof(double) * L);
+        }
+        return e;
+    }
+    RsSlots slots() const {
+        RsSlots P{};
+        for (int i = 0; i < m; ++i) {
+            P.dF[i] = dF[i].get<double>();
+            P.dG[i] = dG[i].get<double>();
+        }
+        return P;
+    }
+};
+
+static cudaError_t rs_enqueue_step(bdc_handle* H, Restricted& rs, RsAA& aa, double* x, double* g, double* xa,
+                                   double* ga) {
+    cudaStream_t s = H->stream;
+    RsAAState* st = aa.st.get<RsAAState>();
+    const uint8_t* w = rs.w.get<uint8_t>();
+    cudaError_t e = rs.enqueue_map(H, x, g, st, 1, 1);
+    if (e != cudaSuccess) return e;
+    k_rs_push_dots<<<aa.nb, 256, 0, s>>>(aa.L, aa.m, w, x, g, aa.f_last.get<double>(), aa.g_last.get<double>(),
+                                         aa.slots(), aa.part.get<double>(), st);
+    k_rs_aa_solve<<<1, 32, 0, s>>>(aa.m, aa.nb, aa.part.get<double>(), st);
+    k_rs_mix<<<aa.nb, 256, 0, s>>>(aa.L, aa.m, w, aa.slots(), aa.g_last.get<double>(), xa, aa.mpart.get<double>(),
+                                   st);
+    k_rs_scale<<<aa.nb, 256, 0, s>>>(aa.L, xa, aa.mpart.get<double>(), aa.nb, st);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = rs.enqueue_map(H, xa, ga, st, 3, 2);
+    if (e != cudaSuccess) return e;
+    k_rs_accept_copy<<<aa.nb, 256, 0, s>>>(aa.L, x, g, ga, st);
+    k_rs_accept_state<<<1, 32, 0, s>>>(aa.m, st);
+    return cudaGetLastError();
+}
+
+// accelerated_ba on the restricted problem, resident on the device: runs
+// until the bracket (started from br) is below gap_bits or about max_evals
+// evaluations (checked once per graph of kRsGraphSteps steps); x holds the
+// start and receives the last accepted point
+static bdc_status rs_accelerated(bdc_handle* H, Restricted& rs, RsAA& aa, double* x, double* g, double* xa,
+                                 double* ga, double gap_bits, int64_t max_evals, Bracket& br, int64_t* evals) {
+    cudaStream_t s = H->stream;
+    RsAAState hs;
+    memset(&hs, 0, sizeof(hs));
+    hs.ub = br.ub;
+    hs.rate = br.rate;
+    hs.target = gap_bits * 0.69314718055994530942;
+    BDC_CUDA_TRY(cudaMemcpyAsync(aa.st.p, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+    BDC_CUDA_TRY(cudaStreamSynchronize(s));
+    // captured on the handle's own stream (the caller's may be the legacy
+    // default stream, which cannot be captured), launched on the caller's
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    H->stream = H->own_stream;
+    cudaError_t e = cudaStreamBeginCapture(H->own_stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        for (int k = 0; k < kRsGraphSteps && e == cudaSuccess; ++k) e = rs_enqueue_step(H, rs, aa, x, g, xa, ga);
+        const cudaError_t e2 = cudaStreamEndCapture(H->own_stream, &graph);
+        if (e == cudaSuccess) e = e2;
+    }
+    H->stream = s;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    while (e == cudaSuccess) {
+        e = cudaGraphLaunch(exec, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, aa.st.p, sizeof(hs), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess || hs.fin || hs.evals >= max_evals) break;
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(BDC_ERR_CUDA, "bdc_solve: restricted loop: %s", cudaGetErrorString(e));
+    br.ub = hs.ub;
+    br.rate = hs.rate;
+    *evals += hs.evals;
+    return BDC_OK;
+}
 
 __global__ void __launch_bounds__(1024) k_ridge(double* __restrict__ M, int n, int ld, double rel) {
     __shared__ double sh[32];
@@ -1033,34 +1385,38 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
             for (double& v : hx) v /= z;
             BDC_CUDA_TRY(cudaMemcpyAsync(ps.p, hx.data(), sizeof(double) * Sn, cudaMemcpyHostToDevice, s));
         }
-        Anderson aa;
+        RsAA aa;
         BDC_CUDA_TRY(aa.init(Sn, kAAMax, sms));
+        DevBuf pbak;
+        BDC_CUDA_TRY(dalloc(pbak, sizeof(double) * Sn));
         Bracket rb;
         int64_t revals = 0;
-        auto rmap = [&](const double* pin, double* pout, double* u, double* r) -> bdc_status {
-            return rs.map(H, pin, pout, u, r);
-        };
         // accelerated restricted BA to a moderate gap, then Newton on the
-        // support to the precision of FP64; BA again if the Newton systems
-        // break down
+        // support to the precision of FP64.  Newton starts from a copy of the
+        // BA iterate: when its systems break down or it stops short of the
+        // target, the copy comes back (its steps set members to zero for
+        // good, which BA could not undo) and BA alone runs to the target.
         const double target = std::min(gap_bits * 1e-2, 1e-11);
-        rc = accelerated_ba(H, aa, rs.w.get<uint8_t>(), rmap, ps.get<double>(), pg.get<double>(), psa.get<double>(),
-                            pga.get<double>(), Sn, std::max(target, kRestrictedSwitchBits), 400000, rb, &revals);
+        rc = rs_accelerated(H, rs, aa, ps.get<double>(), pg.get<double>(), psa.get<double>(), pga.get<double>(),
+                            std::max(target, kRestrictedSwitchBits), 400000, rb, &revals);
         if (rc != BDC_OK) return rc;
-        bool newton_ok = false;
         if (rb.gap_bits() >= target) {
+            BDC_CUDA_TRY(cudaMemcpyAsync(pbak.p, ps.p, sizeof(double) * Sn, cudaMemcpyDeviceToDevice, s));
             Bracket nb;
+            bool newton_ok = false;
             rc = newton_polish(H, rs, ps.get<double>(), pg.get<double>(),
                                std::max(1e-5, 100.0 * rb.gap_bits() * 0.69314718055994530942), nb, &newton_ok);
             if (rc != BDC_OK) return rc;
-            if (newton_ok) rb = nb;
+            const bool done = newton_ok && nb.gap_bits() < target;
             if (H->verbose)
                 printf("bdc: solve round %d: Newton on the support %s, restricted gap %.3e bits (%.3f s)\n", round,
-                       newton_ok ? "done" : "failed", nb.gap_bits(), elapsed());
-            if (!newton_ok || rb.gap_bits() >= target) {
-                aa.clear();
-                rc = accelerated_ba(H, aa, rs.w.get<uint8_t>(), rmap, ps.get<double>(), pg.get<double>(),
-                                    psa.get<double>(), pga.get<double>(), Sn, target, 400000, rb, &revals);
+                       done ? "done" : "stopped short", nb.gap_bits(), elapsed());
+            if (done) {
+                rb.add(nb.ub, nb.rate);
+            } else {
+                BDC_CUDA_TRY(cudaMemcpyAsync(ps.p, pbak.p, sizeof(double) * Sn, cudaMemcpyDeviceToDevice, s));
+                rc = rs_accelerated(H, rs, aa, ps.get<double>(), pg.get<double>(), psa.get<double>(),
+                                    pga.get<double>(), target, 400000, rb, &revals);
                 if (rc != BDC_OK) return rc;
             }
         }
