@@ -70,6 +70,7 @@ struct Launch {
     int* map = nullptr;      // CTA -> descriptor index
     int n = 0, tiles = 0, cfg = CFG_64x64;
     int layout = -1;         // -1: register-staged mainloop; else the cp.async one (see k_mma_store)
+    int grid = 0;            // G only: CTAs launched (0: one per tile; fewer: each loops over tiles)
 };
 
 // q side thin product of one term over a slice [s0, s1) of its contraction:
@@ -172,6 +173,15 @@ struct FactoredState {
     double* snap1 = nullptr;
     double* snap2 = nullptr;
     cudaGraphExec_t cycle = nullptr;
+    // captured single BA maps (factored_map), by their vectors
+    struct MapGraph {
+        const double* pin = nullptr;
+        double* pout = nullptr;
+        double* dout = nullptr;
+        cudaGraphExec_t exec = nullptr;
+    };
+    MapGraph maps[4];
+    int maps_next = 0;
 };
 
 namespace bdc {
@@ -232,18 +242,17 @@ __global__ void __launch_bounds__(256) k_mma_store(const GemmDesc* __restrict__ 
 // rows are x_hi, columns x_lo, x = (x_hi << n2) | x_lo; only representatives
 // are updated; block partials [max D, sum |O| e, max (logW - shift),
 // sum |O| p D, input-zero flag] go to ep.part[blockIdx.x * 8 + 0..4].
+// CTA b takes the tiles b, b + gridDim.x, ... of the ntiles that hold
+// representatives (one each when the grid covers them all); with the cp.async
+// mainloop the next tile's first stages are in flight during this tile's
+// epilogue.
 template <int BM, int BN, int WM, int WN, bool WITH_D, bool CP>
 __global__ void __launch_bounds__(256, (BM * BN <= 4096) ? 3 : 2) k_mma_ba(const GemmDesc* __restrict__ descs, const int* __restrict__ tiles,
-                                                   BaEpilogue ep, const DevState* st) {
+                                                   int ntiles, BaEpilogue ep, const DevState* st) {
     using C = MmaCfg<BM, BN, WM, WN>;
     if (gated(st)) return;
     extern __shared__ __align__(16) double smem[];
     const GemmDesc& d = descs[0];
-    const int t = tiles[blockIdx.x];  // the tiles that hold representatives
-    const int m0 = (t / d.tiles_n) * BM, n0 = (t % d.tiles_n) * BN;
-    double acc[C::MT][C::NT][2];
-    if constexpr (CP) mma_mainloop_cp<BM, BN, WM, WN, false, true, 3>(d, m0, n0, smem, acc);
-    else mma_mainloop<BM, BN, WM, WN>(d, m0, n0, smem, acc);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, tq = lane & 3;
     const int wm0 = (warp / WN) * (8 * C::MT), wn0 = (warp % WN) * (8 * C::NT);
@@ -251,6 +260,26 @@ __global__ void __launch_bounds__(256, (BM * BN <= 4096) ? 3 : 2) k_mma_ba(const
     const double lnz = st->log_z;
     const double inv_z = exp(-lnz);
     double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0, zero = 0.0;
+    int ti = blockIdx.x;
+    if constexpr (CP) {
+        if (ti < ntiles) {
+            const int t = tiles[ti];
+            mma_cp_prologue<BM, BN, false, true, 3>(d, (t / d.tiles_n) * BM, (t % d.tiles_n) * BN, smem);
+        }
+    }
+    for (; ti < ntiles; ti += gridDim.x) {
+    const int t = tiles[ti];
+    const int m0 = (t / d.tiles_n) * BM, n0 = (t % d.tiles_n) * BN;
+    double acc[C::MT][C::NT][2];
+    if constexpr (CP) {
+        mma_cp_body<BM, BN, WM, WN, false, true, 3>(d, m0, n0, smem, acc);
+        if (ti + (int)gridDim.x < ntiles) {
+            const int tn = tiles[ti + gridDim.x];
+            mma_cp_prologue<BM, BN, false, true, 3>(d, (tn / d.tiles_n) * BM, (tn % d.tiles_n) * BN, smem);
+        }
+    } else {
+        mma_mainloop<BM, BN, WM, WN>(d, m0, n0, smem, acc);
+    }
 #pragma unroll
     for (int i = 0; i < C::MT; ++i) {
         const int m = m0 + wm0 + i * 8 + g;
@@ -285,6 +314,7 @@ __global__ void __launch_bounds__(256, (BM * BN <= 4096) ? 3 : 2) k_mma_ba(const
                 sR = fma(pw * inv_z, D, sR);
                 if (zero_in) zero = 1.0;
             }
+    }
     }
     __shared__ double red[5][8];
 #pragma unroll
@@ -427,11 +457,12 @@ static cudaError_t launch_store(const Launch& L, cudaStream_t s, const DevState*
 static cudaError_t launch_ba(const Launch& L, const BaEpilogue& ep, cudaStream_t s, const DevState* st) {
     const bool wd = ep.Dout != nullptr, cp = L.layout == 2;
     const int sm = cfg_smem(L.cfg, cp ? 2 : -1);
-#define GO_(ARGS)                                                                                  \
-    if (wd && cp) k_mma_ba<ARGS, true, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);         \
-    else if (wd) k_mma_ba<ARGS, true, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);         \
-    else if (cp) k_mma_ba<ARGS, false, true><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);         \
-    else k_mma_ba<ARGS, false, false><<<L.tiles, 256, sm, s>>>(L.d, L.map, ep, st);
+    const int grid = (L.grid > 0 && L.grid < L.tiles) ? L.grid : L.tiles;
+#define GO_(ARGS)                                                                                        \
+    if (wd && cp) k_mma_ba<ARGS, true, true><<<grid, 256, sm, s>>>(L.d, L.map, L.tiles, ep, st);         \
+    else if (wd) k_mma_ba<ARGS, true, false><<<grid, 256, sm, s>>>(L.d, L.map, L.tiles, ep, st);         \
+    else if (cp) k_mma_ba<ARGS, false, true><<<grid, 256, sm, s>>>(L.d, L.map, L.tiles, ep, st);         \
+    else k_mma_ba<ARGS, false, false><<<grid, 256, sm, s>>>(L.d, L.map, L.tiles, ep, st);
     switch (L.cfg) {
         case CFG_128x128: GO_(BDC_CFG_ARGS_128x128) break;
         case CFG_128x64: GO_(BDC_CFG_ARGS_128x64) break;
@@ -1027,7 +1058,8 @@ k_fac_finalize(const double* __restrict__ part, int nb, double a, DevState* st) 
 // re-scale after an exp over/underflow: Lt -= s, Pw = |O| exp(Lt), sum
 __global__ void __launch_bounds__(256)
 k_fac_rescale(const uint32_t* __restrict__ reps, int64_t R, int n, double* Lt, double* Pw,
-              double* part, DevState* st) {
+              double* part, DevState* st, int on_shift_error) {
+    if (on_shift_error && st->error != kErrShift) return;  // queued unconditionally in a captured map
     const double s = st->max_logw;  // max of Lt after the failed epilogue
     double sum = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
@@ -1049,8 +1081,9 @@ k_fac_rescale(const uint32_t* __restrict__ reps, int64_t R, int n, double* Lt, d
     if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
-__global__ void k_fac_rescale_finish(const double* part, int nb, double a, DevState* st) {
+__global__ void k_fac_rescale_finish(const double* part, int nb, double a, DevState* st, int on_shift_error) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (on_shift_error && st->error != kErrShift) return;
     double sE = 0.0;
     for (int b = 0; b < nb; ++b) sE += part[b];
     // Lt now holds logW - (shift + s) with maximum 0
@@ -1942,28 +1975,38 @@ bdc_status factored_init(bdc_handle* H) {
         ep.Pw = F->Pw;
         ep.inv_c = H->inv_c;
         ep.part = F->epart;
-        int unused = 0;
-        const bool pinned = tf.get("g", &best_cfg, &unused);
+        // each shape one CTA per tile, or (when the tiles outnumber them) as
+        // many CTAs as fit on the SMs at once, each looping over tiles with
+        // the next tile's loads in flight during the epilogue
+        auto resident = [&](int c) { return H->num_sms * ((kCfgBM[c] * kCfgBN[c] <= 4096) ? 3 : 2); };
+        int best_persist = 0;
+        const bool pinned = tf.get("g", &best_cfg, &best_persist);
         for (int c : cfgs) {
             if (pinned) break;
             Launch T;
             BDC_CUDA_TRY(make_tile_launch(T, d, c, F->colmax));
-            const float ms = time_ms(H, [&] { launch_ba(T, ep, H->stream, H->d_st); });
-            free_launch(T);
-            if (ms < best) {
-                best = ms;
-                best_cfg = c;
+            for (int persist = 0; persist < 2; ++persist) {
+                if (persist && T.tiles <= resident(c)) break;
+                T.grid = persist ? resident(c) : 0;
+                const float ms = time_ms(H, [&] { launch_ba(T, ep, H->stream, H->d_st); });
+                if (ms < best) {
+                    best = ms;
+                    best_cfg = c;
+                    best_persist = persist;
+                }
             }
+            free_launch(T);
         }
-        if (!pinned) tf.put("g", best_cfg, 0);
+        if (!pinned) tf.put("g", best_cfg, best_persist);
         tf.save();
         BDC_CUDA_TRY(make_tile_launch(F->g, d, best_cfg, F->colmax));
-        F->ctas_g = F->g.tiles;
+        F->g.grid = best_persist ? std::min(F->g.tiles, resident(best_cfg)) : 0;
+        F->ctas_g = F->g.grid > 0 ? F->g.grid : F->g.tiles;
         if (H->verbose)
-            printf("bdc: tuned G: tile %dx%d, %d of %d tiles hold representatives, %.1f us%s\n", kCfgBM[best_cfg],
-                   kCfgBN[best_cfg], F->g.tiles,
+            printf("bdc: tuned G: tile %dx%d, %d of %d tiles hold representatives, %d CTAs, %.1f us%s\n",
+                   kCfgBM[best_cfg], kCfgBN[best_cfg], F->g.tiles,
                    ((H1 + kCfgBM[best_cfg] - 1) / kCfgBM[best_cfg]) * ((H2 + kCfgBN[best_cfg] - 1) / kCfgBN[best_cfg]),
-                   pinned ? 0.f : best * 1e3f, pinned ? " (pinned)" : "");
+                   F->ctas_g, pinned ? 0.f : best * 1e3f, pinned ? " (pinned)" : "");
         BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
         BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
         BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
@@ -2006,6 +2049,8 @@ void factored_free(bdc_handle* H) {
     if (F->ev_fork) cudaEventDestroy(F->ev_fork);
     if (F->graph) cudaGraphExecDestroy(F->graph);
     if (F->cycle) cudaGraphExecDestroy(F->cycle);
+    for (auto& m : F->maps)
+        if (m.exec) cudaGraphExecDestroy(m.exec);
     cudaFree(F->snap0);
     cudaFree(F->snap1);
     cudaFree(F->snap2);
@@ -2153,6 +2198,40 @@ static bdc_status rescale(bdc_handle* H, double a);
 // zero entry stays zero) -> p_out.  The bound max_x D(x) and the rate I(p;W)
 // of p_in (nats) are left in H->h_st->max_d / rate; with D_out set, D(x) of
 // p_in per representative.  Leaves the handle's iterate at p_out.
+// the kernels of one map, queued on H->stream: load, iteration, re-scale
+// when the iteration flagged an out-of-range shift (the kernels check the
+// flag themselves), D gather, store, and the state copied to the host mirror
+static cudaError_t enqueue_map(bdc_handle* H, const double* p_in, double* p_out, double* D_out) {
+    FactoredState* F = H->fac;
+    cudaStream_t s = H->stream;
+    cudaError_t e = cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    // (Pw is zero away from the representatives from set-up on: every kernel
+    // writes it only there, and the load below rewrites all of them)
+    const int nb = H->nb_upd;
+    k_fac_load<<<nb, 256, 0, s>>>(H->d_reps, H->R, H->n, p_in, F->Pw, F->Lt, F->epart, 1, H->d_st);
+    k_fac_load_finish<<<1, 32, 0, s>>>(F->epart, nb, H->k, H->d_st);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    F->dout = D_out ? F->Ddense : nullptr;
+    e = enqueue_iteration(H, -INFINITY);
+    F->dout = nullptr;
+    if (e != cudaSuccess) return e;
+    k_fac_rescale<<<nb, 256, 0, s>>>(H->d_reps, H->R, H->n, F->Lt, F->Pw, F->epart, H->d_st, 1);
+    k_fac_rescale_finish<<<1, 32, 0, s>>>(F->epart, nb, -INFINITY, H->d_st, 1);
+    if (D_out) k_gather_dense<<<H->num_sms * 8, 256, 0, s>>>(H->d_reps, H->R, H->n, F->Ddense, D_out);
+    k_fac_store<<<nb, 256, 0, s>>>(H->d_reps, H->R, H->n, F->Pw, p_out, H->d_st);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s);
+}
+
+// One BA map on device vectors: p_in (per representative, sum |O| p = 1; a
+// zero entry stays zero) -> p_out.  The bound max_x D(x) and the rate I(p;W)
+// of p_in (nats) are left in H->h_st->max_d / rate; with D_out set, D(x) of
+// p_in per representative.  The kernels of a map are captured once per
+// (p_in, p_out, D_out) into a CUDA graph (the last four are kept), so a map
+// costs one graph launch and one synchronisation.
 bdc_status factored_map(bdc_handle* H, const double* p_in, double* p_out, double* D_out) {
     FactoredState* F = H->fac;
     const int64_t NX = (int64_t)1 << (H->n - 1);
@@ -2160,31 +2239,36 @@ bdc_status factored_map(bdc_handle* H, const double* p_in, double* p_out, double
         BDC_CUDA_TRY(cudaMalloc(&F->Ddense, sizeof(double) * NX));
         H->bytes += sizeof(double) * NX;
     }
-    BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), H->stream));
-    // (Pw is zero away from the representatives from set-up on: every kernel
-    // writes it only there, and the load below rewrites all of them)
-    const int nb = H->nb_upd;
-    k_fac_load<<<nb, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, p_in, F->Pw, F->Lt, F->epart, 1, H->d_st);
-    k_fac_load_finish<<<1, 32, 0, H->stream>>>(F->epart, nb, H->k, H->d_st);
-    BDC_CUDA_TRY(cudaGetLastError());
-    F->dout = D_out ? F->Ddense : nullptr;
-    cudaError_t e = enqueue_iteration(H, -INFINITY);
-    F->dout = nullptr;
-    BDC_CUDA_TRY(e);
-    BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
-    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
-    if (H->h_st->error) {
-        bdc_status rc = factored_recover(H, -INFINITY);
-        if (rc != BDC_OK) return rc;
+    cudaGraphExec_t exec = nullptr;
+    for (auto& m : F->maps)
+        if (m.exec && m.pin == p_in && m.pout == p_out && m.dout == D_out) exec = m.exec;
+    if (!exec) {
+        // captured on the handle's own stream, launched on the caller's
+        cudaStream_t keep = H->stream;
+        BDC_CUDA_TRY(cudaStreamSynchronize(keep));
+        H->stream = H->own_stream;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(H->own_stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            e = enqueue_map(H, p_in, p_out, D_out);
+            const cudaError_t e2 = cudaStreamEndCapture(H->own_stream, &g);
+            if (e == cudaSuccess) e = e2;
+        }
+        H->stream = keep;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        BDC_CUDA_TRY(e);
+        auto& slot = F->maps[F->maps_next];
+        F->maps_next = (F->maps_next + 1) % 4;
+        if (slot.exec) cudaGraphExecDestroy(slot.exec);
+        slot.pin = p_in;
+        slot.pout = p_out;
+        slot.dout = D_out;
+        slot.exec = exec;
     }
-    if (D_out) {
-        k_gather_dense<<<H->num_sms * 8, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Ddense, D_out);
-        BDC_CUDA_TRY(cudaGetLastError());
-    }
-    k_fac_store<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Pw, p_out, H->d_st);
-    BDC_CUDA_TRY(cudaGetLastError());
-    BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
+    BDC_CUDA_TRY(cudaGraphLaunch(exec, H->stream));
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    if (H->h_st->error) return fail(BDC_ERR_NUMERIC, "factored engine: device error %d", H->h_st->error);
     return BDC_OK;
 }
 
@@ -2195,8 +2279,8 @@ bdc_status factored_recover(bdc_handle* H, double a) {
 
 static bdc_status rescale(bdc_handle* H, double a) {
     FactoredState* F = H->fac;
-    k_fac_rescale<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Lt, F->Pw, F->epart, H->d_st);
-    k_fac_rescale_finish<<<1, 32, 0, H->stream>>>(F->epart, H->nb_upd, a, H->d_st);
+    k_fac_rescale<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Lt, F->Pw, F->epart, H->d_st, 0);
+    k_fac_rescale_finish<<<1, 32, 0, H->stream>>>(F->epart, H->nb_upd, a, H->d_st, 0);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
 }

@@ -226,9 +226,25 @@ __device__ __forceinline__ void cp_stage(const GemmDesc& d, int m0, int n0, int 
     }
 }
 
+// The first STAGES-1 stages of a tile's operands, in flight on return.  Issued
+// by every thread; the shared memory of those stages must be free (after the
+// previous tile's body, which ends with all copies landed and a barrier).
+template <int BM, int BN, bool AK, bool BKM, int STAGES>
+__device__ __forceinline__ void mma_cp_prologue(const GemmDesc& d, int m0, int n0, double* smem) {
+    using C = CpCfg<BM, BN, AK, BKM>;
+    const int nk = (d.K + C::BK - 1) / C::BK;
+#pragma unroll
+    for (int st = 0; st < STAGES - 1; ++st) {
+        if (st < nk) cp_stage<BM, BN, AK, BKM>(d, m0, n0, st * C::BK, smem + st * C::STAGE, smem + st * C::STAGE + C::A_ELEMS);
+        cp_async_commit();
+    }
+}
+
+// The k loop of one tile whose prologue is in flight; returns with every copy
+// landed and the shared memory free.
 template <int BM, int BN, int WM, int WN, bool AK, bool BKM, int STAGES>
-__device__ __forceinline__ void mma_mainloop_cp(const GemmDesc& d, int m0, int n0, double* smem,
-                                                double (&acc)[MmaCfg<BM, BN, WM, WN>::MT][MmaCfg<BM, BN, WM, WN>::NT][2]) {
+__device__ __forceinline__ void mma_cp_body(const GemmDesc& d, int m0, int n0, double* smem,
+                                            double (&acc)[MmaCfg<BM, BN, WM, WN>::MT][MmaCfg<BM, BN, WM, WN>::NT][2]) {
     using M_ = MmaCfg<BM, BN, WM, WN>;
     using C = CpCfg<BM, BN, AK, BKM>;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -239,11 +255,6 @@ __device__ __forceinline__ void mma_mainloop_cp(const GemmDesc& d, int m0, int n
 #pragma unroll
         for (int j = 0; j < M_::NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     const int nk = (d.K + C::BK - 1) / C::BK;
-#pragma unroll
-    for (int st = 0; st < STAGES - 1; ++st) {
-        if (st < nk) cp_stage<BM, BN, AK, BKM>(d, m0, n0, st * C::BK, smem + st * C::STAGE, smem + st * C::STAGE + C::A_ELEMS);
-        cp_async_commit();
-    }
     for (int kt = 0; kt < nk; ++kt) {
         cp_async_wait<STAGES - 2>();
         __syncthreads();
@@ -279,6 +290,13 @@ __device__ __forceinline__ void mma_mainloop_cp(const GemmDesc& d, int m0, int n
     }
     cp_async_wait<0>();
     __syncthreads();
+}
+
+template <int BM, int BN, int WM, int WN, bool AK, bool BKM, int STAGES>
+__device__ __forceinline__ void mma_mainloop_cp(const GemmDesc& d, int m0, int n0, double* smem,
+                                                double (&acc)[MmaCfg<BM, BN, WM, WN>::MT][MmaCfg<BM, BN, WM, WN>::NT][2]) {
+    mma_cp_prologue<BM, BN, AK, BKM, STAGES>(d, m0, n0, smem);
+    mma_cp_body<BM, BN, WM, WN, AK, BKM, STAGES>(d, m0, n0, smem, acc);
 }
 
 }  // namespace bdc

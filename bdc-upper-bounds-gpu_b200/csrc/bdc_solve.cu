@@ -958,12 +958,25 @@ struct RsAA {
     int L = 0, m = 0, nb = 0;
     DevBuf f_last, g_last, part, mpart, st;
     DevBuf dF[kAAMax], dG[kAAMax];
+    RsAAState* host[2] = {nullptr, nullptr};  // pinned copies of the state, one per graph in flight
+    cudaEvent_t copied[2] = {nullptr, nullptr};
 
+    ~RsAA() {
+        for (int i = 0; i < 2; ++i) {
+            if (host[i]) cudaFreeHost(host[i]);
+            if (copied[i]) cudaEventDestroy(copied[i]);
+        }
+    }
     cudaError_t init(int len, int mem, int sms) {
         L = len;
         m = mem;
         nb = std::max(1, std::min(sms * 4, (L + 255) / 256));
-        cudaError_t e = dalloc(f_last, sizeof(double) * L);
+        cudaError_t e = cudaSuccess;
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+            e = cudaMallocHost(&host[i], sizeof(RsAAState));
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&copied[i], cudaEventDisableTiming);
+        }
+        if (e == cudaSuccess) e = dalloc(f_last, sizeof(double) * L);
         if (e == cudaSuccess) e = dalloc(g_last, sizeof(double) * L);
         if (e == cudaSuccess) e = dalloc(part, sizeof(double) * nb * 2 * kAAMax);
         if (e == cudaSuccess) e = dalloc(mpart, sizeof(double) * nb);
@@ -1033,12 +1046,29 @@ static bdc_status rs_accelerated(bdc_handle* H, Restricted& rs, RsAA& aa, double
     }
     H->stream = s;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    // two graphs in flight: while the host reads the state after one, the
+    // next already runs (after the loop finishes every kernel returns at
+    // once, so a graph queued past the end changes nothing)
+    auto queue = [&](int i) -> cudaError_t {
+        cudaError_t r = cudaGraphLaunch(exec, s);
+        if (r == cudaSuccess) r = cudaMemcpyAsync(aa.host[i], aa.st.p, sizeof(RsAAState), cudaMemcpyDeviceToHost, s);
+        if (r == cudaSuccess) r = cudaEventRecord(aa.copied[i], s);
+        return r;
+    };
+    int next = 0;
+    if (e == cudaSuccess) e = queue(0);
+    if (e == cudaSuccess) e = queue(1);
     while (e == cudaSuccess) {
-        e = cudaGraphLaunch(exec, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&hs, aa.st.p, sizeof(hs), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess || hs.fin || hs.evals >= max_evals) break;
+        e = cudaEventSynchronize(aa.copied[next]);
+        if (e != cudaSuccess) break;
+        const RsAAState& h = *aa.host[next];
+        if (h.fin || h.evals >= max_evals) break;
+        e = queue(next);
+        next ^= 1;
     }
+    // the last queued graph wrote the other copy
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) hs = *aa.host[next ^ 1];
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (e != cudaSuccess) return fail(BDC_ERR_CUDA, "bdc_solve: restricted loop: %s", cudaGetErrorString(e));

@@ -250,6 +250,26 @@ def ours_arm(args) -> None:
     e2e = {"value": world * e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": R * 8, "d2h_bytes_per_step": R * 8,
            "call": "bdc_baa_iteration (host p in, host p' out)"}
+    # the copies alone (pinned, same sizes): the end-to-end bound is one H2D,
+    # one iteration and one D2H in sequence (each call depends on the last)
+    d_buf = torch.empty(R, dtype=torch.float64, device="cuda")
+    h2d, d2h = [], []
+    for _ in range(5):
+        c0, c1, c2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        c0.record(stream)
+        d_buf.copy_(p_in, non_blocking=True)
+        c1.record(stream)
+        p_out.copy_(d_buf, non_blocking=True)
+        c2.record(stream)
+        torch.cuda.synchronize()
+        h2d.append(c0.elapsed_time(c1))
+        d2h.append(c1.elapsed_time(c2))
+    h2d_ms, d2h_ms = float(np.median(h2d)), float(np.median(d2h))
+    bound_ms = h2d_ms + ms / args.steps + d2h_ms
+    e2e.update({"pcie_h2d_gbs": R * 8 / (h2d_ms / 1e3) / 1e9, "pcie_d2h_gbs": R * 8 / (d2h_ms / 1e3) / 1e9,
+                "bound": world * 1e3 / bound_ms, "frac": (world * e2e_steps / (e2e_ms / 1e3)) / (world * 1e3 / bound_ms),
+                "bound_model": "median pinned H2D + device iteration + D2H, measured in this run"})
+    del d_buf
 
     # roofline of the dominant kernel, with measured pipe peaks
     peaks, peak_src = load_peaks()
