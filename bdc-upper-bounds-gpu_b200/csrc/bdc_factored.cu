@@ -1532,8 +1532,10 @@ cudaError_t dgemm_nt(const double* A, int lda, const double* B, int ldb, double*
 
 bool factored_supports(int n, int k) {
     // needs k < n (W is not the identity), half tables that fit the uint16
-    // bundles, and a dense 2^{n-1} state that fits comfortably in device memory
-    return k >= 1 && k < n && n >= 2 && n <= 28 && k <= 14;
+    // bundles, a dense 2^{n-1} state that fits comfortably in device memory,
+    // and per-term products of at most 64 small outputs: a term's small side
+    // is 2^min(j, k - j), up to 2^floor(k/2)
+    return k >= 1 && k < n && n >= 2 && n <= 28 && k / 2 <= 6;
 }
 
 bdc_status factored_init(bdc_handle* H) {

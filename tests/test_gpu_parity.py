@@ -231,3 +231,16 @@ def test_underflowed_entries_reenter_like_reference(bdc, O):
             assert np.isinf(st["mx"])
             st = E.iterate(3, -1.0)
             np.testing.assert_allclose(E.get_p(), ref["p"], rtol=1e-11, atol=0)
+
+
+def test_engine_selection_by_size(bdc):
+    # the factored engine's per-term products hold up to 64 small outputs, a
+    # term's small side being 2^min(j, k - j): k <= 13; auto falls back to
+    # the count path above that
+    with bdc.Engine(16, 14) as E:
+        assert E.engine == "count"
+    with pytest.raises(bdc.BDCError) as e:
+        bdc.Engine(16, 14, engine="factored")
+    assert e.value.status == 6
+    with bdc.Engine(16, 13) as E:
+        assert E.engine == "factored"
