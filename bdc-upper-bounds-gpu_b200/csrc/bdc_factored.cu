@@ -1482,8 +1482,12 @@ static bdc_status tune_class(bdc_handle* H, TuneFile& tf, const char* key, const
     const int cfgs[5] = {CFG_128x16, CFG_128x32, CFG_64x64, CFG_128x64, CFG_64x128};
     int best_cfg = -1, unused = 0;
     const bool pinned = tf.get(key, &best_cfg, &unused);
-    const float core_ms = pinned ? 0.f : time_ms(H, core_launch);
-    float best = core_ms;
+    // the CUDA-core kernels hold one accumulator per small output in
+    // registers, up to 64; wider terms always take a tensor-core tile
+    const bool core_ok = lg <= 6;
+    const float core_ms = (pinned || !core_ok) ? 0.f : time_ms(H, core_launch);
+    float best = core_ok ? core_ms : 1e30f;
+    if (pinned && !core_ok && best_cfg < 0) best_cfg = CFG_64x64;
     for (int c : cfgs) {
         if (pinned) break;
         Launch T;
@@ -1533,9 +1537,9 @@ cudaError_t dgemm_nt(const double* A, int lda, const double* B, int ldb, double*
 bool factored_supports(int n, int k) {
     // needs k < n (W is not the identity), half tables that fit the uint16
     // bundles, a dense 2^{n-1} state that fits comfortably in device memory,
-    // and per-term products of at most 64 small outputs: a term's small side
-    // is 2^min(j, k - j), up to 2^floor(k/2)
-    return k >= 1 && k < n && n >= 2 && n <= 28 && k / 2 <= 6;
+    // and per-term products of at most 128 small outputs (a term's small side
+    // is 2^min(j, k - j), up to 2^floor(k/2))
+    return k >= 1 && k < n && n >= 2 && n <= 28 && k <= 14;
 }
 
 bdc_status factored_init(bdc_handle* H) {
@@ -1772,7 +1776,7 @@ bdc_status factored_init(bdc_handle* H) {
             }
             int lg = 0;
             while ((1 << lg) < q.SMALL) ++lg;
-            if (lg > 6) return fail(BDC_ERR_UNSUPPORTED, "factored engine: term with more than 64 small outputs");
+            if (lg > 7) return fail(BDC_ERR_UNSUPPORTED, "factored engine: term with more than 128 small outputs");
             qplan.push_back({ti, lg, q, 1});
             qctas_one += (q.WIDE + 255) / 256;
             td[lg].push_back(d);

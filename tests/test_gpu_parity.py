@@ -177,7 +177,7 @@ def test_reference_shaped_api(bdc, O):
     assert bdc.compute_max_deviation(pn, p) == pytest.approx(O.max_deviation(pn, p), abs=1e-13)
 
 
-@pytest.mark.parametrize("n,k", [(14, 7), (15, 6), (17, 9), (18, 6), (12, 11), (11, 2)])
+@pytest.mark.parametrize("n,k", [(14, 7), (15, 6), (17, 9), (18, 6), (12, 11), (11, 2), (16, 14), (19, 14)])
 def test_factored_equals_count_engine(bdc, O, n, k):
     """The two engines run the same iteration: after 6 iterations from a
     Dirichlet start their iterates and statistics agree to rounding."""
@@ -234,13 +234,11 @@ def test_underflowed_entries_reenter_like_reference(bdc, O):
 
 
 def test_engine_selection_by_size(bdc):
-    # the factored engine's per-term products hold up to 64 small outputs, a
-    # term's small side being 2^min(j, k - j): k <= 13; auto falls back to
-    # the count path above that
-    with bdc.Engine(16, 14) as E:
+    # k = n has no factored form (W is the identity): auto takes the count path
+    with bdc.Engine(12, 12) as E:
         assert E.engine == "count"
     with pytest.raises(bdc.BDCError) as e:
-        bdc.Engine(16, 14, engine="factored")
+        bdc.Engine(12, 12, engine="factored")
     assert e.value.status == 6
-    with bdc.Engine(16, 13) as E:
+    with bdc.Engine(16, 14) as E:
         assert E.engine == "factored"
