@@ -603,6 +603,62 @@ def precision_check(args) -> dict:
     return {"precision": out}
 
 
+def generator_check(args) -> dict:
+    """The cache generator: the reference's CPU program (built from its sources
+    into oracle/_ref/, when present) and this repository's GPU one
+    (generate_bit_transition_cache, same argv, same files), each run as a
+    process in an empty directory, wall clock including the process start (for
+    ours the CUDA context too) and the file writes; the files of both must be
+    identical.  ours_counts_only_s is the GPU generation of the same tables
+    inside this process, copied to host memory, without files.  The reference runs up to N = 12 (its
+    time grows about 4x per N: N = 13 takes about a minute), ours up to 13."""
+    import hashlib
+    import shutil
+
+    ours = os.path.join(REPO, "bdc-upper-bounds-gpu_b200", "generate_bit_transition_cache")
+    ref = os.path.join(REPO, "oracle", "_ref", "generate_bit_transition_cache")
+
+    def run(exe, N):
+        d = tempfile.mkdtemp(prefix="bdc_gen_")
+        try:
+            os.makedirs(os.path.join(d, "transition_counts"))
+            t0 = time.perf_counter()
+            subprocess.run([exe, str(N)], cwd=d, check=True, stdout=subprocess.DEVNULL, timeout=600)
+            sec = time.perf_counter() - t0
+            h = hashlib.sha256()
+            nbytes = 0
+            for f in sorted(os.listdir(os.path.join(d, "transition_counts"))):
+                b = open(os.path.join(d, "transition_counts", f), "rb").read()
+                nbytes += len(b)
+                h.update(f.encode() + b)
+            return sec, h.hexdigest(), nbytes
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+
+    # the counts alone, in this process after a warm-up call (no process start,
+    # no CUDA context creation, no file writes)
+    import bdc_b200
+    bdc_b200.generate_cache(4, 2)
+
+    def counts_only(N):
+        t0 = time.perf_counter()
+        for n in range(N + 1):
+            for k in range(n):
+                bdc_b200.generate_cache(n, k)
+        return time.perf_counter() - t0
+
+    out = []
+    for N in (9, 10, 11, 12, 13):
+        row = {"N": N}
+        sec, dig, nbytes = run(ours, N)
+        row.update({"ours_s": sec, "ours_counts_only_s": counts_only(N), "bytes": nbytes})
+        if N <= 12 and os.path.exists(ref):
+            rsec, rdig, _ = run(ref, N)
+            row.update({"reference_s": rsec, "identical_files": rdig == dig, "speedup": rsec / sec})
+        out.append(row)
+    return {"generator": out, "reference": ref if os.path.exists(ref) else "not built"}
+
+
 def kernels_only(args) -> None:
     """Engine set-up and `steps` iterations, nothing else: the command that
     the ncu captures under profiles/ run."""
@@ -626,7 +682,8 @@ def main() -> None:
     ap.add_argument("--engine", default="auto")
     ap.add_argument("--cpu-sample", type=int, default=20000)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", choices=["bench", "kernels", "ttb", "batch", "adjoint", "precision"], default="bench")
+    ap.add_argument("--mode", choices=["bench", "kernels", "ttb", "batch", "adjoint", "precision", "gen"],
+                    default="bench")
     ap.add_argument("--ttb-budget", type=float, default=15.0,
                     help="device seconds for each of the plain and squarem legs of time-to-bound")
     ap.add_argument("--no-ttb", action="store_true")
@@ -643,6 +700,8 @@ def main() -> None:
         print(json.dumps({"adjoint": adjoint_check(args)}), flush=True)
     elif args.mode == "precision":
         print(json.dumps(precision_check(args)), flush=True)
+    elif args.mode == "gen":
+        print(json.dumps(generator_check(args)), flush=True)
     elif args.mode == "batch":
         res = batched(args)
         if res is not None:
