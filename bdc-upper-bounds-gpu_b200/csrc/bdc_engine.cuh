@@ -92,7 +92,19 @@ cudaError_t factored_enqueue_iteration(bdc_handle* H, double a);
 // any other device error is returned as BDC_ERR_NUMERIC
 bdc_status factored_recover(bdc_handle* H, double a);
 bdc_status factored_map(bdc_handle* H, const double* p_in, double* p_out, double* D_out);
-cudaError_t dgemm_nt(const double* A, int lda, const double* B, int ldb, double* C, int ldc, int M, int N, int K,
-                     double alpha, int accumulate, cudaStream_t s);
+// Device buffers for dgemm_nt: one product descriptor and a tile map (every
+// tile on descriptor 0) of up to `tiles` 64x64 tiles, allocated once by the
+// caller and reused by every call on one stream.
+struct DgemmScratch {
+    void* desc = nullptr;
+    int* map = nullptr;
+    int tiles = 0;
+};
+cudaError_t dgemm_scratch_alloc(DgemmScratch& sc, int max_tiles, cudaStream_t s);
+void dgemm_scratch_free(DgemmScratch& sc);
+// C (M x N) = alpha A B^T (+ C) on the FP64 tensor-core path, queued on s
+// without allocating or synchronising
+cudaError_t dgemm_nt(const DgemmScratch& sc, const double* A, int lda, const double* B, int ldb, double* C, int ldc,
+                     int M, int N, int K, double alpha, int accumulate, cudaStream_t s);
 
 }  // namespace bdc

@@ -1511,26 +1511,49 @@ static bdc_status tune_class(bdc_handle* H, TuneFile& tf, const char* key, const
     return BDC_OK;
 }
 
+cudaError_t dgemm_scratch_alloc(DgemmScratch& sc, int max_tiles, cudaStream_t s) {
+    dgemm_scratch_free(sc);
+    cudaError_t e = cudaMalloc(&sc.desc, sizeof(GemmDesc));
+    if (e == cudaSuccess) e = cudaMalloc(&sc.map, sizeof(int) * (size_t)std::max(1, max_tiles));
+    if (e == cudaSuccess) e = cudaMemsetAsync(sc.map, 0, sizeof(int) * (size_t)std::max(1, max_tiles), s);
+    if (e == cudaSuccess) sc.tiles = max_tiles;
+    return e;
+}
+
+void dgemm_scratch_free(DgemmScratch& sc) {
+    cudaFree(sc.desc);
+    cudaFree(sc.map);
+    sc = DgemmScratch{};
+}
+
 // C (M x N, row stride ldc) = alpha A B^T (+ C when accumulate) for row-major
 // A (M x K, stride lda) and B (N x K, stride ldb) on the FP64 tensor-core
 // path; a helper for small dense work outside the iteration (the certified
-// solver's Newton systems)
-cudaError_t dgemm_nt(const double* A, int lda, const double* B, int ldb, double* C, int ldc, int M, int N, int K,
-                     double alpha, int accumulate, cudaStream_t s) {
+// solver's Newton systems).  The descriptor goes to sc.desc on the same
+// stream, so a call does not overwrite it under the previous call's kernel.
+cudaError_t dgemm_nt(const DgemmScratch& sc, const double* A, int lda, const double* B, int ldb, double* C, int ldc,
+                     int M, int N, int K, double alpha, int accumulate, cudaStream_t s) {
     static bool attrs = false;
     if (!attrs) {
         cudaError_t e = set_smem_attrs();
         if (e != cudaSuccess) return e;
         attrs = true;
     }
-    GemmDesc d = make_desc(op_f64(A, lda, 0), op_f64(B, ldb, 1), C, ldc, 1, M, N, K);
-    d.alpha = alpha;
-    d.accumulate = accumulate;
+    std::vector<GemmDesc> v{make_desc(op_f64(A, lda, 0), op_f64(B, ldb, 1), C, ldc, 1, M, N, K)};
+    v[0].alpha = alpha;
+    v[0].accumulate = accumulate;
     Launch L;
-    cudaError_t e = make_launch(L, {d}, CFG_64x64);
+    L.cfg = CFG_64x64;
+    L.layout = cp_layout(v);
+    L.n = 1;
+    L.tiles = assign_tiles(v, CFG_64x64);
+    if (L.tiles > sc.tiles || !sc.desc) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemcpyAsync(sc.desc, v.data(), sizeof(GemmDesc), cudaMemcpyHostToDevice, s);
+    L.d = (GemmDesc*)sc.desc;
+    L.map = sc.map;
     if (e == cudaSuccess) e = launch_store(L, s, nullptr);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    free_launch(L);
+    L.d = nullptr;  // owned by the scratch
+    L.map = nullptr;
     return e;
 }
 

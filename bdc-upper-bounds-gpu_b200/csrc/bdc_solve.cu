@@ -1114,6 +1114,13 @@ static bdc_status newton_polish(bdc_handle* H, Restricted& rs, double* p, double
     BDC_CUDA_TRY(dalloc(pn, sizeof(double) * S));
     BDC_CUDA_TRY(dalloc(out, sizeof(double) * 4));
     BDC_CUDA_TRY(dalloc(bad, sizeof(int)));
+    // one descriptor and tile map for every product below (at most S x S)
+    struct ScratchHolder {
+        DgemmScratch sc;
+        ~ScratchHolder() { dgemm_scratch_free(sc); }
+    } gh;
+    BDC_CUDA_TRY(dgemm_scratch_alloc(gh.sc, ((S + 63) / 64) * ((S + 63) / 64), s));
+    const DgemmScratch& gsc = gh.sc;
     std::vector<double> hD(S), hp(S);
     auto fetch = [&]() -> bdc_status {
         BDC_CUDA_TRY(cudaMemcpyAsync(hD.data(), rs.D.p, sizeof(double) * S, cudaMemcpyDeviceToHost, s));
@@ -1146,7 +1153,8 @@ static bdc_status newton_polish(bdc_handle* H, Restricted& rs, double* p, double
             k_nt_rows<<<g, 256, 0, s>>>(nF, H->k, dF.get<int>(), rs.rows.get<float>(), rs.acc.get<double>(), H->inv_c,
                                         Bq.get<double>());
             BDC_CUDA_TRY(cudaGetLastError());
-            BDC_CUDA_TRY(dgemm_nt(Bq.get<double>(), ny, Bq.get<double>(), ny, M.get<double>(), nF, nF, nF, ny, 1.0, 0, s));
+            BDC_CUDA_TRY(dgemm_nt(gsc, Bq.get<double>(), ny, Bq.get<double>(), ny, M.get<double>(), nF, nF, nF, ny, 1.0,
+                                  0, s));
             k_ridge<<<1, 1024, 0, s>>>(M.get<double>(), nF, nF, 1e-15);
             BDC_CUDA_TRY(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
             for (int j0 = 0; j0 < nF; j0 += 32) {
@@ -1154,7 +1162,7 @@ static bdc_status newton_polish(bdc_handle* H, Restricted& rs, double* p, double
                 k_chol_panel<<<1, 1024, 0, s>>>(M.get<double>(), nF, nF, j0, j1, bad.get<int>());
                 BDC_CUDA_TRY(cudaGetLastError());
                 if (j1 < nF)
-                    BDC_CUDA_TRY(dgemm_nt(M.get<double>() + (int64_t)j1 * nF + j0, nF, M.get<double>() + (int64_t)j1 * nF + j0,
+                    BDC_CUDA_TRY(dgemm_nt(gsc, M.get<double>() + (int64_t)j1 * nF + j0, nF, M.get<double>() + (int64_t)j1 * nF + j0,
                                           nF, M.get<double>() + (int64_t)j1 * nF + j1, nF, nF - j1, nF - j1, j1 - j0, -1.0,
                                           1, s));
             }
@@ -1346,6 +1354,9 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
         br.add(ub, rate);
         cert_ub = ub;
         cert_rate = rate;
+        if (H->verbose)
+            printf("bdc: solve round %d: full evaluation with D, bracket %.3e bits (%.3f s)\n", round,
+                   (ub - rate) / 0.69314718055994530942, elapsed());
         if ((ub - rate) / 0.69314718055994530942 < gap_bits) {
             certified = true;
             break;
@@ -1392,6 +1403,8 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
         Restricted rs;
         rc = rs.build(H, members);
         if (rc != BDC_OK) return rc;
+        if (H->verbose)
+            printf("bdc: solve round %d: %zu members, rows built (%.3f s)\n", round, members.size(), elapsed());
         const int Sn = rs.S;
         DevBuf ps, pg, psa, pga;
         BDC_CUDA_TRY(dalloc(ps, sizeof(double) * Sn));
@@ -1430,6 +1443,9 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
         rc = rs_accelerated(H, rs, aa, ps.get<double>(), pg.get<double>(), psa.get<double>(), pga.get<double>(),
                             std::max(target, kRestrictedSwitchBits), 400000, rb, &revals);
         if (rc != BDC_OK) return rc;
+        if (H->verbose)
+            printf("bdc: solve round %d: restricted BA, %lld evaluations, restricted gap %.3e bits (%.3f s)\n", round,
+                   (long long)revals, rb.gap_bits(), elapsed());
         if (rb.gap_bits() >= target) {
             BDC_CUDA_TRY(cudaMemcpyAsync(pbak.p, ps.p, sizeof(double) * Sn, cudaMemcpyDeviceToDevice, s));
             Bracket nb;
