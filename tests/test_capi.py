@@ -100,3 +100,27 @@ def test_host_helpers_match_oracle(bdc, O):
     assert abs(np.sum(O.orbits_of(reps, 10) * p) - 1) < 1e-14
     full = dist.expand_to_full(p, 10)
     assert np.allclose(dist.orbit_average(full, 10), p, rtol=0, atol=0)
+
+
+def test_orbit_means_from_representatives_are_bit_identical():
+    # the O(#reps) orbit means (dist.orbit_mean_at_reps) against the O(2^n)
+    # bincount over all strings (dist.orbit_average), odd and even n
+    from bdc_b200 import dist
+    for n in (7, 10, 13, 16):
+        g = np.random.default_rng(n).gamma(0.5, 1.0, size=1 << n)
+        assert np.array_equal(dist.orbit_mean_at_reps(g, n), dist.orbit_average(g, n))
+
+
+def test_bit_reversal_table_matches_bitwise_definition(bdc):
+    rng = np.random.default_rng(3)
+    for n in (1, 5, 8, 12, 17, 24, 31):
+        xs = rng.integers(0, 1 << n, 2000, dtype=np.uint64)
+        want = np.array([int(format(int(x), f"0{n}b")[::-1], 2) for x in xs], dtype=np.uint64)
+        assert np.array_equal(bdc.reverse_bits(xs, n).astype(np.uint64), want)
+
+
+def test_dirichlet_starts_are_seeded():
+    from bdc_b200 import dist
+    a, b, c = dist.dirichlet_start(12, 0.5, 4), dist.dirichlet_start(12, 0.5, 4), dist.dirichlet_start(12, 0.5, 5)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    assert np.all(a > 0)
