@@ -42,7 +42,7 @@ EXPORTED_SYMBOLS = [
     "bdc_write_dist_file", "bdc_work", "bdc_profile", "bdc_set_stream", "bdc_peak_probe",
     "bdc_max_deviation_noalloc", "bdc_accelerate", "bdc_mi_forward", "bdc_mi_backward",
     "bdc_batch_create", "bdc_batch_iterate", "bdc_batch_destroy", "bdc_batch_set_stream", "bdc_solve",
-    "bdc_bound_error",
+    "bdc_bound_error", "bdc_shard_q", "bdc_shard_set_q", "bdc_shard_update_begin", "bdc_shard_update_end",
 ]
 
 
@@ -116,6 +116,11 @@ def library() -> ctypes.CDLL:
     L.bdc_batch_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.bdc_mi_forward.argtypes = [h, _f64p, ctypes.c_int64, _f64p]
     L.bdc_mi_backward.argtypes = [h, _f64p, ctypes.c_int64]
+    L.bdc_bound_error.argtypes = [h, _f64p, _f64p]
+    L.bdc_shard_q.argtypes = [h, ctypes.c_int64, ctypes.c_int64, _f64p, ctypes.c_int64]
+    L.bdc_shard_set_q.argtypes = [h, _f64p, ctypes.c_int64]
+    L.bdc_shard_update_begin.argtypes = [h, ctypes.c_int64, ctypes.c_int64, _f64p]
+    L.bdc_shard_update_end.argtypes = [h, ctypes.c_int64, ctypes.c_int64, ctypes.c_double, _f64p]
     L.bdc_log_q.argtypes = [h, _f64p, ctypes.c_int64]
     L.bdc_log_w.argtypes = [h, _f64p, _f64p, ctypes.c_int64]
     L.bdc_divergence.argtypes = [h, _f64p, _f64p, ctypes.c_int64]
@@ -251,6 +256,32 @@ class Engine:
         st = Stats()
         _check(library().bdc_iterate(self._h, int(max_iters), float(a), ctypes.byref(st)), "bdc_iterate")
         return st.as_dict()
+
+    # ------------------------------------------------ one rank of sharded BA
+    def shard_q(self, r0: int, r1: int) -> np.ndarray:
+        """Partial q sums of representatives [r0, r1): acc[y] over all 2^k y."""
+        acc = np.empty(1 << self.k, dtype=np.float64)
+        _check(library().bdc_shard_q(self._h, ctypes.c_int64(r0), ctypes.c_int64(r1), acc.ctypes.data_as(_f64p),
+                                     ctypes.c_int64(len(acc))), "bdc_shard_q")
+        return acc
+
+    def shard_set_q(self, acc) -> None:
+        acc = np.ascontiguousarray(acc, dtype=np.float64)
+        _check(library().bdc_shard_set_q(self._h, acc.ctypes.data_as(_f64p), ctypes.c_int64(len(acc))),
+               "bdc_shard_set_q")
+
+    def shard_update_begin(self, r0: int, r1: int) -> np.ndarray:
+        """[max logW, sum |O| exp(logW - max), max D, sum |O| p D, zero flag] on the shard."""
+        st = np.empty(5, dtype=np.float64)
+        _check(library().bdc_shard_update_begin(self._h, ctypes.c_int64(r0), ctypes.c_int64(r1),
+                                                st.ctypes.data_as(_f64p)), "bdc_shard_update_begin")
+        return st
+
+    def shard_update_end(self, r0: int, r1: int, log_z: float) -> float:
+        mx = ctypes.c_double()
+        _check(library().bdc_shard_update_end(self._h, ctypes.c_int64(r0), ctypes.c_int64(r1),
+                                              ctypes.c_double(log_z), ctypes.byref(mx)), "bdc_shard_update_end")
+        return mx.value
 
     def bound_error(self) -> tuple[float, float]:
         """(|upper_bound - FP64|, |rate - FP64|) in bits for the last

@@ -254,6 +254,7 @@ void engine_free(bdc_handle* H) {
     cudaFree(H->d_qpart);
     cudaFree(H->d_lnq64);
     cudaFree(H->d_d64);
+    cudaFree(H->d_shard);
     cudaFree(H->d_red);
     cudaFree(H->d_scalar);
     cudaFree(H->d_st);

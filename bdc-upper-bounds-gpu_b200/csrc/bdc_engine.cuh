@@ -44,6 +44,7 @@ struct bdc_handle {
     // reductions / state
     double* d_red = nullptr;
     double* d_scalar = nullptr;
+    double* d_shard = nullptr;   // [2^k] summed q partials of a sharded iteration (on first use)
     bdc::DevState* d_st = nullptr;
     bdc::DevState* h_st = nullptr;  // pinned mirror
     int grid_count = 0;

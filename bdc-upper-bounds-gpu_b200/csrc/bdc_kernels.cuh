@@ -55,6 +55,9 @@ struct UpdateLaunch {
     cudaStream_t stream;
 };
 cudaError_t launch_update(const UpdateLaunch& U);
+// stages 1 (logW, max logW = shift, max D, rate), 2 (e = exp(logW - shift),
+// ln Z) and 3 (p' = e / exp(DevState::log_z), mx, buffer flip): first..last
+cudaError_t launch_update_stages(const UpdateLaunch& U, int first, int last);
 cudaError_t launch_logw(int n, const uint32_t* reps, int64_t R, const double* p, const double* d,
                         double* logw, cudaStream_t stream);
 cudaError_t launch_mi_grad(int n, const uint32_t* reps, int64_t R, const double* d, double* grad,

@@ -181,14 +181,18 @@ k_upd_norm(int64_t R, double* __restrict__ p0, double* __restrict__ p1, double* 
     }
 }
 
-cudaError_t launch_update(const UpdateLaunch& U) {
-    k_upd_logw<<<U.nblocks, kUpdThreads, 0, U.stream>>>(U.n, U.reps, U.R, U.p0, U.p1, U.d, U.logw,
-                                                        U.part, U.st);
-    k_upd_exp<<<U.nblocks, kUpdThreads, 0, U.stream>>>(U.n, U.reps, U.R, U.p0, U.p1, U.logw, U.part,
-                                                       U.st);
-    k_upd_norm<<<U.nblocks, kUpdThreads, 0, U.stream>>>(U.R, U.p0, U.p1, U.part, U.a, U.st);
+cudaError_t launch_update_stages(const UpdateLaunch& U, int first, int last) {
+    if (first <= 1 && last >= 1)
+        k_upd_logw<<<U.nblocks, kUpdThreads, 0, U.stream>>>(U.n, U.reps, U.R, U.p0, U.p1, U.d, U.logw,
+                                                            U.part, U.st);
+    if (first <= 2 && last >= 2)
+        k_upd_exp<<<U.nblocks, kUpdThreads, 0, U.stream>>>(U.n, U.reps, U.R, U.p0, U.p1, U.logw, U.part,
+                                                           U.st);
+    if (first <= 3 && last >= 3) k_upd_norm<<<U.nblocks, kUpdThreads, 0, U.stream>>>(U.R, U.p0, U.p1, U.part, U.a, U.st);
     return cudaGetLastError();
 }
+
+cudaError_t launch_update(const UpdateLaunch& U) { return launch_update_stages(U, 1, 3); }
 
 // ---------------------------------------------------------------- helpers
 __global__ void k_logw(int n, const uint32_t* __restrict__ reps, int64_t R,

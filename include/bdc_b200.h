@@ -147,6 +147,26 @@ bdc_status bdc_mi_backward(bdc_handle_t h, double* grad, int64_t num_reps);
  * engine, n <= 26. */
 bdc_status bdc_solve(bdc_handle_t h, double gap_bits, int64_t max_evals, bdc_stats* stats);
 
+/* Sharded BA (no counterpart in the reference, which runs one (n,k) on one
+ * GPU): rank r of a group owns the representatives [rep_begin, rep_end) of a
+ * count-engine handle (every rank holds the whole problem and sets the same
+ * distribution) and touches p only there.  One iteration:
+ *   bdc_shard_q(acc)             partial q sums, acc[y] for all 2^k raw y
+ *   -- the caller sums acc over the ranks (an all-reduce) --
+ *   bdc_shard_set_q(acc)         ln q from the summed sums
+ *   bdc_shard_update_begin(st)   D and logW on the shard; st = {s = max logW,
+ *                                Z = sum |O| exp(logW - s), max D (nats),
+ *                                sum |O| p D (nats), input-zero flag}
+ *   -- the caller forms S = max s, Z_all = sum Z exp(s - S) over the ranks,
+ *      the bound max D and the rate sum --
+ *   bdc_shard_update_end(ln Z_all + S - s, &mx)   p' on the shard, local mx
+ *   -- the caller takes the max of mx over the ranks (the stopping rule) --
+ * bdc_b200.sharded runs this loop over torch.distributed. */
+bdc_status bdc_shard_q(bdc_handle_t h, int64_t rep_begin, int64_t rep_end, double* acc, int64_t ny);
+bdc_status bdc_shard_set_q(bdc_handle_t h, const double* acc, int64_t ny);
+bdc_status bdc_shard_update_begin(bdc_handle_t h, int64_t rep_begin, int64_t rep_end, double* stats5);
+bdc_status bdc_shard_update_end(bdc_handle_t h, int64_t rep_begin, int64_t rep_end, double log_z, double* mx);
+
 /* Batches (no counterpart in the reference, which runs one (n,k) per
  * process): many handles -- different (n,k) and starting distributions --
  * iterated together from one captured CUDA graph with one branch per handle.
