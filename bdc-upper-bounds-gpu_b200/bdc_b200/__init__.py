@@ -198,6 +198,7 @@ class Engine:
         _check(L.bdc_create(n, k, ctypes.byref(o), ctypes.byref(hdl)), "bdc_create")
         self._h = hdl
         self.n, self.k = n, k
+        self.device = int(device)
         nn, kk, R, eng = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64(), ctypes.c_int()
         _check(L.bdc_info(self._h, ctypes.byref(nn), ctypes.byref(kk), ctypes.byref(R),
                           ctypes.byref(eng)), "bdc_info")

@@ -7,12 +7,16 @@ contiguous range shard_range(R, r, world) of the representatives: the q pass,
 the D pass and the update touch p only there.  Per iteration the ranks
 exchange
   * the 2^k partial q sums (one all-reduce of 2^k doubles),
-  * the update's shift and normaliser, the bound and the rate (two small
-    all-reduces: max, then sum and max),
+  * the update's shift and the bound (one max all-reduce of two values), then
+    the normaliser and the rate (one sum all-reduce of two values),
   * the stopping statistic mx (one max all-reduce),
-over torch.distributed: NCCL with CUDA tensors on GPUs, gloo with CPU tensors.
-The combination of the per-rank update statistics is in combine_update, a
-pure function."""
+over torch.distributed: NCCL with tensors on the handle's own GPU, gloo with
+CPU tensors.  The combination of the per-rank update statistics is in
+combine_update, a pure function.
+
+The handle's own single-GPU statistics (bdc_iterate's bound, rate and mx) are
+not the sharded problem's after a sharded iteration: use what iterate()
+returns."""
 from __future__ import annotations
 
 import math
@@ -49,14 +53,21 @@ def shard_log_z(S: float, log_z: float, shift_r: float) -> float:
     return log_z + S - shift_r
 
 
+def comm_device(backend: str, device: int) -> str:
+    """Where a rank's exchange tensors live: NCCL needs them on the rank's
+    own GPU (the handle's device, which need not be torch's current device),
+    gloo on the host."""
+    return f"cuda:{int(device)}" if backend == "nccl" else "cpu"
+
+
 class _Comm:
-    def __init__(self, group=None):
+    def __init__(self, group=None, device: int = 0):
         import torch
         import torch.distributed as dist
         self.torch, self.dist, self.group = torch, dist, group
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
-        self.device = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+        self.device = comm_device(dist.get_backend(group), device)
 
     def reduce(self, vals, op: str) -> np.ndarray:
         t = self.torch.tensor(np.asarray(vals, dtype=np.float64), device=self.device)
@@ -69,7 +80,7 @@ def iterate(E, max_iters: int, a: float = float("-inf"), group=None) -> dict:
     """BA iterations of a count-engine handle sharded over the ranks of
     `group` (torch.distributed, initialised by the caller), until the global
     mx < a or max_iters; every rank returns the same statistics (bits)."""
-    comm = _Comm(group)
+    comm = _Comm(group, E.device)
     r0, r1 = shard_range(E.R, comm.rank, comm.world)
     out = {"iters": 0, "mx": float("nan"), "upper_bound": float("nan"), "rate": float("nan"),
            "best_upper_bound": float("inf"), "best_rate": float("-inf"), "converged": False,
@@ -78,9 +89,8 @@ def iterate(E, max_iters: int, a: float = float("-inf"), group=None) -> dict:
         acc = comm.reduce(E.shard_q(r0, r1), "sum")
         E.shard_set_q(acc)
         st = E.shard_update_begin(r0, r1)
-        S = float(comm.reduce([st[0]], "max")[0])
+        S, max_d = (float(v) for v in comm.reduce([st[0], st[2]], "max"))
         z_rate = comm.reduce([z_share(st[1], st[0], S), st[3]], "sum")
-        max_d = float(comm.reduce([st[2]], "max")[0])
         mx = E.shard_update_end(r0, r1, shard_log_z(S, math.log(z_rate[0]), st[0]))
         mx = float(comm.reduce([mx], "max")[0])
         out["iters"] += 1
@@ -97,7 +107,7 @@ def iterate(E, max_iters: int, a: float = float("-inf"), group=None) -> dict:
 
 def gather_p(E, group=None) -> np.ndarray | None:
     """The sharded iterate, assembled on rank 0 (None elsewhere)."""
-    comm = _Comm(group)
+    comm = _Comm(group, E.device)
     r0, r1 = shard_range(E.R, comm.rank, comm.world)
     mine = (r0, E.get_p()[r0:r1])
     parts = [None] * comm.world

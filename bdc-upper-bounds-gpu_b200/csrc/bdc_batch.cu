@@ -96,8 +96,8 @@ bdc_status bdc_batch_create(bdc_handle_t* handles, int count, bdc_batch_t* out) 
             }
         B->hs.push_back(handles[i]);
     }
-    cudaSetDevice(B->device);
-    cudaError_t e = cudaStreamCreateWithFlags(&B->origin, cudaStreamNonBlocking);
+    cudaError_t e = cudaSetDevice(B->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&B->origin, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming);
     B->lanes.resize(count, nullptr);
     B->joins.resize(count, nullptr);
@@ -122,7 +122,7 @@ bdc_status bdc_batch_set_stream(bdc_batch_t B, void* stream) {
 
 bdc_status bdc_batch_destroy(bdc_batch_t B) {
     if (!B) return BDC_OK;
-    cudaSetDevice(B->device);
+    BDC_CUDA_TRY(cudaSetDevice(B->device));
     cudaStreamSynchronize(B->launch);
     cudaStreamSynchronize(B->origin);
     batch_free(B);
@@ -131,7 +131,7 @@ bdc_status bdc_batch_destroy(bdc_batch_t B) {
 
 bdc_status bdc_batch_iterate(bdc_batch_t B, int64_t max_iters, double a, bdc_stats* stats) {
     if (!B || max_iters < 0) return fail(BDC_ERR_ARG, "bdc_batch_iterate: bad arguments");
-    cudaSetDevice(B->device);
+    BDC_CUDA_TRY(cudaSetDevice(B->device));
     const size_t N = B->hs.size();
     for (auto* H : B->hs)
         if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_batch_iterate: an instance has no distribution set");

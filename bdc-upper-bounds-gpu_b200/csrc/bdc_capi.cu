@@ -98,7 +98,7 @@ bdc_status bdc_create(int n, int k, const bdc_options* opts, bdc_handle_t* out) 
 
 bdc_status bdc_destroy(bdc_handle_t H) {
     if (!H) return BDC_OK;
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     engine_free(H);
     delete H;
     return BDC_OK;
@@ -116,7 +116,7 @@ bdc_status bdc_info(bdc_handle_t H, int* n, int* k, int64_t* num_reps, int* engi
 bdc_status bdc_get_reps(bdc_handle_t H, uint32_t* reps, int64_t R) {
     if (!H || !reps) return fail(BDC_ERR_ARG, "bdc_get_reps: NULL argument");
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_get_reps: %lld slots for %lld representatives", (long long)R, (long long)H->R);
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     BDC_CUDA_TRY(cudaMemcpyAsync(reps, H->d_reps, sizeof(uint32_t) * R, cudaMemcpyDeviceToHost, H->stream));
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
@@ -127,7 +127,7 @@ bdc_status bdc_set_p(bdc_handle_t H, const double* p, int64_t R) {
     if (R != H->R)
         return fail(BDC_ERR_ARG, "bdc_set_p: distribution has %lld entries, (n=%d) has %lld representatives",
                     (long long)R, H->n, (long long)H->R);
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     BDC_CUDA_TRY(cudaMemcpyAsync(H->d_p[0], p, sizeof(double) * R, cudaMemcpyHostToDevice, H->stream));
     return engine_after_set_p(H);
 }
@@ -135,14 +135,14 @@ bdc_status bdc_set_p(bdc_handle_t H, const double* p, int64_t R) {
 bdc_status bdc_set_p_device(bdc_handle_t H, const double* p, int64_t R) {
     if (!H || !p) return fail(BDC_ERR_ARG, "bdc_set_p_device: NULL argument");
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_set_p_device: size mismatch");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     BDC_CUDA_TRY(cudaMemcpyAsync(H->d_p[0], p, sizeof(double) * R, cudaMemcpyDeviceToDevice, H->stream));
     return engine_after_set_p(H);
 }
 
 bdc_status bdc_set_p_uniform(bdc_handle_t H) {
     if (!H) return fail(BDC_ERR_ARG, "bdc_set_p_uniform: NULL handle");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     std::vector<double> u(H->R, 1.0 / (double)(1ull << H->n));  // backend/main_BAA.cu:64
     BDC_CUDA_TRY(cudaMemcpyAsync(H->d_p[0], u.data(), sizeof(double) * H->R, cudaMemcpyHostToDevice, H->stream));
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
@@ -153,7 +153,7 @@ bdc_status bdc_get_p(bdc_handle_t H, double* p, int64_t R) {
     if (!H || !p) return fail(BDC_ERR_ARG, "bdc_get_p: NULL argument");
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_get_p: size mismatch");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_get_p: no distribution set");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     const double* src = nullptr;
     bdc_status rc = engine_current_p(H, &src);
     if (rc != BDC_OK) return rc;
@@ -166,7 +166,7 @@ bdc_status bdc_get_p_device(bdc_handle_t H, double* p, int64_t R) {
     if (!H || !p) return fail(BDC_ERR_ARG, "bdc_get_p_device: NULL argument");
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_get_p_device: size mismatch");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_get_p_device: no distribution set");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     const double* src = nullptr;
     bdc_status rc = engine_current_p(H, &src);
     if (rc != BDC_OK) return rc;
@@ -179,14 +179,14 @@ bdc_status bdc_iterate(bdc_handle_t H, int64_t max_iters, double a, bdc_stats* s
     if (!H) return fail(BDC_ERR_ARG, "bdc_iterate: NULL handle");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_iterate: no distribution set");
     if (max_iters < 0) return fail(BDC_ERR_ARG, "bdc_iterate: max_iters < 0");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     return engine_iterate(H, max_iters, a, stats);
 }
 
 bdc_status bdc_bound_error(bdc_handle_t H, double* ub_err, double* rate_err) {
     if (!H || !ub_err || !rate_err) return fail(BDC_ERR_ARG, "bdc_bound_error: NULL argument");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_bound_error: no distribution set");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     return engine_bound_error(H, ub_err, rate_err);
 }
 
@@ -196,7 +196,7 @@ bdc_status bdc_accelerate(bdc_handle_t H, int64_t max_evals, double gap_bits, bd
     if (H->engine != BDC_ENGINE_FACTORED)
         return fail(BDC_ERR_UNSUPPORTED, "bdc_accelerate: needs the factored engine (k < n)");
     if (max_evals < 0) return fail(BDC_ERR_ARG, "bdc_accelerate: max_evals < 0");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     return factored_accelerate(H, max_evals, gap_bits, stats);
 }
 
@@ -223,7 +223,7 @@ bdc_status bdc_mi_forward(bdc_handle_t H, const double* p, int64_t R, double* I_
     }
     if (H->engine == BDC_ENGINE_FACTORED) {
         if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_mi_forward: no distribution set");
-        cudaSetDevice(H->device);
+        BDC_CUDA_TRY(cudaSetDevice(H->device));
         bdc_status rc = factored_eval(H, false);
         if (rc != BDC_OK) return rc;
         *I_nats = H->h_st->rate;
@@ -236,7 +236,7 @@ bdc_status bdc_mi_backward(bdc_handle_t H, double* grad, int64_t R) {
     if (!H || !grad) return fail(BDC_ERR_ARG, "bdc_mi_backward: NULL argument");
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_mi_backward: %lld slots for %lld representatives", (long long)R, (long long)H->R);
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_mi_backward: no distribution set");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     bdc_status rc = BDC_OK;
     if (H->engine == BDC_ENGINE_FACTORED) {
         rc = factored_eval(H, true);
@@ -265,7 +265,7 @@ bdc_status bdc_log_q(bdc_handle_t H, double* lnq, int64_t nq) {
     const int64_t want = (H->k >= 1) ? (1ll << (H->k - 1)) : 1;
     if (nq != want) return fail(BDC_ERR_ARG, "bdc_log_q: %lld slots, expected 2^(k-1) = %lld", (long long)nq, (long long)want);
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_log_q: no distribution set");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     bdc_status rc = engine_log_q(H);
     if (rc != BDC_OK) return rc;
     BDC_CUDA_TRY(cudaMemcpyAsync(lnq, H->d_lnq, sizeof(double) * nq, cudaMemcpyDeviceToHost, H->stream));
@@ -276,7 +276,7 @@ bdc_status bdc_log_q(bdc_handle_t H, double* lnq, int64_t nq) {
 static bdc_status divergence_common(bdc_handle_t H, const double* lnq, int64_t R, bool with_lnp, double* out) {
     if (R != H->R) return fail(BDC_ERR_ARG, "size mismatch: %lld for %lld representatives", (long long)R, (long long)H->R);
     if (!H->p_set) return fail(BDC_ERR_STATE, "no distribution set");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     bdc_status rc;
     if (lnq) {
         const int64_t nq = (H->k >= 1) ? (1ll << (H->k - 1)) : 1;
@@ -313,7 +313,7 @@ bdc_status bdc_divergence(bdc_handle_t H, const double* lnq, double* d, int64_t 
 bdc_status bdc_rate(bdc_handle_t H, double* rate_nats) {
     if (!H || !rate_nats) return fail(BDC_ERR_ARG, "bdc_rate: NULL argument");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_rate: no distribution set");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     bdc_status rc = engine_log_q(H);
     if (rc != BDC_OK) return rc;
     rc = engine_divergence(H);
@@ -330,7 +330,7 @@ bdc_status bdc_rate(bdc_handle_t H, double* rate_nats) {
 bdc_status bdc_max_deviation(bdc_handle_t H, const double* p, const double* pb, int64_t R, double* mx) {
     if (!H || !p || !pb || !mx) return fail(BDC_ERR_ARG, "bdc_max_deviation: NULL argument");
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_max_deviation: size mismatch");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     // d_logw and d_d are scratch here
     BDC_CUDA_TRY(cudaMemcpyAsync(H->d_logw, p, sizeof(double) * R, cudaMemcpyHostToDevice, H->stream));
     BDC_CUDA_TRY(cudaMemcpyAsync(H->d_d, pb, sizeof(double) * R, cudaMemcpyHostToDevice, H->stream));
@@ -344,7 +344,7 @@ bdc_status bdc_counts(bdc_handle_t H, const uint32_t* xs, const uint32_t* ys, in
     if (!H || (npairs > 0 && (!xs || !ys || !out)) || npairs < 0)
         return fail(BDC_ERR_ARG, "bdc_counts: bad arguments");
     if (npairs == 0) return BDC_OK;
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     const uint32_t xmask = low_mask(H->n), ymask = low_mask(H->k);
     for (int64_t i = 0; i < npairs; ++i)
         if ((xs[i] & ~xmask) || (ys[i] & ~ymask))
@@ -379,13 +379,13 @@ bdc_status bdc_work(bdc_handle_t H, int64_t* nonzero_pairs, int* split_terms) {
 bdc_status bdc_profile(bdc_handle_t H, int iters, bdc_profile_t* out) {
     if (!H || !out || iters < 1) return fail(BDC_ERR_ARG, "bdc_profile: bad arguments");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_profile: no distribution set");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     return engine_profile(H, iters, out);
 }
 
 bdc_status bdc_set_stream(bdc_handle_t H, void* stream) {
     if (!H) return fail(BDC_ERR_ARG, "bdc_set_stream: NULL handle");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     H->stream = stream ? (cudaStream_t)stream : H->own_stream;
     return BDC_OK;

@@ -17,7 +17,11 @@
 //   -- all-reduce (max) of mx: the stopping statistic --
 //
 // The q and D passes and the update are the single-GPU kernels on a
-// sub-range of the representatives.
+// sub-range of the representatives.  Every call makes the handle's device
+// current on the calling thread (as every other handle call does).  After a
+// sharded iteration the handle's own statistics (its last bound, rate and mx)
+// describe its shard, not the whole problem; its best-bound trackers are left
+// as the handle's own iterations set them.
 #include "bdc_engine.cuh"
 
 namespace bdc {
@@ -38,7 +42,7 @@ static bdc_status shard_check(bdc_handle* H, int64_t r0, int64_t r1, const char*
     if (r0 < 0 || r1 <= r0 || r1 > H->R)
         return fail(BDC_ERR_ARG, "%s: representative range [%lld, %lld) outside [0, %lld)", what, (long long)r0,
                     (long long)r1, (long long)H->R);
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     if (!H->d_shard) {
         BDC_CUDA_TRY(cudaMalloc(&H->d_shard, sizeof(double) << H->k));
         H->bytes += sizeof(double) << H->k;
@@ -105,6 +109,12 @@ bdc_status bdc_shard_update_begin(bdc_handle_t H, int64_t r0, int64_t r1, double
     bdc_status rc = shard_check(H, r0, r1, "bdc_shard_update_begin");
     if (rc != BDC_OK) return rc;
     if (!stats) return fail(BDC_ERR_ARG, "bdc_shard_update_begin: NULL stats");
+    // the update's first stage folds its (shard-local) max D and rate into the
+    // handle's best-bound trackers; they are put back afterwards, so that they
+    // keep describing only the handle's own single-GPU iterations
+    rc = pull_state(H);
+    if (rc != BDC_OK) return rc;
+    const double keep[2] = {H->h_st->best_ub, H->h_st->best_rate};
     BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), H->stream));
     BDC_CUDA_TRY(launch_dpass(shard_launch(H, r0, r1), H->d_lnq, H->d_h + r0, H->inv_c, H->log_c, H->d_d + r0,
                               H->d_st, 0));
@@ -116,7 +126,9 @@ bdc_status bdc_shard_update_begin(bdc_handle_t H, int64_t r0, int64_t r1, double
     stats[2] = H->h_st->max_d;       // max D on the shard (nats)
     stats[3] = H->h_st->rate;        // sum |O| p D on the shard (nats)
     stats[4] = H->h_st->zero_p ? 1.0 : 0.0;
-    return BDC_OK;
+    BDC_CUDA_TRY(cudaMemcpyAsync(&H->d_st->best_ub, &keep[0], sizeof(double), cudaMemcpyHostToDevice, H->stream));
+    BDC_CUDA_TRY(cudaMemcpyAsync(&H->d_st->best_rate, &keep[1], sizeof(double), cudaMemcpyHostToDevice, H->stream));
+    return pull_state(H);
 }
 
 bdc_status bdc_shard_update_end(bdc_handle_t H, int64_t r0, int64_t r1, double log_z, double* mx) {

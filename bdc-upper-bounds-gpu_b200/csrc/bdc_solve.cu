@@ -1291,7 +1291,7 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
     if (H->engine != BDC_ENGINE_FACTORED) return fail(BDC_ERR_UNSUPPORTED, "bdc_solve: needs the factored engine (k < n)");
     if (!(gap_bits > 0.0) || max_evals < 1) return fail(BDC_ERR_ARG, "bdc_solve: need gap_bits > 0 and max_evals >= 1");
     if (H->n > 26) return fail(BDC_ERR_UNSUPPORTED, "bdc_solve: counts of n > 26 do not fit FP32 exactly");
-    cudaSetDevice(H->device);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
     cudaStream_t s = H->stream;
     const int64_t R = H->R;
     const int sms = H->num_sms;

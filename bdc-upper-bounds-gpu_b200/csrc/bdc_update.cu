@@ -14,6 +14,7 @@
 // in a fixed order (deterministic) into DevState.  DevState::done makes every
 // later kernel a no-op once mx < a, so a chunk of iterations can be queued or
 // captured in a graph without a host round trip per iteration.
+#include <atomic>
 #include <cfloat>
 
 #include "bdc_common.cuh"
@@ -343,8 +344,10 @@ k_maxdev_tile(const double* __restrict__ p, const double* __restrict__ pb, int64
     if (threadIdx.x == 0) part[blockIdx.x] = m;
 }
 
-static double* g_noalloc_addr[64];
-static bool g_noalloc_ready[64];
+// the array's device address per device, looked up on the first call there;
+// null until then.  Two threads that make their first call on one device at
+// the same time both look it up and store the same address.
+static std::atomic<double*> g_noalloc_addr[64];
 
 }  // namespace bdc
 
@@ -361,16 +364,17 @@ extern "C" bdc_status bdc_max_deviation_noalloc(const double* p_dev, const doubl
     int dev = 0;
     BDC_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return fail(BDC_ERR_ARG, "bdc_max_deviation_noalloc: device %d out of range", dev);
-    if (!g_noalloc_ready[dev]) {
+    double* part = g_noalloc_addr[dev].load(std::memory_order_acquire);
+    if (!part) {
         void* addr = nullptr;
         BDC_CUDA_TRY(cudaGetSymbolAddress(&addr, g_noalloc_partials));
-        g_noalloc_addr[dev] = (double*)addr;
-        g_noalloc_ready[dev] = true;
+        part = (double*)addr;
+        g_noalloc_addr[dev].store(part, std::memory_order_release);
     }
     cudaStream_t s = (cudaStream_t)cuda_stream;
     const int blocks = (int)((num_reps + kNoAllocTile - 1) / kNoAllocTile);
-    k_maxdev_tile<<<blocks, kUpdThreads, 0, s>>>(p_dev, p_before_dev, num_reps, g_noalloc_addr[dev]);
-    k_fold_max<<<1, kUpdThreads, 0, s>>>(g_noalloc_addr[dev], blocks, mx_dev);
+    k_maxdev_tile<<<blocks, kUpdThreads, 0, s>>>(p_dev, p_before_dev, num_reps, part);
+    k_fold_max<<<1, kUpdThreads, 0, s>>>(part, blocks, mx_dev);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
 }

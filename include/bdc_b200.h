@@ -6,7 +6,8 @@
  *
  * Plain C types only (no torch, no C++).  Every function returns a
  * bdc_status; on failure bdc_last_error() gives a one-line reason.  Nothing
- * calls exit().
+ * calls exit().  Every call on a handle makes the handle's device current on
+ * the calling thread.
  *
  * Layouts (identical to the reference, Pintz45/BDC-Upper-Bounds-GPU):
  *   p[R]       probability of EACH string of an orbit, one entry per canonical
@@ -161,7 +162,10 @@ bdc_status bdc_solve(bdc_handle_t h, double gap_bits, int64_t max_evals, bdc_sta
  *      the bound max D and the rate sum --
  *   bdc_shard_update_end(ln Z_all + S - s, &mx)   p' on the shard, local mx
  *   -- the caller takes the max of mx over the ranks (the stopping rule) --
- * bdc_b200.sharded runs this loop over torch.distributed. */
+ * bdc_b200.sharded runs this loop over torch.distributed.  After a sharded
+ * iteration the handle's own last bound, rate and mx (bdc_iterate's stats)
+ * describe its shard, not the whole problem; the loop's combined values are
+ * the sharded problem's.  The handle's best-bound trackers are not touched. */
 bdc_status bdc_shard_q(bdc_handle_t h, int64_t rep_begin, int64_t rep_end, double* acc, int64_t ny);
 bdc_status bdc_shard_set_q(bdc_handle_t h, const double* acc, int64_t ny);
 bdc_status bdc_shard_update_begin(bdc_handle_t h, int64_t rep_begin, int64_t rep_end, double* stats5);

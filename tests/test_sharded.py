@@ -51,6 +51,25 @@ def test_combined_normaliser_equals_the_whole_vector():
         assert abs(tot - 1.0) < 1e-12
 
 
+def test_exchange_tensors_live_on_the_handles_gpu_under_nccl():
+    # NCCL runs one process per GPU: the exchange buffers must sit on the
+    # handle's device, not on torch's current device (cuda:0 by default)
+    from bdc_b200 import sharded
+    assert sharded.comm_device("nccl", 3) == "cuda:3"
+    assert sharded.comm_device("nccl", 0) == "cuda:0"
+    assert sharded.comm_device("gloo", 3) == "cpu"
+
+
+def test_comm_picks_the_engine_device_for_a_mocked_nccl_group(monkeypatch):
+    import torch.distributed as tdist
+    from bdc_b200 import sharded
+    monkeypatch.setattr(tdist, "get_rank", lambda group=None: 1)
+    monkeypatch.setattr(tdist, "get_world_size", lambda group=None: 2)
+    monkeypatch.setattr(tdist, "get_backend", lambda group=None: "nccl")
+    comm = sharded._Comm(None, device=5)
+    assert comm.device == "cuda:5" and comm.rank == 1 and comm.world == 2
+
+
 def _cpu_rank(rank, world, port, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)

@@ -41,6 +41,28 @@ def test_noalloc_max_deviation_matches_allocating_entry_point(bdc):
             assert got == pytest.approx(float(np.max(np.log2(p) - np.log2(pb))), abs=1e-12)
 
 
+def test_noalloc_ragged_last_tile_and_many_partials(bdc):
+    # 301 blocks of the fixed scratch, the last one holding 17 entries; the
+    # maximum sits in that ragged tile on the first call and elsewhere on
+    # the second, so a stale slot from the first call would show
+    import torch
+
+    R = 8192 * 300 + 17
+    rng = np.random.default_rng(7)
+    for call, where in enumerate((R - 5, 8192 * 150 + 3)):
+        p = rng.random(R) + 0.5
+        pb = rng.random(R) + 0.5
+        p[where] *= 1024.0
+        tp = torch.tensor(p, dtype=torch.float64, device="cuda")
+        tpb = torch.tensor(pb, dtype=torch.float64, device="cuda")
+        out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+        bdc.max_deviation_noalloc(tp.data_ptr(), tpb.data_ptr(), R, out.data_ptr(),
+                                  torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        want = float(np.max(np.log2(p) - np.log2(pb)))
+        assert float(out.item()) == pytest.approx(want, rel=0, abs=1e-12), (call, float(out.item()), want)
+
+
 def test_noalloc_rejects_sizes_beyond_the_limit(bdc):
     L = bdc.library()
     rc = L.bdc_max_deviation_noalloc(ctypes.c_void_p(8), ctypes.c_void_p(8), (1 << 27) + 1,
