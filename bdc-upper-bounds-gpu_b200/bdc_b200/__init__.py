@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = [
     "bdc_log_w", "bdc_divergence", "bdc_rate", "bdc_max_deviation", "bdc_counts",
     "bdc_generate_cache", "bdc_read_cache_file", "bdc_write_cache_file", "bdc_read_dist_file",
     "bdc_write_dist_file", "bdc_work", "bdc_profile", "bdc_set_stream", "bdc_peak_probe",
-    "bdc_max_deviation_noalloc", "bdc_accelerate", "bdc_mi_forward", "bdc_mi_backward",
+    "bdc_max_deviation_noalloc", "bdc_accelerate", "bdc_mi_forward", "bdc_mi_backward", "bdc_mi_backward_device",
     "bdc_batch_create", "bdc_batch_iterate", "bdc_batch_destroy", "bdc_batch_set_stream", "bdc_solve",
     "bdc_bound_error", "bdc_shard_q", "bdc_shard_set_q", "bdc_shard_update_begin", "bdc_shard_update_end",
 ]
@@ -116,6 +116,7 @@ def library() -> ctypes.CDLL:
     L.bdc_batch_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.bdc_mi_forward.argtypes = [h, _f64p, ctypes.c_int64, _f64p]
     L.bdc_mi_backward.argtypes = [h, _f64p, ctypes.c_int64]
+    L.bdc_mi_backward_device.argtypes = [h, ctypes.c_void_p, ctypes.c_int64]
     L.bdc_bound_error.argtypes = [h, _f64p, _f64p]
     L.bdc_shard_q.argtypes = [h, ctypes.c_int64, ctypes.c_int64, _f64p, ctypes.c_int64]
     L.bdc_shard_set_q.argtypes = [h, _f64p, ctypes.c_int64]
@@ -293,9 +294,10 @@ class Engine:
         return ub.value, rate.value
 
     def accelerate(self, max_evals: int, gap_bits: float = 0.0) -> dict:
-        """Accelerated BA on the device (factored engine): runs until the
-        certified gap best_upper_bound - best_rate < gap_bits or max_evals
-        BA map evaluations."""
+        """Nesterov-accelerated exponentiated gradient (adjoint-driven BA with
+        momentum and adaptive restart) on the device (factored engine): runs
+        until the bracket best_upper_bound - best_rate < gap_bits or
+        max_evals evaluations."""
         st = Stats()
         _check(library().bdc_accelerate(self._h, int(max_evals), float(gap_bits), ctypes.byref(st)),
                "bdc_accelerate")
@@ -324,6 +326,11 @@ class Engine:
         out = np.empty(self.R, dtype=np.float64)
         _check(library().bdc_mi_backward(self._h, out.ctypes.data_as(_f64p), self.R), "bdc_mi_backward")
         return out
+
+    def mi_backward_device(self, ptr: int) -> None:
+        """dI/dp per representative (nats) at the current iterate, written to
+        the device buffer at `ptr` (R doubles on the handle's device)."""
+        _check(library().bdc_mi_backward_device(self._h, ctypes.c_void_p(ptr), self.R), "bdc_mi_backward_device")
 
     def baa_iteration(self, p) -> np.ndarray:
         p, pp = _f64(p)

@@ -251,6 +251,26 @@ bdc_status bdc_mi_backward(bdc_handle_t H, double* grad, int64_t R) {
     return BDC_OK;
 }
 
+bdc_status bdc_mi_backward_device(bdc_handle_t H, double* grad_dev, int64_t R) {
+    if (!H || !grad_dev) return fail(BDC_ERR_ARG, "bdc_mi_backward_device: NULL argument");
+    if (R != H->R)
+        return fail(BDC_ERR_ARG, "bdc_mi_backward_device: %lld slots for %lld representatives", (long long)R,
+                    (long long)H->R);
+    if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_mi_backward_device: no distribution set");
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
+    bdc_status rc = BDC_OK;
+    if (H->engine == BDC_ENGINE_FACTORED) {
+        rc = factored_eval(H, true);
+    } else {
+        rc = engine_log_q(H);
+        if (rc == BDC_OK) rc = engine_divergence(H);
+    }
+    if (rc != BDC_OK) return rc;
+    BDC_CUDA_TRY(launch_mi_grad(H->n, H->d_reps, H->R, H->d_d, grad_dev, H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    return BDC_OK;
+}
+
 bdc_status bdc_baa_iteration(bdc_handle_t H, const double* p_in, double* p_out, int64_t R) {
     if (!H || !p_in || !p_out) return fail(BDC_ERR_ARG, "bdc_baa_iteration: NULL argument");
     bdc_status rc = bdc_set_p(H, p_in, R);

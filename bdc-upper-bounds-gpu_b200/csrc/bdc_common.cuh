@@ -140,15 +140,16 @@ struct DevState {
     double lse;          // ln sum |O| p e^D of the last D pass (nats)
     double best_ub;      // min over evaluated iterates of max_x D(x) (nats): still a bound
     double best_rate;    // max over evaluated iterates of I(p;W) (nats): a lower bound
-    double ub_theta1;    // accelerated loop: bound at the middle point of a cycle
-    double sq_alpha;     // accelerated loop: extrapolation step of the current cycle
-    double sq_max;       // accelerated loop: max of the extrapolated log iterate
+    double ng_prev_rate; // accelerated loop: I(p;W) at the last accepted extrapolated point
+    double ng_gap;       // accelerated loop: stop when best_ub - best_rate < this (nats)
+    double ng_max;       // accelerated loop: max of the extrapolated log iterate
+    long long ng_t;      // accelerated loop: steps since the last restart (momentum t / (t + 3))
     long long iter;      // iterations done since the last reset
     int cur;             // which of the two p buffers holds the current iterate
     int done;            // set when mx < a: later iterations do nothing
     int zero_p;          // the current iterate has a zero entry
     int error;           // device-detected error code (0 = none)
-    int restore;         // accelerated loop: the extrapolated point was rejected
+    int ng_mode;         // accelerated loop: 0 fresh start, 1 step accepted, 2 restart
     unsigned int ticket[4];  // last-block counters of the grid reductions
 };
 

@@ -88,6 +88,12 @@ bdc_status factored_store_p(bdc_handle* H, double* p_out);  // dense state -> p 
 bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stats* stats);
 bdc_status factored_profile(bdc_handle* H, int iters, bdc_profile_t* out);
 bdc_status factored_accelerate(bdc_handle* H, int64_t max_evals, double gap_bits, bdc_stats* stats);
+// the accelerated loop's pieces, for callers that queue its steps themselves
+// (batches): the step length, the start (snapshots of the current iterate,
+// the device stop at gap_bits) and `steps` steps queued on H->stream
+double factored_acc_eta();
+bdc_status factored_acc_start(bdc_handle* H, double gap_bits);
+cudaError_t factored_enqueue_acc_steps(bdc_handle* H, int steps, double eta);
 cudaError_t factored_enqueue_iteration(bdc_handle* H, double a);
 // finishes an iteration that stopped on an exp-shift overflow (on H->stream);
 // any other device error is returned as BDC_ERR_NUMERIC

@@ -130,6 +130,7 @@ struct FactoredState {
     uint16_t* Bp = nullptr;   // low-half tables, row c = table row rev(c) (dense column order)
     double* Ddense = nullptr; // [2^{n-1}] D(x) of a map with D output (allocated on first use)
     double* dout = nullptr;   // where the G epilogue writes D (nullptr: nowhere)
+    double eta = 1.0;         // step of the update in the G epilogue (1: the BA map)
     std::vector<int> colmax;  // per dense column: largest x_hi of a representative, -1 if none
     double* LA = nullptr;     // [H1h][Kp]  = [AL | NR]
     double* RB = nullptr;     // [Kp][H2]  = [ML ; BR^T]
@@ -168,11 +169,12 @@ struct FactoredState {
     // a captured chunk of kGraphIters iterations for the threshold graph_a
     cudaGraphExec_t graph = nullptr;
     double graph_a = 0.0;
-    // accelerated loop: snapshots of the normalised log iterate and its graph
+    // accelerated loop: the normalised log iterates x_t and x_{t-1}, and the
+    // graph of kAccSteps steps
     double* snap0 = nullptr;
     double* snap1 = nullptr;
-    double* snap2 = nullptr;
     cudaGraphExec_t cycle = nullptr;
+    double cycle_eta = 0.0;
     // captured single BA maps (factored_map), by their vectors
     struct MapGraph {
         const double* pin = nullptr;
@@ -304,7 +306,7 @@ __global__ void __launch_bounds__(256, (BM * BN <= 4096) ? 3 : 2) k_mma_ba(const
                 const double lt = ep.Lt[xd];
                 const bool zero_in = (lt != lt);
                 const double lnp = zero_in ? 0.0 : lt - lnz;
-                const double lw = lnp + D - shift;
+                const double lw = lnp + ep.eta * D - shift;
                 const double e = exp(lw);
                 ep.Lt[xd] = lw;
                 ep.Pw[xd] = o * e;
@@ -996,7 +998,7 @@ __global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double
 }
 
 __global__ void __launch_bounds__(256)
-k_fac_finalize(const double* __restrict__ part, int nb, double a, DevState* st) {
+k_fac_finalize(const double* __restrict__ part, int nb, double a, double eta, DevState* st) {
     if (gated(st)) return;
     __shared__ double red[5][256];
     double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0, zero = 0.0;
@@ -1036,10 +1038,10 @@ k_fac_finalize(const double* __restrict__ part, int nb, double a, DevState* st) 
         st->rate = sR;
         return;
     }
-    // Lt holds logW - shift, so ln p' - ln p = D - shift - ln Z
+    // Lt holds ln p + eta D - shift, so ln p' - ln p = eta D - shift - ln Z
     const double lnz = log(sE);
     const double ln2 = 0.69314718055994530942;
-    const double mx = st->zero_p ? INFINITY : (mD - st->shift - lnz) / ln2;
+    const double mx = st->zero_p ? INFINITY : (eta * mD - st->shift - lnz) / ln2;
     st->max_d = mD;
     st->rate = sR;
     st->best_ub = fmin(st->best_ub, mD);
@@ -1048,8 +1050,8 @@ k_fac_finalize(const double* __restrict__ part, int nb, double a, DevState* st) 
     st->mx = mx;
     st->max_logw = mL + st->shift;
     st->log_z = lnz;
-    // next shift: the largest new ln p plus the current bound on D
-    st->shift = (mL - lnz) + mD;
+    // next shift: the largest new ln p plus eta times the current bound on D
+    st->shift = (mL - lnz) + eta * mD;
     st->zero_p = 0;
     st->iter += 1;
     st->done = !(mx >= a);
@@ -2004,6 +2006,7 @@ bdc_status factored_init(bdc_handle* H) {
         ep.Pw = F->Pw;
         ep.inv_c = H->inv_c;
         ep.part = F->epart;
+        ep.eta = 1.0;
         // each shape one CTA per tile, or (when the tiles outnumber them) as
         // many CTAs as fit on the SMs at once, each looping over tiles with
         // the next tile's loads in flight during the epilogue
@@ -2082,7 +2085,6 @@ void factored_free(bdc_handle* H) {
         if (m.exec) cudaGraphExecDestroy(m.exec);
     cudaFree(F->snap0);
     cudaFree(F->snap1);
-    cudaFree(F->snap2);
     for (Launch* L : {&F->ul, &F->vr, &F->g}) free_launch(*L);
     for (int lg = 0; lg < 8; ++lg) {
         free_launch(F->mq[lg]);
@@ -2105,6 +2107,7 @@ static BaEpilogue make_epilogue(bdc_handle* H) {
     ep.part = F->epart;
     ep.st = H->d_st;
     ep.Dout = F->dout;
+    ep.eta = F->eta;
     return ep;
 }
 
@@ -2180,7 +2183,7 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
         case ST_G:
             return launch_ba(F->g, make_epilogue(H), s, H->d_st);
         case ST_FIN:
-            k_fac_finalize<<<1, 256, 0, s>>>(F->epart, F->ctas_g, a, H->d_st);
+            k_fac_finalize<<<1, 256, 0, s>>>(F->epart, F->ctas_g, a, F->eta, H->d_st);
             break;
     }
     return cudaGetLastError();
@@ -2393,31 +2396,21 @@ bdc_status factored_iterate(bdc_handle* H, int64_t max_iters, double a, bdc_stat
 }
 
 // ------------------------------------------------------ accelerated loop
-// One cycle (squared extrapolation of the BA map F in ln p):
-//   S0 = ln p; F; S1 = ln p; F (ub1 = bound at S1); S2 = ln p;
-//   alpha = clamp(-|r| / |v|, -64, -1), r = S1 - S0, v = S2 - 2 S1 + S0
-//   ln p' = S0 - 2 alpha r + alpha^2 v; F at p' (bound u');
-//   keep F(p') unless u' > ub1, else go back to S2.
-// Norms are weighted by the orbit sizes (the full-space Euclidean norm).
-constexpr double kSqAlphaMin = -64.0;
-
-__device__ __forceinline__ bool sq_gated(const DevState* st) { return st->error != 0; }
-
-__global__ void __launch_bounds__(256) k_sq_save(const uint32_t* __restrict__ reps, int64_t R, int n,
-                                                 const double* __restrict__ Lt, double* __restrict__ dst,
-                                                 const DevState* st) {
-    if (sq_gated(st)) return;
-    const double lnz = st->log_z;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t xd = fac_pos(reps[i], n >> 1);
-        dst[xd] = Lt[xd] - lnz;
-    }
-}
-
-__global__ void k_sq_mark(DevState* st) {
-    if (sq_gated(st)) return;
-    st->ub_theta1 = st->max_d;
-}
+// Nesterov-accelerated exponentiated gradient on the simplex, driven by the
+// adjoint of I(p;W): its gradient over the probabilities of the strings is
+// dI/dp(x) = D(x) - 1, so the mirror (exponentiated-gradient) step of length
+// eta is ln p' = ln y + eta D(y) - ln Z, which for eta = 1 and y = p is the
+// BA update.  Per step t (all on the device, kAccSteps steps per graph):
+//   y_t     = normalise(exp(x_t + beta_t (x_t - x_{t-1}))),  beta_t = t / (t + 3)
+//   D(y_t), I(y_t)                 the fused forward/backward (G epilogue)
+//   x_{t+1} = ln y_t + eta D(y_t) - ln Z
+// with x the normalised log iterate.  Adaptive restart: when I(y_t) falls
+// below I(y_{t-1}), the step is discarded, the momentum is dropped (t = 0)
+// and the next point is y = x_t.  Every evaluated y gives a valid bracket
+// I(y) <= C <= max_x D(x; y), tracked as best_rate / best_ub; the loop stops
+// on the device when best_ub - best_rate < the requested gap.
+constexpr int kAccSteps = 8;
+constexpr double kAccEta = 1.5;
 
 __device__ __forceinline__ double block_sum256(double v) {
     __shared__ double red[256];
@@ -2445,82 +2438,77 @@ __device__ __forceinline__ double block_max256(double v) {
     return r;
 }
 
-__global__ void __launch_bounds__(256) k_sq_norms(const uint32_t* __restrict__ reps, int64_t R, int n,
-                                                  const double* __restrict__ S0, const double* __restrict__ S1,
-                                                  const double* __restrict__ Lt, double* __restrict__ part,
-                                                  const DevState* st) {
-    if (sq_gated(st)) return;
+__device__ __forceinline__ bool acc_gated(const DevState* st) { return st->error != 0 || st->done; }
+
+// decides what the last evaluation means for the iterate: accept (mode 1),
+// restart (mode 2) or nothing yet (mode 0, the fresh start)
+__global__ void k_acc_decide(DevState* st) {
+    if (acc_gated(st) || threadIdx.x != 0) return;
+    if (st->ng_mode < 0) {  // set by the host: nothing evaluated since the start
+        st->ng_mode = 0;
+        st->ng_t = 0;
+        st->ng_prev_rate = -DBL_MAX;
+        return;
+    }
+    if (st->rate >= st->ng_prev_rate) {
+        st->ng_mode = 1;
+        st->ng_prev_rate = st->rate;
+        st->ng_t += 1;
+    } else {
+        st->ng_mode = 2;
+        st->ng_t = 0;
+        st->ng_prev_rate = -DBL_MAX;
+    }
+}
+
+// x_{t-1}, x_t (dense, at representatives) and the extrapolated ln y into Lt;
+// block max of ln y
+__global__ void __launch_bounds__(256) k_acc_extrap(const uint32_t* __restrict__ reps, int64_t R, int n,
+                                                    double* __restrict__ xa, double* __restrict__ xb,
+                                                    double* __restrict__ Lt, double* __restrict__ part,
+                                                    const DevState* st) {
+    if (acc_gated(st)) return;
+    const int mode = st->ng_mode;
     const double lnz = st->log_z;
-    double rr = 0.0, vv = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
-        const double o = (double)orbit_size(x, n);
-        const double s0 = S0[xd], s1 = S1[xd], s2 = Lt[xd] - lnz;
-        const double r = s1 - s0, v = s2 - 2.0 * s1 + s0;
-        rr = fma(o * r, r, rr);
-        vv = fma(o * v, v, vv);
-    }
-    rr = block_sum256(rr);
-    vv = block_sum256(vv);
-    if (threadIdx.x == 0) {
-        part[2 * blockIdx.x] = rr;
-        part[2 * blockIdx.x + 1] = vv;
-    }
-}
-
-__global__ void k_sq_alpha(const double* __restrict__ part, int nb, DevState* st) {
-    if (sq_gated(st) || threadIdx.x != 0) return;
-    double rr = 0.0, vv = 0.0;
-    for (int b = 0; b < nb; ++b) {
-        rr += part[2 * b];
-        vv += part[2 * b + 1];
-    }
-    double a = (vv > 0.0) ? -sqrt(rr / vv) : -1.0;
-    if (!(a <= -1.0)) a = -1.0;  // also catches NaN
-    if (a < kSqAlphaMin) a = kSqAlphaMin;
-    st->sq_alpha = a;
-}
-
-// S2 = current ln p; Lt = S0 - 2 a (S1 - S0) + a^2 (S2 - 2 S1 + S0); block max
-__global__ void __launch_bounds__(256) k_sq_extrap(const uint32_t* __restrict__ reps, int64_t R, int n,
-                                                   const double* __restrict__ S0, const double* __restrict__ S1,
-                                                   double* __restrict__ S2, double* __restrict__ Lt,
-                                                   double* __restrict__ part, const DevState* st) {
-    if (sq_gated(st)) return;
-    const double a = st->sq_alpha, lnz = st->log_z;
+    const double beta = (double)st->ng_t / ((double)st->ng_t + 3.0);
     double mx = -DBL_MAX;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t xd = fac_pos(reps[i], n >> 1);
-        const double s0 = S0[xd], s1 = S1[xd], s2 = Lt[xd] - lnz;
-        S2[xd] = s2;
-        const double t = s0 - 2.0 * a * (s1 - s0) + a * a * (s2 - 2.0 * s1 + s0);
-        Lt[xd] = t;
-        mx = fmax(mx, t);
+        double y;
+        if (mode == 1) {
+            const double a_old = xa[xd], a_new = Lt[xd] - lnz;
+            xb[xd] = a_old;
+            xa[xd] = a_new;
+            // an input at exact zero (ln p = -inf) stays there
+            y = (a_new == -INFINITY) ? a_new : a_new + beta * (a_new - a_old);
+        } else {
+            y = xa[xd];
+            xb[xd] = y;
+        }
+        Lt[xd] = y;
+        mx = fmax(mx, y);
     }
     mx = block_max256(mx);
     if (threadIdx.x == 0) part[blockIdx.x] = mx;
 }
 
-__global__ void k_sq_max(const double* __restrict__ part, int nb, DevState* st) {
-    if (sq_gated(st) || threadIdx.x != 0) return;
+__global__ void k_acc_max(const double* __restrict__ part, int nb, DevState* st) {
+    if (acc_gated(st) || threadIdx.x != 0) return;
     double m = -DBL_MAX;
     for (int b = 0; b < nb; ++b) m = fmax(m, part[b]);
-    st->sq_max = m;
+    st->ng_max = m;
 }
 
-// Lt -= max, Pw = |O| exp(Lt); block sums of |O| exp(Lt).  With restore set
-// the source is S2 instead (the extrapolated point was rejected).
-__global__ void __launch_bounds__(256) k_sq_pw(const uint32_t* __restrict__ reps, int64_t R, int n,
-                                               const double* __restrict__ S2, double* __restrict__ Lt,
-                                               double* __restrict__ Pw, double* __restrict__ part, int from_s2,
-                                               const DevState* st) {
-    if (sq_gated(st)) return;
-    if (from_s2 && !st->restore) return;
-    const double m = from_s2 ? 0.0 : st->sq_max;
+// Lt -= max, Pw = |O| exp(Lt); block sums of |O| exp(Lt)
+__global__ void __launch_bounds__(256) k_acc_pw(const uint32_t* __restrict__ reps, int64_t R, int n,
+                                                double* __restrict__ Lt, double* __restrict__ Pw,
+                                                double* __restrict__ part, const DevState* st) {
+    if (acc_gated(st)) return;
+    const double m = st->ng_max;
     double sum = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
-        const double l = (from_s2 ? S2[xd] : Lt[xd]) - m;
+        const double l = Lt[xd] - m;
         const double o = (double)orbit_size(x, n);
         const double e = exp(l);
         Lt[xd] = l;
@@ -2531,112 +2519,169 @@ __global__ void __launch_bounds__(256) k_sq_pw(const uint32_t* __restrict__ reps
     if (threadIdx.x == 0) part[blockIdx.x] = sum;
 }
 
-// ln Z of the new point and the next exp shift (max ln p + the last bound)
-__global__ void k_sq_setz(const double* __restrict__ part, int nb, int from_s2, DevState* st) {
-    if (sq_gated(st) || threadIdx.x != 0) return;
-    if (from_s2 && !st->restore) return;
+// ln Z of y and the exp shift of the next update (max ln y + eta * last bound)
+__global__ void k_acc_setz(const double* __restrict__ part, int nb, double eta, DevState* st) {
+    if (acc_gated(st) || threadIdx.x != 0) return;
     double s = 0.0;
     for (int b = 0; b < nb; ++b) s += part[b];
     const double lnz = log(s);
     st->log_z = lnz;
-    st->shift = -lnz + (from_s2 ? st->ub_theta1 : st->max_d);
-    if (from_s2) st->restore = 0;
+    st->shift = -lnz + eta * st->max_d;
 }
 
-__global__ void k_sq_guard(DevState* st) {
-    if (sq_gated(st)) return;
-    st->restore = !(st->max_d <= st->ub_theta1);
+// the device-side stop: the bracket of the evaluated points is below the gap
+__global__ void k_acc_stop(DevState* st) {
+    if (acc_gated(st) || threadIdx.x != 0) return;
+    if (st->best_ub - st->best_rate < st->ng_gap) st->done = 1;
 }
 
-static cudaError_t enqueue_cycle(bdc_handle* H) {
+static cudaError_t enqueue_acc_step(bdc_handle* H, double eta) {
     FactoredState* F = H->fac;
     cudaStream_t s = H->stream;
     const int nb = H->nb_upd;
     const int64_t R = H->R;
-    cudaError_t e;
-    k_sq_save<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->Lt, F->snap0, H->d_st);
-    if ((e = enqueue_iteration(H, -INFINITY)) != cudaSuccess) return e;
-    k_sq_save<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->Lt, F->snap1, H->d_st);
-    if ((e = enqueue_iteration(H, -INFINITY)) != cudaSuccess) return e;
-    k_sq_mark<<<1, 1, 0, s>>>(H->d_st);
-    k_sq_norms<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap0, F->snap1, F->Lt, F->epart, H->d_st);
-    k_sq_alpha<<<1, 32, 0, s>>>(F->epart, nb, H->d_st);
-    k_sq_extrap<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap0, F->snap1, F->snap2, F->Lt, F->epart, H->d_st);
-    k_sq_max<<<1, 32, 0, s>>>(F->epart, nb, H->d_st);
-    k_sq_pw<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap2, F->Lt, F->Pw, F->epart, 0, H->d_st);
-    k_sq_setz<<<1, 32, 0, s>>>(F->epart, nb, 0, H->d_st);
-    if ((e = enqueue_iteration(H, -INFINITY)) != cudaSuccess) return e;
-    k_sq_guard<<<1, 1, 0, s>>>(H->d_st);
-    k_sq_pw<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap2, F->Lt, F->Pw, F->epart, 1, H->d_st);
-    k_sq_setz<<<1, 32, 0, s>>>(F->epart, nb, 1, H->d_st);
+    k_acc_decide<<<1, 32, 0, s>>>(H->d_st);
+    k_acc_extrap<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap0, F->snap1, F->Lt, F->epart, H->d_st);
+    k_acc_max<<<1, 32, 0, s>>>(F->epart, nb, H->d_st);
+    k_acc_pw<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->Lt, F->Pw, F->epart, H->d_st);
+    k_acc_setz<<<1, 32, 0, s>>>(F->epart, nb, eta, H->d_st);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const double keep = F->eta;
+    F->eta = eta;
+    e = enqueue_iteration(H, -INFINITY);
+    F->eta = keep;
+    if (e != cudaSuccess) return e;
+    k_acc_stop<<<1, 32, 0, s>>>(H->d_st);
     return cudaGetLastError();
 }
 
-static bdc_status ensure_cycle_graph(bdc_handle* H) {
+cudaError_t factored_enqueue_acc_steps(bdc_handle* H, int steps, double eta) {
+    for (int i = 0; i < steps; ++i) {
+        cudaError_t e = enqueue_acc_step(H, eta);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// the loop's two snapshot vectors (dense, allocated on first use)
+bdc_status factored_acc_buffers(bdc_handle* H) {
     FactoredState* F = H->fac;
-    if (F->cycle) return BDC_OK;
+    if (F->snap0) return BDC_OK;
     const size_t NX = (size_t)1 << (H->n - 1);
-    if (!F->snap0) {
-        BDC_CUDA_TRY(cudaMalloc(&F->snap0, sizeof(double) * NX));
-        BDC_CUDA_TRY(cudaMalloc(&F->snap1, sizeof(double) * NX));
-        BDC_CUDA_TRY(cudaMalloc(&F->snap2, sizeof(double) * NX));
-        H->bytes += 3 * sizeof(double) * NX;
+    BDC_CUDA_TRY(cudaMalloc(&F->snap0, sizeof(double) * NX));
+    BDC_CUDA_TRY(cudaMalloc(&F->snap1, sizeof(double) * NX));
+    H->bytes += 2 * sizeof(double) * NX;
+    return BDC_OK;
+}
+
+// x_t = x_{t-1} = the current normalised log iterate; nothing evaluated yet
+__global__ void __launch_bounds__(256) k_acc_init(const uint32_t* __restrict__ reps, int64_t R, int n,
+                                                  const double* __restrict__ Lt, double* __restrict__ xa,
+                                                  double* __restrict__ xb, DevState* st, double gap_nats) {
+    const double lnz = st->log_z;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t xd = fac_pos(reps[i], n >> 1);
+        const double l = Lt[xd] - lnz;
+        xa[xd] = l;
+        xb[xd] = l;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->ng_mode = -1;
+        st->ng_gap = gap_nats;
+        st->done = 0;
+    }
+}
+
+bdc_status factored_acc_start(bdc_handle* H, double gap_bits) {
+    bdc_status rc = factored_acc_buffers(H);
+    if (rc != BDC_OK) return rc;
+    FactoredState* F = H->fac;
+    k_acc_init<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Lt, F->snap0, F->snap1, H->d_st,
+                                                 gap_bits * 0.69314718055994530942);
+    BDC_CUDA_TRY(cudaGetLastError());
+    return BDC_OK;
+}
+
+double factored_acc_eta() {
+    const char* e = getenv("BDC_ACCEL_STEP");
+    const double v = (e && *e) ? atof(e) : kAccEta;
+    return (v > 0.0 && v <= 4.0) ? v : kAccEta;
+}
+
+static bdc_status ensure_cycle_graph(bdc_handle* H, double eta) {
+    FactoredState* F = H->fac;
+    if (F->cycle && F->cycle_eta == eta) return BDC_OK;
+    if (F->cycle) {
+        cudaGraphExecDestroy(F->cycle);
+        F->cycle = nullptr;
     }
     cudaStream_t keep = H->stream;
     H->stream = H->own_stream;
     BDC_CUDA_TRY(cudaStreamSynchronize(keep));
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamBeginCapture(H->own_stream, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) e = enqueue_cycle(H);
+    if (e == cudaSuccess) e = factored_enqueue_acc_steps(H, kAccSteps, eta);
     cudaError_t e2 = cudaStreamEndCapture(H->own_stream, &g);
     H->stream = keep;
     if (e == cudaSuccess) e = e2;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&F->cycle, g, 0);
     if (g) cudaGraphDestroy(g);
     BDC_CUDA_TRY(e);
+    F->cycle_eta = eta;
     return BDC_OK;
 }
 
 bdc_status factored_accelerate(bdc_handle* H, int64_t max_evals, double gap_bits, bdc_stats* stats) {
     FactoredState* F = H->fac;
     const double ln2 = 0.69314718055994530942;
+    const double eta = factored_acc_eta();
     BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), H->stream));
     BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     const long long it0 = H->h_st->iter;
-    // a plain step first when the iterate still carries the caller's exact zeros
+    // a plain step first when the iterate still carries the caller's exact
+    // zeros (ln 0 = 0 applies to the first update only)
     if (H->h_st->iter == 0 && max_evals > 0) {
         bdc_status rc = factored_iterate(H, 1, -INFINITY, nullptr);
         if (rc != BDC_OK) return rc;
     }
-    bdc_status rc = ensure_cycle_graph(H);
-    if (rc != BDC_OK) return rc;
-    int64_t chunk = 1;
-    bool converged = false;
-    for (int guard = 0; guard < 1000000; ++guard) {
-        const double gap = (H->h_st->best_ub - H->h_st->best_rate) / ln2;
-        if (gap < gap_bits) {
-            converged = true;
-            break;
-        }
-        const int64_t remaining = max_evals - (H->h_st->iter - it0);
-        if (remaining < 3) break;
-        const int64_t c = std::min<int64_t>(chunk, remaining / 3);
-        for (int64_t i = 0; i < c; ++i) BDC_CUDA_TRY(cudaGraphLaunch(F->cycle, H->stream));
-        BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
-        BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
-        if (H->h_st->error == kErrShift) {
-            // an exp shift went out of range inside a cycle: finish that
-            // evaluation by re-scaling and start the next cycle from there
-            rc = rescale(H, -INFINITY);
-            if (rc != BDC_OK) return rc;
+    bool converged = (H->h_st->best_ub - H->h_st->best_rate) / ln2 < gap_bits;
+    if (!converged && H->h_st->iter - it0 < max_evals) {
+        bdc_status rc = ensure_cycle_graph(H, eta);
+        if (rc != BDC_OK) return rc;
+        rc = factored_acc_start(H, gap_bits);
+        if (rc != BDC_OK) return rc;
+        int64_t chunk = 1;
+        for (int guard = 0; guard < 1000000; ++guard) {
+            const int64_t remaining = max_evals - (H->h_st->iter - it0);
+            // whole graphs while they fit, single steps for the rest
+            if (remaining <= 0) break;
+            if (remaining >= kAccSteps) {
+                const int64_t c = std::min<int64_t>(chunk, remaining / kAccSteps);
+                for (int64_t i = 0; i < c; ++i) BDC_CUDA_TRY(cudaGraphLaunch(F->cycle, H->stream));
+            } else {
+                BDC_CUDA_TRY(factored_enqueue_acc_steps(H, (int)remaining, eta));
+            }
             BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
             BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
-        } else if (H->h_st->error) {
-            return fail(BDC_ERR_NUMERIC, "accelerated loop: device error %d", H->h_st->error);
+            if (H->h_st->error == kErrShift) {
+                // an exp shift went out of range: finish that evaluation by
+                // re-scaling; the next step's decision takes it from there
+                rc = rescale(H, -INFINITY);
+                if (rc != BDC_OK) return rc;
+                BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
+                BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+            } else if (H->h_st->error) {
+                return fail(BDC_ERR_NUMERIC, "accelerated loop: device error %d", H->h_st->error);
+            }
+            if (H->h_st->done) break;
+            if (chunk < 64) chunk *= 2;
         }
-        if (chunk < 64) chunk *= 2;
+        converged = (H->h_st->best_ub - H->h_st->best_rate) / ln2 < gap_bits;
     }
+    BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     fill_stats(H, it0, stats);
     if (stats) stats->converged = converged;
     return BDC_OK;

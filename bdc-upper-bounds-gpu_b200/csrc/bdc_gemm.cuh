@@ -51,6 +51,8 @@ struct BaEpilogue {
     double* part;                // per-CTA partials [ctas][4]
     const DevState* st;
     double* Dout;                // optional: D(x) at every representative (dense layout)
+    double eta;                  // step of the exponentiated-gradient update: ln p' = ln p + eta D - ln Z
+                                 // (1 is the BA update)
 };
 
 }  // namespace bdc

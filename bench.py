@@ -113,6 +113,71 @@ def profile_traffic(kernel: str, n: int, k: int):
     return None
 
 
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_cuda_leg(n: int, k: int, iters: int = 2) -> dict:
+    """The reference's own CUDA BA on this GPU: backend/BAA.cu compiled
+    unchanged (oracle/_ref/ref_harness, built by oracle/Makefile from the
+    reference sources), driven through its host API from the uniform start.
+    The harness times baa_iteration + compute_max_deviation (the body of the
+    reference loop, main_BAA.cu:80-99) with CUDA events; the cache files it
+    loads (transition_counts/cache_{n',k'}, n' <= ceil(n/2)) are written by
+    this repository's generator, byte-identical to the reference's."""
+    import shutil
+    harness = os.path.join(REPO, "oracle", "_ref", "ref_harness")
+    gen = os.path.join(REPO, "bdc-upper-bounds-gpu_b200", "generate_bit_transition_cache")
+    if not (os.path.exists(harness) and os.path.exists(gen)):
+        return {"unavailable": "oracle/_ref/ref_harness not built (make -C oracle ref)"}
+    d = tempfile.mkdtemp(prefix="bdc_refcuda_")
+    try:
+        os.makedirs(os.path.join(d, "transition_counts"))
+        subprocess.run([gen, str((n + 1) // 2)], cwd=d, check=True, stdout=subprocess.DEVNULL, timeout=300)
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        t0 = time.perf_counter()
+        r = subprocess.run([harness, str(n), str(k), str(iters), "uniform", out], cwd=d, capture_output=True,
+                           text=True, timeout=600)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            return {"unavailable": f"ref_harness exited {r.returncode}: {r.stderr.strip()[-200:]}"}
+        times = [float(line.split()[2]) for line in open(os.path.join(out, "meta.txt"))
+                 if line.startswith("time_iter_s")]
+        sec = float(np.median(times))
+        return {"seconds_per_iteration": sec, "iterations_per_s": 1.0 / sec, "iterations_timed": len(times),
+                "per_iteration_s": times, "harness_wall_s": wall,
+                "what": "reference backend/BAA.cu compiled unchanged for sm_100a (oracle/_ref/ref_harness), "
+                        "CUDA events around baa_iteration + compute_max_deviation, uniform start, same GPU"}
+    except (subprocess.SubprocessError, OSError, ValueError) as e:
+        return {"unavailable": f"{type(e).__name__}: {e}"[:200]}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def cpu_full_iteration(n: int, k: int) -> dict:
+    """One whole BA iteration of the CPU oracle port (the reference's
+    per-representative algorithm: per-x DP, distinct subsequences, split
+    identity, orbit factors) over every representative, all host threads,
+    from the uniform start; measured, not extrapolated."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+    reps = O.canonicals(n)
+    p = np.full(len(reps), 1.0 / (1 << n))
+    O.log_q(n, k, p[:8], reps[:8])  # builds the cached half tables (not timed)
+    t0 = time.perf_counter()
+    O.ba_iteration(n, k, p, reps)
+    sec = time.perf_counter() - t0
+    return {"n": n, "k": k, "representatives": int(len(reps)), "seconds_per_iteration": sec,
+            "iterations_per_s": 1.0 / sec, "cores": O.threads(), "kind": "port", "cpu_model": cpu_model()}
+
+
 # --------------------------------------------------------------- CPU legs
 def cpu_ba_iteration_rate(n: int, k: int, sample: int, threads: int | None = None) -> dict:
     """The CPU oracle's q pass + D pass on `sample` evenly spaced
@@ -143,33 +208,54 @@ def cpu_ba_iteration_rate(n: int, k: int, sample: int, threads: int | None = Non
             "sample": f"q pass + D pass on {len(sub)} of {R} representatives (evenly spaced), "
                       f"scaled by {R / len(sub):.1f}, plus the full O(R) normalisation; "
                       f"{t2 - t0:.2f} s of sampled CPU work",
-            "seconds_per_iteration": per_iter}
+            "seconds_per_iteration": per_iter, "representatives": int(R), "sampled": int(len(sub)),
+            "fraction": len(sub) / R}
+
+
+def workload_config(n: int, k: int, R: int) -> dict:
+    """The workload both arms report (same keys and values in both lines)."""
+    return {"workload": f"BA iteration on BDC_{{{n},{k}}}", "n": n, "k": k, "representatives": R,
+            "start": "uniform", "parallelism": "replicas x1",
+            "l2": "working set per iteration > L2 (p, D, logW, h vectors of 33.6 MB each + 32 MB tables)"}
 
 
 def reference_arm(args) -> None:
+    """The reference's algorithm on the host cores.  The reference's BA runs
+    only on a GPU (backend/BAA.cu); its CPU restatement (oracle/bdc_oracle.c:
+    per-x DP, distinct subsequences, split identity, orbit factors, OpenMP
+    over all host threads) stands in.  Each step is a bounded sample of one
+    iteration: the q and D passes over `cpu_sample` evenly spaced
+    representatives plus the full O(R) normalisation.  ms_per_step is the
+    measured time of that sampled step; value is the whole-iteration rate it
+    implies (the sampled passes scaled to every representative)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    steps = []
+    steps, walls = [], []
     meta = None
     for _ in range(max(1, args.warmup)):
         cpu_ba_iteration_rate(args.n, args.k, args.cpu_sample)
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         meta = cpu_ba_iteration_rate(args.n, args.k, args.cpu_sample)
+        walls.append(time.perf_counter() - t0)
         steps.append(1.0 / meta["value"])
     sec = float(np.mean(steps))
     v = 1.0 / sec
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (uniform start)",
-        "config": {"workload": f"BA iteration on BDC_{{{args.n},{args.k}}}", "n": args.n, "k": args.k,
-                   "start": "uniform"},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(walls)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (uniform start; the reference publishes no throughput)",
+        "config": workload_config(args.n, args.k, meta["representatives"]),
+        "engine": "cpu port of the reference's per-representative algorithm (oracle/bdc_oracle.c, OpenMP)",
+        "sampled_step": {"representatives_sampled": meta["sampled"], "fraction": meta["fraction"],
+                         "ms_per_full_iteration_extrapolated": sec * 1e3},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": meta["cores"], "kind": "port",
-                         "sample": meta["sample"]},
+                         "sample": meta["sample"], "cpu_model": cpu_model()},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference has no CPU BA implementation; this is the CPU restatement of its "
-                "BA iteration (oracle/bdc_oracle.c) on all host threads",
+        "note": "the reference has no CPU BA implementation (its BA is CUDA); this is the CPU restatement of its "
+                "BA iteration on all host threads; each step is a bounded sample, value is the full-iteration rate",
     }
     print(json.dumps(line), flush=True)
 
@@ -310,25 +396,46 @@ def ours_arm(args) -> None:
         ttb = time_to_bound(args, E)
 
     cpu = None
+    ref_cuda = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_ba_iteration_rate(args.n, args.k, max(args.cpu_sample, 50000))
-        cpu = {k2: cpu[k2] for k2 in ("value", "unit", "cores", "sample")} | {"kind": "port"}
+        cpu = {k2: cpu[k2] for k2 in ("value", "unit", "cores", "sample")} | {
+            "kind": "port", "cpu_model": cpu_model(), "extrapolated": True}
+        # a whole iteration, measured, at the largest size the CPU finishes in
+        # seconds, next to this engine's iteration at the same size
+        full = cpu_full_iteration(20, 10)
+        with bdc_b200.Engine(20, 10, engine="auto", device=local) as E20:
+            E20.set_stream(stream.cuda_stream)
+            E20.set_uniform()
+            E20.iterate(16, float("-inf"))
+            torch.cuda.synchronize()
+            g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            g0.record(stream)
+            E20.iterate(200, float("-inf"))
+            g1.record(stream)
+            torch.cuda.synchronize()
+            full["gpu_iterations_per_s"] = 200 / (g0.elapsed_time(g1) / 1e3)
+            full["gpu_engine"] = E20.engine
+        cpu["full_iteration_20_10"] = full
+    if rank == 0 and world == 1 and not args.no_ref_cuda:
+        ref_cuda = reference_cuda_leg(args.n, args.k, 2)
+        if "seconds_per_iteration" in ref_cuda:
+            ref_cuda["speedup_of_value"] = value * ref_cuda["seconds_per_iteration"]
+            ref_cuda["speedup_of_e2e"] = e2e["value"] * ref_cuda["seconds_per_iteration"]
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (uniform start; the reference publishes no throughput)",
-        "config": {"workload": f"BA iteration on BDC_{{{args.n},{args.k}}}", "n": args.n, "k": args.k,
-                   "representatives": R, "engine": E.engine, "start": "uniform",
-                   "parallelism": f"replicas x{world}",
-                   "l2": "working set per iteration > L2 (p, D, logW, h vectors of 33.6 MB each + 32 MB tables)"},
+        "config": workload_config(args.n, args.k, R) | {"parallelism": f"replicas x{world}"},
+        "engine": E.engine,
         "gpu_launches": launches_per_iter * args.steps,
         "profile_ms": {k2: prof[k2] for k2 in ("ms_q", "ms_fold", "ms_d", "ms_update", "ms_iter", "ms_main")},
         "roofline": roofline, "roofline_update": roofline_update,
         "peaks_measured": {"int32_madd_tops": imad / 1e12, "fp64_fma_tflops": 2 * dfma / 1e12,
                            "hbm_gbs": peaks.get("hbm_gbs"), "hbm_source": peak_src},
-        "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "time_to_bound": ttb,
+        "e2e": e2e, "cpu_baseline": cpu, "reference_gpu": ref_cuda, "clocks": clocks, "time_to_bound": ttb,
         "bound_bits": st["upper_bound"], "rate_bits": st["rate"],
     }
     E.close()
@@ -687,6 +794,8 @@ def main() -> None:
     ap.add_argument("--ttb-budget", type=float, default=15.0,
                     help="device seconds for each of the plain and squarem legs of time-to-bound")
     ap.add_argument("--no-ttb", action="store_true")
+    ap.add_argument("--no-ref-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA BA (oracle/_ref/ref_harness) on this GPU")
     ap.add_argument("--fd-coords", type=int, default=1024)
     ap.add_argument("--fd-seeds", type=int, default=16)
     args = ap.parse_args()

@@ -115,15 +115,20 @@ bdc_status bdc_iterate(bdc_handle_t h, int64_t max_iters, double a, bdc_stats* s
  * least one iteration since the distribution was set (BDC_ERR_STATE). */
 bdc_status bdc_bound_error(bdc_handle_t h, double* upper_bound_err_bits, double* rate_err_bits);
 
-/* Accelerated BA (no counterpart in the reference): the BA map is the
- * exponentiated-gradient step ln p' = ln p + dI/dp + const with the adjoint
- * gradient dI/dp(x) = D(x) - 1; this loop extrapolates that map in ln p
- * (squared extrapolation: two steps, a step length alpha fitted to them and
- * clamped to [-64, -1], one stabilising step, and a fallback to the plain
- * second step when the bound at the extrapolated point is worse).  Every
- * evaluated iterate gives a valid bound, so best_upper_bound stays an upper
- * bound on C.  Runs until best_upper_bound - best_rate < gap_bits or
- * max_evals BA map evaluations.  Factored engine only. */
+/* Accelerated BA (no counterpart in the reference, whose loop is plain BA,
+ * backend/main_BAA.cu:73-109): Nesterov-accelerated exponentiated gradient
+ * driven by the adjoint of I(p;W).  Over the probabilities of the strings
+ * the gradient is dI/dp(x) = D(x) - 1, and the mirror step of length eta is
+ * ln p' = ln y + eta D(y) - ln Z (eta = 1, y = p: the BA update).  Each step
+ * evaluates D at the extrapolated point y_t = x_t + beta_t (x_t - x_{t-1})
+ * in ln p (beta_t = t / (t + 3)) and steps with eta = 1.5; when I(y_t) falls
+ * below the last accepted I, the step is discarded and the momentum restarts
+ * from x_t.  All on the device (8 steps per CUDA graph, the decisions are
+ * kernels).  Every evaluated point gives a valid bracket, so best_rate <= C
+ * <= best_upper_bound holds throughout.  Runs until best_upper_bound -
+ * best_rate < gap_bits or max_evals evaluations; stats->iters = evaluations.
+ * The handle's iterate is left at the last step's point.  Factored engine
+ * only; BDC_ACCEL_STEP overrides eta (0 < eta <= 4). */
 bdc_status bdc_accelerate(bdc_handle_t h, int64_t max_evals, double gap_bits, bdc_stats* stats);
 
 /* The mutual-information functional and its adjoint (no counterpart in the
@@ -134,6 +139,11 @@ bdc_status bdc_accelerate(bdc_handle_t h, int64_t max_evals, double gap_bits, bd
  * orbit i together: grad[i] = |O_i| (D(x_i) - 1). */
 bdc_status bdc_mi_forward(bdc_handle_t h, const double* p, int64_t num_reps, double* I_nats);
 bdc_status bdc_mi_backward(bdc_handle_t h, double* grad, int64_t num_reps);
+/* The same gradient written to device memory the caller owns (on the
+ * handle's device), for optimisers that keep their iterate on the GPU:
+ * bdc_set_p_device, bdc_mi_forward(h, NULL, ...), bdc_mi_backward_device.
+ * Returns when grad_dev is written. */
+bdc_status bdc_mi_backward_device(bdc_handle_t h, double* grad_dev, int64_t num_reps);
 
 /* Certified solver (no counterpart in the reference, which runs plain BA
  * until max_x log2 p'/p < a, backend/main_BAA.cu:73).  Anderson-accelerated

@@ -31,6 +31,27 @@ def test_adjoint_matches_finite_differences_and_oracle(bdc, O, engine):
             assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])), (i, fd, g[i])
 
 
+def test_device_backward_matches_the_host_backward(bdc, O):
+    # the device-pointer form of the adjoint, for optimisers that keep the
+    # iterate on the GPU: set_p_device -> mi_forward(None) -> mi_backward_device
+    import torch
+    from bdc_b200 import dist
+    n, k = 12, 6
+    reps = O.canonicals(n)
+    p0 = dist.dirichlet_start(n, 1.0, 5)
+    with bdc.Engine(n, k, engine="factored") as E:
+        tp = torch.tensor(p0, dtype=torch.float64, device="cuda")
+        E.set_p_device(tp.data_ptr())
+        I0 = E.mi_forward(None)
+        g = torch.empty_like(tp)
+        E.mi_backward_device(g.data_ptr())
+        host = E.mi_backward()
+        np.testing.assert_array_equal(g.cpu().numpy(), host)
+        lnq = O.log_q(n, k, p0, reps)
+        assert abs(I0 - O.rate(n, k, lnq, p0, reps)) < 1e-12
+        np.testing.assert_allclose(host, O.orbits_of(reps, n) * (O.kl(n, k, lnq, reps) - 1.0), rtol=0, atol=1e-11)
+
+
 def test_accelerated_reaches_the_plain_bound_in_fewer_evaluations(bdc, O):
     n, k, tol = 12, 6, 1e-9
     with bdc.Engine(n, k, engine="factored") as E:
