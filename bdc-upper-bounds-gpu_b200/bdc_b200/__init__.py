@@ -41,7 +41,8 @@ EXPORTED_SYMBOLS = [
     "bdc_generate_cache", "bdc_read_cache_file", "bdc_write_cache_file", "bdc_read_dist_file",
     "bdc_write_dist_file", "bdc_work", "bdc_profile", "bdc_set_stream", "bdc_peak_probe",
     "bdc_max_deviation_noalloc", "bdc_accelerate", "bdc_mi_forward", "bdc_mi_backward", "bdc_mi_backward_device",
-    "bdc_batch_create", "bdc_batch_iterate", "bdc_batch_destroy", "bdc_batch_set_stream", "bdc_solve",
+    "bdc_batch_create", "bdc_batch_iterate", "bdc_batch_destroy", "bdc_batch_set_stream", "bdc_batch_accelerate",
+    "bdc_solve",
     "bdc_bound_error", "bdc_shard_q", "bdc_shard_set_q", "bdc_shard_update_begin", "bdc_shard_update_end",
 ]
 
@@ -112,6 +113,8 @@ def library() -> ctypes.CDLL:
     L.bdc_solve.argtypes = [h, ctypes.c_double, ctypes.c_int64, ctypes.POINTER(Stats)]
     L.bdc_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
     L.bdc_batch_iterate.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats)]
+    L.bdc_batch_accelerate.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Stats),
+                                       _f64p]
     L.bdc_batch_destroy.argtypes = [ctypes.c_void_p]
     L.bdc_batch_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.bdc_mi_forward.argtypes = [h, _f64p, ctypes.c_int64, _f64p]
@@ -421,6 +424,16 @@ class Batch:
         st = (Stats * len(self.engines))()
         _check(library().bdc_batch_iterate(self._b, int(max_iters), float(a), st), "bdc_batch_iterate")
         return [s.as_dict() for s in st]
+
+    def accelerate(self, max_evals: int, gap_bits: float = 1e-9) -> tuple[list, list]:
+        """The accelerated loop for every engine (factored), each stopping on
+        its own bracket < gap_bits; returns (stats per engine, seconds per
+        engine until its bracket fell below gap_bits, -1 if it did not)."""
+        st = (Stats * len(self.engines))()
+        sec = np.empty(len(self.engines), dtype=np.float64)
+        _check(library().bdc_batch_accelerate(self._b, int(max_evals), float(gap_bits), st,
+                                              sec.ctypes.data_as(_f64p)), "bdc_batch_accelerate")
+        return [s.as_dict() for s in st], [float(v) for v in sec]
 
     def set_stream(self, stream: int | None) -> None:
         """Queue the batch's work on a cudaStream_t given as an integer handle."""

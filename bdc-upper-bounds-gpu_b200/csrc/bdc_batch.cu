@@ -25,6 +25,8 @@ struct bdc_batch {
     std::vector<cudaEvent_t> joins;
     cudaGraphExec_t exec = nullptr;
     double a = 0.0;
+    cudaGraphExec_t acc_exec = nullptr;  // accelerated steps of every instance (bdc_batch_accelerate)
+    double acc_eta = 0.0;
 };
 
 namespace bdc {
@@ -33,6 +35,7 @@ constexpr int kBatchIters = 8;
 
 static void batch_free(bdc_batch* B) {
     if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->acc_exec) cudaGraphExecDestroy(B->acc_exec);
     for (auto s : B->lanes) cudaStreamDestroy(s);
     for (auto e : B->joins) cudaEventDestroy(e);
     if (B->fork) cudaEventDestroy(B->fork);
@@ -66,6 +69,37 @@ static bdc_status batch_capture(bdc_batch* B, double a) {
     if (g) cudaGraphDestroy(g);
     BDC_CUDA_TRY(e);
     B->a = a;
+    return BDC_OK;
+}
+
+// kAccBatchSteps accelerated steps of every instance, one branch per instance
+constexpr int kAccBatchSteps = 8;
+
+static bdc_status batch_capture_acc(bdc_batch* B, double eta) {
+    if (B->acc_exec && B->acc_eta == eta) return BDC_OK;
+    if (B->acc_exec) {
+        cudaGraphExecDestroy(B->acc_exec);
+        B->acc_exec = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(B->origin, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaEventRecord(B->fork, B->origin);
+    for (size_t i = 0; i < B->hs.size() && e == cudaSuccess; ++i) {
+        bdc_handle* H = B->hs[i];
+        e = cudaStreamWaitEvent(B->lanes[i], B->fork, 0);
+        cudaStream_t keep = H->stream;
+        H->stream = B->lanes[i];
+        if (e == cudaSuccess) e = factored_enqueue_acc_steps(H, kAccBatchSteps, eta);
+        H->stream = keep;
+        if (e == cudaSuccess) e = cudaEventRecord(B->joins[i], B->lanes[i]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(B->origin, B->joins[i], 0);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(B->origin, &g);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&B->acc_exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    BDC_CUDA_TRY(e);
+    B->acc_eta = eta;
     return BDC_OK;
 }
 
@@ -225,6 +259,109 @@ bdc_status bdc_batch_iterate(bdc_batch_t B, int64_t max_iters, double a, bdc_sta
             o.best_rate = s->best_rate / ln2;
             o.converged = s->done;
         }
+    }
+    return BDC_OK;
+}
+
+bdc_status bdc_batch_accelerate(bdc_batch_t B, int64_t max_evals, double gap_bits, bdc_stats* stats,
+                                double* seconds) {
+    if (!B || max_evals < 0) return fail(BDC_ERR_ARG, "bdc_batch_accelerate: bad arguments");
+    BDC_CUDA_TRY(cudaSetDevice(B->device));
+    const size_t N = B->hs.size();
+    const double ln2 = 0.69314718055994530942;
+    for (auto* H : B->hs) {
+        if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_batch_accelerate: an instance has no distribution set");
+        if (H->engine != BDC_ENGINE_FACTORED)
+            return fail(BDC_ERR_UNSUPPORTED, "bdc_batch_accelerate: every instance needs the factored engine");
+    }
+    const double eta = factored_acc_eta();
+    std::vector<long long> it0(N);
+    std::vector<double> sec(N, -1.0);
+    std::vector<char> fin(N, 0);
+    bdc_status rc = batch_capture_acc(B, eta);
+    if (rc != BDC_OK) return rc;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BDC_CUDA_TRY(cudaEventCreate(&e0));
+    BDC_CUDA_TRY(cudaEventCreate(&e1));
+    // start: the plain first step where the iterate still carries the
+    // caller's exact zeros, then each instance's snapshots and device stop
+    for (auto* H : B->hs) BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    BDC_CUDA_TRY(cudaEventRecord(e0, B->launch));
+    for (size_t i = 0; i < N; ++i) {
+        bdc_handle* H = B->hs[i];
+        cudaStream_t keep = H->stream;
+        H->stream = B->launch;
+        rc = BDC_OK;
+        cudaError_t ce = cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), B->launch);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, B->launch);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(B->launch);
+        if (ce != cudaSuccess) rc = fail(BDC_ERR_CUDA, "bdc_batch_accelerate: %s", cudaGetErrorString(ce));
+        it0[i] = H->h_st->iter;
+        if (rc == BDC_OK && H->h_st->iter == 0 && max_evals > 0) rc = factored_iterate(H, 1, -INFINITY, nullptr);
+        if (rc == BDC_OK) rc = factored_acc_start(H, gap_bits);
+        H->stream = keep;
+        if (rc != BDC_OK) return rc;
+    }
+    static const int kOne = 1;
+    for (int guard = 0; guard < 10000000; ++guard) {
+        // park the instances that are finished or out of evaluations
+        bool any = false;
+        for (size_t i = 0; i < N; ++i) {
+            bdc_handle* H = B->hs[i];
+            if (fin[i]) continue;
+            if (H->h_st->done || H->h_st->iter - it0[i] >= max_evals) {
+                fin[i] = 1;
+                if (!H->h_st->done) {
+                    BDC_CUDA_TRY(cudaMemcpyAsync(&H->d_st->done, &kOne, sizeof(int), cudaMemcpyHostToDevice, B->launch));
+                    H->h_st->done = 1;
+                }
+                continue;
+            }
+            any = true;
+        }
+        if (!any) break;
+        BDC_CUDA_TRY(cudaGraphLaunch(B->acc_exec, B->launch));
+        BDC_CUDA_TRY(cudaEventRecord(e1, B->launch));
+        for (auto* H : B->hs)
+            BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, B->launch));
+        BDC_CUDA_TRY(cudaStreamSynchronize(B->launch));
+        float ms = 0.f;
+        BDC_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        for (size_t i = 0; i < N; ++i) {
+            bdc_handle* H = B->hs[i];
+            if (H->h_st->error) {
+                // an exp shift out of range finishes by re-scaling; any other
+                // device error is returned
+                cudaStream_t keep = H->stream;
+                H->stream = B->launch;
+                bdc_status r2 = factored_recover(H, -INFINITY);
+                H->stream = keep;
+                if (r2 != BDC_OK) return r2;
+                BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, B->launch));
+                BDC_CUDA_TRY(cudaStreamSynchronize(B->launch));
+            }
+            if (!fin[i] && sec[i] < 0 && (H->h_st->best_ub - H->h_st->best_rate) / ln2 < gap_bits) sec[i] = ms * 1e-3;
+        }
+    }
+    for (auto* H : B->hs) BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), B->launch));
+    BDC_CUDA_TRY(cudaStreamSynchronize(B->launch));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (size_t i = 0; i < N; ++i) {
+        const DevState* s = B->hs[i]->h_st;
+        if (stats) {
+            bdc_stats& o = stats[i];
+            o.iters = s->iter - it0[i];
+            o.total_iters = s->iter;
+            o.mx = s->mx;
+            o.upper_bound = s->max_d / ln2;
+            o.rate = s->rate / ln2;
+            o.lse = s->lse / ln2;
+            o.best_upper_bound = s->best_ub / ln2;
+            o.best_rate = s->best_rate / ln2;
+            o.converged = (s->best_ub - s->best_rate) / ln2 < gap_bits;
+        }
+        if (seconds) seconds[i] = sec[i];
     }
     return BDC_OK;
 }

@@ -33,9 +33,12 @@
 #include <string>
 #include <vector>
 
+#include <cstring>
+
 #include "bdc_engine.cuh"
 #include "bdc_gemm.cuh"
 #include "bdc_mma.cuh"
+#include "bdc_ozaki.cuh"
 
 namespace bdc {
 
@@ -160,6 +163,8 @@ struct FactoredState {
     double* lnq_full = nullptr;  // [2^k]
     double* epart = nullptr;  // [ctas][8]
     int ctas_g = 0;
+    bdc::OzakiG* oz = nullptr;  // G on the int8 tensor cores (when set up and chosen)
+    bool use_oz = false;
     bdc::Launch ul, vr, g;
     bdc::FoldTerm* d_fold = nullptr;
     int launches_per_iter = 0;
@@ -2056,8 +2061,27 @@ bdc_status factored_init(bdc_handle* H) {
         nd = 0;
         for (int cl = 0; cl < 4; ++cl) nd += F->n_df[cl] > 0;
     }
-    // U, V, the split sums; q-side terms; three fold kernels; D-side terms; G; finalize
-    F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + nq + 3 + nd + 1 + 1;
+    // G on the int8 tensor cores (bdc_ozaki.cu) where BDC_G_KERNEL=ozaki asks for it
+    {
+        const char* gk = getenv("BDC_G_KERNEL");
+        if (gk && !strcmp(gk, "ozaki")) {
+            const OzakiInput in{F->LA, F->RB, Kp, KL, KR, H1, H2, F->colmax.data()};
+            const char* why = nullptr;
+            bdc_status rc = ozaki_init(H, in, &F->oz, &why);
+            if (rc != BDC_OK) return rc;
+            F->use_oz = F->oz != nullptr;
+            if (H->verbose) {
+                if (F->use_oz)
+                    printf("bdc: G on the int8 tensor cores: %d tiles of %dx%d, %d B shared memory\n", F->oz->tiles,
+                           kOzBM, kOzBN, F->oz->smem);
+                else
+                    printf("bdc: G stays on the FP64 product: %s\n", why ? why : "?");
+            }
+        }
+    }
+    // U, V, the split sums; q-side terms; three fold kernels; D-side terms; G
+    // (plus four operand kernels on the int8 path); finalize
+    F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + nq + 3 + nd + 1 + 1 + (F->use_oz ? 4 : 0);
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
 }
@@ -2091,6 +2115,7 @@ void factored_free(bdc_handle* H) {
         free_launch(F->md[lg]);
     }
     cudaFree(F->d_fold);
+    ozaki_free(F->oz);
     delete F;
     H->fac = nullptr;
 }
@@ -2181,9 +2206,10 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             }
             break;
         case ST_G:
+            if (F->use_oz) return ozaki_enqueue(F->oz, make_epilogue(H), H->d_st, s);
             return launch_ba(F->g, make_epilogue(H), s, H->d_st);
         case ST_FIN:
-            k_fac_finalize<<<1, 256, 0, s>>>(F->epart, F->ctas_g, a, F->eta, H->d_st);
+            k_fac_finalize<<<1, 256, 0, s>>>(F->epart, F->use_oz ? F->oz->tiles : F->ctas_g, a, F->eta, H->d_st);
             break;
     }
     return cudaGetLastError();

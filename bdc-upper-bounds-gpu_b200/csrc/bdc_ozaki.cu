@@ -1,0 +1,631 @@
+// bdc_ozaki.cu -- G = [AL | NR] [ML ; BR^T] with the fused BA update on the
+// int8 tensor cores of sm_100a (tcgen05.mma kind::i8, TMEM accumulators, TMA
+// loads through an mbarrier pipeline).  The splitting of the operands is
+// explained in bdc_ozaki.cuh.
+//
+// Replaces, like the FP64 product it stands beside (k_mma_ba in
+// bdc_factored.cu), the D pass and normalised update of the reference
+// (backend/BAA.cu:487-530 compute_log_W_gpu, 590-639 baa_iteration): per
+// representative D(x) = h(x) - G(x) / C(n,k), logW = ln p + eta D, and the
+// block partials of the update.
+//
+// One CTA per 128 x 64 tile of G that holds a representative (the eight
+// accumulators take all 512 TMEM columns of an SM).  Warp 0 lane 0 loads,
+// warp 1 lane 0 issues the MMAs, then all four warps drain the accumulators
+// (one TMEM lane = one tile row per thread) and run the epilogue.  Every wait
+// on an mbarrier is bounded: on time-out the CTA records an error in
+// DevState::error, skips the epilogue, waits (bounded) for its loads and
+// frees its TMEM.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
+#include "bdc_gemm.cuh"
+#include "bdc_ozaki.cuh"
+
+namespace bdc {
+
+constexpr int kErrOzakiWait = 3;         // DevState::error: an mbarrier wait ran out
+constexpr int kErrOzakiOperand = 4;      // DevState::error: a non-finite FP64 operand
+constexpr uint32_t kOzSpin = 1u << 22;   // polls per wait
+constexpr int kOzTmemCols = kOzW * kOzBN;
+static_assert(kOzTmemCols <= 512, "accumulators exceed tensor memory");
+
+// ------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t sm_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// bounded wait for the phase with the given parity to complete
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kOzSpin; ++i) {
+        uint32_t ok = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major operand in the 128-byte swizzled canonical layout: rows of 128
+// bytes, groups of 8 rows 1024 bytes apart (SBO), the start advanced in
+// 32-byte steps along the contraction inside a 128-byte atom
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t)1 << 16;                          // leading byte offset (unused by swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;                // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;                          // 128-byte swizzle
+    return d;
+}
+
+// instruction descriptor: s8 x s8 -> s32, both K-major, M x N
+__host__ __device__ constexpr uint32_t umma_idesc_i8(int M, int N) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(ad), "l"(bd), "r"(idesc), "r"(accum)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// --------------------------------------------------------------- the product
+struct OzGeomDev {
+    int KLp, KRp;
+    int aS, bS, aD, bD;  // atom columns
+    int M, N;            // rows (H1h) and columns (H2) of G
+    int tiles_n;
+};
+
+__global__ void __launch_bounds__(kOzThreads, 1)
+k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtensorMap tmBs,
+        const __grid_constant__ CUtensorMap tmAd, const __grid_constant__ CUtensorMap tmBd, OzGeomDev g,
+        const int* __restrict__ tiles, const int* __restrict__ d_e, BaEpilogue ep, DevState* st) {
+    extern __shared__ __align__(1024) uint8_t oz_smem_raw[];
+    __shared__ __align__(8) uint64_t bar_static, bar_full[kOzStages], bar_empty[kOzStages], bar_done;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int abort_sh, skip_sh;
+    // one read of the gate for the whole CTA (another CTA may set the error)
+    if (threadIdx.x == 0) skip_sh = (st->done || st->error) ? 1 : 0;
+    __syncthreads();
+    if (skip_sh) return;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = tiles[blockIdx.x];
+    const int m0 = (t / g.tiles_n) * kOzBM, n0 = (t % g.tiles_n) * kOzBN;
+
+    // 1024-byte aligned carve-up: static A, static B, then the stages
+    uint8_t* base = (uint8_t*)(((uintptr_t)oz_smem_raw + 1023) & ~(uintptr_t)1023);
+    const uint32_t sA = sm_addr(base);
+    const uint32_t sB = sA + (uint32_t)g.aS * kOzBM * 128;
+    const uint32_t sStage0 = sB + (uint32_t)g.bS * kOzBN * 128;
+    const uint32_t stageA = (uint32_t)g.aD * kOzBM * 128, stageB = (uint32_t)g.bD * kOzBN * 128;
+    const uint32_t stageBytes = stageA + stageB;
+
+    if (threadIdx.x == 0) {
+        mbar_init(sm_addr(&bar_static), 1);
+        for (int i = 0; i < kOzStages; ++i) {
+            mbar_init(sm_addr(&bar_full[i]), 1);
+            mbar_init(sm_addr(&bar_empty[i]), 1);
+        }
+        mbar_init(sm_addr(&bar_done), 1);
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sm_addr(&tmem_base_sh)),
+                     "r"((uint32_t)kOzTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_sh;
+
+    int issued_loads = 0;  // producer: per-weight loads issued (for the bounded drain on abort)
+
+    if (warp == 0 && lane == 0) {
+        // ---- producer: the static operands once, the per-weight slices through the stages
+        const uint32_t bs = sm_addr(&bar_static);
+        mbar_expect_tx(bs, (uint32_t)(g.aS * kOzBM + g.bS * kOzBN) * 128);
+        for (int c = 0; c < g.aS; ++c) tma_load_2d(sA + c * kOzBM * 128, &tmAs, bs, 128 * c, m0);
+        for (int c = 0; c < g.bS; ++c) tma_load_2d(sB + c * kOzBN * 128, &tmBs, bs, 128 * c, n0);
+        for (int a = 0; a < kOzW; ++a) {
+            const int s = a % kOzStages, use = a / kOzStages;
+            if (use > 0 && !mbar_wait(sm_addr(&bar_empty[s]), (use - 1) & 1)) {
+                atomicExch(&abort_sh, 1);
+                break;
+            }
+            if (*(volatile int*)&abort_sh) break;
+            const uint32_t fb = sm_addr(&bar_full[s]);
+            const uint32_t dA = sStage0 + s * stageBytes, dB = dA + stageA;
+            mbar_expect_tx(fb, stageBytes);
+            // slots a and a + 1 of the sliced operands: [x_{a-1} | x_a]
+            for (int c = 0; c < g.aD; ++c) tma_load_2d(dA + c * kOzBM * 128, &tmAd, fb, a * g.KRp + 128 * c, m0);
+            for (int c = 0; c < g.bD; ++c) tma_load_2d(dB + c * kOzBN * 128, &tmBd, fb, a * g.KLp + 128 * c, n0);
+            ++issued_loads;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer: accumulator a gets [lo | hi] x [x_{a-1} | x_a] over both parts
+        const uint32_t idesc = umma_idesc_i8(kOzBM, kOzBN);
+        bool ok = mbar_wait(sm_addr(&bar_static), 0);
+        for (int a = 0; a < kOzW && ok; ++a) {
+            const int s = a % kOzStages, use = a / kOzStages;
+            if (!mbar_wait(sm_addr(&bar_full[s]), use & 1) || *(volatile int*)&abort_sh) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t dA = sStage0 + s * stageBytes, dB = dA + stageA;
+            const uint32_t tacc = tmem + (uint32_t)(a * kOzBN);
+            uint32_t accum = 0;
+            for (int kb = 0; kb < 2 * g.KLp; kb += 32) {  // L part: static A x per-weight B
+                const uint32_t off = (uint32_t)(kb >> 7), in = (uint32_t)(kb & 127);
+                umma_i8(tacc, umma_desc_sw128(sA + off * kOzBM * 128 + in), umma_desc_sw128(dB + off * kOzBN * 128 + in),
+                        idesc, accum);
+                accum = 1;
+            }
+            for (int kb = 0; kb < 2 * g.KRp; kb += 32) {  // R part: per-weight A x static B
+                const uint32_t off = (uint32_t)(kb >> 7), in = (uint32_t)(kb & 127);
+                umma_i8(tacc, umma_desc_sw128(dA + off * kOzBM * 128 + in), umma_desc_sw128(sB + off * kOzBN * 128 + in),
+                        idesc, accum);
+                accum = 1;
+            }
+            umma_commit(sm_addr(&bar_empty[s]));  // the stage is free once these MMAs are done
+        }
+        if (!ok) atomicExch(&abort_sh, 1);
+        umma_commit(sm_addr(&bar_done));  // arrives when every MMA issued above has completed
+    }
+
+    // ---- everyone: wait for the accumulators
+    const bool done_ok = mbar_wait(sm_addr(&bar_done), 0);
+    tc_fence_after();
+    __syncthreads();
+    if (!done_ok) atomicExch(&abort_sh, 1);
+    __syncthreads();
+    const bool run = (*(volatile int*)&abort_sh == 0);
+
+    double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0, zero = 0.0;
+    if (run) {
+        const double shift = st->shift;
+        const double lnz = st->log_z;
+        const double inv_z = exp(-lnz);
+        const int e = *d_e;
+        const int r = warp * 32 + lane;  // tile row = TMEM lane
+        const int m = m0 + r;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < kOzBN; c0 += 16) {
+            double gsum[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) gsum[j] = 0.0;
+            // smallest weights first: every term is exact, the sum rounds once per step
+#pragma unroll 1
+            for (int a = kOzW - 1; a >= 0; --a) {
+                uint32_t v[16];
+                tmem_ld16(trow + (uint32_t)(a * kOzBN + c0), v);
+                tmem_wait_ld();
+                const double w = ldexp(1.0, e - 7 * a);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) gsum[j] = fma((double)(int32_t)v[j], w, gsum[j]);
+            }
+            if (m >= g.M) continue;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int n = n0 + c0 + j;
+                if (n >= g.N) continue;
+                const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
+                const uint32_t x = (xd & ~low_mask(ep.n2)) | reverse_bits(xd & low_mask(ep.n2), ep.n2);
+                if (!is_rep(x, ep.n)) continue;
+                const double o = (double)orbit_size(x, ep.n);
+                const double D = __ldg(ep.hx + xd) - gsum[j] * ep.inv_c;
+                if (ep.Dout) ep.Dout[xd] = D;
+                // an entry that is exactly 0 in the caller's distribution (Lt
+                // holds NaN) takes ln p = 0, as the reference's apply_log_kernel
+                // leaves ln 0 at 0 (backend/BAA.cu:573-580)
+                const double pw = ep.Pw[xd];
+                const double lt = ep.Lt[xd];
+                const bool zero_in = (lt != lt);
+                const double lnp = zero_in ? 0.0 : lt - lnz;
+                const double lw = lnp + ep.eta * D - shift;
+                const double ex = exp(lw);
+                ep.Lt[xd] = lw;
+                ep.Pw[xd] = o * ex;
+                mD = fmax(mD, D);
+                mL = fmax(mL, lw);
+                sE = fma(o, ex, sE);
+                sR = fma(pw * inv_z, D, sR);
+                if (zero_in) zero = 1.0;
+            }
+        }
+    } else if (threadIdx.x == 0) {
+        st->error = kErrOzakiWait;
+    }
+
+    // ---- block partials, as the FP64 product writes them
+    __shared__ double red[5][kOzThreads / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        mD = fmax(mD, __shfl_xor_sync(0xFFFFFFFFu, mD, off));
+        mL = fmax(mL, __shfl_xor_sync(0xFFFFFFFFu, mL, off));
+        sE += __shfl_xor_sync(0xFFFFFFFFu, sE, off);
+        sR += __shfl_xor_sync(0xFFFFFFFFu, sR, off);
+        zero = fmax(zero, __shfl_xor_sync(0xFFFFFFFFu, zero, off));
+    }
+    if (lane == 0) {
+        red[0][warp] = mD;
+        red[1][warp] = sE;
+        red[2][warp] = mL;
+        red[3][warp] = sR;
+        red[4][warp] = zero;
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = red[0][0], a1 = red[1][0], a2 = red[2][0], a3 = red[3][0], a4 = red[4][0];
+        for (int w = 1; w < kOzThreads / 32; ++w) {
+            a0 = fmax(a0, red[0][w]);
+            a1 += red[1][w];
+            a2 = fmax(a2, red[2][w]);
+            a3 += red[3][w];
+            a4 = fmax(a4, red[4][w]);
+        }
+        double* p = ep.part + (size_t)blockIdx.x * 8;
+        p[0] = a0;
+        p[1] = a1;
+        p[2] = a2;
+        p[3] = a3;
+        p[4] = a4;
+    }
+    // on an abort, wait (bounded) for the loads still in flight before the
+    // shared memory is released; the MMAs were all covered by bar_done
+    if (!run && warp == 0 && lane == 0) {
+        for (int a = 0; a < issued_loads; ++a) {
+            const int s = a % kOzStages, use = a / kOzStages;
+            (void)mbar_wait(sm_addr(&bar_full[s]), use & 1);
+        }
+        (void)mbar_wait(sm_addr(&bar_static), 0);
+    }
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kOzTmemCols)
+                     : "memory");
+}
+
+// ------------------------------------------------------ operand preparation
+// block maxima of |ML| (RB rows [0, KL)) and |NR| (LA columns [KL, KL + KR))
+__global__ void __launch_bounds__(256) k_oz_maxabs(const double* __restrict__ RB, int64_t nml,
+                                                   const double* __restrict__ LA, int Kp, int KL, int KR, int rows,
+                                                   double* __restrict__ part, const DevState* st) {
+    if (st->done || st->error) return;
+    double m = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nml; i += stride) m = fmax(m, fabs(RB[i]));
+    const int64_t nnr = (int64_t)rows * KR;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnr; i += stride)
+        m = fmax(m, fabs(LA[(i / KR) * Kp + KL + (i % KR)]));
+    __shared__ double red[256];
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// e with max |X| < 2^e (frexp); a non-finite operand is a device error
+__global__ void k_oz_exponent(const double* __restrict__ part, int nb, int* __restrict__ e_out, DevState* st) {
+    if (threadIdx.x != 0 || st->done || st->error) return;
+    double m = 0.0;
+    for (int b = 0; b < nb; ++b) m = fmax(m, part[b]);
+    if (!isfinite(m)) {
+        st->error = kErrOzakiOperand;
+        return;
+    }
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);  // m = f 2^e, f in [0.5, 1)
+    *e_out = e;
+}
+
+// J truncated base-128 digits of v 2^{-e} (|v| < 2^e): exact in FP64
+__device__ __forceinline__ void oz_digits(double v, int e, int8_t (&d)[kOzJ]) {
+    double u = ldexp(v, -e);
+#pragma unroll
+    for (int s = 0; s < kOzJ; ++s) {
+        u *= 128.0;
+        const double q = trunc(u);
+        d[s] = (int8_t)(int)q;
+        u -= q;
+    }
+}
+
+__device__ __forceinline__ uint4 pack16(const int8_t (&dig)[16][kOzJ], int s) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        w[q] = (uint32_t)(uint8_t)dig[4 * q][s] | ((uint32_t)(uint8_t)dig[4 * q + 1][s] << 8) |
+               ((uint32_t)(uint8_t)dig[4 * q + 2][s] << 16) | ((uint32_t)(uint8_t)dig[4 * q + 3][s] << 24);
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// NR (LA columns KL + r) -> Ad[m][slot 1 + s][r]; one thread per (row, 16 r)
+__global__ void __launch_bounds__(256) k_oz_slice_a(const double* __restrict__ LA, int Kp, int KL, int KR, int rows,
+                                                    int KRp, uint8_t* __restrict__ Ad, const int* __restrict__ d_e,
+                                                    const DevState* st) {
+    if (st->done || st->error) return;
+    const int e = *d_e;
+    const int chunks = KRp / 16;
+    const int64_t total = (int64_t)rows * chunks;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int m = (int)(i / chunks), c = (int)(i % chunks);
+        int8_t dig[16][kOzJ];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int r = c * 16 + j;
+            const double v = (r < KR) ? LA[(int64_t)m * Kp + KL + r] : 0.0;
+            oz_digits(v, e, dig[j]);
+        }
+        uint8_t* row = Ad + (int64_t)m * kOzP * KRp;
+#pragma unroll
+        for (int s = 0; s < kOzJ; ++s) *(uint4*)(row + (s + 1) * KRp + c * 16) = pack16(dig, s);
+    }
+}
+
+// ML (RB rows k < KL, column n) -> Bd[n][slot 1 + s][k]: a block transposes a
+// 32-column strip of RB through shared memory; thread (column, 16 k) packs
+__global__ void __launch_bounds__(256) k_oz_slice_b(const double* __restrict__ RB, int KL, int cols, int KLp,
+                                                    uint8_t* __restrict__ Bd, const int* __restrict__ d_e,
+                                                    const DevState* st) {
+    if (st->done || st->error) return;
+    extern __shared__ double tile[];  // [KLp][33]
+    const int e = *d_e;
+    const int n0 = blockIdx.x * 32;
+    for (int i = threadIdx.x; i < KLp * 32; i += blockDim.x) {
+        const int k = i / 32, c = i % 32;
+        tile[k * 33 + c] = (k < KL && n0 + c < cols) ? RB[(int64_t)k * cols + n0 + c] : 0.0;
+    }
+    __syncthreads();
+    const int chunks = KLp / 16;
+    for (int i = threadIdx.x; i < 32 * chunks; i += blockDim.x) {
+        const int c = i % 32, ch = i / 32;
+        if (n0 + c >= cols) continue;
+        int8_t dig[16][kOzJ];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) oz_digits(tile[(ch * 16 + j) * 33 + c], e, dig[j]);
+        uint8_t* row = Bd + (int64_t)(n0 + c) * kOzP * KLp;
+#pragma unroll
+        for (int s = 0; s < kOzJ; ++s) *(uint4*)(row + (s + 1) * KLp + ch * 16) = pack16(dig, s);
+    }
+}
+
+// the integer operands, once: As[m] = [lo | hi] of AL[m][k] (LA columns k <
+// KL), Bs[n] = [lo | hi] of BR^T[r][n] (RB rows KL + r); flag set when an
+// entry does not fit two digits
+__global__ void k_oz_static(const double* __restrict__ LA, const double* __restrict__ RB, int Kp, int KL, int KR,
+                            int rows, int cols, int KLp, int KRp, uint8_t* __restrict__ As, uint8_t* __restrict__ Bs,
+                            int* __restrict__ bad) {
+    const int64_t na = (int64_t)rows * KLp, nb = (int64_t)cols * KRp;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < na + nb; i += (int64_t)gridDim.x * blockDim.x) {
+        double v;
+        uint8_t* lo;
+        int len;
+        if (i < na) {
+            const int m = (int)(i / KLp), k = (int)(i % KLp);
+            v = (k < KL) ? LA[(int64_t)m * Kp + k] : 0.0;
+            lo = As + (int64_t)m * 2 * KLp + k;
+            len = KLp;
+        } else {
+            const int64_t j = i - na;
+            const int n = (int)(j / KRp), r = (int)(j % KRp);
+            v = (r < KR) ? RB[(int64_t)(KL + r) * cols + n] : 0.0;
+            lo = Bs + (int64_t)n * 2 * KRp + r;
+            len = KRp;
+        }
+        const int iv = (int)v;
+        if ((double)iv != v || iv < 0 || iv >= 128 * 127) atomicExch(bad, 1);
+        lo[0] = (uint8_t)(iv & 127);
+        lo[len] = (uint8_t)((iv >> 7) & 127);
+    }
+}
+
+// ------------------------------------------------------------------- host
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// a 2-D byte tensor of `rows` rows of `row_bytes` bytes, boxes of 128 bytes x box_rows
+static bool make_map(CUtensorMap* map, const void* base, uint64_t row_bytes, uint64_t rows, uint32_t box_rows) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {row_bytes, rows};
+    const cuuint64_t strides[1] = {row_bytes};
+    const cuuint32_t box[2] = {128, box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+void ozaki_free(OzakiG* oz) {
+    if (!oz) return;
+    cudaFree(oz->As);
+    cudaFree(oz->Bs);
+    cudaFree(oz->Ad);
+    cudaFree(oz->Bd);
+    cudaFree(oz->d_e);
+    cudaFree(oz->mpart);
+    cudaFree(oz->d_tiles);
+    delete oz;
+}
+
+bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const char** why) {
+    *out = nullptr;
+    *why = nullptr;
+    auto round32 = [](int v) { return (v + 31) / 32 * 32; };
+    if (in.KL < 1 || in.KR < 1) {
+        *why = "a part of the contraction is empty";
+        return BDC_OK;
+    }
+    const int KLp = round32(in.KL), KRp = round32(in.KR);
+    if (KLp > 256 || KRp > 256) {
+        *why = "contraction longer than 256";
+        return BDC_OK;
+    }
+    if (!encode_fn()) {
+        *why = "cuTensorMapEncodeTiled unavailable";
+        return BDC_OK;
+    }
+    OzakiG* oz = new OzakiG();
+    oz->in = in;
+    oz->KLp = KLp;
+    oz->KRp = KRp;
+    oz->aS = (2 * KLp + 127) / 128;
+    oz->bS = (2 * KRp + 127) / 128;
+    oz->aD = (2 * KRp + 127) / 128;
+    oz->bD = (2 * KLp + 127) / 128;
+    oz->smem = 1024 + (oz->aS * kOzBM + oz->bS * kOzBN) * 128 + kOzStages * (oz->aD * kOzBM + oz->bD * kOzBN) * 128;
+    int dev_smem = 0;
+    BDC_CUDA_TRY(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, H->device));
+    if (oz->smem + 2048 > dev_smem) {
+        ozaki_free(oz);
+        *why = "tile operands exceed shared memory";
+        return BDC_OK;
+    }
+    const int rows = in.H1h, cols = in.H2;
+    cudaStream_t s = H->stream;
+    auto al = [&](uint8_t** p, size_t bytes) -> cudaError_t {
+        H->bytes += bytes;
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, bytes, s);
+        return e;
+    };
+    BDC_CUDA_TRY(al(&oz->As, (size_t)rows * 2 * KLp));
+    BDC_CUDA_TRY(al(&oz->Bs, (size_t)cols * 2 * KRp));
+    BDC_CUDA_TRY(al(&oz->Ad, (size_t)rows * kOzP * KRp));
+    BDC_CUDA_TRY(al(&oz->Bd, (size_t)cols * kOzP * KLp));
+    BDC_CUDA_TRY(cudaMalloc(&oz->d_e, sizeof(int)));
+    BDC_CUDA_TRY(cudaMemsetAsync(oz->d_e, 0, sizeof(int), s));
+    oz->nmax = H->num_sms * 2;
+    BDC_CUDA_TRY(cudaMalloc(&oz->mpart, sizeof(double) * oz->nmax));
+    {
+        int* bad = nullptr;
+        BDC_CUDA_TRY(cudaMalloc(&bad, sizeof(int)));
+        BDC_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), s));
+        k_oz_static<<<H->num_sms * 4, 256, 0, s>>>(in.LA, in.RB, in.Kp, in.KL, in.KR, rows, cols, KLp, KRp, oz->As,
+                                                   oz->Bs, bad);
+        BDC_CUDA_TRY(cudaGetLastError());
+        int hb = 0;
+        BDC_CUDA_TRY(cudaMemcpyAsync(&hb, bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+        BDC_CUDA_TRY(cudaStreamSynchronize(s));
+        cudaFree(bad);
+        if (hb) {
+            ozaki_free(oz);
+            *why = "a table entry does not fit two base-128 digits";
+            return BDC_OK;
+        }
+    }
+    // tiles that hold a representative
+    const int tiles_m = (rows + kOzBM - 1) / kOzBM, tiles_n = (cols + kOzBN - 1) / kOzBN;
+    std::vector<int> ids;
+    for (int tm = 0; tm < tiles_m; ++tm)
+        for (int tn = 0; tn < tiles_n; ++tn) {
+            int mx = -1;
+            for (int c = tn * kOzBN; c < std::min(cols, (tn + 1) * kOzBN); ++c) mx = std::max(mx, in.colmax[c]);
+            if (mx >= tm * kOzBM) ids.push_back(tm * tiles_n + tn);
+        }
+    oz->tiles = (int)ids.size();
+    oz->tiles_n = tiles_n;
+    if (oz->tiles > 0) {
+        BDC_CUDA_TRY(cudaMalloc(&oz->d_tiles, sizeof(int) * ids.size()));
+        BDC_CUDA_TRY(cudaMemcpy(oz->d_tiles, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+    }
+    const bool ok = make_map(&oz->tmAs, oz->As, 2 * KLp, rows, kOzBM) &&
+                    make_map(&oz->tmBs, oz->Bs, 2 * KRp, cols, kOzBN) &&
+                    make_map(&oz->tmAd, oz->Ad, (uint64_t)kOzP * KRp, rows, kOzBM) &&
+                    make_map(&oz->tmBd, oz->Bd, (uint64_t)kOzP * KLp, cols, kOzBN);
+    if (!ok) {
+        ozaki_free(oz);
+        *why = "tensor map encoding failed";
+        return BDC_OK;
+    }
+    BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smem));
+    BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_slice_b, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(double) * KLp * 33));
+    *out = oz;
+    return BDC_OK;
+}
+
+cudaError_t ozaki_enqueue(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaStream_t s) {
+    const OzakiInput& in = oz->in;
+    k_oz_maxabs<<<oz->nmax, 256, 0, s>>>(in.RB, (int64_t)in.KL * in.H2, in.LA, in.Kp, in.KL, in.KR, in.H1h, oz->mpart,
+                                         st);
+    k_oz_exponent<<<1, 32, 0, s>>>(oz->mpart, oz->nmax, oz->d_e, st);
+    {
+        const int64_t work = (int64_t)in.H1h * (oz->KRp / 16);
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 148 * 8));
+        k_oz_slice_a<<<blocks, 256, 0, s>>>(in.LA, in.Kp, in.KL, in.KR, in.H1h, oz->KRp, oz->Ad, oz->d_e, st);
+    }
+    k_oz_slice_b<<<(in.H2 + 31) / 32, 256, sizeof(double) * oz->KLp * 33, s>>>(in.RB, in.KL, in.H2, oz->KLp, oz->Bd,
+                                                                              oz->d_e, st);
+    if (oz->tiles == 0) return cudaGetLastError();
+    const OzGeomDev g{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_n};
+    k_oz_ba<<<oz->tiles, kOzThreads, oz->smem, s>>>(oz->tmAs, oz->tmBs, oz->tmAd, oz->tmBd, g, oz->d_tiles, oz->d_e,
+                                                    ep, st);
+    return cudaGetLastError();
+}
+
+}  // namespace bdc

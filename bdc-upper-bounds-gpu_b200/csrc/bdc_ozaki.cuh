@@ -1,0 +1,69 @@
+// bdc_ozaki.cuh -- the G product of the factored engine on the integer tensor
+// cores (tcgen05.mma kind::i8, accumulators in tensor memory), exact up to a
+// stated truncation of its FP64 operands.
+//
+// G = AL * ML + NR * BR^T, where AL and BR^T are half-table entries (exact
+// integers < 2^14) and ML, NR are FP64 (ln q contracted with a table).  With
+// one power-of-two exponent e for both FP64 operands (|X| < 2^e):
+//     X = 2^e * sum_{s<J} x_s 2^{-7(s+1)} + r,   x_s in [-127, 127],  |r| < 2^{e-7J}
+//     a = a_lo + 128 a_hi,                         a_lo in [0, 127]
+// and the products regroup by power of two into J + 1 integer sums
+//     acc_w = sum_k a_lo x_w + a_hi x_{w+1}   (L part, x from ML)
+//           + sum_k x_w b_lo + x_{w+1} b_hi   (R part, x from NR),  x_{-1} = x_J = 0
+//     G = sum_{w=-1}^{J-1} 2^{e - 7(w+1)} acc_w  (+ the truncation error)
+// Each acc_w is one int8 product with the contraction [lo | hi] against
+// [x_w | x_{w+1}], exact in int32 (|acc_w| < 2^23 for K <= 256).  The
+// truncation leaves |G - G_exact| < (max row sum of AL + max column sum of
+// BR^T) * 2^{e - 7J}, which is below 1e-13 nats of D(x) at n = 24.
+#pragma once
+
+#include <cuda.h>
+
+#include "bdc_engine.cuh"
+
+namespace bdc {
+
+constexpr int kOzJ = 7;          // int8 slices of each FP64 operand (49 bits)
+constexpr int kOzW = kOzJ + 1;   // accumulators (weights 2^{e - 7a}, a = 0..J)
+constexpr int kOzP = kOzJ + 2;   // slots per row of a sliced operand: zero, x_0..x_{J-1}, zero
+constexpr int kOzBM = 128;       // tile rows (x_hi): one TMEM lane each
+constexpr int kOzBN = 64;        // tile columns (dense x_lo): kOzW * kOzBN = 512 TMEM columns
+constexpr int kOzStages = 3;     // pipeline depth of the per-weight operands
+constexpr int kOzThreads = 128;  // 4 warps: TMA producer, MMA issuer, all four run the epilogue
+
+// what the product reads from the factored engine (bdc_factored.cu)
+struct OzakiInput {
+    const double* LA;               // [H1h][Kp] = [AL | NR]
+    const double* RB;               // [Kp][H2]  = [ML ; BR^T]
+    int Kp, KL, KR, H1h, H2;
+    const int* colmax;              // [H2] largest row of a representative per dense column, -1 if none
+};
+
+struct OzakiG {
+    OzakiInput in{};
+    int KLp = 0, KRp = 0;           // contraction lengths padded to 32
+    int aS = 0, bS = 0, aD = 0, bD = 0;  // 128-byte atom columns: static A / B, per-weight A / B
+    int smem = 0;                   // dynamic shared memory per CTA
+    uint8_t* As = nullptr;          // [H1h][2 KLp]  [a_lo | a_hi] of AL
+    uint8_t* Bs = nullptr;          // [H2][2 KRp]   [b_lo | b_hi] of BR^T
+    uint8_t* Ad = nullptr;          // [H1h][P KRp]  slots of NR
+    uint8_t* Bd = nullptr;          // [H2][P KLp]   slots of ML (transposed)
+    int* d_e = nullptr;             // the exponent e of this iteration's FP64 operands
+    double* mpart = nullptr;        // block maxima of |ML|, |NR|
+    int nmax = 0;
+    int* d_tiles = nullptr;         // tile ids (tm * tiles_n + tn) that hold representatives
+    int tiles = 0, tiles_n = 0;
+    CUtensorMap tmAs, tmBs, tmAd, tmBd;
+};
+
+// set-up: *out stays null (with the reason in *why) when the shapes or the
+// table entries are outside what the kernel covers; the caller then keeps
+// the FP64 product
+bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const char** why);
+void ozaki_free(OzakiG* oz);
+// one G product with the fused BA update, queued on s: the exponent, the
+// slices of ML and NR, then the tensor-core product and epilogue; block
+// partials as the FP64 product writes them (ep.part, one row of 8 per tile)
+cudaError_t ozaki_enqueue(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaStream_t s);
+
+}  // namespace bdc

@@ -195,6 +195,15 @@ bdc_status bdc_batch_destroy(bdc_batch_t batch);
 /* Queue the batch's work on a caller's cudaStream_t (NULL: the batch's own
  * stream); bdc_batch_iterate still returns only when that work is done. */
 bdc_status bdc_batch_set_stream(bdc_batch_t batch, void* stream);
+/* The accelerated loop of bdc_accelerate for every handle of the batch (all
+ * factored engine), 8 steps of each per replay of one captured graph, each
+ * instance stopping on its own bracket (best_upper_bound - best_rate <
+ * gap_bits) or after max_evals evaluations.  seconds (may be NULL) receives
+ * per instance the device time from the start of the call until its bracket
+ * fell below gap_bits (CUDA events on the launch stream, resolution one graph
+ * replay), -1 when it did not. */
+bdc_status bdc_batch_accelerate(bdc_batch_t batch, int64_t max_evals, double gap_bits, bdc_stats* stats,
+                                double* seconds);
 
 /* One reference-shaped iteration with host vectors: p_in -> p_out, like
  * baa_iteration (BAA.cu:590-639, decl. BAA.cuh:295); p_out may equal p_in. */

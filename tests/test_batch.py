@@ -76,3 +76,40 @@ def test_batch_argument_errors(bdc):
         with bdc.Batch([E]) as B:
             with pytest.raises(bdc.BDCError):
                 B.iterate(4, 1e-9)     # no distribution set
+
+
+def test_batch_accelerate_brackets_each_instance_and_times_it(bdc, O):
+    # the accelerated loop of every instance from one graph, each stopping on
+    # its own bracket; the bracket must hold in the oracle at the returned
+    # point and match the same instance accelerated alone
+    gap = 1e-9
+    mix = [(10, 5, ("dirichlet", 0.5, 0)), (12, 6, ("uniform",)), (13, 6, ("dirichlet", 0.5, 1)),
+           (14, 7, ("dirichlet", 1.0, 2))]
+    engines = [bdc.Engine(n, k, engine="factored") for n, k, _ in mix]
+    try:
+        for E, (n, k, spec) in zip(engines, mix):
+            E.set_p(_start(n, spec))
+        with bdc.Batch(engines) as B:
+            stats, secs = B.accelerate(200000, gap)
+        for E, st, sec, (n, k, spec) in zip(engines, stats, secs, mix):
+            assert st["converged"] == 1, (n, k, st)
+            assert 0 <= st["best_upper_bound"] - st["best_rate"] < gap
+            assert sec > 0
+            with bdc.Engine(n, k, engine="factored") as S:
+                S.set_p(_start(n, spec))
+                s1 = S.accelerate(200000, gap)
+            assert s1["converged"] == 1
+            # two certified brackets of the same C overlap
+            assert s1["best_rate"] <= st["best_upper_bound"] + 1e-12
+            assert st["best_rate"] <= s1["best_upper_bound"] + 1e-12
+            # the returned iterate is a distribution whose rate (oracle) is a
+            # lower bound within the bracket's reach
+            reps = O.canonicals(n)
+            p = E.get_p()
+            assert abs(np.sum(O.orbits_of(reps, n) * p) - 1.0) < 1e-12
+            lnq = O.log_q(n, k, p, reps)
+            rate_bits = O.rate(n, k, lnq, p, reps) / np.log(2.0)
+            assert rate_bits <= st["best_upper_bound"] + 1e-12
+    finally:
+        for E in engines:
+            E.close()
