@@ -77,6 +77,11 @@ constexpr int kAccBatchSteps = 8;
 
 static bdc_status batch_capture_acc(bdc_batch* B, double eta) {
     if (B->acc_exec && B->acc_eta == eta) return BDC_OK;
+    // every instance's snapshot vectors exist before its steps are captured
+    for (auto* H : B->hs) {
+        bdc_status rc = factored_acc_buffers(H);
+        if (rc != BDC_OK) return rc;
+    }
     if (B->acc_exec) {
         cudaGraphExecDestroy(B->acc_exec);
         B->acc_exec = nullptr;

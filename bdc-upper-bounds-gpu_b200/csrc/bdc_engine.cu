@@ -240,6 +240,8 @@ bdc_status engine_init(bdc_handle* H) {
 }
 
 void engine_free(bdc_handle* H) {
+    if (H->stream) cudaStreamSynchronize(H->stream);
+    solve_pool_release(H);
     if (H->fac) factored_free(H);
     if (H->stream) cudaStreamSynchronize(H->stream);
     cudaFree(H->d_reps);

@@ -53,6 +53,8 @@ struct bdc_handle {
     int64_t nonzero_pairs = 0;  // sum over reps of distinct length-k subsequences
     // factored engine
     FactoredState* fac = nullptr;
+    // scratch blocks of the certified solver, reused across its calls (bdc_solve.cu)
+    void* solve_pool = nullptr;
 };
 
 namespace bdc {
@@ -78,6 +80,9 @@ cudaError_t engine_enqueue_iteration(bdc_handle* H, double a);  // one iteration
 int count_group_size(int k);
 
 // factored engine (bdc_factored.cu)
+// frees the certified solver's scratch blocks (bdc_solve.cu)
+void solve_pool_release(bdc_handle* H);
+
 bool factored_supports(int n, int k);
 bdc_status factored_init(bdc_handle* H);
 void factored_free(bdc_handle* H);
@@ -93,6 +98,7 @@ bdc_status factored_accelerate(bdc_handle* H, int64_t max_evals, double gap_bits
 // the device stop at gap_bits) and `steps` steps queued on H->stream
 double factored_acc_eta();
 bdc_status factored_acc_start(bdc_handle* H, double gap_bits);
+bdc_status factored_acc_buffers(bdc_handle* H);  // the loop's snapshot vectors (before any capture)
 cudaError_t factored_enqueue_acc_steps(bdc_handle* H, int steps, double eta);
 cudaError_t factored_enqueue_iteration(bdc_handle* H, double a);
 // finishes an iteration that stopped on an exp-shift overflow (on H->stream);

@@ -2563,6 +2563,7 @@ __global__ void k_acc_stop(DevState* st) {
 
 static cudaError_t enqueue_acc_step(bdc_handle* H, double eta) {
     FactoredState* F = H->fac;
+    if (!F->snap0 || !F->snap1) return cudaErrorInvalidValue;  // factored_acc_buffers first
     cudaStream_t s = H->stream;
     const int nb = H->nb_upd;
     const int64_t R = H->R;
@@ -2638,6 +2639,9 @@ double factored_acc_eta() {
 static bdc_status ensure_cycle_graph(bdc_handle* H, double eta) {
     FactoredState* F = H->fac;
     if (F->cycle && F->cycle_eta == eta) return BDC_OK;
+    // the snapshot vectors must exist before the steps are captured
+    bdc_status rc = factored_acc_buffers(H);
+    if (rc != BDC_OK) return rc;
     if (F->cycle) {
         cudaGraphExecDestroy(F->cycle);
         F->cycle = nullptr;

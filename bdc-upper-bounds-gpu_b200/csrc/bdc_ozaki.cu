@@ -169,7 +169,11 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
 
     int issued_loads = 0;  // producer: per-weight loads issued (for the bounded drain on abort)
 
-    if (warp == 0 && lane == 0) {
+    // Lanes 1-31 of the producer and MMA warps wait at __syncwarp while lane 0
+    // works: spinning on an mbarrier on the warp's other path would stall the
+    // working lane's path every time a try_wait suspends.
+    if (warp == 0) {
+      if (lane == 0) {
         // ---- producer: the static operands once, the per-weight slices through the stages
         const uint32_t bs = sm_addr(&bar_static);
         mbar_expect_tx(bs, (uint32_t)(g.aS * kOzBM + g.bS * kOzBN) * 128);
@@ -190,7 +194,10 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
             for (int c = 0; c < g.bD; ++c) tma_load_2d(dB + c * kOzBN * 128, &tmBd, fb, a * g.KLp + 128 * c, n0);
             ++issued_loads;
         }
-    } else if (warp == 1 && lane == 0) {
+      }
+      __syncwarp();
+    } else if (warp == 1) {
+      if (lane == 0) {
         // ---- MMA issuer: accumulator a gets [lo | hi] x [x_{a-1} | x_a] over both parts
         const uint32_t idesc = umma_idesc_i8(kOzBM, kOzBN);
         bool ok = mbar_wait(sm_addr(&bar_static), 0);
@@ -220,6 +227,8 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
         }
         if (!ok) atomicExch(&abort_sh, 1);
         umma_commit(sm_addr(&bar_done));  // arrives when every MMA issued above has completed
+      }
+      __syncwarp();
     }
 
     // ---- everyone: wait for the accumulators

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <vector>
 
 #include "bdc_engine.cuh"
@@ -553,18 +554,60 @@ __global__ void __launch_bounds__(1024) k_newton_apply(int S, int nF, const int*
 }
 
 // ------------------------------------------------------------ host side
+// Scratch of the solver, kept per handle: a block released by a DevBuf goes
+// back to the handle's pool and the next request of the same size takes it,
+// so repeated solves neither allocate nor free (cudaMalloc / cudaFree of
+// hundreds of MB per solve stalled the host for up to seconds) and the
+// solver's vectors keep their addresses, which keeps the captured BA-map
+// graphs valid.  All of the solver's work is ordered on the handle's
+// stream, so a block handed out again is never still in use.
+struct SolvePool {
+    std::multimap<size_t, void*> free_blocks;
+    ~SolvePool() {
+        for (auto& kv : free_blocks) cudaFree(kv.second);
+    }
+};
+
+static thread_local SolvePool* t_pool = nullptr;  // the pool of the solve running on this thread
+
 struct DevBuf {
     void* p = nullptr;
-    ~DevBuf() { cudaFree(p); }
+    size_t bytes = 0;
+    SolvePool* pool = nullptr;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    void release() {
+        if (p && pool) pool->free_blocks.emplace(bytes, p);
+        else if (p) cudaFree(p);
+        p = nullptr;
+    }
+    ~DevBuf() { release(); }
     template <typename T>
     T* get() const { return (T*)p; }
 };
 
 static cudaError_t dalloc(DevBuf& b, size_t bytes) {
-    cudaFree(b.p);
-    b.p = nullptr;
-    return cudaMalloc(&b.p, bytes > 0 ? bytes : 16);
+    b.release();
+    bytes = bytes > 0 ? bytes : 16;
+    b.bytes = bytes;
+    b.pool = t_pool;
+    if (t_pool) {
+        auto it = t_pool->free_blocks.find(bytes);
+        if (it != t_pool->free_blocks.end()) {
+            b.p = it->second;
+            t_pool->free_blocks.erase(it);
+            return cudaSuccess;
+        }
+    }
+    return cudaMalloc(&b.p, bytes);
 }
+
+// sets the thread's pool for the duration of one solve
+struct PoolScope {
+    explicit PoolScope(SolvePool* p) { t_pool = p; }
+    ~PoolScope() { t_pool = nullptr; }
+};
 
 // Anderson mixing on vectors of length L with orbit weights w; the Gram
 // matrix of the stored differences lives on the host (m <= kAAMax numbers a
@@ -1292,6 +1335,9 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
     if (!(gap_bits > 0.0) || max_evals < 1) return fail(BDC_ERR_ARG, "bdc_solve: need gap_bits > 0 and max_evals >= 1");
     if (H->n > 26) return fail(BDC_ERR_UNSUPPORTED, "bdc_solve: counts of n > 26 do not fit FP32 exactly");
     BDC_CUDA_TRY(cudaSetDevice(H->device));
+    if (!H->solve_pool) H->solve_pool = new SolvePool();
+    // declared before every DevBuf of this call, so it outlives them
+    PoolScope pool_scope((SolvePool*)H->solve_pool);
     cudaStream_t s = H->stream;
     const int64_t R = H->R;
     const int sms = H->num_sms;
@@ -1494,3 +1540,10 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
     (void)certified;
     return BDC_OK;
 }
+
+namespace bdc {
+void solve_pool_release(bdc_handle* H) {
+    delete (SolvePool*)H->solve_pool;
+    H->solve_pool = nullptr;
+}
+}  // namespace bdc
