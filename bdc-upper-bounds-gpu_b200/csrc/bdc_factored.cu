@@ -2064,16 +2064,18 @@ bdc_status factored_init(bdc_handle* H) {
     // G on the int8 tensor cores (bdc_ozaki.cu) where BDC_G_KERNEL=ozaki asks for it
     {
         const char* gk = getenv("BDC_G_KERNEL");
-        if (gk && !strcmp(gk, "ozaki")) {
+        if (gk && (!strcmp(gk, "ozaki") || !strcmp(gk, "ozaki-p"))) {
             const OzakiInput in{F->LA, F->RB, Kp, KL, KR, H1, H2, F->colmax.data()};
             const char* why = nullptr;
-            bdc_status rc = ozaki_init(H, in, &F->oz, &why);
+            bdc_status rc = ozaki_init(H, in, !strcmp(gk, "ozaki-p"), &F->oz, &why);
             if (rc != BDC_OK) return rc;
             F->use_oz = F->oz != nullptr;
             if (H->verbose) {
                 if (F->use_oz)
-                    printf("bdc: G on the int8 tensor cores: %d tiles of %dx%d, %d B shared memory\n", F->oz->tiles,
-                           kOzBM, kOzBN, F->oz->smem);
+                    printf("bdc: G on the int8 tensor cores: %d tiles of %dx%d, %d B shared memory%s\n",
+                           F->oz->persistent ? F->oz->tilesP : F->oz->tiles, kOzBM, F->oz->persistent ? 32 : kOzBN,
+                           F->oz->persistent ? F->oz->smemP : F->oz->smem,
+                           F->oz->persistent ? ", persistent (one CTA per SM)" : "");
                 else
                     printf("bdc: G stays on the FP64 product: %s\n", why ? why : "?");
             }
@@ -2209,7 +2211,7 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             if (F->use_oz) return ozaki_enqueue(F->oz, make_epilogue(H), H->d_st, s);
             return launch_ba(F->g, make_epilogue(H), s, H->d_st);
         case ST_FIN:
-            k_fac_finalize<<<1, 256, 0, s>>>(F->epart, F->use_oz ? F->oz->tiles : F->ctas_g, a, F->eta, H->d_st);
+            k_fac_finalize<<<1, 256, 0, s>>>(F->epart, F->use_oz ? ozaki_partials(F->oz) : F->ctas_g, a, F->eta, H->d_st);
             break;
     }
     return cudaGetLastError();

@@ -346,6 +346,289 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
                      : "memory");
 }
 
+// ------------------------------------------- the persistent, overlapped form
+// One CTA per SM loops over 128 x 32 tiles.  Two TMEM buffers of eight
+// 32-column accumulators (2 x 256 = 512 columns): while warps 2-5 drain and
+// finish tile i from one buffer, warp 1 issues tile i + 1's MMAs into the
+// other.  The static operands of a tile are double-buffered, the per-weight
+// slices go through a ring of kOzStages stages that continues across tiles.
+// Barriers: sfull/sempty (static operands), full/empty (ring), tfull/tempty
+// (TMEM buffers; tempty takes one arrival per epilogue warp).
+constexpr int kOzPBN = 32;
+constexpr int kOzPThreads = 192;
+constexpr int kOzPBuf = kOzW * kOzPBN;  // TMEM columns of one buffer
+static_assert(2 * kOzPBuf <= 512, "two accumulator buffers exceed tensor memory");
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__global__ void __launch_bounds__(kOzPThreads, 1)
+k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtensorMap tmBs,
+          const __grid_constant__ CUtensorMap tmAd, const __grid_constant__ CUtensorMap tmBd, OzGeomDev g,
+          const int* __restrict__ tiles, int ntiles, const int* __restrict__ d_e, BaEpilogue ep, DevState* st) {
+    extern __shared__ __align__(1024) uint8_t ozp_smem_raw[];
+    __shared__ __align__(8) uint64_t sfull[2], sempty[2], full[kOzStages], empty[kOzStages], tfull[2], tempty[2],
+        bar_done;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int abort_sh, skip_sh;
+    if (threadIdx.x == 0) skip_sh = (st->done || st->error) ? 1 : 0;
+    __syncthreads();
+    if (skip_sh) return;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nmine = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    uint8_t* base = (uint8_t*)(((uintptr_t)ozp_smem_raw + 1023) & ~(uintptr_t)1023);
+    const uint32_t sA0 = sm_addr(base);
+    const uint32_t bytesA = (uint32_t)g.aS * kOzBM * 128, bytesB = (uint32_t)g.bS * kOzPBN * 128;
+    const uint32_t sB0 = sA0 + 2 * bytesA;
+    const uint32_t ring0 = sB0 + 2 * bytesB;
+    const uint32_t stageA = (uint32_t)g.aD * kOzBM * 128, stageB = (uint32_t)g.bD * kOzPBN * 128;
+    const uint32_t stageBytes = stageA + stageB;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(sm_addr(&sfull[i]), 1);
+            mbar_init(sm_addr(&sempty[i]), 1);
+            mbar_init(sm_addr(&tfull[i]), 1);
+            mbar_init(sm_addr(&tempty[i]), 4);
+        }
+        for (int i = 0; i < kOzStages; ++i) {
+            mbar_init(sm_addr(&full[i]), 1);
+            mbar_init(sm_addr(&empty[i]), 1);
+        }
+        mbar_init(sm_addr(&bar_done), 1);
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sm_addr(&tmem_base_sh)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_sh;
+    auto aborted = [&]() { return *(volatile int*)&abort_sh != 0; };
+    auto give_up = [&]() { atomicExch(&abort_sh, 1); };
+
+    double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0, zero = 0.0;
+    // producer bookkeeping for the bounded drain on an abort
+    int last_use[kOzStages], last_static[2];
+    for (int i = 0; i < kOzStages; ++i) last_use[i] = -1;
+    last_static[0] = last_static[1] = -1;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int wc = 0;
+            for (int it = 0; it < nmine && !aborted(); ++it) {
+                const int t = tiles[blockIdx.x + it * gridDim.x];
+                const int m0 = (t / g.tiles_n) * kOzBM, n0 = (t % g.tiles_n) * kOzPBN;
+                const int sb = it & 1;
+                if (it >= 2 && !mbar_wait(sm_addr(&sempty[sb]), ((it >> 1) - 1) & 1)) {
+                    give_up();
+                    break;
+                }
+                const uint32_t sfb = sm_addr(&sfull[sb]);
+                mbar_expect_tx(sfb, bytesA + bytesB);
+                for (int c = 0; c < g.aS; ++c) tma_load_2d(sA0 + sb * bytesA + c * kOzBM * 128, &tmAs, sfb, 128 * c, m0);
+                for (int c = 0; c < g.bS; ++c)
+                    tma_load_2d(sB0 + sb * bytesB + c * kOzPBN * 128, &tmBs, sfb, 128 * c, n0);
+                last_static[sb] = it >> 1;
+                bool ok = true;
+                for (int a = 0; a < kOzW; ++a, ++wc) {
+                    const int s = wc % kOzStages, use = wc / kOzStages;
+                    if (use > 0 && !mbar_wait(sm_addr(&empty[s]), (use - 1) & 1)) {
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t fb = sm_addr(&full[s]);
+                    const uint32_t dA = ring0 + s * stageBytes, dB = dA + stageA;
+                    mbar_expect_tx(fb, stageBytes);
+                    for (int c = 0; c < g.aD; ++c) tma_load_2d(dA + c * kOzBM * 128, &tmAd, fb, a * g.KRp + 128 * c, m0);
+                    for (int c = 0; c < g.bD; ++c)
+                        tma_load_2d(dB + c * kOzPBN * 128, &tmBd, fb, a * g.KLp + 128 * c, n0);
+                    last_use[s] = use;
+                }
+                if (!ok) {
+                    give_up();
+                    break;
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = umma_idesc_i8(kOzBM, kOzPBN);
+            int wc = 0;
+            for (int it = 0; it < nmine && !aborted(); ++it) {
+                const int tb = it & 1, sb = it & 1;
+                if (it >= 2 && !mbar_wait(sm_addr(&tempty[tb]), ((it >> 1) - 1) & 1)) {
+                    give_up();
+                    break;
+                }
+                if (!mbar_wait(sm_addr(&sfull[sb]), (it >> 1) & 1)) {
+                    give_up();
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t sA = sA0 + sb * bytesA, sB = sB0 + sb * bytesB;
+                bool ok = true;
+                for (int a = 0; a < kOzW; ++a, ++wc) {
+                    const int s = wc % kOzStages, use = wc / kOzStages;
+                    if (!mbar_wait(sm_addr(&full[s]), use & 1) || aborted()) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t dA = ring0 + s * stageBytes, dB = dA + stageA;
+                    const uint32_t tacc = tmem + (uint32_t)(tb * kOzPBuf + a * kOzPBN);
+                    uint32_t accum = 0;
+                    for (int kb = 0; kb < 2 * g.KLp; kb += 32) {
+                        const uint32_t off = (uint32_t)(kb >> 7), in = (uint32_t)(kb & 127);
+                        umma_i8(tacc, umma_desc_sw128(sA + off * kOzBM * 128 + in),
+                                umma_desc_sw128(dB + off * kOzPBN * 128 + in), idesc, accum);
+                        accum = 1;
+                    }
+                    for (int kb = 0; kb < 2 * g.KRp; kb += 32) {
+                        const uint32_t off = (uint32_t)(kb >> 7), in = (uint32_t)(kb & 127);
+                        umma_i8(tacc, umma_desc_sw128(dA + off * kOzBM * 128 + in),
+                                umma_desc_sw128(sB + off * kOzPBN * 128 + in), idesc, accum);
+                        accum = 1;
+                    }
+                    umma_commit(sm_addr(&empty[s]));
+                }
+                if (!ok) {
+                    give_up();
+                    break;
+                }
+                umma_commit(sm_addr(&sempty[sb]));
+                umma_commit(sm_addr(&tfull[tb]));
+            }
+            umma_commit(sm_addr(&bar_done));  // every MMA issued above has completed
+        }
+        __syncwarp();
+    } else {
+        // ---- epilogue warps: TMEM lanes 32 (warp % 4) .. + 31 = tile rows
+        const int q = warp & 3;
+        const int r = q * 32 + lane;
+        const double shift = st->shift;
+        const double lnz = st->log_z;
+        const double inv_z = exp(-lnz);
+        const int e = *d_e;
+        for (int it = 0; it < nmine; ++it) {
+            const int tb = it & 1;
+            if (!mbar_wait(sm_addr(&tfull[tb]), (it >> 1) & 1) || aborted()) {
+                give_up();
+                break;
+            }
+            tc_fence_after();
+            const int t = tiles[blockIdx.x + it * gridDim.x];
+            const int m = (t / g.tiles_n) * kOzBM + r, n0 = (t % g.tiles_n) * kOzPBN;
+            const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tb * kOzPBuf);
+            double gsum[kOzPBN];
+#pragma unroll
+            for (int j = 0; j < kOzPBN; ++j) gsum[j] = 0.0;
+#pragma unroll 1
+            for (int a = kOzW - 1; a >= 0; --a) {
+                const double w = ldexp(1.0, e - 7 * a);
+#pragma unroll
+                for (int c0 = 0; c0 < kOzPBN; c0 += 16) {
+                    uint32_t v[16];
+                    tmem_ld16(trow + (uint32_t)(a * kOzPBN + c0), v);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) gsum[c0 + j] = fma((double)(int32_t)v[j], w, gsum[c0 + j]);
+                }
+            }
+            // the buffer is free for the tile after next
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(sm_addr(&tempty[tb]));
+            if (m >= g.M) continue;
+#pragma unroll
+            for (int j = 0; j < kOzPBN; ++j) {
+                const int n = n0 + j;
+                if (n >= g.N) continue;
+                const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
+                const uint32_t x = (xd & ~low_mask(ep.n2)) | reverse_bits(xd & low_mask(ep.n2), ep.n2);
+                if (!is_rep(x, ep.n)) continue;
+                const double o = (double)orbit_size(x, ep.n);
+                const double D = __ldg(ep.hx + xd) - gsum[j] * ep.inv_c;
+                if (ep.Dout) ep.Dout[xd] = D;
+                // exact zeros of the caller's distribution (Lt = NaN) take ln p = 0
+                // (backend/BAA.cu:573-580)
+                const double pw = ep.Pw[xd];
+                const double lt = ep.Lt[xd];
+                const bool zero_in = (lt != lt);
+                const double lnp = zero_in ? 0.0 : lt - lnz;
+                const double lw = lnp + ep.eta * D - shift;
+                const double ex = exp(lw);
+                ep.Lt[xd] = lw;
+                ep.Pw[xd] = o * ex;
+                mD = fmax(mD, D);
+                mL = fmax(mL, lw);
+                sE = fma(o, ex, sE);
+                sR = fma(pw * inv_z, D, sR);
+                if (zero_in) zero = 1.0;
+            }
+        }
+    }
+
+    // ---- teardown: every MMA done, then the partials, the loads, the TMEM
+    const bool mma_done = mbar_wait(sm_addr(&bar_done), 0);
+    tc_fence_after();
+    if (!mma_done) give_up();
+    __syncthreads();
+    const bool ran = !aborted();
+    if (!ran && threadIdx.x == 0) st->error = kErrOzakiWait;
+    __shared__ double red[5][kOzPThreads / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        mD = fmax(mD, __shfl_xor_sync(0xFFFFFFFFu, mD, off));
+        mL = fmax(mL, __shfl_xor_sync(0xFFFFFFFFu, mL, off));
+        sE += __shfl_xor_sync(0xFFFFFFFFu, sE, off);
+        sR += __shfl_xor_sync(0xFFFFFFFFu, sR, off);
+        zero = fmax(zero, __shfl_xor_sync(0xFFFFFFFFu, zero, off));
+    }
+    if (lane == 0) {
+        red[0][warp] = mD;
+        red[1][warp] = sE;
+        red[2][warp] = mL;
+        red[3][warp] = sR;
+        red[4][warp] = zero;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = red[0][0], a1 = red[1][0], a2 = red[2][0], a3 = red[3][0], a4 = red[4][0];
+        for (int w = 1; w < kOzPThreads / 32; ++w) {
+            a0 = fmax(a0, red[0][w]);
+            a1 += red[1][w];
+            a2 = fmax(a2, red[2][w]);
+            a3 += red[3][w];
+            a4 = fmax(a4, red[4][w]);
+        }
+        double* p = ep.part + (size_t)blockIdx.x * 8;
+        p[0] = a0;
+        p[1] = a1;
+        p[2] = a2;
+        p[3] = a3;
+        p[4] = a4;
+    }
+    if (!ran && warp == 0 && lane == 0) {
+        for (int s = 0; s < kOzStages; ++s)
+            if (last_use[s] >= 0) (void)mbar_wait(sm_addr(&full[s]), last_use[s] & 1);
+        for (int b = 0; b < 2; ++b)
+            if (last_static[b] >= 0) (void)mbar_wait(sm_addr(&sfull[b]), last_static[b] & 1);
+    }
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+}
+
 // ------------------------------------------------------ operand preparation
 // block maxima of |ML| (RB rows [0, KL)) and |NR| (LA columns [KL, KL + KR))
 __global__ void __launch_bounds__(256) k_oz_maxabs(const double* __restrict__ RB, int64_t nml,
@@ -518,10 +801,27 @@ void ozaki_free(OzakiG* oz) {
     cudaFree(oz->d_e);
     cudaFree(oz->mpart);
     cudaFree(oz->d_tiles);
+    cudaFree(oz->d_tilesP);
     delete oz;
 }
 
-bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const char** why) {
+int ozaki_partials(const OzakiG* oz) { return oz->persistent ? oz->gridP : oz->tiles; }
+
+// tile ids (tm * tiles_n + tn) of BM x bn tiles that hold a representative
+static std::vector<int> rep_tiles(const OzakiInput& in, int bn, int* tiles_n) {
+    const int tiles_m = (in.H1h + kOzBM - 1) / kOzBM;
+    *tiles_n = (in.H2 + bn - 1) / bn;
+    std::vector<int> ids;
+    for (int tm = 0; tm < tiles_m; ++tm)
+        for (int tn = 0; tn < *tiles_n; ++tn) {
+            int mx = -1;
+            for (int c = tn * bn; c < std::min(in.H2, (tn + 1) * bn); ++c) mx = std::max(mx, in.colmax[c]);
+            if (mx >= tm * kOzBM) ids.push_back(tm * *tiles_n + tn);
+        }
+    return ids;
+}
+
+bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, OzakiG** out, const char** why) {
     *out = nullptr;
     *why = nullptr;
     auto round32 = [](int v) { return (v + 31) / 32 * 32; };
@@ -547,9 +847,12 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const c
     oz->aD = (2 * KRp + 127) / 128;
     oz->bD = (2 * KLp + 127) / 128;
     oz->smem = 1024 + (oz->aS * kOzBM + oz->bS * kOzBN) * 128 + kOzStages * (oz->aD * kOzBM + oz->bD * kOzBN) * 128;
+    oz->smemP = 1024 + 2 * (oz->aS * kOzBM + oz->bS * kOzPBN) * 128 +
+                kOzStages * (oz->aD * kOzBM + oz->bD * kOzPBN) * 128;
+    oz->persistent = persistent;
     int dev_smem = 0;
     BDC_CUDA_TRY(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, H->device));
-    if (oz->smem + 2048 > dev_smem) {
+    if ((persistent ? oz->smemP : oz->smem) + 2048 > dev_smem) {
         ozaki_free(oz);
         *why = "tile operands exceed shared memory";
         return BDC_OK;
@@ -587,31 +890,36 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const c
             return BDC_OK;
         }
     }
-    // tiles that hold a representative
-    const int tiles_m = (rows + kOzBM - 1) / kOzBM, tiles_n = (cols + kOzBN - 1) / kOzBN;
-    std::vector<int> ids;
-    for (int tm = 0; tm < tiles_m; ++tm)
-        for (int tn = 0; tn < tiles_n; ++tn) {
-            int mx = -1;
-            for (int c = tn * kOzBN; c < std::min(cols, (tn + 1) * kOzBN); ++c) mx = std::max(mx, in.colmax[c]);
-            if (mx >= tm * kOzBM) ids.push_back(tm * tiles_n + tn);
+    // tiles that hold a representative, for both tile widths
+    {
+        std::vector<int> ids = rep_tiles(in, kOzBN, &oz->tiles_n);
+        oz->tiles = (int)ids.size();
+        if (oz->tiles > 0) {
+            BDC_CUDA_TRY(cudaMalloc(&oz->d_tiles, sizeof(int) * ids.size()));
+            BDC_CUDA_TRY(cudaMemcpy(oz->d_tiles, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
         }
-    oz->tiles = (int)ids.size();
-    oz->tiles_n = tiles_n;
-    if (oz->tiles > 0) {
-        BDC_CUDA_TRY(cudaMalloc(&oz->d_tiles, sizeof(int) * ids.size()));
-        BDC_CUDA_TRY(cudaMemcpy(oz->d_tiles, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
+        std::vector<int> idsP = rep_tiles(in, kOzPBN, &oz->tiles_nP);
+        oz->tilesP = (int)idsP.size();
+        oz->gridP = std::min(oz->tilesP, H->num_sms);
+        if (oz->tilesP > 0) {
+            BDC_CUDA_TRY(cudaMalloc(&oz->d_tilesP, sizeof(int) * idsP.size()));
+            BDC_CUDA_TRY(cudaMemcpy(oz->d_tilesP, idsP.data(), sizeof(int) * idsP.size(), cudaMemcpyHostToDevice));
+        }
     }
     const bool ok = make_map(&oz->tmAs, oz->As, 2 * KLp, rows, kOzBM) &&
                     make_map(&oz->tmBs, oz->Bs, 2 * KRp, cols, kOzBN) &&
                     make_map(&oz->tmAd, oz->Ad, (uint64_t)kOzP * KRp, rows, kOzBM) &&
-                    make_map(&oz->tmBd, oz->Bd, (uint64_t)kOzP * KLp, cols, kOzBN);
+                    make_map(&oz->tmBd, oz->Bd, (uint64_t)kOzP * KLp, cols, kOzBN) &&
+                    make_map(&oz->tmBsP, oz->Bs, 2 * KRp, cols, kOzPBN) &&
+                    make_map(&oz->tmBdP, oz->Bd, (uint64_t)kOzP * KLp, cols, kOzPBN);
     if (!ok) {
         ozaki_free(oz);
         *why = "tensor map encoding failed";
         return BDC_OK;
     }
     BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smem));
+    if (oz->smemP + 2048 <= dev_smem)
+        BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba_p, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smemP));
     BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_slice_b, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(double) * KLp * 33));
     *out = oz;
@@ -630,6 +938,13 @@ cudaError_t ozaki_enqueue(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaSt
     }
     k_oz_slice_b<<<(in.H2 + 31) / 32, 256, sizeof(double) * oz->KLp * 33, s>>>(in.RB, in.KL, in.H2, oz->KLp, oz->Bd,
                                                                               oz->d_e, st);
+    if (oz->persistent) {
+        if (oz->tilesP == 0) return cudaGetLastError();
+        const OzGeomDev gp{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_nP};
+        k_oz_ba_p<<<oz->gridP, kOzPThreads, oz->smemP, s>>>(oz->tmAs, oz->tmBsP, oz->tmAd, oz->tmBdP, gp,
+                                                           oz->d_tilesP, oz->tilesP, oz->d_e, ep, st);
+        return cudaGetLastError();
+    }
     if (oz->tiles == 0) return cudaGetLastError();
     const OzGeomDev g{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_n};
     k_oz_ba<<<oz->tiles, kOzThreads, oz->smem, s>>>(oz->tmAs, oz->tmBs, oz->tmAd, oz->tmBd, g, oz->d_tiles, oz->d_e,

@@ -54,12 +54,20 @@ struct OzakiG {
     int* d_tiles = nullptr;         // tile ids (tm * tiles_n + tn) that hold representatives
     int tiles = 0, tiles_n = 0;
     CUtensorMap tmAs, tmBs, tmAd, tmBd;
+    // the persistent form: 128 x 32 tiles, one CTA per SM, two TMEM buffers
+    bool persistent = false;
+    int smemP = 0, gridP = 0;
+    int* d_tilesP = nullptr;
+    int tilesP = 0, tiles_nP = 0;
+    CUtensorMap tmBsP, tmBdP;
 };
 
 // set-up: *out stays null (with the reason in *why) when the shapes or the
 // table entries are outside what the kernel covers; the caller then keeps
 // the FP64 product
-bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const char** why);
+bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, OzakiG** out, const char** why);
+// rows of block partials the product writes (the finalize's count)
+int ozaki_partials(const OzakiG* oz);
 void ozaki_free(OzakiG* oz);
 // one G product with the fused BA update, queued on s: the exponent, the
 // slices of ML and NR, then the tensor-core product and epilogue; block
