@@ -42,6 +42,7 @@ EXPORTED_SYMBOLS = [
     "bdc_write_dist_file", "bdc_work", "bdc_profile", "bdc_set_stream", "bdc_peak_probe",
     "bdc_max_deviation_noalloc", "bdc_accelerate", "bdc_mi_forward", "bdc_mi_backward", "bdc_mi_backward_device",
     "bdc_batch_create", "bdc_batch_iterate", "bdc_batch_destroy", "bdc_batch_set_stream", "bdc_batch_accelerate",
+    "bdc_create_sharded", "bdc_fshard_range", "bdc_fshard_q", "bdc_fshard_d", "bdc_fshard_finish", "bdc_fshard_get_p",
     "bdc_solve",
     "bdc_bound_error", "bdc_shard_q", "bdc_shard_set_q", "bdc_shard_update_begin", "bdc_shard_update_end",
 ]
@@ -120,6 +121,14 @@ def library() -> ctypes.CDLL:
     L.bdc_mi_forward.argtypes = [h, _f64p, ctypes.c_int64, _f64p]
     L.bdc_mi_backward.argtypes = [h, _f64p, ctypes.c_int64]
     L.bdc_mi_backward_device.argtypes = [h, ctypes.c_void_p, ctypes.c_int64]
+    L.bdc_create_sharded.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(Options), ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(h)]
+    L.bdc_fshard_range.argtypes = [h, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                   ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    L.bdc_fshard_q.argtypes = [h, _f64p, ctypes.c_int64]
+    L.bdc_fshard_d.argtypes = [h, _f64p, ctypes.c_int64, _f64p]
+    L.bdc_fshard_finish.argtypes = [h, _f64p, ctypes.c_double, ctypes.POINTER(Stats)]
+    L.bdc_fshard_get_p.argtypes = [h, _f64p, ctypes.c_int64]
     L.bdc_bound_error.argtypes = [h, _f64p, _f64p]
     L.bdc_shard_q.argtypes = [h, ctypes.c_int64, ctypes.c_int64, _f64p, ctypes.c_int64]
     L.bdc_shard_set_q.argtypes = [h, _f64p, ctypes.c_int64]
@@ -189,7 +198,7 @@ class Engine:
     """
 
     def __init__(self, n: int, k: int, engine: str = "auto", device: int = 0,
-                 cache_dir: str | None = None, verbose: bool = False):
+                 cache_dir: str | None = None, verbose: bool = False, shard: tuple[int, int] | None = None):
         L = library()
         o = Options()
         L.bdc_default_options(ctypes.byref(o))
@@ -199,7 +208,13 @@ class Engine:
         o.cache_dir = self._cache_dir
         o.verbose = 1 if verbose else 0
         hdl = ctypes.c_void_p()
-        _check(L.bdc_create(n, k, ctypes.byref(o), ctypes.byref(hdl)), "bdc_create")
+        if shard is None:
+            _check(L.bdc_create(n, k, ctypes.byref(o), ctypes.byref(hdl)), "bdc_create")
+        else:
+            # the factored engine holding rank shard[0]'s window of the rows out of shard[1]
+            _check(L.bdc_create_sharded(n, k, ctypes.byref(o), int(shard[0]), int(shard[1]), ctypes.byref(hdl)),
+                   "bdc_create_sharded")
+        self.shard = shard
         self._h = hdl
         self.n, self.k = n, k
         self.device = int(device)
@@ -263,6 +278,37 @@ class Engine:
         return st.as_dict()
 
     # ------------------------------------------------ one rank of sharded BA
+    # ------------------------------------------- rows sharded (factored engine)
+    def fshard_range(self) -> tuple[int, int, int, int]:
+        """(first row, rows, first representative, end representative) held."""
+        r0, rows, i0, i1 = ctypes.c_int(), ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64()
+        _check(library().bdc_fshard_range(self._h, ctypes.byref(r0), ctypes.byref(rows), ctypes.byref(i0),
+                                          ctypes.byref(i1)), "bdc_fshard_range")
+        return r0.value, rows.value, int(i0.value), int(i1.value)
+
+    def fshard_q(self) -> np.ndarray:
+        out = np.empty(1 << self.k, dtype=np.float64)
+        _check(library().bdc_fshard_q(self._h, out.ctypes.data_as(_f64p), len(out)), "bdc_fshard_q")
+        return out
+
+    def fshard_d(self, acc) -> np.ndarray:
+        acc, pa = _f64(acc)
+        out = np.empty(5, dtype=np.float64)
+        _check(library().bdc_fshard_d(self._h, pa, len(acc), out.ctypes.data_as(_f64p)), "bdc_fshard_d")
+        return out
+
+    def fshard_finish(self, part5, a: float = float("-inf")) -> dict:
+        part5, pp = _f64(part5)
+        st = Stats()
+        _check(library().bdc_fshard_finish(self._h, pp, float(a), ctypes.byref(st)), "bdc_fshard_finish")
+        return st.as_dict()
+
+    def fshard_get_p(self) -> np.ndarray:
+        _, _, i0, i1 = self.fshard_range()
+        out = np.empty(i1 - i0, dtype=np.float64)
+        _check(library().bdc_fshard_get_p(self._h, out.ctypes.data_as(_f64p), len(out)), "bdc_fshard_get_p")
+        return out
+
     def shard_q(self, r0: int, r1: int) -> np.ndarray:
         """Partial q sums of representatives [r0, r1): acc[y] over all 2^k y."""
         acc = np.empty(1 << self.k, dtype=np.float64)

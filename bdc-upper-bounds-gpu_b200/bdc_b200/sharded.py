@@ -105,6 +105,51 @@ def iterate(E, max_iters: int, a: float = float("-inf"), group=None) -> dict:
     return out
 
 
+def combine_part5(parts) -> np.ndarray:
+    """The update statistics of row shards combined: [max D, sum |O| e,
+    max logW, sum |O| p D, input-zero flag] -> max, sum, max, sum, max."""
+    P = np.asarray(parts, dtype=np.float64).reshape(-1, 5)
+    return np.array([P[:, 0].max(), P[:, 1].sum(), P[:, 2].max(), P[:, 3].sum(), P[:, 4].max()])
+
+
+def iterate_rows(E, max_iters: int, a: float = float("-inf"), group=None) -> dict:
+    """BA iterations of a factored-engine handle created with shard=(rank,
+    world) (each rank holds a window of whole rows of the dense iterate),
+    until mx < a or max_iters.  Per iteration: one sum all-reduce of the 2^k
+    partial q sums, then one max all-reduce of [max D, max logW, zero flag]
+    and one sum all-reduce of [sum |O| e, sum |O| p D] (the shift that scales
+    e is the same on every rank).  Every rank returns the same statistics
+    (bits)."""
+    comm = _Comm(group, E.device)
+    out = {"iters": 0, "world": comm.world, "rows": E.fshard_range()}
+    for _ in range(int(max_iters)):
+        acc = comm.reduce(E.fshard_q(), "sum")
+        part = E.fshard_d(acc)
+        mx3 = comm.reduce([part[0], part[2], part[4]], "max")
+        sm2 = comm.reduce([part[1], part[3]], "sum")
+        st = E.fshard_finish([mx3[0], sm2[0], mx3[1], sm2[1], mx3[2]], a)
+        out["iters"] += 1
+        out.update({key: st[key] for key in ("mx", "upper_bound", "rate", "best_upper_bound", "best_rate")})
+        out["converged"] = bool(st["converged"])
+        if out["converged"]:
+            break
+    return out
+
+
+def gather_p_rows(E, group=None) -> np.ndarray | None:
+    """The iterate of a row-sharded handle assembled on rank 0 (None elsewhere)."""
+    comm = _Comm(group, E.device)
+    _, _, i0, i1 = E.fshard_range()
+    parts = [None] * comm.world
+    comm.dist.all_gather_object(parts, (i0, E.fshard_get_p()), group=group)
+    if comm.rank != 0:
+        return None
+    p = np.empty(E.R, dtype=np.float64)
+    for lo, v in parts:
+        p[lo:lo + len(v)] = v
+    return p
+
+
 def gather_p(E, group=None) -> np.ndarray | None:
     """The sharded iterate, assembled on rank 0 (None elsewhere)."""
     comm = _Comm(group, E.device)

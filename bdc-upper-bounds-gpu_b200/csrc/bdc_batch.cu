@@ -124,6 +124,10 @@ bdc_status bdc_batch_create(bdc_handle_t* handles, int count, bdc_batch_t* out) 
             batch_free(B);
             return fail(BDC_ERR_ARG, "bdc_batch_create: handle %d is NULL", i);
         }
+        if (handles[i]->shard_world > 1) {
+            batch_free(B);
+            return fail(BDC_ERR_STATE, "bdc_batch_create: handle %d holds a shard of the rows", i);
+        }
         if (handles[i]->device != B->device) {
             batch_free(B);
             return fail(BDC_ERR_ARG, "bdc_batch_create: handles on different devices");

@@ -52,7 +52,33 @@ void bdc_default_options(bdc_options* o) {
 
 const char* bdc_version(void) { return "bdc-b200 0.1.0 (sm_100a)"; }
 
+static bdc_status create_handle(int n, int k, const bdc_options* opts, int rank, int world, bdc_handle_t* out);
+
+// a handle that holds only a window of the rows (bdc_create_sharded) runs
+// the sharded iteration only
+static bdc_status refuse_sharded(bdc_handle_t H, const char* what) {
+    if (H && H->shard_world > 1)
+        return fail(BDC_ERR_STATE, "%s: this handle holds a shard of the rows; use the bdc_fshard_* calls", what);
+    return BDC_OK;
+}
+
 bdc_status bdc_create(int n, int k, const bdc_options* opts, bdc_handle_t* out) {
+    return create_handle(n, k, opts, 0, 1, out);
+}
+
+bdc_status bdc_create_sharded(int n, int k, const bdc_options* opts, int rank, int world, bdc_handle_t* out) {
+    if (world < 1 || rank < 0 || rank >= world)
+        return fail(BDC_ERR_ARG, "bdc_create_sharded: rank %d of %d", rank, world);
+    bdc_options o;
+    bdc_default_options(&o);
+    if (opts) o = *opts;
+    if (o.engine != BDC_ENGINE_AUTO && o.engine != BDC_ENGINE_FACTORED)
+        return fail(BDC_ERR_UNSUPPORTED, "bdc_create_sharded: rows are sharded on the factored engine only");
+    o.engine = BDC_ENGINE_FACTORED;
+    return create_handle(n, k, &o, rank, world, out);
+}
+
+static bdc_status create_handle(int n, int k, const bdc_options* opts, int rank, int world, bdc_handle_t* out) {
     if (!out) return fail(BDC_ERR_ARG, "bdc_create: out is NULL");
     *out = nullptr;
     bdc_options o;
@@ -72,6 +98,8 @@ bdc_status bdc_create(int n, int k, const bdc_options* opts, bdc_handle_t* out) 
     H->k = k;
     H->s = s;
     H->device = o.device;
+    H->shard_rank = rank;
+    H->shard_world = world;
     H->verbose = o.verbose;
     H->cache_dir = o.cache_dir ? std::string(o.cache_dir) : std::string();
     H->C = (double)binom(n, k);
@@ -151,6 +179,7 @@ bdc_status bdc_set_p_uniform(bdc_handle_t H) {
 
 bdc_status bdc_get_p(bdc_handle_t H, double* p, int64_t R) {
     if (!H || !p) return fail(BDC_ERR_ARG, "bdc_get_p: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_get_p")) return rs;
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_get_p: size mismatch");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_get_p: no distribution set");
     BDC_CUDA_TRY(cudaSetDevice(H->device));
@@ -164,6 +193,7 @@ bdc_status bdc_get_p(bdc_handle_t H, double* p, int64_t R) {
 
 bdc_status bdc_get_p_device(bdc_handle_t H, double* p, int64_t R) {
     if (!H || !p) return fail(BDC_ERR_ARG, "bdc_get_p_device: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_get_p_device")) return rs;
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_get_p_device: size mismatch");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_get_p_device: no distribution set");
     BDC_CUDA_TRY(cudaSetDevice(H->device));
@@ -177,6 +207,7 @@ bdc_status bdc_get_p_device(bdc_handle_t H, double* p, int64_t R) {
 
 bdc_status bdc_iterate(bdc_handle_t H, int64_t max_iters, double a, bdc_stats* stats) {
     if (!H) return fail(BDC_ERR_ARG, "bdc_iterate: NULL handle");
+    if (bdc_status rs = refuse_sharded(H, "bdc_iterate")) return rs;
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_iterate: no distribution set");
     if (max_iters < 0) return fail(BDC_ERR_ARG, "bdc_iterate: max_iters < 0");
     BDC_CUDA_TRY(cudaSetDevice(H->device));
@@ -185,6 +216,7 @@ bdc_status bdc_iterate(bdc_handle_t H, int64_t max_iters, double a, bdc_stats* s
 
 bdc_status bdc_bound_error(bdc_handle_t H, double* ub_err, double* rate_err) {
     if (!H || !ub_err || !rate_err) return fail(BDC_ERR_ARG, "bdc_bound_error: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_bound_error")) return rs;
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_bound_error: no distribution set");
     BDC_CUDA_TRY(cudaSetDevice(H->device));
     return engine_bound_error(H, ub_err, rate_err);
@@ -192,6 +224,7 @@ bdc_status bdc_bound_error(bdc_handle_t H, double* ub_err, double* rate_err) {
 
 bdc_status bdc_accelerate(bdc_handle_t H, int64_t max_evals, double gap_bits, bdc_stats* stats) {
     if (!H) return fail(BDC_ERR_ARG, "bdc_accelerate: NULL handle");
+    if (bdc_status rs = refuse_sharded(H, "bdc_accelerate")) return rs;
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_accelerate: no distribution set");
     if (H->engine != BDC_ENGINE_FACTORED)
         return fail(BDC_ERR_UNSUPPORTED, "bdc_accelerate: needs the factored engine (k < n)");
@@ -217,6 +250,7 @@ static bdc_status factored_eval(bdc_handle_t H, bool with_d) {
 
 bdc_status bdc_mi_forward(bdc_handle_t H, const double* p, int64_t R, double* I_nats) {
     if (!H || !I_nats) return fail(BDC_ERR_ARG, "bdc_mi_forward: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_mi_forward")) return rs;
     if (p) {
         bdc_status rc = bdc_set_p(H, p, R);
         if (rc != BDC_OK) return rc;
@@ -234,6 +268,7 @@ bdc_status bdc_mi_forward(bdc_handle_t H, const double* p, int64_t R, double* I_
 
 bdc_status bdc_mi_backward(bdc_handle_t H, double* grad, int64_t R) {
     if (!H || !grad) return fail(BDC_ERR_ARG, "bdc_mi_backward: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_mi_backward")) return rs;
     if (R != H->R) return fail(BDC_ERR_ARG, "bdc_mi_backward: %lld slots for %lld representatives", (long long)R, (long long)H->R);
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_mi_backward: no distribution set");
     BDC_CUDA_TRY(cudaSetDevice(H->device));
@@ -253,6 +288,7 @@ bdc_status bdc_mi_backward(bdc_handle_t H, double* grad, int64_t R) {
 
 bdc_status bdc_mi_backward_device(bdc_handle_t H, double* grad_dev, int64_t R) {
     if (!H || !grad_dev) return fail(BDC_ERR_ARG, "bdc_mi_backward_device: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_mi_backward_device")) return rs;
     if (R != H->R)
         return fail(BDC_ERR_ARG, "bdc_mi_backward_device: %lld slots for %lld representatives", (long long)R,
                     (long long)H->R);
@@ -273,6 +309,7 @@ bdc_status bdc_mi_backward_device(bdc_handle_t H, double* grad_dev, int64_t R) {
 
 bdc_status bdc_baa_iteration(bdc_handle_t H, const double* p_in, double* p_out, int64_t R) {
     if (!H || !p_in || !p_out) return fail(BDC_ERR_ARG, "bdc_baa_iteration: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_baa_iteration")) return rs;
     bdc_status rc = bdc_set_p(H, p_in, R);
     if (rc != BDC_OK) return rc;
     rc = engine_iterate(H, 1, -INFINITY, nullptr);
@@ -282,6 +319,7 @@ bdc_status bdc_baa_iteration(bdc_handle_t H, const double* p_in, double* p_out, 
 
 bdc_status bdc_log_q(bdc_handle_t H, double* lnq, int64_t nq) {
     if (!H || !lnq) return fail(BDC_ERR_ARG, "bdc_log_q: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_log_q")) return rs;
     const int64_t want = (H->k >= 1) ? (1ll << (H->k - 1)) : 1;
     if (nq != want) return fail(BDC_ERR_ARG, "bdc_log_q: %lld slots, expected 2^(k-1) = %lld", (long long)nq, (long long)want);
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_log_q: no distribution set");
@@ -322,16 +360,19 @@ static bdc_status divergence_common(bdc_handle_t H, const double* lnq, int64_t R
 
 bdc_status bdc_log_w(bdc_handle_t H, const double* lnq, double* logw, int64_t R) {
     if (!H || !logw) return fail(BDC_ERR_ARG, "bdc_log_w: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_log_w")) return rs;
     return divergence_common(H, lnq, R, true, logw);
 }
 
 bdc_status bdc_divergence(bdc_handle_t H, const double* lnq, double* d, int64_t R) {
     if (!H || !d) return fail(BDC_ERR_ARG, "bdc_divergence: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_divergence")) return rs;
     return divergence_common(H, lnq, R, false, d);
 }
 
 bdc_status bdc_rate(bdc_handle_t H, double* rate_nats) {
     if (!H || !rate_nats) return fail(BDC_ERR_ARG, "bdc_rate: NULL argument");
+    if (bdc_status rs = refuse_sharded(H, "bdc_rate")) return rs;
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_rate: no distribution set");
     BDC_CUDA_TRY(cudaSetDevice(H->device));
     bdc_status rc = engine_log_q(H);
@@ -398,6 +439,7 @@ bdc_status bdc_work(bdc_handle_t H, int64_t* nonzero_pairs, int* split_terms) {
 
 bdc_status bdc_profile(bdc_handle_t H, int iters, bdc_profile_t* out) {
     if (!H || !out || iters < 1) return fail(BDC_ERR_ARG, "bdc_profile: bad arguments");
+    if (bdc_status rs = refuse_sharded(H, "bdc_profile")) return rs;
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_profile: no distribution set");
     BDC_CUDA_TRY(cudaSetDevice(H->device));
     return engine_profile(H, iters, out);

@@ -16,6 +16,7 @@ struct bdc_handle {
     int64_t R = 0;
     // placement / options
     int device = 0;
+    int shard_rank = 0, shard_world = 1;  // factored engine over several GPUs: this handle's share of the rows
     int engine = BDC_ENGINE_COUNT;
     int c32 = 0;  // count engine with compensated-FP32 sums (BDC_ENGINE_COUNT_FP32C)
     int verbose = 0;
@@ -80,6 +81,13 @@ cudaError_t engine_enqueue_iteration(bdc_handle* H, double a);  // one iteration
 int count_group_size(int k);
 
 // factored engine (bdc_factored.cu)
+// factored engine sharded by rows (bdc_factored.cu): this handle's window,
+// and one iteration in three parts around the two exchanges
+void factored_shard_range(const bdc_handle* H, int* row0, int* rows, int64_t* i0, int64_t* i1);
+bdc_status factored_shard_q(bdc_handle* H, double* acc);
+bdc_status factored_shard_d(bdc_handle* H, const double* acc, double* part5);
+bdc_status factored_shard_finish(bdc_handle* H, const double* part5, double a);
+
 // frees the certified solver's scratch blocks (bdc_solve.cu)
 void solve_pool_release(bdc_handle* H);
 

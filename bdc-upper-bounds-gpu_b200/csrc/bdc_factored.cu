@@ -125,7 +125,9 @@ struct ThinDF {
 
 struct FactoredState {
     int H1 = 0, H2 = 0, KL = 0, KR = 0, Kp = 0, T = 0;
-    int H1h = 0;              // rows that hold representatives: x_hi < H1 / 2
+    int H1h = 0;              // rows held: x_hi in [row0, row0 + H1h) (all x_hi < H1 / 2 on one GPU)
+    int row0 = 0;             // first row held (a shard of the rows over several GPUs; 0 on one GPU)
+    int64_t i0 = 0, Rl = 0;   // the representatives in those rows: [i0, i0 + Rl) of the ascending list
     std::vector<bdc::Term> terms;
     double* Pw = nullptr;     // [2^{n-1}]  |O(x)| e(x) at representatives, 0 elsewhere
     double* Lt = nullptr;     // [2^{n-1}]  ln e(x) (p = e / Z)
@@ -206,6 +208,12 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a);
 __host__ __device__ __forceinline__ uint32_t fac_pos(uint32_t x, int n2) {
     const uint32_t m = low_mask(n2);
     return (x & ~m) | reverse_bits(x & m, n2);
+}
+
+// the index of representative x in a dense buffer that holds the rows
+// x_hi >= row0 (a shard of the rows; row0 = 0 on one GPU)
+__host__ __device__ __forceinline__ uint32_t fac_loc(uint32_t x, int n, int row0) {
+    return fac_pos(x, n >> 1) - ((uint32_t)row0 << (n >> 1));
 }
 
 
@@ -298,7 +306,7 @@ __global__ void __launch_bounds__(256, (BM * BN <= 4096) ? 3 : 2) k_mma_ba(const
                 const int n = n0 + wn0 + j * 8 + 2 * tq + h;
                 if (n >= d.N) continue;
                 const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
-                const uint32_t x = fac_pos(xd, ep.n2);
+                const uint32_t x = fac_pos(xd + ((uint32_t)ep.row0 << ep.n2), ep.n2);
                 if (!is_rep(x, ep.n)) continue;
                 const double o = (double)orbit_size(x, ep.n);
                 const double D = __ldg(ep.hx + xd) - acc[i][j][h] * ep.inv_c;
@@ -932,11 +940,13 @@ __global__ void k_qsum(const FoldTerm* __restrict__ terms, int T, const double* 
 // only the rows x_hi < H1h; the rows above are zero)
 __device__ __forceinline__ double term_value(const FoldTerm& f, const double* qsum, int t, int ny,
                                              const double* ULt, int KL, const double* VR, int KR, int H1h,
-                                             uint32_t y) {
+                                             int row0, uint32_t y) {
     if (f.kind == 0) return qsum[(size_t)t * ny + y];
     const uint32_t yh = y >> f.m, yl = y & ((1u << f.m) - 1u);
     if (f.kind == 1) return ULt[(size_t)reverse_bits(yl, f.m) * KL + f.off + yh];  // Q_t = U_t (rows: rev x_lo)
-    return yh < (uint32_t)H1h ? VR[(size_t)yh * KR + f.off + yl] : 0.0;  // Q_t = V_t
+    // Q_t = V_t at row x_hi = yh: held rows only (the others are another shard's)
+    const uint32_t r = yh - (uint32_t)row0;
+    return (yh >= (uint32_t)row0 && r < (uint32_t)H1h) ? VR[(size_t)r * KR + f.off + yl] : 0.0;
 }
 
 // phase 2: acc[y] = sum_t Q_t[y]: CTA = 32 consecutive y, warp w reads the
@@ -944,8 +954,8 @@ __device__ __forceinline__ double term_value(const FoldTerm& f, const double* qs
 // in a fixed order
 __global__ void __launch_bounds__(256) k_fold_acc(const FoldTerm* __restrict__ terms, int T,
                                                   const double* __restrict__ qsum, const double* __restrict__ ULt,
-                                                  int KL, const double* __restrict__ VR, int KR, int H1h, int k,
-                                                  double* __restrict__ acc, const DevState* st) {
+                                                  int KL, const double* __restrict__ VR, int KR, int H1h, int row0,
+                                                  int k, double* __restrict__ acc, const DevState* st) {
     if (gated(st)) return;
     __shared__ double part[8][33];
     const int ny = 1 << k;
@@ -953,7 +963,7 @@ __global__ void __launch_bounds__(256) k_fold_acc(const FoldTerm* __restrict__ t
     const int y = blockIdx.x * 32 + yy;
     double a = 0.0;
     if (y < ny)
-        for (int t = w; t < T; t += 8) a += term_value(terms[t], qsum, t, ny, ULt, KL, VR, KR, H1h, (uint32_t)y);
+        for (int t = w; t < T; t += 8) a += term_value(terms[t], qsum, t, ny, ULt, KL, VR, KR, H1h, row0, (uint32_t)y);
     part[w][yy] = a;
     __syncthreads();
     if (w == 0 && y < ny) {
@@ -968,7 +978,7 @@ __global__ void __launch_bounds__(256) k_fold_acc(const FoldTerm* __restrict__ t
 // and copied into RB / LA where a D-side product is the identity.
 __global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double* __restrict__ accv, int k,
                          double inv_c, double* __restrict__ lnq_full, double* __restrict__ lnq, double* __restrict__ RB,
-                         int H2, double* __restrict__ LA, int Kp, int KL, int H1h, const DevState* st) {
+                         int H2, double* __restrict__ LA, int Kp, int KL, int H1h, int row0, const DevState* st) {
     if (gated(st)) return;
     const int ny = 1 << k;
     const int y = blockIdx.x * blockDim.x + threadIdx.x;
@@ -998,7 +1008,8 @@ __global__ void k_fold_q(const FoldTerm* __restrict__ terms, int T, const double
         const FoldTerm& f = terms[t];
         const uint32_t yh = (uint32_t)y >> f.m, yl = (uint32_t)y & ((1u << f.m) - 1u);
         if (f.idB_left) RB[(size_t)(f.off + yh) * H2 + reverse_bits(yl, f.m)] = lq;  // M_t = Lq_t
-        if (f.idA_right && yh < (uint32_t)H1h) LA[(size_t)yh * Kp + KL + f.off + yl] = lq;  // N_t = Lq_t
+        const uint32_t r = yh - (uint32_t)row0;  // the held rows of N_t = Lq_t
+        if (f.idA_right && yh >= (uint32_t)row0 && r < (uint32_t)H1h) LA[(size_t)r * Kp + KL + f.off + yl] = lq;
     }
 }
 
@@ -1064,13 +1075,13 @@ k_fac_finalize(const double* __restrict__ part, int nb, double a, double eta, De
 
 // re-scale after an exp over/underflow: Lt -= s, Pw = |O| exp(Lt), sum
 __global__ void __launch_bounds__(256)
-k_fac_rescale(const uint32_t* __restrict__ reps, int64_t R, int n, double* Lt, double* Pw,
+k_fac_rescale(const uint32_t* __restrict__ reps, int64_t R, int n, int row0, double* Lt, double* Pw,
               double* part, DevState* st, int on_shift_error) {
     if (on_shift_error && st->error != kErrShift) return;  // queued unconditionally in a captured map
     const double s = st->max_logw;  // max of Lt after the failed epilogue
     double sum = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
+        const uint32_t x = reps[i], xd = fac_loc(x, n, row0);
         const double l = Lt[xd] - s;
         const double o = (double)orbit_size(x, n);
         Lt[xd] = l;
@@ -1113,12 +1124,12 @@ __global__ void k_fac_rescale_finish(const double* part, int nb, double a, DevSt
 
 // p -> (Pw, Lt) at representatives; block max of ln p for the first shift
 __global__ void __launch_bounds__(256)
-k_fac_load(const uint32_t* __restrict__ reps, int64_t R, int n, const double* __restrict__ p,
+k_fac_load(const uint32_t* __restrict__ reps, int64_t R, int n, int row0, const double* __restrict__ p,
            double* Pw, double* Lt, double* part, int strict_zero, DevState* st) {
     double mx = -DBL_MAX;
     int zero = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
+        const uint32_t x = reps[i], xd = fac_loc(x, n, row0);
         const double v = p[i];
         Pw[xd] = (double)orbit_size(x, n) * v;
         if (strict_zero) {
@@ -1164,20 +1175,20 @@ __global__ void k_fac_load_finish(const double* part, int nb, int k, DevState* s
 }
 
 // p per representative from the dense state: p = Pw / (|O| Z)
-__global__ void k_fac_store(const uint32_t* __restrict__ reps, int64_t R, int n,
+__global__ void k_fac_store(const uint32_t* __restrict__ reps, int64_t R, int n, int row0,
                             const double* __restrict__ Pw, double* __restrict__ p, const DevState* st) {
     const double inv_z = exp(-st->log_z);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t x = reps[i];
-        p[i] = Pw[fac_pos(x, n >> 1)] * inv_z / (double)orbit_size(x, n);
+        p[i] = Pw[fac_loc(x, n, row0)] * inv_z / (double)orbit_size(x, n);
     }
 }
 
 // scatter h per representative into the dense layout
-__global__ void k_scatter(const uint32_t* __restrict__ reps, int64_t R, int n, const double* __restrict__ v,
+__global__ void k_scatter(const uint32_t* __restrict__ reps, int64_t R, int n, int row0, const double* __restrict__ v,
                           double* __restrict__ dense) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
-        dense[fac_pos(reps[i], n >> 1)] = v[i];
+        dense[fac_loc(reps[i], n, row0)] = v[i];
 }
 
 // constant parts of LA (AL columns) and RB (BR^T rows) from the bundles
@@ -1584,6 +1595,39 @@ bdc_status factored_init(bdc_handle* H) {
     // every representative is <= its complement, so its top bit is 0 and
     // x_hi < H1 / 2: only those rows of the iterate and of G are needed
     F->H1h = F->H1 / 2;
+    // the rows this handle holds: all of them on one GPU; a window of whole
+    // rows, balanced by the number of representatives, for shard rank r of w
+    // (representatives ascend, and x_hi = x >> n2, so a row window is one
+    // contiguous range of them)
+    std::vector<uint32_t> hr((size_t)H->R);
+    BDC_CUDA_TRY(cudaMemcpyAsync(hr.data(), H->d_reps, sizeof(uint32_t) * hr.size(), cudaMemcpyDeviceToHost,
+                                 H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    {
+        const int w = H->shard_world, r = H->shard_rank;
+        if (w < 1 || r < 0 || r >= w || w > F->H1h)
+            return fail(BDC_ERR_ARG, "factored engine: shard %d of %d over %d rows", r, w, F->H1h);
+        auto below = [&](int row) {  // representatives with x_hi < row
+            return (int64_t)(std::lower_bound(hr.begin(), hr.end(), (uint32_t)row << s.n2) - hr.begin());
+        };
+        auto cut = [&](int q) {  // first row of shard q
+            if (q <= 0) return 0;
+            if (q >= w) return F->H1h;
+            const int64_t target = H->R * q / w;
+            int lo = 0, hi = F->H1h;
+            while (lo < hi) {
+                const int mid = (lo + hi) / 2;
+                if (below(mid) >= target) hi = mid;
+                else lo = mid + 1;
+            }
+            return std::max(lo, q);  // at least one row per shard
+        };
+        const int c0 = std::min(cut(r), F->H1h - (w - r)), c1 = (r + 1 == w) ? F->H1h : std::min(cut(r + 1), F->H1h - (w - r - 1));
+        F->row0 = c0;
+        F->H1h = c1 - c0;
+        F->i0 = below(c0);
+        F->Rl = below(c1) - F->i0;
+    }
     const int k = H->k;
     int KL = 0, KR = 0;
     for (int j = s.jlo; j <= s.jhi; ++j) {
@@ -1604,7 +1648,7 @@ bdc_status factored_init(bdc_handle* H) {
     F->KR = KR;
     F->Kp = (KL + KR + 7) / 8 * 8;
     F->T = (int)F->terms.size();
-    const int64_t NX = (int64_t)1 << (H->n - 1);
+    const int64_t NX = (int64_t)F->H1h * F->H2;  // the dense rows held
     const int ny = 1 << k;
     const int H1 = F->H1h, H2 = F->H2, Kp = F->Kp;  // H1: the rows kept
     const int KLa = KL > 0 ? KL : 1, KRa = KR > 0 ? KR : 1;
@@ -1639,14 +1683,10 @@ bdc_status factored_init(bdc_handle* H) {
         H->bytes += cnt * sizeof(uint16_t);
         k_permute_rows<<<H->num_sms * 8, 256, 0, H->stream>>>(H->B.rows, H->B.stride, H2, s.n2, F->Bp);
         BDC_CUDA_TRY(cudaGetLastError());
-        std::vector<uint32_t> hr((size_t)H->R);
-        BDC_CUDA_TRY(cudaMemcpyAsync(hr.data(), H->d_reps, sizeof(uint32_t) * hr.size(), cudaMemcpyDeviceToHost,
-                                     H->stream));
-        BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
         F->colmax.assign(H2, -1);
-        for (uint32_t x : hr) {
-            const uint32_t xd = fac_pos(x, s.n2);
-            const int c = (int)(xd & low_mask(s.n2)), xh = (int)(xd >> s.n2);
+        for (int64_t i = F->i0; i < F->i0 + F->Rl; ++i) {
+            const uint32_t xd = fac_pos(hr[i], s.n2);
+            const int c = (int)(xd & low_mask(s.n2)), xh = (int)(xd >> s.n2) - F->row0;
             if (xh > F->colmax[c]) F->colmax[c] = xh;
         }
     }
@@ -1662,13 +1702,14 @@ bdc_status factored_init(bdc_handle* H) {
         int* d_cm = nullptr;
         BDC_CUDA_TRY(cudaMalloc(&d_cm, sizeof(int) * colmap.size()));
         BDC_CUDA_TRY(cudaMemcpy(d_cm, colmap.data(), sizeof(int) * colmap.size(), cudaMemcpyHostToDevice));
-        k_fill_tables<<<H->num_sms * 8, 256, 0, H->stream>>>(H1, H2, Kp, H->A.rows, H->A.stride, F->Bp,
+        k_fill_tables<<<H->num_sms * 8, 256, 0, H->stream>>>(H1, H2, Kp, H->A.rows + (size_t)F->row0 * H->A.stride,
+                                                            H->A.stride, F->Bp,
                                                             H->B.stride, d_cm, KL, KR, F->LA, F->RB);
         BDC_CUDA_TRY(cudaGetLastError());
         BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
         cudaFree(d_cm);
     }
-    k_scatter<<<H->num_sms * 8, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, H->d_h, F->hx);
+    k_scatter<<<H->num_sms * 8, 256, 0, H->stream>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, H->d_h + F->i0, F->hx);
     BDC_CUDA_TRY(cudaGetLastError());
 
     // ---- the two thin products: U^T (H2 x KL) = (AL^T Pw)^T, V (H1h x KR) = Pw BR
@@ -1786,7 +1827,7 @@ bdc_status factored_init(bdc_handle* H) {
                 q.small = F->VR + t.off;
                 q.small_stride = KR;
                 q.small_u16 = 0;
-                q.wide = H->A.rows + bundle_offset(t.j);
+                q.wide = H->A.rows + (size_t)F->row0 * H->A.stride + bundle_offset(t.j);
                 q.wide_stride = H->A.stride;
                 q.wide_u16 = 1;
                 q.SMALL = 1 << t.m;
@@ -1794,7 +1835,7 @@ bdc_status factored_init(bdc_handle* H) {
                 q.s1 = H1;
                 q.out_trans = 1;
                 // N_t[x_hi][yl] = sum_yh A_j[x_hi][yh] Lq[yh][yl] -> LA[x_hi][KL + off + yl]
-                d.wide = H->A.rows + bundle_offset(t.j);
+                d.wide = H->A.rows + (size_t)F->row0 * H->A.stride + bundle_offset(t.j);
                 d.wide_stride = H->A.stride;
                 d.SMALL = 1 << t.m;
                 d.WIDE = 1 << t.j;
@@ -2012,6 +2053,7 @@ bdc_status factored_init(bdc_handle* H) {
         ep.inv_c = H->inv_c;
         ep.part = F->epart;
         ep.eta = 1.0;
+        ep.row0 = F->row0;
         // each shape one CTA per tile, or (when the tiles outnumber them) as
         // many CTAs as fit on the SMs at once, each looping over tiles with
         // the next tile's loads in flight during the epilogue
@@ -2135,6 +2177,7 @@ static BaEpilogue make_epilogue(bdc_handle* H) {
     ep.st = H->d_st;
     ep.Dout = F->dout;
     ep.eta = F->eta;
+    ep.row0 = F->row0;
     return ep;
 }
 
@@ -2177,9 +2220,10 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             const int nqs = (F->T * ny + 255) / 256;
             k_qsum<<<nqs < 4096 ? nqs : 4096, 256, 0, s>>>(F->d_fold, F->T, F->qparts, H->k, F->qsum, H->d_st);
             k_fold_acc<<<(ny + 31) / 32, 256, 0, s>>>(F->d_fold, F->T, F->qsum, F->UL, F->KL, F->VR, F->KR,
-                                                       F->H1h, H->k, F->qacc, H->d_st);
+                                                       F->H1h, F->row0, H->k, F->qacc, H->d_st);
             k_fold_q<<<(ny + 127) / 128, 128, 0, s>>>(F->d_fold, F->T, F->qacc, H->k, H->inv_c, F->lnq_full,
-                                                       H->d_lnq, F->RB, F->H2, F->LA, F->Kp, F->KL, F->H1h, H->d_st);
+                                                       H->d_lnq, F->RB, F->H2, F->LA, F->Kp, F->KL, F->H1h, F->row0,
+                                                       H->d_st);
             break;
         }
         case ST_DSMALL:
@@ -2227,29 +2271,143 @@ static cudaError_t enqueue_iteration(bdc_handle* H, double a) {
 
 cudaError_t factored_enqueue_iteration(bdc_handle* H, double a) { return enqueue_iteration(H, a); }
 
+// the first shift's inputs over every representative (as k_fac_load writes
+// them for its own): a shard sets the same p on every rank, so each one
+// derives the same shift without an exchange
+__global__ void __launch_bounds__(256) k_lnp_all(const double* __restrict__ p, int64_t R, int strict_zero,
+                                                 double* __restrict__ part) {
+    double mx = -DBL_MAX;
+    int zero = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = p[i];
+        if (strict_zero) {
+            if (v > 0.0) mx = fmax(mx, log(v));
+            continue;
+        }
+        mx = fmax(mx, (v != 0.0) ? log(v) : 0.0);
+        if (v == 0.0) zero = 1;
+    }
+    __shared__ double red[256];
+    __shared__ int zr[256];
+    red[threadIdx.x] = mx;
+    zr[threadIdx.x] = zero;
+    __syncthreads();
+    for (int t = 128; t > 0; t >>= 1) {
+        if (threadIdx.x < t) {
+            red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + t]);
+            zr[threadIdx.x] |= zr[threadIdx.x + t];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = red[0];
+        part[2 * blockIdx.x + 1] = (double)zr[0];
+    }
+}
+
 bdc_status factored_load_p(bdc_handle* H, int strict_zero) {
     FactoredState* F = H->fac;
-    const int64_t NX = (int64_t)1 << (H->n - 1);  // representatives have x < 2^{n-1}
+    const int64_t NX = (int64_t)F->H1h * F->H2;  // the dense rows held
     BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
     const int nb = H->nb_upd;
-    k_fac_load<<<nb, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, H->d_p[0], F->Pw, F->Lt, F->epart, strict_zero,
-                                          H->d_st);
+    k_fac_load<<<nb, 256, 0, H->stream>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, H->d_p[0] + F->i0, F->Pw, F->Lt,
+                                          F->epart, strict_zero, H->d_st);
+    if (H->shard_world > 1) k_lnp_all<<<nb, 256, 0, H->stream>>>(H->d_p[0], H->R, strict_zero, F->epart);
     k_fac_load_finish<<<1, 32, 0, H->stream>>>(F->epart, nb, H->k, H->d_st);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
 }
 
+// ----------------------------------------------- rows over several GPUs
+void factored_shard_range(const bdc_handle* H, int* row0, int* rows, int64_t* i0, int64_t* i1) {
+    const FactoredState* F = H->fac;
+    *row0 = F->row0;
+    *rows = F->H1h;
+    *i0 = F->i0;
+    *i1 = F->i0 + F->Rl;
+}
+
+// q side on the held rows: partial sums acc[y] = sum_{held x} |O(x)| e(x) N(x, y)
+// of every term (the fold's first two phases), to the host
+bdc_status factored_shard_q(bdc_handle* H, double* acc) {
+    FactoredState* F = H->fac;
+    cudaStream_t s = H->stream;
+    BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), s));
+    BDC_CUDA_TRY(enqueue_stage(H, ST_QBIG, -INFINITY));
+    BDC_CUDA_TRY(enqueue_stage(H, ST_QSMALL, -INFINITY));
+    const int ny = 1 << H->k;
+    const int nqs = (F->T * ny + 255) / 256;
+    k_qsum<<<nqs < 4096 ? nqs : 4096, 256, 0, s>>>(F->d_fold, F->T, F->qparts, H->k, F->qsum, H->d_st);
+    k_fold_acc<<<(ny + 31) / 32, 256, 0, s>>>(F->d_fold, F->T, F->qsum, F->UL, F->KL, F->VR, F->KR, F->H1h, F->row0,
+                                               H->k, F->qacc, H->d_st);
+    BDC_CUDA_TRY(cudaGetLastError());
+    BDC_CUDA_TRY(cudaMemcpyAsync(acc, F->qacc, sizeof(double) * ny, cudaMemcpyDeviceToHost, s));
+    BDC_CUDA_TRY(cudaStreamSynchronize(s));
+    return BDC_OK;
+}
+
+// from the summed acc: ln q, the D side and G with the update on the held
+// rows; part5 = this shard's [max D, sum |O| e, max logW, sum |O| p D, zero]
+bdc_status factored_shard_d(bdc_handle* H, const double* acc, double* part5) {
+    FactoredState* F = H->fac;
+    cudaStream_t s = H->stream;
+    const int ny = 1 << H->k;
+    BDC_CUDA_TRY(cudaMemcpyAsync(F->qacc, acc, sizeof(double) * ny, cudaMemcpyHostToDevice, s));
+    k_fold_q<<<(ny + 127) / 128, 128, 0, s>>>(F->d_fold, F->T, F->qacc, H->k, H->inv_c, F->lnq_full, H->d_lnq, F->RB,
+                                              F->H2, F->LA, F->Kp, F->KL, F->H1h, F->row0, H->d_st);
+    BDC_CUDA_TRY(cudaGetLastError());
+    BDC_CUDA_TRY(enqueue_stage(H, ST_DSMALL, -INFINITY));
+    BDC_CUDA_TRY(enqueue_stage(H, ST_G, -INFINITY));
+    const int nb = F->use_oz ? ozaki_partials(F->oz) : F->ctas_g;
+    std::vector<double> part((size_t)nb * 8);
+    BDC_CUDA_TRY(cudaMemcpyAsync(part.data(), F->epart, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, s));
+    BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    BDC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (H->h_st->error) return fail(BDC_ERR_NUMERIC, "sharded iteration: device error %d", H->h_st->error);
+    double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0, zero = 0.0;
+    for (int b = 0; b < nb; ++b) {
+        mD = std::max(mD, part[(size_t)b * 8 + 0]);
+        sE += part[(size_t)b * 8 + 1];
+        mL = std::max(mL, part[(size_t)b * 8 + 2]);
+        sR += part[(size_t)b * 8 + 3];
+        zero = std::max(zero, part[(size_t)b * 8 + 4]);
+    }
+    part5[0] = mD;
+    part5[1] = sE;
+    part5[2] = mL;
+    part5[3] = sR;
+    part5[4] = zero;
+    return BDC_OK;
+}
+
+// the update's finish from the combined part5 (max, sum, max, sum, max over
+// the shards): ln Z, mx, the bound, the stop test and the next shift, the
+// same on every shard
+bdc_status factored_shard_finish(bdc_handle* H, const double* part5, double a) {
+    FactoredState* F = H->fac;
+    cudaStream_t s = H->stream;
+    double row[8] = {part5[0], part5[1], part5[2], part5[3], part5[4], 0.0, 0.0, 0.0};
+    BDC_CUDA_TRY(cudaMemcpyAsync(F->epart, row, sizeof(row), cudaMemcpyHostToDevice, s));
+    k_fac_finalize<<<1, 256, 0, s>>>(F->epart, 1, a, 1.0, H->d_st);
+    BDC_CUDA_TRY(cudaGetLastError());
+    BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+    BDC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (H->h_st->error)
+        return fail(BDC_ERR_NUMERIC, "sharded iteration: exp shift out of range (device error %d)", H->h_st->error);
+    return BDC_OK;
+}
+
 bdc_status factored_store_p(bdc_handle* H, double* p_out) {
     FactoredState* F = H->fac;
-    k_fac_store<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Pw, p_out, H->d_st);
+    k_fac_store<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Pw, p_out + F->i0, H->d_st);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
 }
 
-__global__ void k_gather_dense(const uint32_t* __restrict__ reps, int64_t R, int n, const double* __restrict__ dense,
+__global__ void k_gather_dense(const uint32_t* __restrict__ reps, int64_t R, int n, int row0, const double* __restrict__ dense,
                                double* __restrict__ out) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = dense[fac_pos(reps[i], n >> 1)];
+        out[i] = dense[fac_loc(reps[i], n, row0)];
 }
 
 static bdc_status rescale(bdc_handle* H, double a);
@@ -2269,7 +2427,7 @@ static cudaError_t enqueue_map(bdc_handle* H, const double* p_in, double* p_out,
     // (Pw is zero away from the representatives from set-up on: every kernel
     // writes it only there, and the load below rewrites all of them)
     const int nb = H->nb_upd;
-    k_fac_load<<<nb, 256, 0, s>>>(H->d_reps, H->R, H->n, p_in, F->Pw, F->Lt, F->epart, 1, H->d_st);
+    k_fac_load<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, p_in + F->i0, F->Pw, F->Lt, F->epart, 1, H->d_st);
     k_fac_load_finish<<<1, 32, 0, s>>>(F->epart, nb, H->k, H->d_st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -2277,10 +2435,10 @@ static cudaError_t enqueue_map(bdc_handle* H, const double* p_in, double* p_out,
     e = enqueue_iteration(H, -INFINITY);
     F->dout = nullptr;
     if (e != cudaSuccess) return e;
-    k_fac_rescale<<<nb, 256, 0, s>>>(H->d_reps, H->R, H->n, F->Lt, F->Pw, F->epart, H->d_st, 1);
+    k_fac_rescale<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Lt, F->Pw, F->epart, H->d_st, 1);
     k_fac_rescale_finish<<<1, 32, 0, s>>>(F->epart, nb, -INFINITY, H->d_st, 1);
-    if (D_out) k_gather_dense<<<H->num_sms * 8, 256, 0, s>>>(H->d_reps, H->R, H->n, F->Ddense, D_out);
-    k_fac_store<<<nb, 256, 0, s>>>(H->d_reps, H->R, H->n, F->Pw, p_out, H->d_st);
+    if (D_out) k_gather_dense<<<H->num_sms * 8, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Ddense, D_out + F->i0);
+    k_fac_store<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Pw, p_out + F->i0, H->d_st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s);
@@ -2294,7 +2452,7 @@ static cudaError_t enqueue_map(bdc_handle* H, const double* p_in, double* p_out,
 // costs one graph launch and one synchronisation.
 bdc_status factored_map(bdc_handle* H, const double* p_in, double* p_out, double* D_out) {
     FactoredState* F = H->fac;
-    const int64_t NX = (int64_t)1 << (H->n - 1);
+    const int64_t NX = (int64_t)F->H1h * F->H2;
     if (D_out && !F->Ddense) {
         BDC_CUDA_TRY(cudaMalloc(&F->Ddense, sizeof(double) * NX));
         H->bytes += sizeof(double) * NX;
@@ -2339,7 +2497,7 @@ bdc_status factored_recover(bdc_handle* H, double a) {
 
 static bdc_status rescale(bdc_handle* H, double a) {
     FactoredState* F = H->fac;
-    k_fac_rescale<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Lt, F->Pw, F->epart, H->d_st, 0);
+    k_fac_rescale<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Lt, F->Pw, F->epart, H->d_st, 0);
     k_fac_rescale_finish<<<1, 32, 0, H->stream>>>(F->epart, H->nb_upd, a, H->d_st, 0);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
@@ -2491,7 +2649,7 @@ __global__ void k_acc_decide(DevState* st) {
 
 // x_{t-1}, x_t (dense, at representatives) and the extrapolated ln y into Lt;
 // block max of ln y
-__global__ void __launch_bounds__(256) k_acc_extrap(const uint32_t* __restrict__ reps, int64_t R, int n,
+__global__ void __launch_bounds__(256) k_acc_extrap(const uint32_t* __restrict__ reps, int64_t R, int n, int row0,
                                                     double* __restrict__ xa, double* __restrict__ xb,
                                                     double* __restrict__ Lt, double* __restrict__ part,
                                                     const DevState* st) {
@@ -2501,7 +2659,7 @@ __global__ void __launch_bounds__(256) k_acc_extrap(const uint32_t* __restrict__
     const double beta = (double)st->ng_t / ((double)st->ng_t + 3.0);
     double mx = -DBL_MAX;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t xd = fac_pos(reps[i], n >> 1);
+        const uint32_t xd = fac_loc(reps[i], n, row0);
         double y;
         if (mode == 1) {
             const double a_old = xa[xd], a_new = Lt[xd] - lnz;
@@ -2528,14 +2686,14 @@ __global__ void k_acc_max(const double* __restrict__ part, int nb, DevState* st)
 }
 
 // Lt -= max, Pw = |O| exp(Lt); block sums of |O| exp(Lt)
-__global__ void __launch_bounds__(256) k_acc_pw(const uint32_t* __restrict__ reps, int64_t R, int n,
+__global__ void __launch_bounds__(256) k_acc_pw(const uint32_t* __restrict__ reps, int64_t R, int n, int row0,
                                                 double* __restrict__ Lt, double* __restrict__ Pw,
                                                 double* __restrict__ part, const DevState* st) {
     if (acc_gated(st)) return;
     const double m = st->ng_max;
     double sum = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i], xd = fac_pos(x, n >> 1);
+        const uint32_t x = reps[i], xd = fac_loc(x, n, row0);
         const double l = Lt[xd] - m;
         const double o = (double)orbit_size(x, n);
         const double e = exp(l);
@@ -2568,11 +2726,10 @@ static cudaError_t enqueue_acc_step(bdc_handle* H, double eta) {
     if (!F->snap0 || !F->snap1) return cudaErrorInvalidValue;  // factored_acc_buffers first
     cudaStream_t s = H->stream;
     const int nb = H->nb_upd;
-    const int64_t R = H->R;
     k_acc_decide<<<1, 32, 0, s>>>(H->d_st);
-    k_acc_extrap<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->snap0, F->snap1, F->Lt, F->epart, H->d_st);
+    k_acc_extrap<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->snap0, F->snap1, F->Lt, F->epart, H->d_st);
     k_acc_max<<<1, 32, 0, s>>>(F->epart, nb, H->d_st);
-    k_acc_pw<<<nb, 256, 0, s>>>(H->d_reps, R, H->n, F->Lt, F->Pw, F->epart, H->d_st);
+    k_acc_pw<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Lt, F->Pw, F->epart, H->d_st);
     k_acc_setz<<<1, 32, 0, s>>>(F->epart, nb, eta, H->d_st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -2597,7 +2754,7 @@ cudaError_t factored_enqueue_acc_steps(bdc_handle* H, int steps, double eta) {
 bdc_status factored_acc_buffers(bdc_handle* H) {
     FactoredState* F = H->fac;
     if (F->snap0) return BDC_OK;
-    const size_t NX = (size_t)1 << (H->n - 1);
+    const size_t NX = (size_t)F->H1h * F->H2;
     BDC_CUDA_TRY(cudaMalloc(&F->snap0, sizeof(double) * NX));
     BDC_CUDA_TRY(cudaMalloc(&F->snap1, sizeof(double) * NX));
     H->bytes += 2 * sizeof(double) * NX;
@@ -2605,12 +2762,12 @@ bdc_status factored_acc_buffers(bdc_handle* H) {
 }
 
 // x_t = x_{t-1} = the current normalised log iterate; nothing evaluated yet
-__global__ void __launch_bounds__(256) k_acc_init(const uint32_t* __restrict__ reps, int64_t R, int n,
+__global__ void __launch_bounds__(256) k_acc_init(const uint32_t* __restrict__ reps, int64_t R, int n, int row0,
                                                   const double* __restrict__ Lt, double* __restrict__ xa,
                                                   double* __restrict__ xb, DevState* st, double gap_nats) {
     const double lnz = st->log_z;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t xd = fac_pos(reps[i], n >> 1);
+        const uint32_t xd = fac_loc(reps[i], n, row0);
         const double l = Lt[xd] - lnz;
         xa[xd] = l;
         xb[xd] = l;
@@ -2626,7 +2783,7 @@ bdc_status factored_acc_start(bdc_handle* H, double gap_bits) {
     bdc_status rc = factored_acc_buffers(H);
     if (rc != BDC_OK) return rc;
     FactoredState* F = H->fac;
-    k_acc_init<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps, H->R, H->n, F->Lt, F->snap0, F->snap1, H->d_st,
+    k_acc_init<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Lt, F->snap0, F->snap1, H->d_st,
                                                  gap_bits * 0.69314718055994530942);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;

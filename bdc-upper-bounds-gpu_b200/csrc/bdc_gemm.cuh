@@ -53,6 +53,7 @@ struct BaEpilogue {
     double* Dout;                // optional: D(x) at every representative (dense layout)
     double eta;                  // step of the exponentiated-gradient update: ln p' = ln p + eta D - ln Z
                                  // (1 is the BA update)
+    int row0;                    // global x_hi of the product's row 0 (a shard of the rows; 0 on one GPU)
 };
 
 }  // namespace bdc

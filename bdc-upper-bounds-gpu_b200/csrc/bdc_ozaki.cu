@@ -268,7 +268,8 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
                 const int n = n0 + c0 + j;
                 if (n >= g.N) continue;
                 const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
-                const uint32_t x = (xd & ~low_mask(ep.n2)) | reverse_bits(xd & low_mask(ep.n2), ep.n2);
+                const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);  // the global dense index
+                const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
                 if (!is_rep(x, ep.n)) continue;
                 const double o = (double)orbit_size(x, ep.n);
                 const double D = __ldg(ep.hx + xd) - gsum[j] * ep.inv_c;
@@ -553,7 +554,8 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
                 const int n = n0 + j;
                 if (n >= g.N) continue;
                 const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
-                const uint32_t x = (xd & ~low_mask(ep.n2)) | reverse_bits(xd & low_mask(ep.n2), ep.n2);
+                const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);  // the global dense index
+                const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
                 if (!is_rep(x, ep.n)) continue;
                 const double o = (double)orbit_size(x, ep.n);
                 const double D = __ldg(ep.hx + xd) - gsum[j] * ep.inv_c;

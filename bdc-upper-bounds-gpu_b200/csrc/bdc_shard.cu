@@ -143,4 +143,75 @@ bdc_status bdc_shard_update_end(bdc_handle_t H, int64_t r0, int64_t r1, double l
     return BDC_OK;
 }
 
+// ---------------------------------------------- factored engine, rows sharded
+static bdc_status fshard_check(bdc_handle* H, const char* what) {
+    if (!H) return fail(BDC_ERR_ARG, "%s: NULL handle", what);
+    if (H->engine != BDC_ENGINE_FACTORED || !H->fac)
+        return fail(BDC_ERR_UNSUPPORTED, "%s: needs a handle from bdc_create_sharded", what);
+    if (!H->p_set) return fail(BDC_ERR_STATE, "%s: no distribution set", what);
+    BDC_CUDA_TRY(cudaSetDevice(H->device));
+    return BDC_OK;
+}
+
+bdc_status bdc_fshard_range(bdc_handle_t H, int* row0, int* rows, int64_t* rep_begin, int64_t* rep_end) {
+    if (!H || !H->fac || !row0 || !rows || !rep_begin || !rep_end)
+        return fail(BDC_ERR_ARG, "bdc_fshard_range: NULL argument or not a factored handle");
+    factored_shard_range(H, row0, rows, rep_begin, rep_end);
+    return BDC_OK;
+}
+
+bdc_status bdc_fshard_q(bdc_handle_t H, double* acc, int64_t ny) {
+    bdc_status rc = fshard_check(H, "bdc_fshard_q");
+    if (rc != BDC_OK) return rc;
+    if (!acc || ny != ((int64_t)1 << H->k)) return fail(BDC_ERR_ARG, "bdc_fshard_q: acc must hold 2^k values");
+    return factored_shard_q(H, acc);
+}
+
+bdc_status bdc_fshard_d(bdc_handle_t H, const double* acc, int64_t ny, double* part5) {
+    bdc_status rc = fshard_check(H, "bdc_fshard_d");
+    if (rc != BDC_OK) return rc;
+    if (!acc || !part5 || ny != ((int64_t)1 << H->k))
+        return fail(BDC_ERR_ARG, "bdc_fshard_d: acc must hold 2^k values, part5 five");
+    return factored_shard_d(H, acc, part5);
+}
+
+bdc_status bdc_fshard_finish(bdc_handle_t H, const double* part5, double a, bdc_stats* stats) {
+    bdc_status rc = fshard_check(H, "bdc_fshard_finish");
+    if (rc != BDC_OK) return rc;
+    if (!part5) return fail(BDC_ERR_ARG, "bdc_fshard_finish: NULL part5");
+    rc = factored_shard_finish(H, part5, a);
+    if (rc != BDC_OK) return rc;
+    if (stats) {
+        const double ln2 = 0.69314718055994530942;
+        const DevState* s = H->h_st;
+        stats->iters = 1;
+        stats->total_iters = s->iter;
+        stats->mx = s->mx;
+        stats->upper_bound = s->max_d / ln2;
+        stats->rate = s->rate / ln2;
+        stats->lse = s->lse / ln2;
+        stats->best_upper_bound = s->best_ub / ln2;
+        stats->best_rate = s->best_rate / ln2;
+        stats->converged = s->done;
+    }
+    return BDC_OK;
+}
+
+bdc_status bdc_fshard_get_p(bdc_handle_t H, double* p, int64_t count) {
+    bdc_status rc = fshard_check(H, "bdc_fshard_get_p");
+    if (rc != BDC_OK) return rc;
+    int row0 = 0, rows = 0;
+    int64_t i0 = 0, i1 = 0;
+    factored_shard_range(H, &row0, &rows, &i0, &i1);
+    if (!p || count != i1 - i0) return fail(BDC_ERR_ARG, "bdc_fshard_get_p: %lld slots for %lld representatives",
+                                            (long long)count, (long long)(i1 - i0));
+    // the dense state of the held rows -> p of their representatives
+    BDC_CUDA_TRY(cudaMemsetAsync(H->d_d, 0, sizeof(double) * H->R, H->stream));
+    rc = factored_store_p(H, H->d_d);
+    if (rc != BDC_OK) return rc;
+    BDC_CUDA_TRY(cudaMemcpyAsync(p, H->d_d + i0, sizeof(double) * count, cudaMemcpyDeviceToHost, H->stream));
+    BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
+    return BDC_OK;
+}
+
 }  // extern "C"

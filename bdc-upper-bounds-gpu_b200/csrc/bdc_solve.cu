@@ -1332,6 +1332,7 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
     if (!H) return fail(BDC_ERR_ARG, "bdc_solve: NULL handle");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_solve: no distribution set");
     if (H->engine != BDC_ENGINE_FACTORED) return fail(BDC_ERR_UNSUPPORTED, "bdc_solve: needs the factored engine (k < n)");
+    if (H->shard_world > 1) return fail(BDC_ERR_STATE, "bdc_solve: this handle holds a shard of the rows");
     if (!(gap_bits > 0.0) || max_evals < 1) return fail(BDC_ERR_ARG, "bdc_solve: need gap_bits > 0 and max_evals >= 1");
     if (H->n > 26) return fail(BDC_ERR_UNSUPPORTED, "bdc_solve: counts of n > 26 do not fit FP32 exactly");
     BDC_CUDA_TRY(cudaSetDevice(H->device));

@@ -181,6 +181,30 @@ bdc_status bdc_shard_set_q(bdc_handle_t h, const double* acc, int64_t ny);
 bdc_status bdc_shard_update_begin(bdc_handle_t h, int64_t rep_begin, int64_t rep_end, double* stats5);
 bdc_status bdc_shard_update_end(bdc_handle_t h, int64_t rep_begin, int64_t rep_end, double log_z, double* mx);
 
+/* The factored engine with its rows sharded over several GPUs (no
+ * counterpart in the reference, which runs one (n,k) on one GPU).  Rank r of
+ * `world` holds a window of whole rows x_hi (about R / world representatives,
+ * a contiguous range of the ascending list): the dense iterate, h(x) and the
+ * G product exist only for those rows.  Every rank sets the same
+ * distribution (bdc_set_p with the full vector).  One iteration:
+ *   bdc_fshard_q(acc)              partial q sums of the held rows, 2^k values
+ *   -- the caller sums acc over the ranks (an all-reduce) --
+ *   bdc_fshard_d(acc, part5)       ln q, the D side and G with the update on the
+ *                                  held rows; part5 = [max D, sum |O| e,
+ *                                  max logW, sum |O| p D, input-zero flag]
+ *   -- the caller combines part5 over the ranks: max, sum, max, sum, max --
+ *   bdc_fshard_finish(part5, a, stats)   ln Z, mx, the bound and the stop test,
+ *                                  identical on every rank (stats->converged: mx < a)
+ * A sharded handle refuses the single-GPU calls (bdc_iterate, bdc_get_p, ...);
+ * bdc_fshard_get_p returns p of its own representatives.  bdc_b200.sharded
+ * runs this loop over torch.distributed. */
+bdc_status bdc_create_sharded(int n, int k, const bdc_options* opts, int rank, int world, bdc_handle_t* out);
+bdc_status bdc_fshard_range(bdc_handle_t h, int* row0, int* rows, int64_t* rep_begin, int64_t* rep_end);
+bdc_status bdc_fshard_q(bdc_handle_t h, double* acc, int64_t ny);
+bdc_status bdc_fshard_d(bdc_handle_t h, const double* acc, int64_t ny, double* part5);
+bdc_status bdc_fshard_finish(bdc_handle_t h, const double* part5, double a, bdc_stats* stats);
+bdc_status bdc_fshard_get_p(bdc_handle_t h, double* p, int64_t count);
+
 /* Batches (no counterpart in the reference, which runs one (n,k) per
  * process): many handles -- different (n,k) and starting distributions --
  * iterated together from one captured CUDA graph with one branch per handle.

@@ -161,3 +161,163 @@ def test_two_ranks_match_one_engine(bdc, O):
     reps = O.canonicals(10)
     ref = O.run_ba(10, 5, np.full(len(reps), 1.0 / (1 << 10)), reps, 1e-3, 100000)
     assert res["stop"][0]["iters"] == ref["iters"]
+
+
+# ------------------------------------- the factored engine, rows sharded
+def test_combine_part5_is_max_sum_max_sum_max():
+    from bdc_b200 import sharded
+    parts = [[1.0, 2.0, -3.0, 0.5, 0.0], [4.0, 1.0, -5.0, 0.25, 1.0], [2.0, 0.5, -1.0, 0.0, 0.0]]
+    np.testing.assert_array_equal(sharded.combine_part5(parts), [4.0, 3.5, -1.0, 0.75, 1.0])
+
+
+class _RowShardStandIn:
+    """The three calls of a row-sharded factored handle restated in numpy on
+    the full input space (every orbit of size one), for testing the exchange
+    logic of sharded.iterate_rows without a GPU: fshard_q returns the held
+    rows' partial sums acc[y] = sum_x e(x) N(x, y), fshard_d the update
+    statistics of the held rows with the shift every rank shares, and
+    fshard_finish the normaliser, the stopping statistic and the next shift
+    from the combined statistics (the device finalize's arithmetic)."""
+
+    def __init__(self, n, k, rank, world, p0, O):
+        xs = np.arange(1 << n, dtype=np.uint32)
+        self.N = O.count_rows(n, k, xs).reshape(1 << n, 1 << k).astype(np.float64)
+        self.C = float(O.nck(n, k))
+        W = self.N / self.C
+        self.h = np.where(W > 0, W * np.log(np.where(W > 0, W, 1.0)), 0.0).sum(1)
+        self.k, self.R, self.device = k, 1 << n, 0
+        self.i0, self.i1 = (1 << n) * rank // world, (1 << n) * (rank + 1) // world
+        self.lt = np.log(p0)                 # ln e (unnormalised), all rows (only held ones are used)
+        self.log_z, self.shift = 0.0, float(np.log(p0).max()) + k * np.log(2.0)
+
+    def fshard_range(self):
+        return (self.i0, self.i1 - self.i0, self.i0, self.i1)
+
+    def fshard_q(self):
+        sl = slice(self.i0, self.i1)
+        return np.exp(self.lt[sl] - self.log_z) @ self.N[sl]
+
+    def fshard_d(self, acc):
+        sl = slice(self.i0, self.i1)
+        q = acc / self.C
+        lnq = np.log(np.where(q > 0, q, 1.0))
+        D = self.h[sl] - (self.N[sl] @ lnq) / self.C
+        p = np.exp(self.lt[sl] - self.log_z)
+        lw = (self.lt[sl] - self.log_z) + D - self.shift
+        self.lt[sl] = lw
+        return np.array([D.max(), np.exp(lw).sum(), lw.max(), (p * D).sum(), 0.0])
+
+    def fshard_finish(self, part5, a):
+        mD, sE, mL, sR, _ = part5
+        lnz = np.log(sE)
+        mx = (mD - self.shift - lnz) / np.log(2.0)
+        # ln e carries the shift: ln p = lt - ln Z from here on
+        self.shift, self.log_z = (mL - lnz) + mD, lnz
+        return {"mx": mx, "upper_bound": mD / np.log(2.0), "rate": sR / np.log(2.0),
+                "best_upper_bound": mD / np.log(2.0), "best_rate": sR / np.log(2.0), "converged": not mx >= a}
+
+    def p(self):
+        return np.exp(self.lt - self.log_z)
+
+
+def _rows_rank(rank, world, port, q):
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(PKG), "oracle"))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import oracle as O
+        from bdc_b200 import sharded
+        n, k = 8, 4
+        p0 = np.random.default_rng(3).dirichlet(np.ones(1 << n))
+        E = _RowShardStandIn(n, k, rank, world, p0, O)
+        st = sharded.iterate_rows(E, 25, float("-inf"))
+        parts = [None] * world
+        dist.all_gather_object(parts, (E.i0, E.p()[E.i0:E.i1]))
+        if rank == 0:
+            p = np.concatenate([v for _, v in sorted(parts, key=lambda t: t[0])])
+            q.put((st, p))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_row_shards_over_gloo_world_2_match_one_process(O):
+    # the same 25 BA iterations on the full space of n = 8 in one process
+    n, k = 8, 4
+    p = np.random.default_rng(3).dirichlet(np.ones(1 << n))
+    N = O.count_rows(n, k, np.arange(1 << n, dtype=np.uint32)).reshape(1 << n, 1 << k).astype(np.float64)
+    W = N / O.nck(n, k)
+    for _ in range(25):
+        qv = p @ W
+        D = (W * np.log(np.where(W > 0, W / qv, 1.0))).sum(1)
+        bound, rate = D.max() / np.log(2.0), (p * D).sum() / np.log(2.0)
+        pn = p * np.exp(D)
+        pn /= pn.sum()
+        mx = np.max(np.log2(pn) - np.log2(p))
+        p = pn
+    ctx = mp.get_context("spawn")
+    qq = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rows_rank, args=(r, 2, port, qq)) for r in range(2)]
+    for pr in procs:
+        pr.start()
+    st, got = qq.get(timeout=120)
+    for pr in procs:
+        pr.join(timeout=120)
+        assert pr.exitcode == 0
+    assert st["iters"] == 25 and st["world"] == 2
+    np.testing.assert_allclose(got, p, rtol=1e-12, atol=0)
+    assert abs(st["upper_bound"] - bound) < 1e-12 and abs(st["rate"] - rate) < 1e-12
+    assert abs(st["mx"] - mx) < 1e-10
+
+
+ROW_CASES = [(20, 10, ("dirichlet", 1.0, 0), 12), (24, 12, ("uniform",), 6)]
+
+
+def _gpu_rows_rank(rank, world, port, q):
+    import sys
+    sys.path.insert(0, PKG)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300))
+    try:
+        import bdc_b200
+        from bdc_b200 import sharded
+        res = {}
+        for n, k, spec, iters in ROW_CASES:
+            with bdc_b200.Engine(n, k, engine="factored", device=0, shard=(rank, world)) as E:
+                E.set_p(_start(n, spec))
+                st = sharded.iterate_rows(E, iters)
+                p = sharded.gather_p_rows(E)
+            res[(n, k)] = (st, p)
+        if rank == 0:
+            q.put(res)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_row_sharded_factored_engine_two_ranks_match_one_engine(bdc):
+    # two ranks, each holding half of the representatives' rows, as two
+    # processes on one device exchanging over gloo (no kernel waits on another)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gpu_rows_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = q.get(timeout=600)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    for n, k, spec, iters in ROW_CASES:
+        st, p = res[(n, k)]
+        assert st["world"] == 2 and st["iters"] == iters
+        with bdc.Engine(n, k, engine="factored") as E:
+            E.set_p(_start(n, spec))
+            s1 = E.iterate(iters, float("-inf"))
+            p1 = E.get_p()
+        np.testing.assert_allclose(p, p1, rtol=1e-11, atol=0)
+        assert abs(st["upper_bound"] - s1["upper_bound"]) < 1e-11
+        assert abs(st["rate"] - s1["rate"]) < 1e-11
+        assert abs(st["mx"] - s1["mx"]) < 1e-10
