@@ -55,6 +55,33 @@ struct Tile {
     }
 };
 
+// N consecutive uint16 entries (N <= 8) from an address aligned to 2N bytes,
+// in one load
+template <int N>
+__device__ __forceinline__ void ld_u16(const uint16_t* __restrict__ p, uint32_t (&o)[N]) {
+    if constexpr (N == 8) {
+        const uint4 v = __ldg((const uint4*)p);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            o[2 * i] = w[i] & 0xFFFFu;
+            o[2 * i + 1] = w[i] >> 16;
+        }
+    } else if constexpr (N == 4) {
+        const uint2 v = __ldg((const uint2*)p);
+        o[0] = v.x & 0xFFFFu;
+        o[1] = v.x >> 16;
+        o[2] = v.y & 0xFFFFu;
+        o[3] = v.y >> 16;
+    } else if constexpr (N == 2) {
+        const uint32_t v = __ldg((const unsigned int*)p);
+        o[0] = v & 0xFFFFu;
+        o[1] = v >> 16;
+    } else {
+        o[0] = __ldg(p);
+    }
+}
+
 // One split point J of the dense row: N[t][b] += A_J[xh][y >> M] * B_M[xl][y & (2^M-1)].
 template <int K, int TB, int BB, int J>
 __device__ __forceinline__ void tile_term(const Split& s, const uint16_t* __restrict__ ar,
@@ -87,16 +114,26 @@ __device__ __forceinline__ void tile_term(const Split& s, const uint16_t* __rest
                 const uint32_t b = (M >= BB) ? 0 : (ba << M);
                 av[ta][ba] = (uint32_t)(xh == gA + ((t << (K - TB)) >> M) + (b >> M));
             }
+    } else if constexpr (J >= TB) {
+        // the A row is stored rotated (rotate_bundle): the T entries of one
+        // thread, y_hi = (t << (J - TB)) | low, sit at (low << TB) | t, one
+        // vector load for all t
+#pragma unroll
+        for (int ba = 0; ba < AB; ++ba) {
+            const uint32_t low = gA + ((M >= BB) ? 0u : (uint32_t)ba);
+            uint32_t v[T];
+            ld_u16<T>(ar + bundle_offset(J) + (low << TB), v);
+#pragma unroll
+            for (int ta = 0; ta < AT; ++ta) av[ta][ba] = v[ta];
+        }
     } else {
-        const uint16_t* __restrict__ pa = ar + bundle_offset(J) + gA;
+        // J < TB: the 2^J entries y_hi = 0 .. 2^J - 1 are contiguous (gA = 0)
+        uint32_t v[AT];
+        ld_u16<AT>(ar + bundle_offset(J), v);
 #pragma unroll
         for (int ta = 0; ta < AT; ++ta)
 #pragma unroll
-            for (int ba = 0; ba < AB; ++ba) {
-                const uint32_t t = (J >= TB) ? ta : (ta << (TB - J));
-                const uint32_t b = (M >= BB) ? 0 : (ba << M);
-                av[ta][ba] = (uint32_t)__ldg(pa + (((t << (K - TB)) >> M) + (b >> M)));
-            }
+            for (int ba = 0; ba < AB; ++ba) av[ta][ba] = v[ta];
     }
     if (M == s.n2) {
 #pragma unroll
@@ -107,14 +144,16 @@ __device__ __forceinline__ void tile_term(const Split& s, const uint16_t* __rest
                 bv[tb][bb] = (uint32_t)(xl == gB + ((t << (K - TB)) & mlo) + ((uint32_t)bb & mlo));
             }
     } else {
+        // the BN entries of one t are contiguous and aligned to BN: one vector load
         const uint16_t* __restrict__ pb = br + bundle_offset(M) + gB;
 #pragma unroll
-        for (int tb = 0; tb < BT; ++tb)
+        for (int tb = 0; tb < BT; ++tb) {
+            const uint32_t t = (J >= TB) ? 0 : tb;
+            uint32_t v[BN];
+            ld_u16<BN>(pb + ((t << (K - TB)) & mlo), v);
 #pragma unroll
-            for (int bb = 0; bb < BN; ++bb) {
-                const uint32_t t = (J >= TB) ? 0 : tb;
-                bv[tb][bb] = (uint32_t)__ldg(pb + (((t << (K - TB)) & mlo) + ((uint32_t)bb & mlo)));
-            }
+            for (int bb = 0; bb < BN; ++bb) bv[tb][bb] = v[bb];
+        }
     }
 #pragma unroll
     for (int t = 0; t < T; ++t)
@@ -442,6 +481,38 @@ __global__ void k_qfold(const double* __restrict__ part, int nparts, int k, doub
     }
 }
 
+// ------------------------------------------------------- rotated A bundle
+// Copy of a high-half bundle in which each segment j >= tb stores entry y at
+// ((y mod 2^{j-tb}) << tb) | (y >> (j - tb)): the top tb bits of y become the
+// bottom ones, so the entries a dense tile reads together (its t values, the
+// top bits of y) are adjacent.  Segments j < tb are copied as they are.
+__global__ void k_rotate_bundle(const uint16_t* __restrict__ src, int64_t rows, int stride, int mmax, int tb,
+                                uint16_t* __restrict__ dst) {
+    const int64_t total = rows * stride;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = e / stride;
+        const int i = (int)(e % stride);
+        uint32_t dpos = (uint32_t)i;
+        if (i >= 1) {
+            const int j = 31 - __clz(i);  // segment: 2^j <= i < 2^{j+1}
+            const uint32_t y = (uint32_t)i - (1u << j);
+            if (j <= mmax && j >= tb) {
+                const int lo = j - tb;
+                dpos = (1u << j) + (((y & ((1u << lo) - 1u)) << tb) | (y >> lo));
+            }
+        }
+        dst[row * stride + dpos] = src[e];
+    }
+}
+
+cudaError_t launch_rotate_bundle(const HalfTables& A, int tb, uint16_t* dst, cudaStream_t stream) {
+    const int64_t total = ((int64_t)A.stride) << A.h;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_rotate_bundle<<<(int)blocks, 256, 0, stream>>>(A.rows, (int64_t)1 << A.h, A.stride, A.mmax, tb, dst);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------ dispatch
 // (TB, BB) per output length K: 16 words per thread for K >= 4.
 // (TB, BB) per output length K: 16 words per thread for 4 <= K <= 12, and
@@ -490,6 +561,15 @@ static cudaError_t launch_dpass_k(const CountLaunch& L, const double* lnq, const
 int count_group_size(int k) {
     switch (k) {
 #define C_(K) case K: return Tile<K, TileChoice<K>::TB, TileChoice<K>::BB>::GROUP;
+        BDC_K_CASES(C_)
+#undef C_
+        default: return 0;
+    }
+}
+
+int count_tile_tb(int k) {
+    switch (k) {
+#define C_(K) case K: return TileChoice<K>::TB;
         BDC_K_CASES(C_)
 #undef C_
         default: return 0;

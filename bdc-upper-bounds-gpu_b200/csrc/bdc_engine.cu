@@ -103,7 +103,7 @@ int select_engine(int requested, int n, int k) {
 CountLaunch count_launch(const bdc_handle* H) {
     CountLaunch L;
     L.s = H->s;
-    L.A = H->A;
+    L.A = H->Ar;
     L.B = H->B;
     L.reps = H->d_reps;
     L.R = H->R;
@@ -133,7 +133,7 @@ bdc_status engine_init(bdc_handle* H) {
     // assert, backend/BAA.cu:31-44, which vanishes under NDEBUG)
     const int mA = mmax_for_high(s), mB = mmax_for_low(s);
     size_t need = 0;
-    need += ((size_t)bundle_stride(mA) << s.n1) * 2;
+    need += ((size_t)bundle_stride(mA) << s.n1) * 2 * 2;  // and its rotated copy
     if (s.n2 != s.n1) need += ((size_t)bundle_stride(mB) << s.n2) * 2;
     need += (size_t)R * (4 + 8 * 5);
     size_t free_b = 0, total_b = 0;
@@ -177,6 +177,17 @@ bdc_status engine_init(bdc_handle* H) {
         if (rc != BDC_OK) return rc;
         H->A = HalfTables{H->d_bundle_hi, s.n1, mA, strideA};
         H->B = HalfTables{H->d_bundle_lo, s.n2, mB, strideB};
+    }
+
+    // the A bundle rotated for the count passes (their tiles read 2^TB
+    // entries of one row at once)
+    {
+        const size_t cnt = ((size_t)H->A.stride) << H->A.h;
+        BDC_CUDA_TRY(cudaMalloc(&H->d_bundle_rot, cnt * sizeof(uint16_t)));
+        H->bytes += cnt * sizeof(uint16_t);
+        BDC_CUDA_TRY(launch_rotate_bundle(H->A, count_tile_tb(H->k), H->d_bundle_rot, H->stream));
+        H->Ar = H->A;
+        H->Ar.rows = H->d_bundle_rot;
     }
 
     // per-representative vectors and reductions
@@ -247,6 +258,7 @@ void engine_free(bdc_handle* H) {
     cudaFree(H->d_reps);
     if (H->d_bundle_lo && H->d_bundle_lo != H->d_bundle_hi) cudaFree(H->d_bundle_lo);
     cudaFree(H->d_bundle_hi);
+    cudaFree(H->d_bundle_rot);
     for (int b = 0; b < 2; ++b) cudaFree(H->d_p[b]);
     cudaFree(H->d_h);
     cudaFree(H->d_d);

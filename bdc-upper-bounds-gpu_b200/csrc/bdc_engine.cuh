@@ -30,6 +30,8 @@ struct bdc_handle {
     uint16_t* d_bundle_hi = nullptr;
     uint16_t* d_bundle_lo = nullptr;  // equal to d_bundle_hi when n is even
     bdc::HalfTables A{}, B{};
+    uint16_t* d_bundle_rot = nullptr;  // the A bundle rotated for the count passes' vector loads
+    bdc::HalfTables Ar{};
     // per-representative vectors
     double* d_p[2] = {nullptr, nullptr};
     double* d_h = nullptr;     // sum_y W ln W

@@ -7,7 +7,8 @@ namespace bdc {
 
 struct CountLaunch {
     Split s;
-    HalfTables A;             // cache_{n1, j} bundles, rows indexed by x_hi
+    HalfTables A;             // cache_{n1, j} bundles, rows indexed by x_hi, stored rotated
+                              // (launch_rotate_bundle with count_tile_tb(k))
     HalfTables B;             // cache_{n2, m} bundles, rows indexed by x_lo
     const uint32_t* reps;     // canonical representatives, ascending
     int64_t R;
@@ -19,6 +20,9 @@ struct CountLaunch {
 // ---- count path (bdc_count.cu)
 int count_cta_threads(int k);
 int count_ctas_per_sm(int k);  // CTAs per SM in the grid of the q / D passes
+int count_tile_tb(int k);      // top bits of y per thread tile (the rotation of the A bundle)
+// the A bundle with each segment j >= tb rotated so that a tile's entries are adjacent
+cudaError_t launch_rotate_bundle(const HalfTables& A, int tb, uint16_t* dst, cudaStream_t stream);
 cudaError_t launch_count_pairs(const Split& s, const HalfTables& A, const HalfTables& B,
                                const uint32_t* xs, const uint32_t* ys, int64_t npairs,
                                uint32_t* out, cudaStream_t stream);
