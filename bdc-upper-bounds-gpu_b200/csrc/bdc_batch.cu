@@ -284,6 +284,11 @@ bdc_status bdc_batch_accelerate(bdc_batch_t B, int64_t max_evals, double gap_bit
             return fail(BDC_ERR_UNSUPPORTED, "bdc_batch_accelerate: every instance needs the factored engine");
     }
     const double eta = factored_acc_eta();
+    // a target below the support switch: the batched momentum phase runs to
+    // the switch, then each instance's support phases finish (n <= 26)
+    bool support = gap_bits > 0.0 && gap_bits < kSupportSwitchBits;
+    for (auto* H : B->hs) support = support && H->n <= 26;
+    const double phase_gap = support ? kSupportSwitchBits : gap_bits;
     std::vector<long long> it0(N);
     std::vector<double> sec(N, -1.0);
     std::vector<char> fin(N, 0);
@@ -307,7 +312,7 @@ bdc_status bdc_batch_accelerate(bdc_batch_t B, int64_t max_evals, double gap_bit
         if (ce != cudaSuccess) rc = fail(BDC_ERR_CUDA, "bdc_batch_accelerate: %s", cudaGetErrorString(ce));
         it0[i] = H->h_st->iter;
         if (rc == BDC_OK && H->h_st->iter == 0 && max_evals > 0) rc = factored_iterate(H, 1, -INFINITY, nullptr);
-        if (rc == BDC_OK) rc = factored_acc_start(H, gap_bits);
+        if (rc == BDC_OK) rc = factored_acc_start(H, phase_gap);
         H->stream = keep;
         if (rc != BDC_OK) return rc;
     }
@@ -349,15 +354,48 @@ bdc_status bdc_batch_accelerate(bdc_batch_t B, int64_t max_evals, double gap_bit
                 BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, B->launch));
                 BDC_CUDA_TRY(cudaStreamSynchronize(B->launch));
             }
-            if (!fin[i] && sec[i] < 0 && (H->h_st->best_ub - H->h_st->best_rate) / ln2 < gap_bits) sec[i] = ms * 1e-3;
+            if (!fin[i] && sec[i] < 0 && (H->h_st->best_ub - H->h_st->best_rate) / ln2 < phase_gap) sec[i] = ms * 1e-3;
         }
     }
     for (auto* H : B->hs) BDC_CUDA_TRY(cudaMemsetAsync(&H->d_st->done, 0, sizeof(int), B->launch));
     BDC_CUDA_TRY(cudaStreamSynchronize(B->launch));
+    // the support phases, instance by instance on the launch stream; an
+    // instance's time is its momentum phase in the batch plus its own
+    // support phases
+    std::vector<bdc_stats> sup(N);
+    std::vector<char> used_sup(N, 0);
+    std::vector<long long> mom(N);
+    for (size_t i = 0; i < N; ++i) mom[i] = B->hs[i]->h_st->iter - it0[i];  // momentum-phase evaluations
+    if (support) {
+        for (size_t i = 0; i < N; ++i) {
+            bdc_handle* H = B->hs[i];
+            if (sec[i] < 0) continue;  // the momentum phase did not reach the switch
+            cudaStream_t keep = H->stream;
+            H->stream = B->launch;
+            BDC_CUDA_TRY(cudaEventRecord(e0, B->launch));
+            bdc_status r2 = solve_impl(H, gap_bits, max_evals, &sup[i], 2);
+            BDC_CUDA_TRY(cudaEventRecord(e1, B->launch));
+            H->stream = keep;
+            if (r2 != BDC_OK) return r2;
+            BDC_CUDA_TRY(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            BDC_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+            used_sup[i] = 1;
+            sec[i] = sup[i].converged ? sec[i] + ms * 1e-3 : -1.0;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     for (size_t i = 0; i < N; ++i) {
         const DevState* s = B->hs[i]->h_st;
+        if (used_sup[i]) {
+            if (stats) {
+                stats[i] = sup[i];
+                stats[i].iters += mom[i];  // the batched momentum evaluations too
+            }
+            if (seconds) seconds[i] = sec[i];
+            continue;
+        }
         if (stats) {
             bdc_stats& o = stats[i];
             o.iters = s->iter - it0[i];

@@ -230,6 +230,11 @@ bdc_status bdc_accelerate(bdc_handle_t H, int64_t max_evals, double gap_bits, bd
         return fail(BDC_ERR_UNSUPPORTED, "bdc_accelerate: needs the factored engine (k < n)");
     if (max_evals < 0) return fail(BDC_ERR_ARG, "bdc_accelerate: max_evals < 0");
     BDC_CUDA_TRY(cudaSetDevice(H->device));
+    // a target below the support switch: the momentum phase, then the
+    // support phases (restricted BA, Newton on the support, the full-space
+    // check) finish, as in the certified solver (counts exact in FP32: n <= 26)
+    if (gap_bits > 0.0 && gap_bits < kSupportSwitchBits && H->n <= 26 && max_evals > 0)
+        return solve_impl(H, gap_bits, max_evals, stats, 1);
     return factored_accelerate(H, max_evals, gap_bits, stats);
 }
 

@@ -90,6 +90,12 @@ bdc_status factored_shard_q(bdc_handle* H, double* acc);
 bdc_status factored_shard_d(bdc_handle* H, const double* acc, double* part5);
 bdc_status factored_shard_finish(bdc_handle* H, const double* part5, double a);
 
+// the certified solver (bdc_solve.cu) with its first phase chosen: 0 Anderson
+// (bdc_solve), 1 the momentum loop (bdc_accelerate), 2 none (the handle's
+// iterate is already near the optimum: support phases only)
+constexpr double kSupportSwitchBits = 1e-4;  // bracket at which the support phases take over
+bdc_status solve_impl(bdc_handle* H, double gap_bits, int64_t max_evals, bdc_stats* stats, int phase1);
+
 // frees the certified solver's scratch blocks (bdc_solve.cu)
 void solve_pool_release(bdc_handle* H);
 

@@ -2238,6 +2238,7 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
                     if ((e = cudaEventRecord(F->ev_join[cl], F->side[cl])) != cudaSuccess) return e;
                     if ((e = cudaStreamWaitEvent(s, F->ev_join[cl], 0)) != cudaSuccess) return e;
                 }
+                if (F->use_oz) return ozaki_prepare(F->oz, H->d_st, s);
                 break;
             }
             for (int lg = 0; lg < 8; ++lg) {
@@ -2250,9 +2251,10 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
                 if ((e = cudaEventRecord(F->ev_join[lg], F->side[lg])) != cudaSuccess) return e;
                 if ((e = cudaStreamWaitEvent(s, F->ev_join[lg], 0)) != cudaSuccess) return e;
             }
+            if (F->use_oz) return ozaki_prepare(F->oz, H->d_st, s);
             break;
         case ST_G:
-            if (F->use_oz) return ozaki_enqueue(F->oz, make_epilogue(H), H->d_st, s);
+            if (F->use_oz) return ozaki_product(F->oz, make_epilogue(H), H->d_st, s);
             return launch_ba(F->g, make_epilogue(H), s, H->d_st);
         case ST_FIN:
             k_fac_finalize<<<1, 256, 0, s>>>(F->epart, F->use_oz ? ozaki_partials(F->oz) : F->ctas_g, a, F->eta, H->d_st);

@@ -928,7 +928,7 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, Ozak
     return BDC_OK;
 }
 
-cudaError_t ozaki_enqueue(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaStream_t s) {
+cudaError_t ozaki_prepare(OzakiG* oz, DevState* st, cudaStream_t s) {
     const OzakiInput& in = oz->in;
     k_oz_maxabs<<<oz->nmax, 256, 0, s>>>(in.RB, (int64_t)in.KL * in.H2, in.LA, in.Kp, in.KL, in.KR, in.H1h, oz->mpart,
                                          st);
@@ -940,6 +940,11 @@ cudaError_t ozaki_enqueue(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaSt
     }
     k_oz_slice_b<<<(in.H2 + 31) / 32, 256, sizeof(double) * oz->KLp * 33, s>>>(in.RB, in.KL, in.H2, oz->KLp, oz->Bd,
                                                                               oz->d_e, st);
+    return cudaGetLastError();
+}
+
+cudaError_t ozaki_product(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaStream_t s) {
+    const OzakiInput& in = oz->in;
     if (oz->persistent) {
         if (oz->tilesP == 0) return cudaGetLastError();
         const OzGeomDev gp{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_nP};

@@ -69,9 +69,11 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, Ozak
 // rows of block partials the product writes (the finalize's count)
 int ozaki_partials(const OzakiG* oz);
 void ozaki_free(OzakiG* oz);
-// one G product with the fused BA update, queued on s: the exponent, the
-// slices of ML and NR, then the tensor-core product and epilogue; block
-// partials as the FP64 product writes them (ep.part, one row of 8 per tile)
-cudaError_t ozaki_enqueue(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaStream_t s);
+// the operands of one G product, queued on s once ML and NR are final: the
+// exponent of the FP64 operands and their int8 slices
+cudaError_t ozaki_prepare(OzakiG* oz, DevState* st, cudaStream_t s);
+// the tensor-core product with the fused BA update; block partials as the
+// FP64 product writes them (ep.part, one row of 8 per tile or per CTA)
+cudaError_t ozaki_product(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaStream_t s);
 
 }  // namespace bdc

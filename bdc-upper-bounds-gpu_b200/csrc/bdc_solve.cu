@@ -1328,7 +1328,16 @@ static bdc_status accelerated_ba(bdc_handle* H, Anderson& aa, const uint8_t* w, 
 
 using namespace bdc;
 
-extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_evals, bdc_stats* stats) {
+namespace bdc {
+
+// The solver with a choice of its first phase: SOLVE_ANDERSON (bdc_solve),
+// SOLVE_MOMENTUM (the accelerated loop of factored_accelerate, run on the
+// handle's own iterate to the switch bracket) or SOLVE_FROM_POINT (the caller
+// has brought the handle's iterate near the optimum already: only the
+// support phases run, starting from the best bounds the handle has seen).
+enum SolvePhase1 { SOLVE_ANDERSON = 0, SOLVE_MOMENTUM = 1, SOLVE_FROM_POINT = 2 };
+
+bdc_status solve_impl(bdc_handle_t H, double gap_bits, int64_t max_evals, bdc_stats* stats, int phase1) {
     if (!H) return fail(BDC_ERR_ARG, "bdc_solve: NULL handle");
     if (!H->p_set) return fail(BDC_ERR_STATE, "bdc_solve: no distribution set");
     if (H->engine != BDC_ENGINE_FACTORED) return fail(BDC_ERR_UNSUPPORTED, "bdc_solve: needs the factored engine (k < n)");
@@ -1346,9 +1355,28 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
     const auto t_start = std::chrono::steady_clock::now();
     auto elapsed = [&] { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count(); };
 
+    Bracket br;
+    int64_t evals = 0;
+    const double switch_bits = std::max(gap_bits, kSupportSwitchBits);
+    bdc_status rc = BDC_OK;
+    if (phase1 == SOLVE_MOMENTUM) {
+        // the momentum phase on the handle's dense state, then its point
+        bdc_stats s1{};
+        rc = factored_accelerate(H, max_evals, switch_bits, &s1);
+        if (rc != BDC_OK) return rc;
+        evals += s1.iters;
+    }
+    if (phase1 != SOLVE_ANDERSON) {
+        BDC_CUDA_TRY(cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+        BDC_CUDA_TRY(cudaStreamSynchronize(s));
+        br.add(H->h_st->best_ub, H->h_st->best_rate);
+        if (H->verbose)
+            printf("bdc: solve phase 1 (momentum): %lld full evaluations, gap %.3e bits (%.3f s)\n", (long long)evals,
+                   br.gap_bits(), elapsed());
+    }
     // start: the handle's current iterate
     const double* cur = nullptr;
-    bdc_status rc = engine_current_p(H, &cur);
+    rc = engine_current_p(H, &cur);
     if (rc != BDC_OK) return rc;
     DevBuf x, g, xa, ga, D, wts, in_s, cnt, sel, mpart;
     BDC_CUDA_TRY(dalloc(x, sizeof(double) * R));
@@ -1367,8 +1395,6 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
     BDC_CUDA_TRY(cudaMemsetAsync(in_s.p, 0, R, s));
     BDC_CUDA_TRY(cudaGetLastError());
 
-    Bracket br;
-    int64_t evals = 0;
     auto full_map = [&](const double* pin, double* pout, double* u, double* r) -> bdc_status {
         bdc_status e = factored_map(H, pin, pout, nullptr);
         *u = H->h_st->max_d;
@@ -1376,15 +1402,14 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
         return e;
     };
     // ---- phase 1
-    const double switch_bits = std::max(gap_bits, 1e-4);
-    {
+    if (phase1 == SOLVE_ANDERSON) {
         Anderson aa;
         BDC_CUDA_TRY(aa.init(R, 8, sms));
         rc = accelerated_ba(H, aa, wts.get<uint8_t>(), full_map, x.get<double>(), g.get<double>(), xa.get<double>(),
                             ga.get<double>(), R, switch_bits, max_evals, br, &evals);
         if (rc != BDC_OK) return rc;
     }
-    if (H->verbose)
+    if (H->verbose && phase1 == SOLVE_ANDERSON)
         printf("bdc: solve phase 1: %lld full evaluations, gap %.3e bits (%.3f s)\n", (long long)evals, br.gap_bits(),
                elapsed());
 
@@ -1540,6 +1565,12 @@ extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_eva
     }
     (void)certified;
     return BDC_OK;
+}
+
+}  // namespace bdc
+
+extern "C" bdc_status bdc_solve(bdc_handle_t H, double gap_bits, int64_t max_evals, bdc_stats* stats) {
+    return solve_impl(H, gap_bits, max_evals, stats, SOLVE_ANDERSON);
 }
 
 namespace bdc {

@@ -127,8 +127,14 @@ bdc_status bdc_bound_error(bdc_handle_t h, double* upper_bound_err_bits, double*
  * kernels).  Every evaluated point gives a valid bracket, so best_rate <= C
  * <= best_upper_bound holds throughout.  Runs until best_upper_bound -
  * best_rate < gap_bits or max_evals evaluations; stats->iters = evaluations.
- * The handle's iterate is left at the last step's point.  Factored engine
- * only; BDC_ACCEL_STEP overrides eta (0 < eta <= 4). */
+ * With 0 < gap_bits < 1e-4 (and n <= 26) the momentum phase stops at a
+ * 1e-4-bit bracket and the support phases of bdc_solve finish: BA
+ * restricted to the inputs that can carry mass, Newton on that support, and
+ * a full-space evaluation proving that no other input can (the momentum
+ * phase alone converges sublinearly on the small-mass members of the
+ * support).  gap_bits <= 0 runs the momentum loop for max_evals.  The
+ * handle's iterate is left at the final point.  Factored engine only;
+ * BDC_ACCEL_STEP overrides eta (0 < eta <= 4). */
 bdc_status bdc_accelerate(bdc_handle_t h, int64_t max_evals, double gap_bits, bdc_stats* stats);
 
 /* The mutual-information functional and its adjoint (no counterpart in the
@@ -225,7 +231,10 @@ bdc_status bdc_batch_set_stream(bdc_batch_t batch, void* stream);
  * gap_bits) or after max_evals evaluations.  seconds (may be NULL) receives
  * per instance the device time from the start of the call until its bracket
  * fell below gap_bits (CUDA events on the launch stream, resolution one graph
- * replay), -1 when it did not. */
+ * replay), -1 when it did not.  With 0 < gap_bits < 1e-4 the batched
+ * momentum phase runs to a 1e-4-bit bracket and then each instance's support
+ * phases finish it, one instance after another; its time is then its
+ * momentum phase in the batch plus its own support phases. */
 bdc_status bdc_batch_accelerate(bdc_batch_t batch, int64_t max_evals, double gap_bits, bdc_stats* stats,
                                 double* seconds);
 
