@@ -119,6 +119,7 @@ struct OzGeomDev {
     int aS, bS, aD, bD;  // atom columns
     int M, N;            // rows (H1h) and columns (H2) of G
     int tiles_n;
+    int stages;          // ring depth of the per-weight operands (persistent form; <= kOzStages)
 };
 
 __global__ void __launch_bounds__(kOzThreads, 1)
@@ -349,19 +350,34 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
 
 // ------------------------------------------- the persistent, overlapped form
 // One CTA per SM loops over 128 x 32 tiles.  Two TMEM buffers of eight
-// 32-column accumulators (2 x 256 = 512 columns): while warps 2-5 drain and
+// 32-column accumulators (2 x 256 = 512 columns): while warps 2-9 drain and
 // finish tile i from one buffer, warp 1 issues tile i + 1's MMAs into the
 // other.  The static operands of a tile are double-buffered, the per-weight
-// slices go through a ring of kOzStages stages that continues across tiles.
+// slices go through a ring of g.stages stages that continues across tiles.
 // Barriers: sfull/sempty (static operands), full/empty (ring), tfull/tempty
 // (TMEM buffers; tempty takes one arrival per epilogue warp).
+//
+// The epilogue streams three vectors of the iterate (h, Pw, Lt: 40 bytes per
+// representative), so it is bound by memory, and a CTA is alone on its SM:
+// eight epilogue warps (two per TMEM lane quadrant, splitting the columns)
+// drain the accumulators into an FP64 tile in shared memory, then walk it
+// row by row with the lanes along the columns (coalesced), issuing the loads
+// of eight elements before computing them.
 constexpr int kOzPBN = 32;
-constexpr int kOzPThreads = 192;
-constexpr int kOzPBuf = kOzW * kOzPBN;  // TMEM columns of one buffer
+constexpr int kOzPEpiWarps = 8;
+constexpr int kOzPThreads = 64 + 32 * kOzPEpiWarps;  // producer, MMA, epilogue warps
+constexpr int kOzPBuf = kOzW * kOzPBN;               // TMEM columns of one buffer
+constexpr int kOzPTileLd = kOzPBN + 1;                // row pitch of the FP64 tile in shared memory
+constexpr int kOzPTileBytes = kOzBM * kOzPTileLd * 8;
 static_assert(2 * kOzPBuf <= 512, "two accumulator buffers exceed tensor memory");
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// barrier 1 among the epilogue warps only
+__device__ __forceinline__ void epi_sync() {
+    asm volatile("bar.sync 1, %0;" ::"r"(32 * kOzPEpiWarps) : "memory");
 }
 
 __global__ void __launch_bounds__(kOzPThreads, 1)
@@ -378,6 +394,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
     if (skip_sh) return;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int NS = g.stages;
     const int nmine = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
     uint8_t* base = (uint8_t*)(((uintptr_t)ozp_smem_raw + 1023) & ~(uintptr_t)1023);
     const uint32_t sA0 = sm_addr(base);
@@ -386,15 +403,16 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
     const uint32_t ring0 = sB0 + 2 * bytesB;
     const uint32_t stageA = (uint32_t)g.aD * kOzBM * 128, stageB = (uint32_t)g.bD * kOzPBN * 128;
     const uint32_t stageBytes = stageA + stageB;
+    double* gt = (double*)(base + (ring0 - sA0) + (size_t)NS * stageBytes);  // [kOzBM][kOzPTileLd]
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < 2; ++i) {
             mbar_init(sm_addr(&sfull[i]), 1);
             mbar_init(sm_addr(&sempty[i]), 1);
             mbar_init(sm_addr(&tfull[i]), 1);
-            mbar_init(sm_addr(&tempty[i]), 4);
+            mbar_init(sm_addr(&tempty[i]), kOzPEpiWarps);
         }
-        for (int i = 0; i < kOzStages; ++i) {
+        for (int i = 0; i < NS; ++i) {
             mbar_init(sm_addr(&full[i]), 1);
             mbar_init(sm_addr(&empty[i]), 1);
         }
@@ -440,7 +458,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
                 last_static[sb] = it >> 1;
                 bool ok = true;
                 for (int a = 0; a < kOzW; ++a, ++wc) {
-                    const int s = wc % kOzStages, use = wc / kOzStages;
+                    const int s = wc % NS, use = wc / NS;
                     if (use > 0 && !mbar_wait(sm_addr(&empty[s]), (use - 1) & 1)) {
                         ok = false;
                         break;
@@ -478,7 +496,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
                 const uint32_t sA = sA0 + sb * bytesA, sB = sB0 + sb * bytesB;
                 bool ok = true;
                 for (int a = 0; a < kOzW; ++a, ++wc) {
-                    const int s = wc % kOzStages, use = wc / kOzStages;
+                    const int s = wc % NS, use = wc / NS;
                     if (!mbar_wait(sm_addr(&full[s]), use & 1) || aborted()) {
                         ok = false;
                         break;
@@ -512,69 +530,90 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
         }
         __syncwarp();
     } else {
-        // ---- epilogue warps: TMEM lanes 32 (warp % 4) .. + 31 = tile rows
+        // ---- epilogue warps: quadrant q of the TMEM lanes, half of the columns
         const int q = warp & 3;
-        const int r = q * 32 + lane;
+        const int half = (warp - 2) >> 2;
+        const int r = q * 32 + lane;          // the tile row this thread drains
+        const int et = threadIdx.x - 64;      // 0 .. 255 in the coalesced pass
         const double shift = st->shift;
         const double lnz = st->log_z;
         const double inv_z = exp(-lnz);
         const int e = *d_e;
         for (int it = 0; it < nmine; ++it) {
             const int tb = it & 1;
-            if (!mbar_wait(sm_addr(&tfull[tb]), (it >> 1) & 1) || aborted()) {
-                give_up();
-                break;
-            }
+            const bool got = mbar_wait(sm_addr(&tfull[tb]), (it >> 1) & 1) && !aborted();
+            if (!got) give_up();
             tc_fence_after();
-            const int t = tiles[blockIdx.x + it * gridDim.x];
-            const int m = (t / g.tiles_n) * kOzBM + r, n0 = (t % g.tiles_n) * kOzPBN;
-            const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tb * kOzPBuf);
-            double gsum[kOzPBN];
+            constexpr int HC = kOzPBN / 2;  // columns per half
+            double gsum[HC];
 #pragma unroll
-            for (int j = 0; j < kOzPBN; ++j) gsum[j] = 0.0;
+            for (int j = 0; j < HC; ++j) gsum[j] = 0.0;
+            if (got) {
+                const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tb * kOzPBuf + half * HC);
 #pragma unroll 1
-            for (int a = kOzW - 1; a >= 0; --a) {
-                const double w = ldexp(1.0, e - 7 * a);
-#pragma unroll
-                for (int c0 = 0; c0 < kOzPBN; c0 += 16) {
+                for (int a = kOzW - 1; a >= 0; --a) {
+                    const double w = ldexp(1.0, e - 7 * a);
                     uint32_t v[16];
-                    tmem_ld16(trow + (uint32_t)(a * kOzPBN + c0), v);
+                    tmem_ld16(trow + (uint32_t)(a * kOzPBN), v);
                     tmem_wait_ld();
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) gsum[c0 + j] = fma((double)(int32_t)v[j], w, gsum[c0 + j]);
+                    for (int j = 0; j < HC; ++j) gsum[j] = fma((double)(int32_t)v[j], w, gsum[j]);
                 }
             }
-            // the buffer is free for the tile after next
+            // the TMEM buffer is free for the tile after next
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(sm_addr(&tempty[tb]));
-            if (m >= g.M) continue;
+            epi_sync();  // the previous tile's pass is done with the shared tile
+            if (aborted()) break;  // uniform: read after the barrier
 #pragma unroll
-            for (int j = 0; j < kOzPBN; ++j) {
-                const int n = n0 + j;
-                if (n >= g.N) continue;
-                const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
-                const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);  // the global dense index
-                const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
-                if (!is_rep(x, ep.n)) continue;
-                const double o = (double)orbit_size(x, ep.n);
-                const double D = __ldg(ep.hx + xd) - gsum[j] * ep.inv_c;
-                if (ep.Dout) ep.Dout[xd] = D;
-                // exact zeros of the caller's distribution (Lt = NaN) take ln p = 0
-                // (backend/BAA.cu:573-580)
-                const double pw = ep.Pw[xd];
-                const double lt = ep.Lt[xd];
-                const bool zero_in = (lt != lt);
-                const double lnp = zero_in ? 0.0 : lt - lnz;
-                const double lw = lnp + ep.eta * D - shift;
-                const double ex = exp(lw);
-                ep.Lt[xd] = lw;
-                ep.Pw[xd] = o * ex;
-                mD = fmax(mD, D);
-                mL = fmax(mL, lw);
-                sE = fma(o, ex, sE);
-                sR = fma(pw * inv_z, D, sR);
-                if (zero_in) zero = 1.0;
+            for (int j = 0; j < HC; ++j) gt[r * kOzPTileLd + half * HC + j] = gsum[j];
+            epi_sync();
+            // coalesced pass: element (row, col) = (i / 32, lane), 16 per thread
+            const int t = tiles[blockIdx.x + it * gridDim.x];
+            const int m0 = (t / g.tiles_n) * kOzBM, n = (t % g.tiles_n) * kOzPBN + lane;
+#pragma unroll 1
+            for (int i0 = 0; i0 < kOzBM * kOzPBN / (32 * kOzPEpiWarps); i0 += 8) {
+                uint32_t xdv[8];
+                bool rep[8];
+                double hv[8], pwv[8], ltv[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int row = (et >> 5) + (i0 + u) * kOzPEpiWarps;
+                    const int m = m0 + row;
+                    const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
+                    const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);
+                    const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
+                    rep[u] = (m < g.M) && (n < g.N) && is_rep(x, ep.n);
+                    xdv[u] = xd;
+                    hv[u] = rep[u] ? __ldg(ep.hx + xd) : 0.0;
+                    pwv[u] = rep[u] ? ep.Pw[xd] : 0.0;
+                    ltv[u] = rep[u] ? ep.Lt[xd] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (!rep[u]) continue;
+                    const int row = (et >> 5) + (i0 + u) * kOzPEpiWarps;
+                    const uint32_t xd = xdv[u];
+                    const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);
+                    const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
+                    const double o = (double)orbit_size(x, ep.n);
+                    const double D = hv[u] - gt[row * kOzPTileLd + lane] * ep.inv_c;
+                    if (ep.Dout) ep.Dout[xd] = D;
+                    // exact zeros of the caller's distribution (Lt = NaN) take ln p = 0
+                    // (backend/BAA.cu:573-580)
+                    const bool zero_in = (ltv[u] != ltv[u]);
+                    const double lnp = zero_in ? 0.0 : ltv[u] - lnz;
+                    const double lw = lnp + ep.eta * D - shift;
+                    const double ex = exp(lw);
+                    ep.Lt[xd] = lw;
+                    ep.Pw[xd] = o * ex;
+                    mD = fmax(mD, D);
+                    mL = fmax(mL, lw);
+                    sE = fma(o, ex, sE);
+                    sR = fma(pwv[u] * inv_z, D, sR);
+                    if (zero_in) zero = 1.0;
+                }
             }
         }
     }
@@ -620,7 +659,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
         p[4] = a4;
     }
     if (!ran && warp == 0 && lane == 0) {
-        for (int s = 0; s < kOzStages; ++s)
+        for (int s = 0; s < NS; ++s)
             if (last_use[s] >= 0) (void)mbar_wait(sm_addr(&full[s]), last_use[s] & 1);
         for (int b = 0; b < 2; ++b)
             if (last_static[b] >= 0) (void)mbar_wait(sm_addr(&sfull[b]), last_static[b] & 1);
@@ -849,11 +888,15 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, Ozak
     oz->aD = (2 * KRp + 127) / 128;
     oz->bD = (2 * KLp + 127) / 128;
     oz->smem = 1024 + (oz->aS * kOzBM + oz->bS * kOzBN) * 128 + kOzStages * (oz->aD * kOzBM + oz->bD * kOzBN) * 128;
-    oz->smemP = 1024 + 2 * (oz->aS * kOzBM + oz->bS * kOzPBN) * 128 +
-                kOzStages * (oz->aD * kOzBM + oz->bD * kOzPBN) * 128;
     oz->persistent = persistent;
     int dev_smem = 0;
     BDC_CUDA_TRY(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, H->device));
+    // the persistent form: the deepest ring (<= kOzStages) that fits with the FP64 tile
+    for (oz->stagesP = kOzStages; oz->stagesP >= 2; --oz->stagesP) {
+        oz->smemP = 1024 + 2 * (oz->aS * kOzBM + oz->bS * kOzPBN) * 128 +
+                    oz->stagesP * (oz->aD * kOzBM + oz->bD * kOzPBN) * 128 + kOzPTileBytes;
+        if (oz->smemP + 2048 <= dev_smem) break;
+    }
     if ((persistent ? oz->smemP : oz->smem) + 2048 > dev_smem) {
         ozaki_free(oz);
         *why = "tile operands exceed shared memory";
@@ -947,13 +990,13 @@ cudaError_t ozaki_product(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaSt
     const OzakiInput& in = oz->in;
     if (oz->persistent) {
         if (oz->tilesP == 0) return cudaGetLastError();
-        const OzGeomDev gp{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_nP};
+        const OzGeomDev gp{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_nP, oz->stagesP};
         k_oz_ba_p<<<oz->gridP, kOzPThreads, oz->smemP, s>>>(oz->tmAs, oz->tmBsP, oz->tmAd, oz->tmBdP, gp,
                                                            oz->d_tilesP, oz->tilesP, oz->d_e, ep, st);
         return cudaGetLastError();
     }
     if (oz->tiles == 0) return cudaGetLastError();
-    const OzGeomDev g{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_n};
+    const OzGeomDev g{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_n, kOzStages};
     k_oz_ba<<<oz->tiles, kOzThreads, oz->smem, s>>>(oz->tmAs, oz->tmBs, oz->tmAd, oz->tmBd, g, oz->d_tiles, oz->d_e,
                                                     ep, st);
     return cudaGetLastError();

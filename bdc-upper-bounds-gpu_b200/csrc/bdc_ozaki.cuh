@@ -56,7 +56,7 @@ struct OzakiG {
     CUtensorMap tmAs, tmBs, tmAd, tmBd;
     // the persistent form: 128 x 32 tiles, one CTA per SM, two TMEM buffers
     bool persistent = false;
-    int smemP = 0, gridP = 0;
+    int smemP = 0, gridP = 0, stagesP = 0;
     int* d_tilesP = nullptr;
     int tilesP = 0, tiles_nP = 0;
     CUtensorMap tmBsP, tmBdP;
