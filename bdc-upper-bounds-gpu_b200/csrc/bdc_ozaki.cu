@@ -693,10 +693,20 @@ __global__ void __launch_bounds__(256) k_oz_maxabs(const double* __restrict__ RB
 }
 
 // e with max |X| < 2^e (frexp); a non-finite operand is a device error
-__global__ void k_oz_exponent(const double* __restrict__ part, int nb, int* __restrict__ e_out, DevState* st) {
-    if (threadIdx.x != 0 || st->done || st->error) return;
+__global__ void __launch_bounds__(256) k_oz_exponent(const double* __restrict__ part, int nb, int* __restrict__ e_out,
+                                                     DevState* st) {
+    if (st->done || st->error) return;
     double m = 0.0;
-    for (int b = 0; b < nb; ++b) m = fmax(m, part[b]);
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) m = fmax(m, part[b]);
+    __shared__ double red[256];
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    m = red[0];
     if (!isfinite(m)) {
         st->error = kErrOzakiOperand;
         return;
@@ -975,7 +985,7 @@ cudaError_t ozaki_prepare(OzakiG* oz, DevState* st, cudaStream_t s) {
     const OzakiInput& in = oz->in;
     k_oz_maxabs<<<oz->nmax, 256, 0, s>>>(in.RB, (int64_t)in.KL * in.H2, in.LA, in.Kp, in.KL, in.KR, in.H1h, oz->mpart,
                                          st);
-    k_oz_exponent<<<1, 32, 0, s>>>(oz->mpart, oz->nmax, oz->d_e, st);
+    k_oz_exponent<<<1, 256, 0, s>>>(oz->mpart, oz->nmax, oz->d_e, st);
     {
         const int64_t work = (int64_t)in.H1h * (oz->KRp / 16);
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 148 * 8));
