@@ -57,9 +57,32 @@ struct Tile {
 
 // N consecutive uint16 entries (N <= 8) from an address aligned to 2N bytes,
 // in one load
-template <int N>
+template <int N, bool SH = false>
 __device__ __forceinline__ void ld_u16(const uint16_t* __restrict__ p, uint32_t (&o)[N]) {
-    if constexpr (N == 8) {
+    if constexpr (SH) {
+        // a row staged in shared memory
+        if constexpr (N == 8) {
+            const uint4 v = *(const uint4*)p;
+            const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                o[2 * i] = w[i] & 0xFFFFu;
+                o[2 * i + 1] = w[i] >> 16;
+            }
+        } else if constexpr (N == 4) {
+            const uint2 v = *(const uint2*)p;
+            o[0] = v.x & 0xFFFFu;
+            o[1] = v.x >> 16;
+            o[2] = v.y & 0xFFFFu;
+            o[3] = v.y >> 16;
+        } else if constexpr (N == 2) {
+            const uint32_t v = *(const uint32_t*)p;
+            o[0] = v & 0xFFFFu;
+            o[1] = v >> 16;
+        } else {
+            o[0] = *p;
+        }
+    } else if constexpr (N == 8) {
         const uint4 v = __ldg((const uint4*)p);
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
@@ -83,7 +106,7 @@ __device__ __forceinline__ void ld_u16(const uint16_t* __restrict__ p, uint32_t 
 }
 
 // One split point J of the dense row: N[t][b] += A_J[xh][y >> M] * B_M[xl][y & (2^M-1)].
-template <int K, int TB, int BB, int J>
+template <int K, int TB, int BB, int J, bool SH>
 __device__ __forceinline__ void tile_term(const Split& s, const uint16_t* __restrict__ ar,
                                           const uint16_t* __restrict__ br, uint32_t xh, uint32_t xl,
                                           uint32_t g, uint32_t (&N)[1 << TB][1 << BB]) {
@@ -122,14 +145,14 @@ __device__ __forceinline__ void tile_term(const Split& s, const uint16_t* __rest
         for (int ba = 0; ba < AB; ++ba) {
             const uint32_t low = gA + ((M >= BB) ? 0u : (uint32_t)ba);
             uint32_t v[T];
-            ld_u16<T>(ar + bundle_offset(J) + (low << TB), v);
+            ld_u16<T, SH>(ar + bundle_offset(J) + (low << TB), v);
 #pragma unroll
             for (int ta = 0; ta < AT; ++ta) av[ta][ba] = v[ta];
         }
     } else {
         // J < TB: the 2^J entries y_hi = 0 .. 2^J - 1 are contiguous (gA = 0)
         uint32_t v[AT];
-        ld_u16<AT>(ar + bundle_offset(J), v);
+        ld_u16<AT, SH>(ar + bundle_offset(J), v);
 #pragma unroll
         for (int ta = 0; ta < AT; ++ta)
 #pragma unroll
@@ -150,7 +173,7 @@ __device__ __forceinline__ void tile_term(const Split& s, const uint16_t* __rest
         for (int tb = 0; tb < BT; ++tb) {
             const uint32_t t = (J >= TB) ? 0 : tb;
             uint32_t v[BN];
-            ld_u16<BN>(pb + ((t << (K - TB)) & mlo), v);
+            ld_u16<BN, SH>(pb + ((t << (K - TB)) & mlo), v);
 #pragma unroll
             for (int bb = 0; bb < BN; ++bb) bv[tb][bb] = v[bb];
         }
@@ -167,12 +190,24 @@ __device__ __forceinline__ void tile_term(const Split& s, const uint16_t* __rest
         }
 }
 
-template <int K, int TB, int BB, int... Js>
+template <int K, int TB, int BB, bool SH, int... Js>
 __device__ __forceinline__ void tile_row_impl(const Split& s, const uint16_t* ar, const uint16_t* br,
                                               uint32_t xh, uint32_t xl, uint32_t g,
                                               uint32_t (&N)[1 << TB][1 << BB],
                                               std::integer_sequence<int, Js...>) {
-    (tile_term<K, TB, BB, Js>(s, ar, br, xh, xl, g, N), ...);
+    (tile_term<K, TB, BB, Js, SH>(s, ar, br, xh, xl, g, N), ...);
+}
+
+// the same from the two rows of x already staged in shared memory
+template <int K, int TB, int BB>
+__device__ __forceinline__ void tile_row_staged(const Split& s, const uint16_t* ar, const uint16_t* br, uint32_t x,
+                                                uint32_t g, uint32_t (&N)[1 << TB][1 << BB]) {
+#pragma unroll
+    for (int t = 0; t < (1 << TB); ++t)
+#pragma unroll
+        for (int b = 0; b < (1 << BB); ++b) N[t][b] = 0u;
+    const uint32_t xh = x >> s.n2, xl = x & low_mask(s.n2);
+    tile_row_impl<K, TB, BB, true>(s, ar, br, xh, xl, g, N, std::make_integer_sequence<int, K + 1>{});
 }
 
 // Dense counts N(x, y(t,b)) for all of this thread's y.
@@ -186,8 +221,58 @@ __device__ __forceinline__ void tile_row(const Split& s, const HalfTables& A, co
     const uint32_t xh = x >> s.n2, xl = x & low_mask(s.n2);
     const uint16_t* ar = A.rows + (size_t)xh * A.stride;
     const uint16_t* br = B.rows + (size_t)xl * B.stride;
-    tile_row_impl<K, TB, BB>(s, ar, br, xh, xl, g, N, std::make_integer_sequence<int, K + 1>{});
+    tile_row_impl<K, TB, BB, false>(s, ar, br, xh, xl, g, N, std::make_integer_sequence<int, K + 1>{});
 }
+
+// ------------------------------------------------ rows staged in shared memory
+// For k >= 12 a whole CTA (256 threads) works on one x at a time, and every
+// entry of the x's A row and B row is read by some thread.  One thread copies
+// the next x's two rows into shared memory (cp.async.bulk, completion on an
+// mbarrier) while the CTA computes the current x from the previous copy;
+// the table reads then come from shared memory instead of waiting on L2.
+constexpr uint32_t kStageSpin = 1u << 22;  // polls of a bounded mbarrier wait
+constexpr int kErrCountStage = 5;          // DevState::error: a staging wait ran out
+
+__device__ __forceinline__ uint32_t cnt_smem(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cnt_mbar_init(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool cnt_mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kStageSpin; ++i) {
+        uint32_t ok = 0;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// the A row (rotated bundle) and the B row of x into buffer dst, bytes
+// counted on bar; rows start 16-byte aligned and are multiples of 16 bytes
+__device__ __forceinline__ void stage_rows(const Split& s, const HalfTables& A, const HalfTables& B, uint32_t x,
+                                           uint16_t* dst, uint32_t bar) {
+    const uint32_t xh = x >> s.n2, xl = x & low_mask(s.n2);
+    const uint32_t ba = (uint32_t)A.stride * 2u, bb = (uint32_t)B.stride * 2u;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(ba + bb) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     cnt_smem(dst)),
+                 "l"(A.rows + (size_t)xh * A.stride), "r"(ba), "r"(bar)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     cnt_smem(dst + A.stride)),
+                 "l"(B.rows + (size_t)xl * B.stride), "r"(bb), "r"(bar)
+                 : "memory");
+}
+
+__host__ __device__ constexpr bool staged_rows(int group) { return group == 256; }
 
 // Residency of the two passes.  They wait on L1/L2 table loads, so
 // occupancy pays: tiles of 16 words per thread are compiled for 4 CTAs of 256
@@ -284,6 +369,49 @@ __global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_qpass(Spl
 #pragma unroll
                 for (int b = 0; b < TL::NB; ++b) acc[t][b] += acc32[t][b].value();
         }
+    } else if constexpr (staged_rows(TL::GROUP)) {
+        // the CTA is one x-group: rows staged through shared memory, after sh_acc
+        extern __shared__ __align__(16) double sh_dyn[];
+        uint16_t* rows = (uint16_t*)(sh_dyn + (1 << K));  // [2][A.stride + B.stride]
+        __shared__ __align__(8) uint64_t rbar[2];
+        const int rs = A.stride + B.stride;
+        if (threadIdx.x == 0) {
+            cnt_mbar_init(cnt_smem(&rbar[0]));
+            cnt_mbar_init(cnt_smem(&rbar[1]));
+        }
+        __syncthreads();
+        int bad = 0, failed = 0;  // this thread's wait ran out; some thread's did (uniform)
+        const int64_t nx = i1 - i0;
+        if (threadIdx.x == 0 && nx > 0) stage_rows(s, A, B, __ldg(reps + i0), rows, cnt_smem(&rbar[0]));
+        int64_t ix = 0;
+        for (; ix < nx; ++ix) {
+            const int b = (int)(ix & 1);
+            if (threadIdx.x == 0 && ix + 1 < nx)
+                stage_rows(s, A, B, __ldg(reps + i0 + ix + 1), rows + (b ^ 1) * rs, cnt_smem(&rbar[b ^ 1]));
+            if (!cnt_mbar_wait(cnt_smem(&rbar[b]), (uint32_t)(ix >> 1) & 1u)) bad = 1;
+            const uint32_t x = __ldg(reps + i0 + ix);
+            const double w = (double)orbit_size(x, s.n) * __ldg(p + i0 + ix);
+            uint32_t N[TL::T][TL::NB];
+            tile_row_staged<K, TB, BB>(s, rows + b * rs, rows + b * rs + A.stride, x, g, N);
+#pragma unroll
+            for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+                for (int bb = 0; bb < TL::NB; ++bb) acc[t][bb] = fma(w, (double)N[t][bb], acc[t][bb]);
+            failed = __syncthreads_or(bad);  // buffer b is free for x_{ix+2}
+            if (failed) break;
+        }
+        if (failed) {
+            // a copy that never completed: wait (bounded) for the one still in
+            // flight, record the error, and leave NaN sums behind
+            if (threadIdx.x == 0) {
+                if (ix + 1 < nx) (void)cnt_mbar_wait(cnt_smem(&rbar[(ix + 1) & 1]), (uint32_t)((ix + 1) >> 1) & 1u);
+                if (st) ((DevState*)st)->error = kErrCountStage;
+            }
+#pragma unroll
+            for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+                for (int bb = 0; bb < TL::NB; ++bb) acc[t][bb] = __longlong_as_double(0x7ff8000000000000ll);
+        }
     } else {
         for (int64_t i = i0; i < i1; ++i) {
             const uint32_t x = __ldg(reps + i);
@@ -358,6 +486,95 @@ __global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_dpass(Spl
     __shared__ double sh_part[XC][8];            // [x slot][warp of the CTA]
     __shared__ uint32_t sh_nz[XC][8];
     const int warp = threadIdx.x >> 5;
+    // this thread's share of one x: sum_y N ln q (MODE 0) or sum N ln N and
+    // the nonzero count (MODE 1)
+    auto per_x = [&](const uint32_t (&N)[TL::T][TL::NB], double& v, uint32_t& nz) {
+        if constexpr (C32) {
+            F32Pair sv;
+#pragma unroll
+            for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+                for (int b = 0; b < TL::NB; ++b) sv.add_prod(lqh[t][b], lql[t][b], (float)N[t][b]);
+            v = sv.value();
+        } else {
+#pragma unroll
+            for (int t = 0; t < TL::T; ++t)
+#pragma unroll
+                for (int b = 0; b < TL::NB; ++b) {
+                    if (MODE == 0) {
+                        v = fma((double)N[t][b], lq[t][b], v);
+                    } else {
+                        const uint32_t c = N[t][b];
+                        if (c) {
+                            v = fma((double)c, log((double)c), v);
+                            ++nz;
+                        }
+                    }
+                }
+        }
+    };
+    auto finish_x = [&](int64_t i, double v, uint32_t nz) {
+        out_d[i] = (MODE == 0) ? (__ldg(h + i) - v * inv_c) : (v * inv_c - log_c);
+        if (MODE == 1) out_nnz[i] = nz;
+    };
+    if constexpr (staged_rows(TL::GROUP)) {
+        // the CTA is one x-group: each x's two rows staged through shared memory
+        extern __shared__ __align__(16) uint16_t rows[];  // [2][A.stride + B.stride]
+        __shared__ __align__(8) uint64_t rbar[2];
+        const int rs = A.stride + B.stride;
+        if (threadIdx.x == 0) {
+            cnt_mbar_init(cnt_smem(&rbar[0]));
+            cnt_mbar_init(cnt_smem(&rbar[1]));
+        }
+        __syncthreads();
+        int bad = 0, failed = 0;  // this thread's wait ran out; some thread's did (uniform)
+        const int64_t nx = i1 - i0;
+        if (threadIdx.x == 0 && nx > 0) stage_rows(s, A, B, __ldg(reps + i0), rows, cnt_smem(&rbar[0]));
+        int64_t ix = 0;
+        for (; ix < nx; ++ix) {
+            const int b = (int)(ix & 1);
+            if (threadIdx.x == 0 && ix + 1 < nx)
+                stage_rows(s, A, B, __ldg(reps + i0 + ix + 1), rows + (b ^ 1) * rs, cnt_smem(&rbar[b ^ 1]));
+            if (!cnt_mbar_wait(cnt_smem(&rbar[b]), (uint32_t)(ix >> 1) & 1u)) bad = 1;
+            const uint32_t x = __ldg(reps + i0 + ix);
+            uint32_t N[TL::T][TL::NB];
+            tile_row_staged<K, TB, BB>(s, rows + b * rs, rows + b * rs + A.stride, x, g, N);
+            double v = 0.0;
+            uint32_t nz = 0;
+            per_x(N, v, nz);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                v += __shfl_xor_sync(0xFFFFFFFFu, v, off);
+                if (MODE == 1) nz += __shfl_xor_sync(0xFFFFFFFFu, nz, off);
+            }
+            const int slot = (int)(ix % XC);
+            if (lane == 0) {
+                sh_part[slot][warp] = v;
+                sh_nz[slot][warp] = nz;
+            }
+            failed = __syncthreads_or(bad);  // buffer b is free for x_{ix+2}; the slot is written
+            if (slot == XC - 1 || ix == nx - 1) {
+                if (threadIdx.x <= slot) {
+                    const int xs = threadIdx.x;
+                    double vv = 0.0;
+                    uint32_t nn = 0;
+                    for (int w = 0; w < WPG; ++w) {
+                        vv += sh_part[xs][w];
+                        nn += sh_nz[xs][w];
+                    }
+                    finish_x(i0 + ix - slot + xs, vv, nn);
+                }
+                __syncthreads();
+            }
+            if (failed) break;
+        }
+        if (failed && threadIdx.x == 0) {
+            // a copy that never completed: wait (bounded) for the one still in
+            // flight and record the error (the D values of this CTA are stale)
+            if (ix + 1 < nx) (void)cnt_mbar_wait(cnt_smem(&rbar[(ix + 1) & 1]), (uint32_t)((ix + 1) >> 1) & 1u);
+            if (st) ((DevState*)st)->error = kErrCountStage;
+        }
+    } else {
     // All groups of a CTA run the same number of rounds so that the
     // barriers below are uniform.
     for (int64_t r0 = 0; r0 < chunk; r0 += XC) {
@@ -369,29 +586,7 @@ __global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_dpass(Spl
                 const uint32_t x = __ldg(reps + i);
                 uint32_t N[TL::T][TL::NB];
                 tile_row<K, TB, BB>(s, A, B, x, g, N);
-                if constexpr (C32) {
-                    F32Pair sv;
-#pragma unroll
-                    for (int t = 0; t < TL::T; ++t)
-#pragma unroll
-                        for (int b = 0; b < TL::NB; ++b) sv.add_prod(lqh[t][b], lql[t][b], (float)N[t][b]);
-                    v = sv.value();
-                } else {
-#pragma unroll
-                    for (int t = 0; t < TL::T; ++t)
-#pragma unroll
-                        for (int b = 0; b < TL::NB; ++b) {
-                            if (MODE == 0) {
-                                v = fma((double)N[t][b], lq[t][b], v);
-                            } else {
-                                const uint32_t c = N[t][b];
-                                if (c) {
-                                    v = fma((double)c, log((double)c), v);
-                                    ++nz;
-                                }
-                            }
-                        }
-                }
+                per_x(N, v, nz);
             }
             if (TL::GROUP <= 32) {
                 // the group is a lane-aligned slice of one warp
@@ -400,10 +595,7 @@ __global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_dpass(Spl
                     v += __shfl_xor_sync(0xFFFFFFFFu, v, off);
                     if (MODE == 1) nz += __shfl_xor_sync(0xFFFFFFFFu, nz, off);
                 }
-                if (g == 0 && i < i1) {
-                    out_d[i] = (MODE == 0) ? (__ldg(h + i) - v * inv_c) : (v * inv_c - log_c);
-                    if (MODE == 1) out_nnz[i] = nz;
-                }
+                if (g == 0 && i < i1) finish_x(i, v, nz);
             } else {
 #pragma unroll
                 for (int off = 16; off > 0; off >>= 1) {
@@ -430,12 +622,12 @@ __global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_dpass(Spl
                         v += sh_part[xs][gg * WPG + w];
                         nz += sh_nz[xs][gg * WPG + w];
                     }
-                    out_d[i] = (MODE == 0) ? (__ldg(h + i) - v * inv_c) : (v * inv_c - log_c);
-                    if (MODE == 1) out_nnz[i] = nz;
+                    finish_x(i, v, nz);
                 }
             }
             __syncthreads();
         }
+    }
     }
 }
 
@@ -534,7 +726,10 @@ static cudaError_t launch_qpass_k(const CountLaunch& L, const double* p0, const 
                                   double* part, const DevState* st, int use_state) {
     constexpr int TB = TileChoice<K>::TB, BB = TileChoice<K>::BB;
     const int threads = cta_threads<K>();
-    const size_t shm = sizeof(double) << K;
+    // the partial sums, then (staged rows, FP64 sums) two buffers of the A and B rows
+    constexpr bool staged = staged_rows(Tile<K, TB, BB>::GROUP);
+    const size_t rows_b = (staged && !L.c32) ? 2 * (size_t)(L.A.stride + L.B.stride) * sizeof(uint16_t) : 0;
+    const size_t shm = (sizeof(double) << K) + rows_b;
     auto kern = L.c32 ? k_qpass<K, TB, BB, true> : k_qpass<K, TB, BB, false>;
     if (shm > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
@@ -551,8 +746,15 @@ static cudaError_t launch_dpass_k(const CountLaunch& L, const double* lnq, const
     constexpr int TB = TileChoice<K>::TB, BB = TileChoice<K>::BB;
     const int threads = cta_threads<K>();
     auto kern = (MODE == 0 && L.c32) ? k_dpass<K, TB, BB, MODE, MODE == 0> : k_dpass<K, TB, BB, MODE, false>;
-    kern<<<L.grid, threads, 0, L.stream>>>(L.s, L.A, L.B, L.reps, L.R, lnq, h, inv_c, log_c, out, nnz, st,
-                                           use_state);
+    // staged rows: two buffers of the A and B rows
+    constexpr bool staged = staged_rows(Tile<K, TB, BB>::GROUP);
+    const size_t shm = staged ? 2 * (size_t)(L.A.stride + L.B.stride) * sizeof(uint16_t) : 0;
+    if (shm > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<L.grid, threads, shm, L.stream>>>(L.s, L.A, L.B, L.reps, L.R, lnq, h, inv_c, log_c, out, nnz, st,
+                                             use_state);
     return cudaGetLastError();
 }
 

@@ -1409,12 +1409,13 @@ struct TuneFile {
         snprintf(line, sizeof(line), "%d %d %s %d %d\n", n, k, key, a, b);
         fresh.push_back(line);
     }
-    void save() const {
+    void save() {
         if (path.empty() || fresh.empty()) return;
         FILE* f = fopen(path.c_str(), "a");
         if (!f) return;
         for (auto& l : fresh) fputs(l.c_str(), f);
         fclose(f);
+        fresh.clear();
     }
 };
 
@@ -1582,6 +1583,8 @@ bool factored_supports(int n, int k) {
     // is 2^min(j, k - j), up to 2^floor(k/2))
     return k >= 1 && k < n && n >= 2 && n <= 28 && k <= 14;
 }
+
+static BaEpilogue make_epilogue(bdc_handle* H);
 
 bdc_status factored_init(bdc_handle* H) {
     BDC_CUDA_TRY(set_smem_attrs());
@@ -2103,29 +2106,60 @@ bdc_status factored_init(bdc_handle* H) {
         nd = 0;
         for (int cl = 0; cl < 4; ++cl) nd += F->n_df[cl] > 0;
     }
-    // G on the int8 tensor cores (bdc_ozaki.cu) where BDC_G_KERNEL=ozaki asks for it
+    // G on the int8 tensor cores (bdc_ozaki.cu), with the slicing of its FP64
+    // operands, where that times faster than the FP64 product chosen above;
+    // BDC_G_KERNEL=dmma or ozaki forces one of the two
     {
         const char* gk = getenv("BDC_G_KERNEL");
-        if (gk && (!strcmp(gk, "ozaki") || !strcmp(gk, "ozaki-p"))) {
-            const OzakiInput in{F->LA, F->RB, Kp, KL, KR, H1, H2, F->colmax.data()};
+        const bool force_fp = gk && !strcmp(gk, "dmma");
+        const bool force_oz = gk && !strcmp(gk, "ozaki");
+        int pick = -1, unused = 0;
+        const bool pinned = !force_oz && tf.get("oz", &pick, &unused);
+        if (!force_fp && !(pinned && pick == 0)) {
+            // an entry of ML (NR) is ln q against a row of B_m (A_j), whose
+            // entries add up to C(n2, m) (C(n1, j)); 1 for an identity table
+            double cmax = 1.0;
+            for (const Term& t : F->terms)
+                if (t.left && !t.idB) cmax = std::max(cmax, (double)binom(s.n2, t.m));
+                else if (!t.left && !t.idA) cmax = std::max(cmax, (double)binom(s.n1, t.j));
+            const OzakiInput in{F->LA, F->RB, Kp, KL, KR, H1, H2, F->colmax.data(), F->lnq_full, H->k, cmax};
             const char* why = nullptr;
-            bdc_status rc = ozaki_init(H, in, !strcmp(gk, "ozaki-p"), &F->oz, &why);
+            bdc_status rc = ozaki_init(H, in, &F->oz, &why);
             if (rc != BDC_OK) return rc;
+            float t_fp = 0.f, t_oz = 0.f;
+            if (F->oz && !force_oz && !pinned) {
+                // both on the zeroed state (the products' cost does not depend on the values)
+                const BaEpilogue ep = make_epilogue(H);
+                t_fp = time_ms(H, [&] { launch_ba(F->g, ep, H->stream, H->d_st); });
+                t_oz = time_ms(H, [&] {
+                    ozaki_prepare(F->oz, H->d_st, H->stream);
+                    ozaki_product(F->oz, ep, H->d_st, H->stream);
+                });
+                tf.put("oz", t_oz < t_fp ? 1 : 0, 0);
+                tf.save();
+                BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
+                BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
+                BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
+                if (t_oz >= t_fp) {
+                    ozaki_free(F->oz);
+                    F->oz = nullptr;
+                }
+            }
             F->use_oz = F->oz != nullptr;
             if (H->verbose) {
                 if (F->use_oz)
-                    printf("bdc: G on the int8 tensor cores: %d tiles of %dx%d, %d B shared memory%s\n",
-                           F->oz->persistent ? F->oz->tilesP : F->oz->tiles, kOzBM, F->oz->persistent ? 32 : kOzBN,
-                           F->oz->persistent ? F->oz->smemP : F->oz->smem,
-                           F->oz->persistent ? ", persistent (one CTA per SM)" : "");
+                    printf("bdc: G on the int8 tensor cores: %d tiles of %dx%d over %d CTAs, %d B shared memory, "
+                           "ring of %d%s\n", F->oz->tiles, kOzBM, kOzTN, F->oz->grid, F->oz->smem, F->oz->stages,
+                           t_oz > 0.f ? "" : " (forced or pinned)");
                 else
-                    printf("bdc: G stays on the FP64 product: %s\n", why ? why : "?");
+                    printf("bdc: G stays on the FP64 product: %s\n", why ? why : "timed slower");
+                if (t_oz > 0.f) printf("bdc: G timed: FP64 %.1f us, int8 with slicing %.1f us\n", t_fp * 1e3f, t_oz * 1e3f);
             }
         }
     }
     // U, V, the split sums; q-side terms; three fold kernels; D-side terms; G
-    // (plus four operand kernels on the int8 path); finalize
-    F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + nq + 3 + nd + 1 + 1 + (F->use_oz ? 4 : 0);
+    // (plus the slicing kernel on the int8 path); finalize
+    F->launches_per_iter = (F->ul.n > 0) + (F->vr.n > 0) + 1 + nq + 3 + nd + 1 + 1 + (F->use_oz ? 1 : 0);
     BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
     return BDC_OK;
 }

@@ -9,12 +9,16 @@
 // representative D(x) = h(x) - G(x) / C(n,k), logW = ln p + eta D, and the
 // block partials of the update.
 //
-// One CTA per 128 x 64 tile of G that holds a representative (the eight
-// accumulators take all 512 TMEM columns of an SM).  Warp 0 lane 0 loads,
-// warp 1 lane 0 issues the MMAs, then all four warps drain the accumulators
-// (one TMEM lane = one tile row per thread) and run the epilogue.  Every wait
-// on an mbarrier is bounded: on time-out the CTA records an error in
-// DevState::error, skips the epilogue, waits (bounded) for its loads and
+// One persistent CTA per SM loops over the 128 x 32 tiles of G that hold a
+// representative.  Warp 0 lane 0 loads by TMA (the static table slices of a
+// tile into one of two buffers, the per-weight slices of the FP64 operands
+// through a ring), warp 1 lane 0 issues the MMAs into one of two TMEM
+// accumulator buffers (8 weights x 32 columns each), and 16 epilogue warps
+// drain the other buffer: a thread owns one tile row (its TMEM lane) and 8
+// adjacent columns, i.e. 64 contiguous bytes of each dense array, so the
+// update runs on 16-byte loads and stores with no barrier among the warps.
+// Every wait on an mbarrier is bounded: on time-out the CTA records an error
+// in DevState::error, skips the rest, waits (bounded) for its loads and
 // frees its TMEM.
 #include <cudaTypedefs.h>
 
@@ -31,8 +35,6 @@ namespace bdc {
 constexpr int kErrOzakiWait = 3;         // DevState::error: an mbarrier wait ran out
 constexpr int kErrOzakiOperand = 4;      // DevState::error: a non-finite FP64 operand
 constexpr uint32_t kOzSpin = 1u << 22;   // polls per wait
-constexpr int kOzTmemCols = kOzW * kOzBN;
-static_assert(kOzTmemCols <= 512, "accumulators exceed tensor memory");
 
 // ------------------------------------------------------------- PTX helpers
 __device__ __forceinline__ uint32_t sm_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -111,6 +113,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
         : "r"(taddr));
 }
 
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // --------------------------------------------------------------- the product
@@ -119,269 +127,21 @@ struct OzGeomDev {
     int aS, bS, aD, bD;  // atom columns
     int M, N;            // rows (H1h) and columns (H2) of G
     int tiles_n;
-    int stages;          // ring depth of the per-weight operands (persistent form; <= kOzStages)
+    int stages;          // ring depth of the per-weight operands (<= kOzStages)
 };
 
-__global__ void __launch_bounds__(kOzThreads, 1)
-k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtensorMap tmBs,
-        const __grid_constant__ CUtensorMap tmAd, const __grid_constant__ CUtensorMap tmBd, OzGeomDev g,
-        const int* __restrict__ tiles, const int* __restrict__ d_e, BaEpilogue ep, DevState* st) {
-    extern __shared__ __align__(1024) uint8_t oz_smem_raw[];
-    __shared__ __align__(8) uint64_t bar_static, bar_full[kOzStages], bar_empty[kOzStages], bar_done;
-    __shared__ uint32_t tmem_base_sh;
-    __shared__ int abort_sh, skip_sh;
-    // one read of the gate for the whole CTA (another CTA may set the error)
-    if (threadIdx.x == 0) skip_sh = (st->done || st->error) ? 1 : 0;
-    __syncthreads();
-    if (skip_sh) return;
-
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int t = tiles[blockIdx.x];
-    const int m0 = (t / g.tiles_n) * kOzBM, n0 = (t % g.tiles_n) * kOzBN;
-
-    // 1024-byte aligned carve-up: static A, static B, then the stages
-    uint8_t* base = (uint8_t*)(((uintptr_t)oz_smem_raw + 1023) & ~(uintptr_t)1023);
-    const uint32_t sA = sm_addr(base);
-    const uint32_t sB = sA + (uint32_t)g.aS * kOzBM * 128;
-    const uint32_t sStage0 = sB + (uint32_t)g.bS * kOzBN * 128;
-    const uint32_t stageA = (uint32_t)g.aD * kOzBM * 128, stageB = (uint32_t)g.bD * kOzBN * 128;
-    const uint32_t stageBytes = stageA + stageB;
-
-    if (threadIdx.x == 0) {
-        mbar_init(sm_addr(&bar_static), 1);
-        for (int i = 0; i < kOzStages; ++i) {
-            mbar_init(sm_addr(&bar_full[i]), 1);
-            mbar_init(sm_addr(&bar_empty[i]), 1);
-        }
-        mbar_init(sm_addr(&bar_done), 1);
-        abort_sh = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sm_addr(&tmem_base_sh)),
-                     "r"((uint32_t)kOzTmemCols)
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = tmem_base_sh;
-
-    int issued_loads = 0;  // producer: per-weight loads issued (for the bounded drain on abort)
-
-    // Lanes 1-31 of the producer and MMA warps wait at __syncwarp while lane 0
-    // works: spinning on an mbarrier on the warp's other path would stall the
-    // working lane's path every time a try_wait suspends.
-    if (warp == 0) {
-      if (lane == 0) {
-        // ---- producer: the static operands once, the per-weight slices through the stages
-        const uint32_t bs = sm_addr(&bar_static);
-        mbar_expect_tx(bs, (uint32_t)(g.aS * kOzBM + g.bS * kOzBN) * 128);
-        for (int c = 0; c < g.aS; ++c) tma_load_2d(sA + c * kOzBM * 128, &tmAs, bs, 128 * c, m0);
-        for (int c = 0; c < g.bS; ++c) tma_load_2d(sB + c * kOzBN * 128, &tmBs, bs, 128 * c, n0);
-        for (int a = 0; a < kOzW; ++a) {
-            const int s = a % kOzStages, use = a / kOzStages;
-            if (use > 0 && !mbar_wait(sm_addr(&bar_empty[s]), (use - 1) & 1)) {
-                atomicExch(&abort_sh, 1);
-                break;
-            }
-            if (*(volatile int*)&abort_sh) break;
-            const uint32_t fb = sm_addr(&bar_full[s]);
-            const uint32_t dA = sStage0 + s * stageBytes, dB = dA + stageA;
-            mbar_expect_tx(fb, stageBytes);
-            // slots a and a + 1 of the sliced operands: [x_{a-1} | x_a]
-            for (int c = 0; c < g.aD; ++c) tma_load_2d(dA + c * kOzBM * 128, &tmAd, fb, a * g.KRp + 128 * c, m0);
-            for (int c = 0; c < g.bD; ++c) tma_load_2d(dB + c * kOzBN * 128, &tmBd, fb, a * g.KLp + 128 * c, n0);
-            ++issued_loads;
-        }
-      }
-      __syncwarp();
-    } else if (warp == 1) {
-      if (lane == 0) {
-        // ---- MMA issuer: accumulator a gets [lo | hi] x [x_{a-1} | x_a] over both parts
-        const uint32_t idesc = umma_idesc_i8(kOzBM, kOzBN);
-        bool ok = mbar_wait(sm_addr(&bar_static), 0);
-        for (int a = 0; a < kOzW && ok; ++a) {
-            const int s = a % kOzStages, use = a / kOzStages;
-            if (!mbar_wait(sm_addr(&bar_full[s]), use & 1) || *(volatile int*)&abort_sh) {
-                ok = false;
-                break;
-            }
-            tc_fence_after();
-            const uint32_t dA = sStage0 + s * stageBytes, dB = dA + stageA;
-            const uint32_t tacc = tmem + (uint32_t)(a * kOzBN);
-            uint32_t accum = 0;
-            for (int kb = 0; kb < 2 * g.KLp; kb += 32) {  // L part: static A x per-weight B
-                const uint32_t off = (uint32_t)(kb >> 7), in = (uint32_t)(kb & 127);
-                umma_i8(tacc, umma_desc_sw128(sA + off * kOzBM * 128 + in), umma_desc_sw128(dB + off * kOzBN * 128 + in),
-                        idesc, accum);
-                accum = 1;
-            }
-            for (int kb = 0; kb < 2 * g.KRp; kb += 32) {  // R part: per-weight A x static B
-                const uint32_t off = (uint32_t)(kb >> 7), in = (uint32_t)(kb & 127);
-                umma_i8(tacc, umma_desc_sw128(dA + off * kOzBM * 128 + in), umma_desc_sw128(sB + off * kOzBN * 128 + in),
-                        idesc, accum);
-                accum = 1;
-            }
-            umma_commit(sm_addr(&bar_empty[s]));  // the stage is free once these MMAs are done
-        }
-        if (!ok) atomicExch(&abort_sh, 1);
-        umma_commit(sm_addr(&bar_done));  // arrives when every MMA issued above has completed
-      }
-      __syncwarp();
-    }
-
-    // ---- everyone: wait for the accumulators
-    const bool done_ok = mbar_wait(sm_addr(&bar_done), 0);
-    tc_fence_after();
-    __syncthreads();
-    if (!done_ok) atomicExch(&abort_sh, 1);
-    __syncthreads();
-    const bool run = (*(volatile int*)&abort_sh == 0);
-
-    double mD = -DBL_MAX, sE = 0.0, mL = -DBL_MAX, sR = 0.0, zero = 0.0;
-    if (run) {
-        const double shift = st->shift;
-        const double lnz = st->log_z;
-        const double inv_z = exp(-lnz);
-        const int e = *d_e;
-        const int r = warp * 32 + lane;  // tile row = TMEM lane
-        const int m = m0 + r;
-        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-        for (int c0 = 0; c0 < kOzBN; c0 += 16) {
-            double gsum[16];
-#pragma unroll
-            for (int j = 0; j < 16; ++j) gsum[j] = 0.0;
-            // smallest weights first: every term is exact, the sum rounds once per step
-#pragma unroll 1
-            for (int a = kOzW - 1; a >= 0; --a) {
-                uint32_t v[16];
-                tmem_ld16(trow + (uint32_t)(a * kOzBN + c0), v);
-                tmem_wait_ld();
-                const double w = ldexp(1.0, e - 7 * a);
-#pragma unroll
-                for (int j = 0; j < 16; ++j) gsum[j] = fma((double)(int32_t)v[j], w, gsum[j]);
-            }
-            if (m >= g.M) continue;
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int n = n0 + c0 + j;
-                if (n >= g.N) continue;
-                const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
-                const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);  // the global dense index
-                const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
-                if (!is_rep(x, ep.n)) continue;
-                const double o = (double)orbit_size(x, ep.n);
-                const double D = __ldg(ep.hx + xd) - gsum[j] * ep.inv_c;
-                if (ep.Dout) ep.Dout[xd] = D;
-                // an entry that is exactly 0 in the caller's distribution (Lt
-                // holds NaN) takes ln p = 0, as the reference's apply_log_kernel
-                // leaves ln 0 at 0 (backend/BAA.cu:573-580)
-                const double pw = ep.Pw[xd];
-                const double lt = ep.Lt[xd];
-                const bool zero_in = (lt != lt);
-                const double lnp = zero_in ? 0.0 : lt - lnz;
-                const double lw = lnp + ep.eta * D - shift;
-                const double ex = exp(lw);
-                ep.Lt[xd] = lw;
-                ep.Pw[xd] = o * ex;
-                mD = fmax(mD, D);
-                mL = fmax(mL, lw);
-                sE = fma(o, ex, sE);
-                sR = fma(pw * inv_z, D, sR);
-                if (zero_in) zero = 1.0;
-            }
-        }
-    } else if (threadIdx.x == 0) {
-        st->error = kErrOzakiWait;
-    }
-
-    // ---- block partials, as the FP64 product writes them
-    __shared__ double red[5][kOzThreads / 32];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        mD = fmax(mD, __shfl_xor_sync(0xFFFFFFFFu, mD, off));
-        mL = fmax(mL, __shfl_xor_sync(0xFFFFFFFFu, mL, off));
-        sE += __shfl_xor_sync(0xFFFFFFFFu, sE, off);
-        sR += __shfl_xor_sync(0xFFFFFFFFu, sR, off);
-        zero = fmax(zero, __shfl_xor_sync(0xFFFFFFFFu, zero, off));
-    }
-    if (lane == 0) {
-        red[0][warp] = mD;
-        red[1][warp] = sE;
-        red[2][warp] = mL;
-        red[3][warp] = sR;
-        red[4][warp] = zero;
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a0 = red[0][0], a1 = red[1][0], a2 = red[2][0], a3 = red[3][0], a4 = red[4][0];
-        for (int w = 1; w < kOzThreads / 32; ++w) {
-            a0 = fmax(a0, red[0][w]);
-            a1 += red[1][w];
-            a2 = fmax(a2, red[2][w]);
-            a3 += red[3][w];
-            a4 = fmax(a4, red[4][w]);
-        }
-        double* p = ep.part + (size_t)blockIdx.x * 8;
-        p[0] = a0;
-        p[1] = a1;
-        p[2] = a2;
-        p[3] = a3;
-        p[4] = a4;
-    }
-    // on an abort, wait (bounded) for the loads still in flight before the
-    // shared memory is released; the MMAs were all covered by bar_done
-    if (!run && warp == 0 && lane == 0) {
-        for (int a = 0; a < issued_loads; ++a) {
-            const int s = a % kOzStages, use = a / kOzStages;
-            (void)mbar_wait(sm_addr(&bar_full[s]), use & 1);
-        }
-        (void)mbar_wait(sm_addr(&bar_static), 0);
-    }
-    __syncthreads();
-    tc_fence_after();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kOzTmemCols)
-                     : "memory");
-}
-
-// ------------------------------------------- the persistent, overlapped form
-// One CTA per SM loops over 128 x 32 tiles.  Two TMEM buffers of eight
-// 32-column accumulators (2 x 256 = 512 columns): while warps 2-9 drain and
-// finish tile i from one buffer, warp 1 issues tile i + 1's MMAs into the
-// other.  The static operands of a tile are double-buffered, the per-weight
-// slices go through a ring of g.stages stages that continues across tiles.
-// Barriers: sfull/sempty (static operands), full/empty (ring), tfull/tempty
-// (TMEM buffers; tempty takes one arrival per epilogue warp).
-//
-// The epilogue streams three vectors of the iterate (h, Pw, Lt: 40 bytes per
-// representative), so it is bound by memory, and a CTA is alone on its SM:
-// eight epilogue warps (two per TMEM lane quadrant, splitting the columns)
-// drain the accumulators into an FP64 tile in shared memory, then walk it
-// row by row with the lanes along the columns (coalesced), issuing the loads
-// of eight elements before computing them.
-constexpr int kOzPBN = 32;
-constexpr int kOzPEpiWarps = 8;
-constexpr int kOzPThreads = 64 + 32 * kOzPEpiWarps;  // producer, MMA, epilogue warps
-constexpr int kOzPBuf = kOzW * kOzPBN;               // TMEM columns of one buffer
-constexpr int kOzPTileLd = kOzPBN + 1;                // row pitch of the FP64 tile in shared memory
-constexpr int kOzPTileBytes = kOzBM * kOzPTileLd * 8;
-static_assert(2 * kOzPBuf <= 512, "two accumulator buffers exceed tensor memory");
+constexpr int kOzThreads = 64 + 32 * kOzEpiWarps;  // producer, MMA, epilogue warps
+constexpr int kOzBuf = kOzW * kOzTN;               // TMEM columns of one accumulator buffer
+constexpr int kOzCols = kOzTN / (kOzEpiWarps / 4);  // columns one epilogue warp drains
+static_assert(kOzCols == 8 && kOzW % 2 == 0, "the drain reads accumulator pairs, 8 columns at a time");
+static_assert(2 * kOzBuf <= 512, "two accumulator buffers exceed tensor memory");
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// barrier 1 among the epilogue warps only
-__device__ __forceinline__ void epi_sync() {
-    asm volatile("bar.sync 1, %0;" ::"r"(32 * kOzPEpiWarps) : "memory");
-}
-
-__global__ void __launch_bounds__(kOzPThreads, 1)
-k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtensorMap tmBs,
+__global__ void __maxnreg__(112)
+k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtensorMap tmBs,
           const __grid_constant__ CUtensorMap tmAd, const __grid_constant__ CUtensorMap tmBd, OzGeomDev g,
           const int* __restrict__ tiles, int ntiles, const int* __restrict__ d_e, BaEpilogue ep, DevState* st) {
     extern __shared__ __align__(1024) uint8_t ozp_smem_raw[];
@@ -398,19 +158,18 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
     const int nmine = (ntiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
     uint8_t* base = (uint8_t*)(((uintptr_t)ozp_smem_raw + 1023) & ~(uintptr_t)1023);
     const uint32_t sA0 = sm_addr(base);
-    const uint32_t bytesA = (uint32_t)g.aS * kOzBM * 128, bytesB = (uint32_t)g.bS * kOzPBN * 128;
+    const uint32_t bytesA = (uint32_t)g.aS * kOzBM * 128, bytesB = (uint32_t)g.bS * kOzTN * 128;
     const uint32_t sB0 = sA0 + 2 * bytesA;
     const uint32_t ring0 = sB0 + 2 * bytesB;
-    const uint32_t stageA = (uint32_t)g.aD * kOzBM * 128, stageB = (uint32_t)g.bD * kOzPBN * 128;
+    const uint32_t stageA = (uint32_t)g.aD * kOzBM * 128, stageB = (uint32_t)g.bD * kOzTN * 128;
     const uint32_t stageBytes = stageA + stageB;
-    double* gt = (double*)(base + (ring0 - sA0) + (size_t)NS * stageBytes);  // [kOzBM][kOzPTileLd]
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < 2; ++i) {
             mbar_init(sm_addr(&sfull[i]), 1);
             mbar_init(sm_addr(&sempty[i]), 1);
             mbar_init(sm_addr(&tfull[i]), 1);
-            mbar_init(sm_addr(&tempty[i]), kOzPEpiWarps);
+            mbar_init(sm_addr(&tempty[i]), kOzEpiWarps);
         }
         for (int i = 0; i < NS; ++i) {
             mbar_init(sm_addr(&full[i]), 1);
@@ -444,7 +203,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
             int wc = 0;
             for (int it = 0; it < nmine && !aborted(); ++it) {
                 const int t = tiles[blockIdx.x + it * gridDim.x];
-                const int m0 = (t / g.tiles_n) * kOzBM, n0 = (t % g.tiles_n) * kOzPBN;
+                const int m0 = (t / g.tiles_n) * kOzBM, n0 = (t % g.tiles_n) * kOzTN;
                 const int sb = it & 1;
                 if (it >= 2 && !mbar_wait(sm_addr(&sempty[sb]), ((it >> 1) - 1) & 1)) {
                     give_up();
@@ -454,7 +213,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
                 mbar_expect_tx(sfb, bytesA + bytesB);
                 for (int c = 0; c < g.aS; ++c) tma_load_2d(sA0 + sb * bytesA + c * kOzBM * 128, &tmAs, sfb, 128 * c, m0);
                 for (int c = 0; c < g.bS; ++c)
-                    tma_load_2d(sB0 + sb * bytesB + c * kOzPBN * 128, &tmBs, sfb, 128 * c, n0);
+                    tma_load_2d(sB0 + sb * bytesB + c * kOzTN * 128, &tmBs, sfb, 128 * c, n0);
                 last_static[sb] = it >> 1;
                 bool ok = true;
                 for (int a = 0; a < kOzW; ++a, ++wc) {
@@ -468,7 +227,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
                     mbar_expect_tx(fb, stageBytes);
                     for (int c = 0; c < g.aD; ++c) tma_load_2d(dA + c * kOzBM * 128, &tmAd, fb, a * g.KRp + 128 * c, m0);
                     for (int c = 0; c < g.bD; ++c)
-                        tma_load_2d(dB + c * kOzPBN * 128, &tmBd, fb, a * g.KLp + 128 * c, n0);
+                        tma_load_2d(dB + c * kOzTN * 128, &tmBd, fb, a * g.KLp + 128 * c, n0);
                     last_use[s] = use;
                 }
                 if (!ok) {
@@ -480,7 +239,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
         __syncwarp();
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = umma_idesc_i8(kOzBM, kOzPBN);
+            const uint32_t idesc = umma_idesc_i8(kOzBM, kOzTN);
             int wc = 0;
             for (int it = 0; it < nmine && !aborted(); ++it) {
                 const int tb = it & 1, sb = it & 1;
@@ -503,18 +262,18 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
                     }
                     tc_fence_after();
                     const uint32_t dA = ring0 + s * stageBytes, dB = dA + stageA;
-                    const uint32_t tacc = tmem + (uint32_t)(tb * kOzPBuf + a * kOzPBN);
+                    const uint32_t tacc = tmem + (uint32_t)(tb * kOzBuf + a * kOzTN);
                     uint32_t accum = 0;
                     for (int kb = 0; kb < 2 * g.KLp; kb += 32) {
                         const uint32_t off = (uint32_t)(kb >> 7), in = (uint32_t)(kb & 127);
                         umma_i8(tacc, umma_desc_sw128(sA + off * kOzBM * 128 + in),
-                                umma_desc_sw128(dB + off * kOzPBN * 128 + in), idesc, accum);
+                                umma_desc_sw128(dB + off * kOzTN * 128 + in), idesc, accum);
                         accum = 1;
                     }
                     for (int kb = 0; kb < 2 * g.KRp; kb += 32) {
                         const uint32_t off = (uint32_t)(kb >> 7), in = (uint32_t)(kb & 127);
                         umma_i8(tacc, umma_desc_sw128(dA + off * kOzBM * 128 + in),
-                                umma_desc_sw128(sB + off * kOzPBN * 128 + in), idesc, accum);
+                                umma_desc_sw128(sB + off * kOzTN * 128 + in), idesc, accum);
                         accum = 1;
                     }
                     umma_commit(sm_addr(&empty[s]));
@@ -530,90 +289,93 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
         }
         __syncwarp();
     } else {
-        // ---- epilogue warps: quadrant q of the TMEM lanes, half of the columns
+        // ---- epilogue warps: TMEM lane quadrant q (warp % 4) and a quarter
+        // of the columns each; a thread owns one tile row and 8 adjacent
+        // columns (64 contiguous bytes of each dense array), so the warps
+        // need no barrier among themselves
         const int q = warp & 3;
-        const int half = (warp - 2) >> 2;
-        const int r = q * 32 + lane;          // the tile row this thread drains
-        const int et = threadIdx.x - 64;      // 0 .. 255 in the coalesced pass
+        const int part = (warp - 2) >> 2;
+        const int r = q * 32 + lane;
         const double shift = st->shift;
         const double lnz = st->log_z;
         const double inv_z = exp(-lnz);
         const int e = *d_e;
         for (int it = 0; it < nmine; ++it) {
             const int tb = it & 1;
+            const int t = tiles[blockIdx.x + it * gridDim.x];
+            const int m = (t / g.tiles_n) * kOzBM + r;
+            const int n0 = (t % g.tiles_n) * kOzTN + part * kOzCols;
+            const uint32_t xd0 = ((uint32_t)m << ep.n2) | (uint32_t)n0;
+            const bool row_in = m < g.M;
+            // the row's entropy, log iterate and weighted iterate, loaded
+            // while its accumulators are produced (16-byte pieces: n0 is a
+            // multiple of 8 and the dense rows are 2^n2 >= 32 wide)
+            double2 hv[kOzCols / 2], pwv[kOzCols / 2], ltv[kOzCols / 2];
+            if (row_in) {
+#pragma unroll
+                for (int j = 0; j < kOzCols / 2; ++j) {
+                    hv[j] = __ldg((const double2*)(ep.hx + xd0) + j);
+                    pwv[j] = ((const double2*)(ep.Pw + xd0))[j];
+                    ltv[j] = ((const double2*)(ep.Lt + xd0))[j];
+                }
+            }
             const bool got = mbar_wait(sm_addr(&tfull[tb]), (it >> 1) & 1) && !aborted();
             if (!got) give_up();
             tc_fence_after();
-            constexpr int HC = kOzPBN / 2;  // columns per half
-            double gsum[HC];
+            double gsum[kOzCols];
 #pragma unroll
-            for (int j = 0; j < HC; ++j) gsum[j] = 0.0;
+            for (int j = 0; j < kOzCols; ++j) gsum[j] = 0.0;
             if (got) {
-                const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tb * kOzPBuf + half * HC);
-#pragma unroll 1
-                for (int a = kOzW - 1; a >= 0; --a) {
-                    const double w = ldexp(1.0, e - 7 * a);
-                    uint32_t v[16];
-                    tmem_ld16(trow + (uint32_t)(a * kOzPBN), v);
+                const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tb * kOzBuf + part * kOzCols);
+#pragma unroll
+                for (int b = kOzW / 2 - 1; b >= 0; --b) {
+                    uint32_t v0[kOzCols], v1[kOzCols];
+                    tmem_ld8(trow + (uint32_t)(2 * b * kOzTN), v0);
+                    tmem_ld8(trow + (uint32_t)((2 * b + 1) * kOzTN), v1);
+                    // 2^{e - 7(2b+1)} from its exponent bits (e >= -900, so normal)
+                    const double w = __hiloint2double((1023 + e - 7 * (2 * b + 1)) << 20, 0);
                     tmem_wait_ld();
 #pragma unroll
-                    for (int j = 0; j < HC; ++j) gsum[j] = fma((double)(int32_t)v[j], w, gsum[j]);
+                    for (int j = 0; j < kOzCols; ++j)
+                        gsum[j] = fma((double)((int32_t)v0[j] * 128 + (int32_t)v1[j]), w, gsum[j]);
                 }
             }
-            // the TMEM buffer is free for the tile after next
+            // this warp's part of the TMEM buffer is free for the tile after next
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(sm_addr(&tempty[tb]));
-            epi_sync();  // the previous tile's pass is done with the shared tile
-            if (aborted()) break;  // uniform: read after the barrier
+            if (!got || !row_in) continue;
+            // the BA update; positions that hold no representative keep their
+            // values, so every 16-byte piece is written whole
 #pragma unroll
-            for (int j = 0; j < HC; ++j) gt[r * kOzPTileLd + half * HC + j] = gsum[j];
-            epi_sync();
-            // coalesced pass: element (row, col) = (i / 32, lane), 16 per thread
-            const int t = tiles[blockIdx.x + it * gridDim.x];
-            const int m0 = (t / g.tiles_n) * kOzBM, n = (t % g.tiles_n) * kOzPBN + lane;
-#pragma unroll 1
-            for (int i0 = 0; i0 < kOzBM * kOzPBN / (32 * kOzPEpiWarps); i0 += 8) {
-                uint32_t xdv[8];
-                bool rep[8];
-                double hv[8], pwv[8], ltv[8];
+            for (int j = 0; j < kOzCols / 2; ++j) {
+                double lo[2] = {ltv[j].x, ltv[j].y}, po[2] = {pwv[j].x, pwv[j].y};
+                const double hh[2] = {hv[j].x, hv[j].y};
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int row = (et >> 5) + (i0 + u) * kOzPEpiWarps;
-                    const int m = m0 + row;
-                    const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t xd = xd0 + 2 * j + h;
                     const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);
                     const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
-                    rep[u] = (m < g.M) && (n < g.N) && is_rep(x, ep.n);
-                    xdv[u] = xd;
-                    hv[u] = rep[u] ? __ldg(ep.hx + xd) : 0.0;
-                    pwv[u] = rep[u] ? ep.Pw[xd] : 0.0;
-                    ltv[u] = rep[u] ? ep.Lt[xd] : 0.0;
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    if (!rep[u]) continue;
-                    const int row = (et >> 5) + (i0 + u) * kOzPEpiWarps;
-                    const uint32_t xd = xdv[u];
-                    const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);
-                    const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
+                    if (!is_rep(x, ep.n)) continue;
                     const double o = (double)orbit_size(x, ep.n);
-                    const double D = hv[u] - gt[row * kOzPTileLd + lane] * ep.inv_c;
+                    const double D = hh[h] - gsum[2 * j + h] * ep.inv_c;
                     if (ep.Dout) ep.Dout[xd] = D;
                     // exact zeros of the caller's distribution (Lt = NaN) take ln p = 0
                     // (backend/BAA.cu:573-580)
-                    const bool zero_in = (ltv[u] != ltv[u]);
-                    const double lnp = zero_in ? 0.0 : ltv[u] - lnz;
+                    const bool zero_in = (lo[h] != lo[h]);
+                    const double lnp = zero_in ? 0.0 : lo[h] - lnz;
                     const double lw = lnp + ep.eta * D - shift;
                     const double ex = exp(lw);
-                    ep.Lt[xd] = lw;
-                    ep.Pw[xd] = o * ex;
                     mD = fmax(mD, D);
                     mL = fmax(mL, lw);
                     sE = fma(o, ex, sE);
-                    sR = fma(pwv[u] * inv_z, D, sR);
+                    sR = fma(po[h] * inv_z, D, sR);
                     if (zero_in) zero = 1.0;
+                    lo[h] = lw;
+                    po[h] = o * ex;
                 }
+                ((double2*)(ep.Lt + xd0))[j] = make_double2(lo[0], lo[1]);
+                ((double2*)(ep.Pw + xd0))[j] = make_double2(po[0], po[1]);
             }
         }
     }
@@ -625,7 +387,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
     __syncthreads();
     const bool ran = !aborted();
     if (!ran && threadIdx.x == 0) st->error = kErrOzakiWait;
-    __shared__ double red[5][kOzPThreads / 32];
+    __shared__ double red[5][kOzThreads / 32];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         mD = fmax(mD, __shfl_xor_sync(0xFFFFFFFFu, mD, off));
@@ -644,7 +406,7 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
     __syncthreads();
     if (threadIdx.x == 0) {
         double a0 = red[0][0], a1 = red[1][0], a2 = red[2][0], a3 = red[3][0], a4 = red[4][0];
-        for (int w = 1; w < kOzPThreads / 32; ++w) {
+        for (int w = 1; w < kOzThreads / 32; ++w) {
             a0 = fmax(a0, red[0][w]);
             a1 += red[1][w];
             a2 = fmax(a2, red[2][w]);
@@ -671,103 +433,88 @@ k_oz_ba_p(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUte
 }
 
 // ------------------------------------------------------ operand preparation
-// block maxima of |ML| (RB rows [0, KL)) and |NR| (LA columns [KL, KL + KR))
-__global__ void __launch_bounds__(256) k_oz_maxabs(const double* __restrict__ RB, int64_t nml,
-                                                   const double* __restrict__ LA, int Kp, int KL, int KR, int rows,
-                                                   double* __restrict__ part, const DevState* st) {
-    if (st->done || st->error) return;
-    double m = 0.0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nml; i += stride) m = fmax(m, fabs(RB[i]));
-    const int64_t nnr = (int64_t)rows * KR;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nnr; i += stride)
-        m = fmax(m, fabs(LA[(i / KR) * Kp + KL + (i % KR)]));
-    __shared__ double red[256];
-    red[threadIdx.x] = m;
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
-        __syncthreads();
+// The J truncated base-128 digits of v 2^{-e} (|v| < 2^e), sign included:
+// with N = trunc(v 2^{7J - e}) (a power-of-two scaling, exact, then a
+// truncating conversion, exact since |N| < 2^{7J}), digit s is the sign of v
+// times bits [7(J-1-s), 7(J-s)) of |N| -- the digits that repeated
+// "multiply by 128, truncate, subtract" would give.  Four values' digit s
+// packed into one 32-bit word per call.
+__device__ __forceinline__ uint32_t oz_pack4(const long long (&N)[4], int s) {
+    uint32_t w = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const unsigned long long a = (unsigned long long)(N[j] < 0 ? -N[j] : N[j]);
+        const int d = (int)((a >> (7 * (kOzJ - 1 - s))) & 127u);
+        w |= (uint32_t)(uint8_t)(int8_t)(N[j] < 0 ? -d : d) << (8 * j);
     }
-    if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+    return w;
 }
 
-// e with max |X| < 2^e (frexp); a non-finite operand is a device error
-__global__ void __launch_bounds__(256) k_oz_exponent(const double* __restrict__ part, int nb, int* __restrict__ e_out,
-                                                     DevState* st) {
-    if (st->done || st->error) return;
-    double m = 0.0;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) m = fmax(m, part[b]);
-    __shared__ double red[256];
-    red[threadIdx.x] = m;
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
-        __syncthreads();
-    }
-    if (threadIdx.x != 0) return;
-    m = red[0];
-    if (!isfinite(m)) {
-        st->error = kErrOzakiOperand;
-        return;
-    }
-    int e = 0;
-    if (m > 0.0) frexp(m, &e);  // m = f 2^e, f in [0.5, 1)
-    *e_out = e;
-}
-
-// J truncated base-128 digits of v 2^{-e} (|v| < 2^e): exact in FP64
-__device__ __forceinline__ void oz_digits(double v, int e, int8_t (&d)[kOzJ]) {
-    double u = ldexp(v, -e);
+// 16 values -> their J digit slices as 16-byte words dst[s * pitch] (s < J)
+__device__ __forceinline__ void oz_slice16(const double (&v)[16], double scale, uint8_t* dst, int pitch) {
+    long long N[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) N[j] = __double2ll_rz(v[j] * scale);
 #pragma unroll
     for (int s = 0; s < kOzJ; ++s) {
-        u *= 128.0;
-        const double q = trunc(u);
-        d[s] = (int8_t)(int)q;
-        u -= q;
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const long long n4[4] = {N[4 * q], N[4 * q + 1], N[4 * q + 2], N[4 * q + 3]};
+            w[q] = oz_pack4(n4, s);
+        }
+        *(uint4*)(dst + (size_t)s * pitch) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
-__device__ __forceinline__ uint4 pack16(const int8_t (&dig)[16][kOzJ], int s) {
-    uint32_t w[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-        w[q] = (uint32_t)(uint8_t)dig[4 * q][s] | ((uint32_t)(uint8_t)dig[4 * q + 1][s] << 8) |
-               ((uint32_t)(uint8_t)dig[4 * q + 2][s] << 16) | ((uint32_t)(uint8_t)dig[4 * q + 3][s] << 24);
-    return make_uint4(w[0], w[1], w[2], w[3]);
+// The operands' exponent e (max |X| < 2^e, frexp) from the bound |ML|, |NR|
+// <= max |ln q| * cmax: each operand entry is ln q summed against a table row
+// whose entries add up to at most cmax.  Every block of the slicing launch
+// reduces the 2^k values of ln q (from L2) itself; false on a non-finite ln q.
+__device__ __forceinline__ bool oz_exponent(const double* __restrict__ lnq, int ny, double cmax, int* e_out) {
+    __shared__ double red[256];
+    double m = 0.0;
+    for (int y = threadIdx.x; y < ny; y += blockDim.x) m = fmax(m, fabs(lnq[y]));
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + h]);
+        __syncthreads();
+    }
+    // headroom for the rounding of the FP64 operands (sums of at most cmax
+    // terms, relative error far below 2^-30), so that |X| < 2^e holds for the
+    // computed values too
+    m = red[0] * cmax * (1.0 + 0x1p-30);
+    if (!isfinite(m)) return false;
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);  // m = f 2^e, f in [0.5, 1)
+    // raising e keeps |X| < 2^e; the weights 2^{e - 7a} stay normal numbers
+    *e_out = e < -900 ? -900 : e;
+    return true;
 }
 
-// NR (LA columns KL + r) -> Ad[m][slot 1 + s][r]; one thread per (row, 16 r)
-__global__ void __launch_bounds__(256) k_oz_slice_a(const double* __restrict__ LA, int Kp, int KL, int KR, int rows,
-                                                    int KRp, uint8_t* __restrict__ Ad, const int* __restrict__ d_e,
-                                                    const DevState* st) {
-    if (st->done || st->error) return;
-    const int e = *d_e;
+// NR (LA columns KL + r) -> Ad[m][slot 1 + s][r]; one thread per (row, 16 r),
+// over blocks [b0, b0 + nb) of the launch
+__device__ __forceinline__ void oz_slice_a(const double* __restrict__ LA, int Kp, int KL, int KR, int rows, int KRp,
+                                           uint8_t* __restrict__ Ad, double scale, int b0, int nb) {
     const int chunks = KRp / 16;
     const int64_t total = (int64_t)rows * chunks;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = (blockIdx.x - b0) * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)nb * blockDim.x) {
         const int m = (int)(i / chunks), c = (int)(i % chunks);
-        int8_t dig[16][kOzJ];
+        double v[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int r = c * 16 + j;
-            const double v = (r < KR) ? LA[(int64_t)m * Kp + KL + r] : 0.0;
-            oz_digits(v, e, dig[j]);
+            v[j] = (r < KR) ? LA[(int64_t)m * Kp + KL + r] : 0.0;
         }
-        uint8_t* row = Ad + (int64_t)m * kOzP * KRp;
-#pragma unroll
-        for (int s = 0; s < kOzJ; ++s) *(uint4*)(row + (s + 1) * KRp + c * 16) = pack16(dig, s);
+        oz_slice16(v, scale, Ad + (int64_t)m * kOzP * KRp + KRp + c * 16, KRp);
     }
 }
 
 // ML (RB rows k < KL, column n) -> Bd[n][slot 1 + s][k]: a block transposes a
-// 32-column strip of RB through shared memory; thread (column, 16 k) packs
-__global__ void __launch_bounds__(256) k_oz_slice_b(const double* __restrict__ RB, int KL, int cols, int KLp,
-                                                    uint8_t* __restrict__ Bd, const int* __restrict__ d_e,
-                                                    const DevState* st) {
-    if (st->done || st->error) return;
-    extern __shared__ double tile[];  // [KLp][33]
-    const int e = *d_e;
+// 32-column strip of RB through shared memory; thread (column, 16 k) slices
+__device__ __forceinline__ void oz_slice_b(const double* __restrict__ RB, int KL, int cols, int KLp,
+                                           uint8_t* __restrict__ Bd, double scale, double* tile) {
     const int n0 = blockIdx.x * 32;
     for (int i = threadIdx.x; i < KLp * 32; i += blockDim.x) {
         const int k = i / 32, c = i % 32;
@@ -778,13 +525,31 @@ __global__ void __launch_bounds__(256) k_oz_slice_b(const double* __restrict__ R
     for (int i = threadIdx.x; i < 32 * chunks; i += blockDim.x) {
         const int c = i % 32, ch = i / 32;
         if (n0 + c >= cols) continue;
-        int8_t dig[16][kOzJ];
+        double v[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) oz_digits(tile[(ch * 16 + j) * 33 + c], e, dig[j]);
-        uint8_t* row = Bd + (int64_t)(n0 + c) * kOzP * KLp;
-#pragma unroll
-        for (int s = 0; s < kOzJ; ++s) *(uint4*)(row + (s + 1) * KLp + ch * 16) = pack16(dig, s);
+        for (int j = 0; j < 16; ++j) v[j] = tile[(ch * 16 + j) * 33 + c];
+        oz_slice16(v, scale, Bd + (int64_t)(n0 + c) * kOzP * KLp + KLp + ch * 16, KLp);
     }
+}
+
+// the exponent and both slicings in one launch: blocks [0, nb_b) the
+// 32-column strips of ML, the rest NR; block 0 publishes e for the product
+__global__ void __launch_bounds__(256) k_oz_slice(const double* __restrict__ RB, const double* __restrict__ LA, int Kp,
+                                                  int KL, int KR, int rows, int cols, int KLp, int KRp,
+                                                  uint8_t* __restrict__ Ad, uint8_t* __restrict__ Bd, int nb_b,
+                                                  const double* __restrict__ lnq, int ny, double cmax,
+                                                  int* __restrict__ d_e, DevState* st) {
+    if (st->done || st->error) return;
+    extern __shared__ double tile[];  // [KLp][33]
+    int e = 0;
+    if (!oz_exponent(lnq, ny, cmax, &e)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) st->error = kErrOzakiOperand;
+        return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d_e = e;
+    const double scale = ldexp(1.0, 7 * kOzJ - e);
+    if ((int)blockIdx.x < nb_b) oz_slice_b(RB, KL, cols, KLp, Bd, scale, tile);
+    else oz_slice_a(LA, Kp, KL, KR, rows, KRp, Ad, scale, nb_b, (int)gridDim.x - nb_b);
 }
 
 // the integer operands, once: As[m] = [lo | hi] of AL[m][k] (LA columns k <
@@ -850,13 +615,11 @@ void ozaki_free(OzakiG* oz) {
     cudaFree(oz->Ad);
     cudaFree(oz->Bd);
     cudaFree(oz->d_e);
-    cudaFree(oz->mpart);
     cudaFree(oz->d_tiles);
-    cudaFree(oz->d_tilesP);
     delete oz;
 }
 
-int ozaki_partials(const OzakiG* oz) { return oz->persistent ? oz->gridP : oz->tiles; }
+int ozaki_partials(const OzakiG* oz) { return oz->grid; }
 
 // tile ids (tm * tiles_n + tn) of BM x bn tiles that hold a representative
 static std::vector<int> rep_tiles(const OzakiInput& in, int bn, int* tiles_n) {
@@ -872,7 +635,7 @@ static std::vector<int> rep_tiles(const OzakiInput& in, int bn, int* tiles_n) {
     return ids;
 }
 
-bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, OzakiG** out, const char** why) {
+bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const char** why) {
     *out = nullptr;
     *why = nullptr;
     auto round32 = [](int v) { return (v + 31) / 32 * 32; };
@@ -897,17 +660,20 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, Ozak
     oz->bS = (2 * KRp + 127) / 128;
     oz->aD = (2 * KRp + 127) / 128;
     oz->bD = (2 * KLp + 127) / 128;
-    oz->smem = 1024 + (oz->aS * kOzBM + oz->bS * kOzBN) * 128 + kOzStages * (oz->aD * kOzBM + oz->bD * kOzBN) * 128;
-    oz->persistent = persistent;
     int dev_smem = 0;
     BDC_CUDA_TRY(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, H->device));
-    // the persistent form: the deepest ring (<= kOzStages) that fits with the FP64 tile
-    for (oz->stagesP = kOzStages; oz->stagesP >= 2; --oz->stagesP) {
-        oz->smemP = 1024 + 2 * (oz->aS * kOzBM + oz->bS * kOzPBN) * 128 +
-                    oz->stagesP * (oz->aD * kOzBM + oz->bD * kOzPBN) * 128 + kOzPTileBytes;
-        if (oz->smemP + 2048 <= dev_smem) break;
+    // the deepest ring (<= kOzStages) that fits
+    for (oz->stages = kOzStages; oz->stages >= 2; --oz->stages) {
+        oz->smem = 1024 + 2 * (oz->aS * kOzBM + oz->bS * kOzTN) * 128 +
+                    oz->stages * (oz->aD * kOzBM + oz->bD * kOzTN) * 128;
+        if (oz->smem + 2048 <= dev_smem) break;
     }
-    if ((persistent ? oz->smemP : oz->smem) + 2048 > dev_smem) {
+    if (in.H2 % kOzTN) {
+        ozaki_free(oz);
+        *why = "dense rows narrower than a tile";
+        return BDC_OK;
+    }
+    if (oz->smem + 2048 > dev_smem) {
         ozaki_free(oz);
         *why = "tile operands exceed shared memory";
         return BDC_OK;
@@ -926,8 +692,6 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, Ozak
     BDC_CUDA_TRY(al(&oz->Bd, (size_t)cols * kOzP * KLp));
     BDC_CUDA_TRY(cudaMalloc(&oz->d_e, sizeof(int)));
     BDC_CUDA_TRY(cudaMemsetAsync(oz->d_e, 0, sizeof(int), s));
-    oz->nmax = H->num_sms * 2;
-    BDC_CUDA_TRY(cudaMalloc(&oz->mpart, sizeof(double) * oz->nmax));
     {
         int* bad = nullptr;
         BDC_CUDA_TRY(cudaMalloc(&bad, sizeof(int)));
@@ -945,37 +709,27 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, Ozak
             return BDC_OK;
         }
     }
-    // tiles that hold a representative, for both tile widths
+    // tiles that hold a representative
     {
-        std::vector<int> ids = rep_tiles(in, kOzBN, &oz->tiles_n);
-        oz->tiles = (int)ids.size();
+        std::vector<int> idsP = rep_tiles(in, kOzTN, &oz->tiles_n);
+        oz->tiles = (int)idsP.size();
+        oz->grid = std::min(oz->tiles, H->num_sms);
         if (oz->tiles > 0) {
-            BDC_CUDA_TRY(cudaMalloc(&oz->d_tiles, sizeof(int) * ids.size()));
-            BDC_CUDA_TRY(cudaMemcpy(oz->d_tiles, ids.data(), sizeof(int) * ids.size(), cudaMemcpyHostToDevice));
-        }
-        std::vector<int> idsP = rep_tiles(in, kOzPBN, &oz->tiles_nP);
-        oz->tilesP = (int)idsP.size();
-        oz->gridP = std::min(oz->tilesP, H->num_sms);
-        if (oz->tilesP > 0) {
-            BDC_CUDA_TRY(cudaMalloc(&oz->d_tilesP, sizeof(int) * idsP.size()));
-            BDC_CUDA_TRY(cudaMemcpy(oz->d_tilesP, idsP.data(), sizeof(int) * idsP.size(), cudaMemcpyHostToDevice));
+            BDC_CUDA_TRY(cudaMalloc(&oz->d_tiles, sizeof(int) * idsP.size()));
+            BDC_CUDA_TRY(cudaMemcpy(oz->d_tiles, idsP.data(), sizeof(int) * idsP.size(), cudaMemcpyHostToDevice));
         }
     }
     const bool ok = make_map(&oz->tmAs, oz->As, 2 * KLp, rows, kOzBM) &&
-                    make_map(&oz->tmBs, oz->Bs, 2 * KRp, cols, kOzBN) &&
                     make_map(&oz->tmAd, oz->Ad, (uint64_t)kOzP * KRp, rows, kOzBM) &&
-                    make_map(&oz->tmBd, oz->Bd, (uint64_t)kOzP * KLp, cols, kOzBN) &&
-                    make_map(&oz->tmBsP, oz->Bs, 2 * KRp, cols, kOzPBN) &&
-                    make_map(&oz->tmBdP, oz->Bd, (uint64_t)kOzP * KLp, cols, kOzPBN);
+                    make_map(&oz->tmBs, oz->Bs, 2 * KRp, cols, kOzTN) &&
+                    make_map(&oz->tmBd, oz->Bd, (uint64_t)kOzP * KLp, cols, kOzTN);
     if (!ok) {
         ozaki_free(oz);
         *why = "tensor map encoding failed";
         return BDC_OK;
     }
     BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smem));
-    if (oz->smemP + 2048 <= dev_smem)
-        BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba_p, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smemP));
-    BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_slice_b, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_slice, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(double) * KLp * 33));
     *out = oz;
     return BDC_OK;
@@ -983,32 +737,21 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, Ozak
 
 cudaError_t ozaki_prepare(OzakiG* oz, DevState* st, cudaStream_t s) {
     const OzakiInput& in = oz->in;
-    k_oz_maxabs<<<oz->nmax, 256, 0, s>>>(in.RB, (int64_t)in.KL * in.H2, in.LA, in.Kp, in.KL, in.KR, in.H1h, oz->mpart,
-                                         st);
-    k_oz_exponent<<<1, 256, 0, s>>>(oz->mpart, oz->nmax, oz->d_e, st);
-    {
-        const int64_t work = (int64_t)in.H1h * (oz->KRp / 16);
-        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, 148 * 8));
-        k_oz_slice_a<<<blocks, 256, 0, s>>>(in.LA, in.Kp, in.KL, in.KR, in.H1h, oz->KRp, oz->Ad, oz->d_e, st);
-    }
-    k_oz_slice_b<<<(in.H2 + 31) / 32, 256, sizeof(double) * oz->KLp * 33, s>>>(in.RB, in.KL, in.H2, oz->KLp, oz->Bd,
-                                                                              oz->d_e, st);
+    const int nb_b = (in.H2 + 31) / 32;
+    const int64_t work_a = (int64_t)in.H1h * (oz->KRp / 16);
+    const int nb_a = (int)std::max<int64_t>(1, std::min<int64_t>((work_a + 255) / 256, 148 * 4));
+    k_oz_slice<<<nb_b + nb_a, 256, sizeof(double) * oz->KLp * 33, s>>>(
+        in.RB, in.LA, in.Kp, in.KL, in.KR, in.H1h, in.H2, oz->KLp, oz->KRp, oz->Ad, oz->Bd, nb_b, in.lnq, 1 << in.k,
+        in.cmax, oz->d_e, st);
     return cudaGetLastError();
 }
 
 cudaError_t ozaki_product(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaStream_t s) {
     const OzakiInput& in = oz->in;
-    if (oz->persistent) {
-        if (oz->tilesP == 0) return cudaGetLastError();
-        const OzGeomDev gp{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_nP, oz->stagesP};
-        k_oz_ba_p<<<oz->gridP, kOzPThreads, oz->smemP, s>>>(oz->tmAs, oz->tmBsP, oz->tmAd, oz->tmBdP, gp,
-                                                           oz->d_tilesP, oz->tilesP, oz->d_e, ep, st);
-        return cudaGetLastError();
-    }
     if (oz->tiles == 0) return cudaGetLastError();
-    const OzGeomDev g{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_n, kOzStages};
-    k_oz_ba<<<oz->tiles, kOzThreads, oz->smem, s>>>(oz->tmAs, oz->tmBs, oz->tmAd, oz->tmBd, g, oz->d_tiles, oz->d_e,
-                                                    ep, st);
+    const OzGeomDev gp{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_n, oz->stages};
+    k_oz_ba<<<oz->grid, kOzThreads, oz->smem, s>>>(oz->tmAs, oz->tmBs, oz->tmAd, oz->tmBd, gp,
+                                                       oz->d_tiles, oz->tiles, oz->d_e, ep, st);
     return cudaGetLastError();
 }
 

@@ -27,9 +27,9 @@ constexpr int kOzJ = 7;          // int8 slices of each FP64 operand (49 bits)
 constexpr int kOzW = kOzJ + 1;   // accumulators (weights 2^{e - 7a}, a = 0..J)
 constexpr int kOzP = kOzJ + 2;   // slots per row of a sliced operand: zero, x_0..x_{J-1}, zero
 constexpr int kOzBM = 128;       // tile rows (x_hi): one TMEM lane each
-constexpr int kOzBN = 64;        // tile columns (dense x_lo): kOzW * kOzBN = 512 TMEM columns
-constexpr int kOzStages = 3;     // pipeline depth of the per-weight operands
-constexpr int kOzThreads = 128;  // 4 warps: TMA producer, MMA issuer, all four run the epilogue
+constexpr int kOzTN = 32;        // tile columns (dense x_lo): two buffers of kOzW * kOzTN TMEM columns
+constexpr int kOzStages = 6;     // deepest ring of the per-weight operands
+constexpr int kOzEpiWarps = 16;  // epilogue warps (beside one TMA producer warp and one MMA warp)
 
 // what the product reads from the factored engine (bdc_factored.cu)
 struct OzakiInput {
@@ -37,35 +37,33 @@ struct OzakiInput {
     const double* RB;               // [Kp][H2]  = [ML ; BR^T]
     int Kp, KL, KR, H1h, H2;
     const int* colmax;              // [H2] largest row of a representative per dense column, -1 if none
+    const double* lnq;              // [2^k] ln q over every output (the operands are ln q contracted with tables)
+    int k;
+    double cmax;                    // the largest row sum of a table the FP64 operands contract ln q with:
+                                    // |ML|, |NR| <= max |ln q| * cmax
 };
 
 struct OzakiG {
     OzakiInput in{};
     int KLp = 0, KRp = 0;           // contraction lengths padded to 32
     int aS = 0, bS = 0, aD = 0, bD = 0;  // 128-byte atom columns: static A / B, per-weight A / B
-    int smem = 0;                   // dynamic shared memory per CTA
     uint8_t* As = nullptr;          // [H1h][2 KLp]  [a_lo | a_hi] of AL
     uint8_t* Bs = nullptr;          // [H2][2 KRp]   [b_lo | b_hi] of BR^T
     uint8_t* Ad = nullptr;          // [H1h][P KRp]  slots of NR
     uint8_t* Bd = nullptr;          // [H2][P KLp]   slots of ML (transposed)
     int* d_e = nullptr;             // the exponent e of this iteration's FP64 operands
-    double* mpart = nullptr;        // block maxima of |ML|, |NR|
-    int nmax = 0;
-    int* d_tiles = nullptr;         // tile ids (tm * tiles_n + tn) that hold representatives
+    // persistent product: one CTA per SM over the 128 x 32 tiles that hold
+    // representatives, two TMEM accumulator buffers
+    int smem = 0, grid = 0, stages = 0;
+    int* d_tiles = nullptr;         // tile ids (tm * tiles_n + tn)
     int tiles = 0, tiles_n = 0;
     CUtensorMap tmAs, tmBs, tmAd, tmBd;
-    // the persistent form: 128 x 32 tiles, one CTA per SM, two TMEM buffers
-    bool persistent = false;
-    int smemP = 0, gridP = 0, stagesP = 0;
-    int* d_tilesP = nullptr;
-    int tilesP = 0, tiles_nP = 0;
-    CUtensorMap tmBsP, tmBdP;
 };
 
 // set-up: *out stays null (with the reason in *why) when the shapes or the
 // table entries are outside what the kernel covers; the caller then keeps
 // the FP64 product
-bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, bool persistent, OzakiG** out, const char** why);
+bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const char** why);
 // rows of block partials the product writes (the finalize's count)
 int ozaki_partials(const OzakiG* oz);
 void ozaki_free(OzakiG* oz);
@@ -73,7 +71,7 @@ void ozaki_free(OzakiG* oz);
 // exponent of the FP64 operands and their int8 slices
 cudaError_t ozaki_prepare(OzakiG* oz, DevState* st, cudaStream_t s);
 // the tensor-core product with the fused BA update; block partials as the
-// FP64 product writes them (ep.part, one row of 8 per tile or per CTA)
+// FP64 product writes them (ep.part, one row of 8 per CTA)
 cudaError_t ozaki_product(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaStream_t s);
 
 }  // namespace bdc

@@ -417,6 +417,7 @@ def ours_arm(args) -> None:
             full["gpu_iterations_per_s"] = 200 / (g0.elapsed_time(g1) / 1e3)
             full["gpu_engine"] = E20.engine
         cpu["full_iteration_20_10"] = full
+        cpu["cache_generator"] = generator_leg(11)
     configs = None
     if rank == 0 and world == 1 and not args.no_configs:
         import copy
@@ -780,6 +781,50 @@ def precision_check(args) -> dict:
     return {"precision": out}
 
 
+GEN_OURS = os.path.join(REPO, "bdc-upper-bounds-gpu_b200", "generate_bit_transition_cache")
+GEN_REF = os.path.join(REPO, "oracle", "_ref", "generate_bit_transition_cache")
+
+
+def _gen_run(exe: str, N: int):
+    """One generator process for every cache_{n,k}, n <= N, in an empty
+    directory: wall seconds, sha256 over the files (names and bytes), bytes."""
+    import hashlib
+    import shutil
+    d = tempfile.mkdtemp(prefix="bdc_gen_")
+    try:
+        os.makedirs(os.path.join(d, "transition_counts"))
+        t0 = time.perf_counter()
+        subprocess.run([exe, str(N)], cwd=d, check=True, stdout=subprocess.DEVNULL, timeout=600)
+        sec = time.perf_counter() - t0
+        h = hashlib.sha256()
+        nbytes = 0
+        for f in sorted(os.listdir(os.path.join(d, "transition_counts"))):
+            b = open(os.path.join(d, "transition_counts", f), "rb").read()
+            nbytes += len(b)
+            h.update(f.encode() + b)
+        return sec, h.hexdigest(), nbytes
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def generator_leg(N: int = 11) -> dict:
+    """The reference's CPU cache generator (one host thread, built from its
+    sources) beside this repository's GPU generator, both as processes with
+    the same argv writing every cache_{n,k} for n <= N; the files must be
+    identical."""
+    if not os.path.exists(GEN_OURS):
+        return {"unavailable": "generate_bit_transition_cache not built"}
+    sec, dig, nbytes = _gen_run(GEN_OURS, N)
+    row = {"N": N, "bytes": nbytes, "ours_s": sec}
+    if os.path.exists(GEN_REF):
+        rsec, rdig, _ = _gen_run(GEN_REF, N)
+        row.update({"reference_s": rsec, "reference_cores": 1, "identical_files": rdig == dig,
+                    "speedup": rsec / sec})
+    else:
+        row["reference"] = "not built (oracle/Makefile ref)"
+    return row
+
+
 def generator_check(args) -> dict:
     """The cache generator: the reference's CPU program (built from its sources
     into oracle/_ref/, when present) and this repository's GPU one
@@ -789,28 +834,8 @@ def generator_check(args) -> dict:
     identical.  ours_counts_only_s is the GPU generation of the same tables
     inside this process, copied to host memory, without files.  The reference runs up to N = 12 (its
     time grows about 4x per N: N = 13 takes about a minute), ours up to 13."""
-    import hashlib
-    import shutil
-
-    ours = os.path.join(REPO, "bdc-upper-bounds-gpu_b200", "generate_bit_transition_cache")
-    ref = os.path.join(REPO, "oracle", "_ref", "generate_bit_transition_cache")
-
-    def run(exe, N):
-        d = tempfile.mkdtemp(prefix="bdc_gen_")
-        try:
-            os.makedirs(os.path.join(d, "transition_counts"))
-            t0 = time.perf_counter()
-            subprocess.run([exe, str(N)], cwd=d, check=True, stdout=subprocess.DEVNULL, timeout=600)
-            sec = time.perf_counter() - t0
-            h = hashlib.sha256()
-            nbytes = 0
-            for f in sorted(os.listdir(os.path.join(d, "transition_counts"))):
-                b = open(os.path.join(d, "transition_counts", f), "rb").read()
-                nbytes += len(b)
-                h.update(f.encode() + b)
-            return sec, h.hexdigest(), nbytes
-        finally:
-            shutil.rmtree(d, ignore_errors=True)
+    ours, ref = GEN_OURS, GEN_REF
+    run = _gen_run
 
     # the counts alone, in this process after a warm-up call (no process start,
     # no CUDA context creation, no file writes)
