@@ -5,9 +5,11 @@
 // (backend/main_BAA.cu:46-50): representatives are compacted on the device,
 // the two half-table bundles are built (from cache files or by the device
 // generator), and the entropy term h(x) = sum_y W ln W is computed once.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "bdc_engine.cuh"
@@ -121,26 +123,60 @@ static int64_t num_reps_of(int n) {
     return (all + fixed_r + fixed_rc) / 4;
 }
 
-bdc_status engine_init(bdc_handle* H) {
-    BDC_CUDA_TRY(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
-    H->stream = H->own_stream;
-    BDC_CUDA_TRY(cudaDeviceGetAttribute(&H->num_sms, cudaDevAttrMultiProcessorCount, H->device));
+// The p-independent data of a handle -- the representatives, the half-table
+// bundles, the rotated A bundle and h(x) per representative -- is read-only
+// after set-up and the same for every handle of one n, k and table source on
+// one device (the seeds of a batch, the ranks of a sharded problem on one
+// device), so those handles share one set, freed with its last handle.
+struct TableSet {
+    int device = 0, n = 0, k = 0;
+    std::string source;  // the cache directory, empty for the device generator
+    int refs = 0;
+    uint32_t* reps = nullptr;
+    uint16_t *hi = nullptr, *lo = nullptr, *rot = nullptr;
+    double* h = nullptr;
+    HalfTables A{}, B{}, Ar{};
+    int64_t nonzero_pairs = 0;
+};
+static std::mutex g_tables_mu;
+static std::vector<TableSet*> g_tables;
+
+static TableSet* find_tables(const bdc_handle* H) {
+    for (TableSet* t : g_tables)
+        if (t->device == H->device && t->n == H->n && t->k == H->k && t->source == H->cache_dir) return t;
+    return nullptr;
+}
+
+static void release_tables(bdc_handle* H) {
+    std::lock_guard<std::mutex> lock(g_tables_mu);
+    TableSet* t = (TableSet*)H->tables;
+    H->tables = nullptr;
+    if (!t) {
+        // set-up failed before its tables were published: they are the handle's own
+        cudaFree(H->d_reps);
+        if (H->d_bundle_lo && H->d_bundle_lo != H->d_bundle_hi) cudaFree(H->d_bundle_lo);
+        cudaFree(H->d_bundle_hi);
+        cudaFree(H->d_bundle_rot);
+        cudaFree(H->d_h);
+    } else if (--t->refs == 0) {
+        cudaFree(t->reps);
+        if (t->lo && t->lo != t->hi) cudaFree(t->lo);
+        cudaFree(t->hi);
+        cudaFree(t->rot);
+        cudaFree(t->h);
+        g_tables.erase(std::find(g_tables.begin(), g_tables.end(), t));
+        delete t;
+    }
+    H->d_reps = nullptr;
+    H->d_bundle_hi = H->d_bundle_lo = H->d_bundle_rot = nullptr;
+    H->d_h = nullptr;
+}
+
+// the representatives, the half-table bundles and the rotated A bundle of a
+// new table set
+static bdc_status build_tables(bdc_handle* H, int mA, int mB) {
     const Split& s = H->s;
-    const int64_t R = num_reps_of(H->n);
-    H->R = R;
-
-    // memory estimate (the reference checks 95% of free memory with an
-    // assert, backend/BAA.cu:31-44, which vanishes under NDEBUG)
-    const int mA = mmax_for_high(s), mB = mmax_for_low(s);
-    size_t need = 0;
-    need += ((size_t)bundle_stride(mA) << s.n1) * 2 * 2;  // and its rotated copy
-    if (s.n2 != s.n1) need += ((size_t)bundle_stride(mB) << s.n2) * 2;
-    need += (size_t)R * (4 + 8 * 5);
-    size_t free_b = 0, total_b = 0;
-    BDC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-    if (need > (size_t)(0.95 * (double)free_b))
-        return fail(BDC_ERR_NOMEM, "need about %zu MB of device memory, %zu MB free", need >> 20, free_b >> 20);
-
+    const int64_t R = H->R;
     // representatives
     BDC_CUDA_TRY(dalloc(H, &H->d_reps, (size_t)R));
     {
@@ -189,10 +225,60 @@ bdc_status engine_init(bdc_handle* H) {
         H->Ar = H->A;
         H->Ar.rows = H->d_bundle_rot;
     }
+    return BDC_OK;
+}
+
+bdc_status engine_init(bdc_handle* H) {
+    BDC_CUDA_TRY(cudaStreamCreateWithFlags(&H->own_stream, cudaStreamNonBlocking));
+    H->stream = H->own_stream;
+    BDC_CUDA_TRY(cudaDeviceGetAttribute(&H->num_sms, cudaDevAttrMultiProcessorCount, H->device));
+    const Split& s = H->s;
+    const int64_t R = num_reps_of(H->n);
+    H->R = R;
+
+    // the table set is looked up and, when new, built and published under
+    // the registry's lock
+    std::unique_lock<std::mutex> tables_lock(g_tables_mu);
+    TableSet* shared = find_tables(H);
+
+    // memory estimate (the reference checks 95% of free memory with an
+    // assert, backend/BAA.cu:31-44, which vanishes under NDEBUG)
+    const int mA = mmax_for_high(s), mB = mmax_for_low(s);
+    size_t need = 0;
+    if (!shared) {
+        need += ((size_t)bundle_stride(mA) << s.n1) * 2 * 2;  // and its rotated copy
+        if (s.n2 != s.n1) need += ((size_t)bundle_stride(mB) << s.n2) * 2;
+        need += (size_t)R * (4 + 8);
+    }
+    need += (size_t)R * 8 * 4;
+    size_t free_b = 0, total_b = 0;
+    BDC_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    if (need > (size_t)(0.95 * (double)free_b))
+        return fail(BDC_ERR_NOMEM, "need about %zu MB of device memory, %zu MB free", need >> 20, free_b >> 20);
+
+    if (shared) {
+        ++shared->refs;
+        H->tables = shared;
+        H->d_reps = shared->reps;
+        H->d_bundle_hi = shared->hi;
+        H->d_bundle_lo = shared->lo;
+        H->d_bundle_rot = shared->rot;
+        H->d_h = shared->h;
+        H->A = shared->A;
+        H->B = shared->B;
+        H->Ar = shared->Ar;
+        H->nonzero_pairs = shared->nonzero_pairs;
+        tables_lock.unlock();
+    }
+
+    if (!shared) {
+        bdc_status rc = build_tables(H, mA, mB);
+        if (rc != BDC_OK) return rc;
+    }
 
     // per-representative vectors and reductions
     for (int b = 0; b < 2; ++b) BDC_CUDA_TRY(dalloc(H, &H->d_p[b], (size_t)R));
-    BDC_CUDA_TRY(dalloc(H, &H->d_h, (size_t)R));
+    if (!shared) BDC_CUDA_TRY(dalloc(H, &H->d_h, (size_t)R));
     BDC_CUDA_TRY(dalloc(H, &H->d_d, (size_t)R));
     BDC_CUDA_TRY(dalloc(H, &H->d_logw, (size_t)R));
     const size_t nq = (size_t)1 << (H->k >= 1 ? H->k - 1 : 0);
@@ -222,9 +308,9 @@ bdc_status engine_init(bdc_handle* H) {
     BDC_CUDA_TRY(cudaMallocHost(&H->h_st, sizeof(DevState)));
     memset(H->h_st, 0, sizeof(DevState));
 
-    // h(x) = (1/C) sum_y N ln N - ln C, once per handle; the same pass
+    // h(x) = (1/C) sum_y N ln N - ln C, once per table set; the same pass
     // counts the distinct subsequences of every representative
-    {
+    if (!shared) {
         uint32_t* d_nnz = nullptr;
         BDC_CUDA_TRY(cudaMalloc(&d_nnz, sizeof(uint32_t) * R + 16));
         cudaError_t e = launch_hpass(count_launch(H), H->inv_c, H->log_c, H->d_h, d_nnz);
@@ -237,10 +323,29 @@ bdc_status engine_init(bdc_handle* H) {
         int64_t tot = 0;
         for (uint32_t v : nnz) tot += v;
         H->nonzero_pairs = tot;
+        // publish the set (every kernel that wrote it has completed)
+        TableSet* t = new TableSet();
+        t->device = H->device;
+        t->n = H->n;
+        t->k = H->k;
+        t->source = H->cache_dir;
+        t->refs = 1;
+        t->reps = H->d_reps;
+        t->hi = H->d_bundle_hi;
+        t->lo = H->d_bundle_lo;
+        t->rot = H->d_bundle_rot;
+        t->h = H->d_h;
+        t->A = H->A;
+        t->B = H->B;
+        t->Ar = H->Ar;
+        t->nonzero_pairs = tot;
+        g_tables.push_back(t);
+        H->tables = t;
+        tables_lock.unlock();
     }
 
     if (H->engine == BDC_ENGINE_FACTORED) {
-        rc = factored_init(H);
+        bdc_status rc = factored_init(H);
         if (rc != BDC_OK) return rc;
     }
     if (H->verbose)
@@ -255,12 +360,8 @@ void engine_free(bdc_handle* H) {
     solve_pool_release(H);
     if (H->fac) factored_free(H);
     if (H->stream) cudaStreamSynchronize(H->stream);
-    cudaFree(H->d_reps);
-    if (H->d_bundle_lo && H->d_bundle_lo != H->d_bundle_hi) cudaFree(H->d_bundle_lo);
-    cudaFree(H->d_bundle_hi);
-    cudaFree(H->d_bundle_rot);
+    release_tables(H);
     for (int b = 0; b < 2; ++b) cudaFree(H->d_p[b]);
-    cudaFree(H->d_h);
     cudaFree(H->d_d);
     cudaFree(H->d_logw);
     cudaFree(H->d_lnq);

@@ -25,7 +25,10 @@ struct bdc_handle {
     cudaStream_t stream = nullptr;      // where work is queued
     cudaStream_t own_stream = nullptr;  // created by the handle
     size_t bytes = 0;  // device bytes held
-    // tables
+    // tables (the representatives, the bundles and h below are shared by
+    // every handle of the same n, k and table source on the device:
+    // bdc_engine.cu, TableSet)
+    void* tables = nullptr;
     uint32_t* d_reps = nullptr;
     uint16_t* d_bundle_hi = nullptr;
     uint16_t* d_bundle_lo = nullptr;  // equal to d_bundle_hi when n is even

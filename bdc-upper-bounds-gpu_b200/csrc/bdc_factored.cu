@@ -31,6 +31,7 @@
 #include <cmath>
 #include <map>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cstring>
@@ -606,7 +607,7 @@ __global__ void __launch_bounds__(64) k_thin_d(const ThinD* __restrict__ descs, 
                 if (wb >= d.WIDE) break;
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
-                    const double wv = (double)((pk[u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+                    const double wv = u32_to_f64((pk[u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
                     const double* lr = lqs + (wb + u) * SMALL;
 #pragma unroll
                     for (int i = 0; i < SMALL; ++i) acc[i] = fma(wv, lr[i], acc[i]);
@@ -615,7 +616,7 @@ __global__ void __launch_bounds__(64) k_thin_d(const ThinD* __restrict__ descs, 
         }
     } else if (live) {
         for (int w = q; w < d.WIDE; w += 4) {
-            const double wv = (double)__ldg(v + w);
+            const double wv = u32_to_f64(__ldg(v + w));
             const double* lr = lqs + w * SMALL;
 #pragma unroll
             for (int i = 0; i < SMALL; ++i) acc[i] = fma(wv, lr[i], acc[i]);
@@ -669,15 +670,16 @@ static cudaError_t launch_thin_d(int lg, const ThinD* d, int n, int ctas, int ny
 // and a slice [s0, s1) of its contraction), 2^k / 16 threads, each owning IT
 // (1 or 2) small indices x 16 / IT consecutive wide indices, the latter read
 // as 16-byte pieces of the table row; 16 FP64 FMAs per row and thread.
+__device__ __forceinline__ void unpack2(const uint32_t p, double* v) {
+    v[0] = u32_to_f64(p & 0xFFFFu);
+    v[1] = u32_to_f64(p >> 16);
+}
+
 __device__ __forceinline__ void unpack8(const uint4 p, double* v) {
-    v[0] = (double)(p.x & 0xFFFFu);
-    v[1] = (double)(p.x >> 16);
-    v[2] = (double)(p.y & 0xFFFFu);
-    v[3] = (double)(p.y >> 16);
-    v[4] = (double)(p.z & 0xFFFFu);
-    v[5] = (double)(p.z >> 16);
-    v[6] = (double)(p.w & 0xFFFFu);
-    v[7] = (double)(p.w >> 16);
+    unpack2(p.x, v);
+    unpack2(p.y, v + 2);
+    unpack2(p.z, v + 4);
+    unpack2(p.w, v + 6);
 }
 
 // The slice's rows stream through shared memory with cp.async, kQtRows rows a
@@ -692,12 +694,32 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
 }
 
-__global__ void __launch_bounds__(256) k_qthin(const ThinQ* __restrict__ descs, int stage_bytes, const DevState* st) {
-    if (gated(st)) return;
-    extern __shared__ __align__(16) uint8_t qsm[];
-    const ThinQ& q = descs[blockIdx.x];
-    const int IT = q.SMALL >= 2 ? 2 : 1;
-    const int WT = 16 / IT;
+// small indices a thread covers: up to 8, so that each table entry it
+// converts feeds up to 8 FMAs; the thread's 16 outputs are IT small x 16 / IT
+// wide indices
+__host__ __device__ constexpr int qthin_it(int SMALL) { return SMALL < 8 ? SMALL : 8; }
+
+// the WT = 16 / IT table entries of a thread in one staged row
+template <int WT>
+__device__ __forceinline__ void qthin_entries(const uint8_t* p, double (&v)[WT]) {
+    if constexpr (WT == 16) {
+        const uint4* q = reinterpret_cast<const uint4*>(p);
+        unpack8(q[0], v);
+        unpack8(q[1], v + 8);
+    } else if constexpr (WT == 8) {
+        unpack8(*reinterpret_cast<const uint4*>(p), v);
+    } else if constexpr (WT == 4) {
+        const uint2 q = *reinterpret_cast<const uint2*>(p);
+        unpack2(q.x, v);
+        unpack2(q.y, v + 2);
+    } else {
+        unpack2(*reinterpret_cast<const uint32_t*>(p), v);
+    }
+}
+
+template <int IT>
+__device__ __forceinline__ void qthin_run(const ThinQ& q, int stage_bytes, uint8_t* qsm) {
+    constexpr int WT = 16 / IT;
     const int nwb = q.WIDE / WT;
     const int tid = threadIdx.x;
     const int wb = tid % nwb, ib = tid / nwb;
@@ -730,7 +752,6 @@ __global__ void __launch_bounds__(256) k_qthin(const ThinQ* __restrict__ descs, 
         if (p < nst) issue(p);
         cp_async_commit();
     }
-    double v[16];
     for (int stg = 0; stg < nst; ++stg) {
         cp_async_wait<kQtStages - 2>();
         __syncthreads();
@@ -740,26 +761,14 @@ __global__ void __launch_bounds__(256) k_qthin(const ThinQ* __restrict__ descs, 
         const double* sb = reinterpret_cast<const double*>(base + kQtRows * wbytes);
         const int nr = min(kQtRows, q.s1 - (q.s0 + stg * kQtRows));
         if (i0 < q.SMALL) {
-            if (IT == 2) {
-                for (int r = 0; r < nr; ++r) {
-                    const uint4 pk = *reinterpret_cast<const uint4*>(base + r * wbytes + w0 * 2);
-                    const double a0 = sb[r * q.SMALL + i0], a1 = sb[r * q.SMALL + i0 + 1];
-                    unpack8(pk, v);
+            for (int r = 0; r < nr; ++r) {
+                double v[WT];
+                qthin_entries<WT>(base + r * wbytes + w0 * 2, v);
 #pragma unroll
-                    for (int e = 0; e < 8; ++e) {
-                        acc[e] = fma(a0, v[e], acc[e]);
-                        acc[8 + e] = fma(a1, v[e], acc[8 + e]);
-                    }
-                }
-            } else {
-                for (int r = 0; r < nr; ++r) {
-                    const uint4* wr = reinterpret_cast<const uint4*>(base + r * wbytes + w0 * 2);
-                    const uint4 p0 = wr[0], p1 = wr[1];
-                    const double a0 = sb[r * q.SMALL + i0];
-                    unpack8(p0, v);
-                    unpack8(p1, v + 8);
+                for (int t = 0; t < IT; ++t) {
+                    const double a = sb[r * q.SMALL + i0 + t];
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) acc[e] = fma(a0, v[e], acc[e]);
+                    for (int e = 0; e < WT; ++e) acc[t * WT + e] = fma(a, v[e], acc[t * WT + e]);
                 }
             }
         }
@@ -768,9 +777,21 @@ __global__ void __launch_bounds__(256) k_qthin(const ThinQ* __restrict__ descs, 
     if (i0 >= q.SMALL) return;
 #pragma unroll
     for (int e = 0; e < 16; ++e) {
-        const int i = i0 + (IT == 2 ? e / 8 : 0), w = w0 + (IT == 2 ? e % 8 : e);
+        const int i = i0 + e / WT, w = w0 + e % WT;
         if (q.out_trans) q.out[(int64_t)w * q.SMALL + i] = acc[e];
         else q.out[(int64_t)i * q.WIDE + w] = acc[e];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_qthin(const ThinQ* __restrict__ descs, int stage_bytes, const DevState* st) {
+    if (gated(st)) return;
+    extern __shared__ __align__(16) uint8_t qsm[];
+    const ThinQ& q = descs[blockIdx.x];
+    switch (qthin_it(q.SMALL)) {
+        case 1: qthin_run<1>(q, stage_bytes, qsm); break;
+        case 2: qthin_run<2>(q, stage_bytes, qsm); break;
+        case 4: qthin_run<4>(q, stage_bytes, qsm); break;
+        default: qthin_run<8>(q, stage_bytes, qsm); break;
     }
 }
 
@@ -834,7 +855,7 @@ __global__ void __launch_bounds__(256) k_dthin(const ThinDF* __restrict__ descs,
             for (int u = 0; u < 8; ++u) {
                 double v[kDfRT];
 #pragma unroll
-                for (int r = 0; r < kDfRT; ++r) v[r] = (double)((pk[c][r][u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+                for (int r = 0; r < kDfRT; ++r) v[r] = u32_to_f64((pk[c][r][u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
 #pragma unroll
                 for (int i = 0; i < IT; ++i) {
                     const double l = lc[u * SMALL + i];
@@ -1324,16 +1345,27 @@ static cudaError_t make_launch(Launch& L, std::vector<GemmDesc> v, int cfg) {
 }
 
 template <typename F>
-static float time_ms(bdc_handle* H, F&& launch) {
-    // the best of three rounds of three launches, after a warm-up launch
+static float time_ms(bdc_handle* H, F&& launch, cudaError_t* err = nullptr) {
+    // the best of three rounds of three launches, after a warm-up launch; a
+    // launch that returns an error (or leaves one) makes the time 1e30 and
+    // the error is passed out through err
+    cudaError_t first = cudaSuccess;
+    auto run = [&] {
+        if constexpr (std::is_same_v<decltype(launch()), cudaError_t>) {
+            const cudaError_t e = launch();
+            if (first == cudaSuccess) first = e;
+        } else {
+            launch();
+        }
+    };
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
-    launch();
+    run();
     float best = 1e30f;
     for (int round = 0; round < 3; ++round) {
         cudaEventRecord(a, H->stream);
-        for (int r = 0; r < 3; ++r) launch();
+        for (int r = 0; r < 3; ++r) run();
         cudaEventRecord(b, H->stream);
         cudaEventSynchronize(b);
         float ms = 0.f;
@@ -1342,7 +1374,10 @@ static float time_ms(bdc_handle* H, F&& launch) {
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    return (cudaGetLastError() == cudaSuccess) ? best : 1e30f;
+    const cudaError_t last = cudaGetLastError();
+    if (first == cudaSuccess) first = last;
+    if (err) *err = first;
+    return first == cudaSuccess ? best : 1e30f;
 }
 
 // G with only the tiles that hold representatives (colmax: per dense column
@@ -1441,8 +1476,9 @@ static bdc_status tune_thin(bdc_handle* H, TuneFile& tf, const char* key, Launch
             }
             // the product and the sum of its S split slices
             const float ms = time_ms(H, [&] {
-                launch_store(T, H->stream, nullptr);
+                const cudaError_t e = launch_store(T, H->stream, nullptr);
                 post(S);
+                return e;
             });
             free_launch(T);
             if (ms < best) {
@@ -1511,7 +1547,7 @@ static bdc_status tune_class(bdc_handle* H, TuneFile& tf, const char* key, const
         if (pinned) break;
         Launch T;
         BDC_CUDA_TRY(make_launch(T, descs, c));
-        const float ms = time_ms(H, [&] { launch_store(T, H->stream, nullptr); });
+        const float ms = time_ms(H, [&] { return launch_store(T, H->stream, nullptr); });
         free_launch(T);
         if (ms < best) {
             best = ms;
@@ -1948,9 +1984,9 @@ bdc_status factored_init(bdc_handle* H) {
         std::vector<ThinQ> all_q;
         for (int lg = 0; lg < 8; ++lg)
             for (auto& q : tq[lg]) {
-                const int IT = q.SMALL >= 2 ? 2 : 1;
+                const int IT = qthin_it(q.SMALL);
                 const int WT = 16 / IT;
-                if (q.WIDE % WT != 0 || (q.WIDE / WT) * (q.SMALL / IT) != ny / 16 ||
+                if ((q.SMALL & (q.SMALL - 1)) != 0 || q.WIDE % WT != 0 || (q.WIDE / WT) * (q.SMALL / IT) != ny / 16 ||
                     ((uintptr_t)q.wide & 15) != 0 || (q.wide_stride % 8) != 0 || q.wide_u16 != 1 || q.small_u16 != 0)
                     qok = false;
                 all_q.push_back(q);
@@ -1995,8 +2031,8 @@ bdc_status factored_init(bdc_handle* H) {
             if (pinned_q >= 0) {
                 F->use_qf = pinned_q != 0;
             } else {
-                const float tc = time_ms(H, [&] { enqueue_stage(H, ST_QSMALL, -INFINITY); });
-                const float tfu = time_ms(H, [&] { launch_qthin(F->d_qf, F->n_qf, F->qf_stage, H->stream, nullptr); });
+                const float tc = time_ms(H, [&] { return enqueue_stage(H, ST_QSMALL, -INFINITY); });
+                const float tfu = time_ms(H, [&] { return launch_qthin(F->d_qf, F->n_qf, F->qf_stage, H->stream, nullptr); });
                 F->use_qf = tfu < tc;
                 tf.put("qf", F->use_qf ? 1 : 0, 0);
                 if (H->verbose)
@@ -2023,9 +2059,9 @@ bdc_status factored_init(bdc_handle* H) {
                 F->use_df = pinned_d != 0;
             } else {
                 F->use_df = false;
-                const float tc = time_ms(H, [&] { enqueue_stage(H, ST_DSMALL, -INFINITY); });
+                const float tc = time_ms(H, [&] { return enqueue_stage(H, ST_DSMALL, -INFINITY); });
                 F->use_df = true;
-                const float tfu = time_ms(H, [&] { enqueue_stage(H, ST_DSMALL, -INFINITY); });
+                const float tfu = time_ms(H, [&] { return enqueue_stage(H, ST_DSMALL, -INFINITY); });
                 F->use_df = tfu < tc;
                 tf.put("df", F->use_df ? 1 : 0, 0);
                 if (H->verbose)
@@ -2070,7 +2106,7 @@ bdc_status factored_init(bdc_handle* H) {
             for (int persist = 0; persist < 2; ++persist) {
                 if (persist && T.tiles <= resident(c)) break;
                 T.grid = persist ? resident(c) : 0;
-                const float ms = time_ms(H, [&] { launch_ba(T, ep, H->stream, H->d_st); });
+                const float ms = time_ms(H, [&] { return launch_ba(T, ep, H->stream, H->d_st); });
                 if (ms < best) {
                     best = ms;
                     best_cfg = c;
@@ -2126,21 +2162,35 @@ bdc_status factored_init(bdc_handle* H) {
             const char* why = nullptr;
             bdc_status rc = ozaki_init(H, in, &F->oz, &why);
             if (rc != BDC_OK) return rc;
-            float t_fp = 0.f, t_oz = 0.f;
-            if (F->oz && !force_oz && !pinned) {
-                // both on the zeroed state (the products' cost does not depend on the values)
+            float t_fp = 0.f, t_oz[2] = {0.f, 0.f};
+            if (F->oz && pinned) {
+                F->oz->epi = pick == 8 ? 8 : 16;
+            } else if (F->oz) {
+                // both on the zeroed state (the products' cost does not depend
+                // on the values); the int8 product with 16 and with 8
+                // epilogue warps
                 const BaEpilogue ep = make_epilogue(H);
-                t_fp = time_ms(H, [&] { launch_ba(F->g, ep, H->stream, H->d_st); });
-                t_oz = time_ms(H, [&] {
-                    ozaki_prepare(F->oz, H->d_st, H->stream);
-                    ozaki_product(F->oz, ep, H->d_st, H->stream);
-                });
-                tf.put("oz", t_oz < t_fp ? 1 : 0, 0);
+                cudaError_t e = cudaSuccess;
+                if (!force_oz) {
+                    t_fp = time_ms(H, [&] { return launch_ba(F->g, ep, H->stream, H->d_st); }, &e);
+                    BDC_CUDA_TRY(e);
+                }
+                for (int v = 0; v < 2; ++v) {
+                    F->oz->epi = v == 0 ? 16 : 8;
+                    t_oz[v] = time_ms(H, [&] {
+                        const cudaError_t e1 = ozaki_prepare(F->oz, H->d_st, H->stream);
+                        return e1 != cudaSuccess ? e1 : ozaki_product(F->oz, ep, H->d_st, H->stream);
+                    }, &e);
+                    BDC_CUDA_TRY(e);
+                }
+                F->oz->epi = t_oz[1] < t_oz[0] ? 8 : 16;
+                const bool use = force_oz || std::min(t_oz[0], t_oz[1]) < t_fp;
+                tf.put("oz", use ? F->oz->epi : 0, 0);
                 tf.save();
                 BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
                 BDC_CUDA_TRY(cudaMemsetAsync(F->Lt, 0, sizeof(double) * NX, H->stream));
                 BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
-                if (t_oz >= t_fp) {
+                if (!use) {
                     ozaki_free(F->oz);
                     F->oz = nullptr;
                 }
@@ -2148,12 +2198,15 @@ bdc_status factored_init(bdc_handle* H) {
             F->use_oz = F->oz != nullptr;
             if (H->verbose) {
                 if (F->use_oz)
-                    printf("bdc: G on the int8 tensor cores: %d tiles of %dx%d over %d CTAs, %d B shared memory, "
-                           "ring of %d%s\n", F->oz->tiles, kOzBM, kOzTN, F->oz->grid, F->oz->smem, F->oz->stages,
-                           t_oz > 0.f ? "" : " (forced or pinned)");
+                    printf("bdc: G on the int8 tensor cores: %d tiles of %dx%d over %d CTAs, %d epilogue warps, "
+                           "%d B shared memory, ring of %d, %d FP64 tile%s%s\n", F->oz->tiles, kOzBM, kOzTN,
+                           F->oz->grid, F->oz->epi, F->oz->smem, F->oz->stages, 1 + F->oz->two_tiles,
+                           F->oz->two_tiles ? "s" : "", t_oz[0] > 0.f ? "" : " (pinned)");
                 else
                     printf("bdc: G stays on the FP64 product: %s\n", why ? why : "timed slower");
-                if (t_oz > 0.f) printf("bdc: G timed: FP64 %.1f us, int8 with slicing %.1f us\n", t_fp * 1e3f, t_oz * 1e3f);
+                if (t_oz[0] > 0.f)
+                    printf("bdc: G timed: FP64 %.1f us, int8 with slicing %.1f us (16 epilogue warps), %.1f us (8)\n",
+                           t_fp * 1e3f, t_oz[0] * 1e3f, t_oz[1] * 1e3f);
             }
         }
     }

@@ -13,13 +13,14 @@
 // representative.  Warp 0 lane 0 loads by TMA (the static table slices of a
 // tile into one of two buffers, the per-weight slices of the FP64 operands
 // through a ring), warp 1 lane 0 issues the MMAs into one of two TMEM
-// accumulator buffers (8 weights x 32 columns each), and 16 epilogue warps
-// drain the other buffer: a thread owns one tile row (its TMEM lane) and 8
-// adjacent columns, i.e. 64 contiguous bytes of each dense array, so the
-// update runs on 16-byte loads and stores with no barrier among the warps.
-// Every wait on an mbarrier is bounded: on time-out the CTA records an error
-// in DevState::error, skips the rest, waits (bounded) for its loads and
-// frees its TMEM.
+// accumulator buffers (8 weights x 32 columns each), and 8 or 16 epilogue
+// warps drain the other buffer (a thread per tile row, its TMEM lane) into an
+// FP64 tile in shared memory, then run the BA update over the tile in a
+// coalesced order (a warp per 256 contiguous bytes of a dense row).  The
+// entropy and log iterate of the next tile are loaded before its
+// accumulators are drained.  Every wait on an mbarrier is bounded: on
+// time-out the CTA records an error in DevState::error, skips the rest, waits
+// (bounded) for its loads and frees its TMEM.
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -113,10 +114,19 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
         : "r"(taddr));
 }
 
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-                 : "r"(taddr));
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&v)[N]) {
+    if constexpr (N == 16) tmem_ld16(taddr, v);
+    else if constexpr (N == 4) {
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+                     : "r"(taddr));
+    } else {
+        static_assert(N == 8, "4, 8 or 16 columns");
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                     : "r"(taddr));
+    }
 }
 
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -128,22 +138,35 @@ struct OzGeomDev {
     int M, N;            // rows (H1h) and columns (H2) of G
     int tiles_n;
     int stages;          // ring depth of the per-weight operands (<= kOzStages)
+    int two_tiles;       // 1: two FP64 tiles in shared memory (one epilogue barrier per tile), 0: one (two)
 };
 
-constexpr int kOzThreads = 64 + 32 * kOzEpiWarps;  // producer, MMA, epilogue warps
-constexpr int kOzBuf = kOzW * kOzTN;               // TMEM columns of one accumulator buffer
-constexpr int kOzCols = kOzTN / (kOzEpiWarps / 4);  // columns one epilogue warp drains
-static_assert(kOzCols == 8 && kOzW % 2 == 0, "the drain reads accumulator pairs, 8 columns at a time");
+constexpr int kOzBuf = kOzW * kOzTN;  // TMEM columns of one accumulator buffer
 static_assert(2 * kOzBuf <= 512, "two accumulator buffers exceed tensor memory");
+static_assert(kOzW % 2 == 0, "the drain reads accumulator pairs");
+// threads of the product with EPI epilogue warps (beside one TMA producer
+// warp and one MMA warp)
+__host__ __device__ constexpr int oz_threads(int EPI) { return 64 + 32 * EPI; }
+constexpr int kOzTileLd = kOzTN + 1;                  // row pitch of an FP64 tile in shared memory
+constexpr int kOzTileBytes = kOzBM * kOzTileLd * 8;  // one FP64 tile
+
+// named barrier 1 among the EPI epilogue warps only
+__device__ __forceinline__ void epi_sync(int EPI) {
+    asm volatile("bar.sync 1, %0;" ::"r"(32 * EPI) : "memory");
+}
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-__global__ void __maxnreg__(112)
+// EPI epilogue warps (8 or 16): four per TMEM lane quadrant or two, each
+// draining 32 / (EPI / 4) columns of its 32 rows
+template <int EPI>
+__global__ void __launch_bounds__(oz_threads(EPI), 1)
 k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtensorMap tmBs,
           const __grid_constant__ CUtensorMap tmAd, const __grid_constant__ CUtensorMap tmBd, OzGeomDev g,
           const int* __restrict__ tiles, int ntiles, const int* __restrict__ d_e, BaEpilogue ep, DevState* st) {
+    constexpr int kOzCols = kOzTN / (EPI / 4);  // columns one epilogue warp drains
     extern __shared__ __align__(1024) uint8_t ozp_smem_raw[];
     __shared__ __align__(8) uint64_t sfull[2], sempty[2], full[kOzStages], empty[kOzStages], tfull[2], tempty[2],
         bar_done;
@@ -163,13 +186,16 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
     const uint32_t ring0 = sB0 + 2 * bytesB;
     const uint32_t stageA = (uint32_t)g.aD * kOzBM * 128, stageB = (uint32_t)g.bD * kOzTN * 128;
     const uint32_t stageBytes = stageA + stageB;
+    // two FP64 tiles [kOzBM][kOzTileLd] after the ring: the drain of one tile
+    // writes one while the pass of the previous tile reads the other
+    double* gt = (double*)(base + (ring0 - sA0) + (size_t)NS * stageBytes);
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < 2; ++i) {
             mbar_init(sm_addr(&sfull[i]), 1);
             mbar_init(sm_addr(&sempty[i]), 1);
             mbar_init(sm_addr(&tfull[i]), 1);
-            mbar_init(sm_addr(&tempty[i]), kOzEpiWarps);
+            mbar_init(sm_addr(&tempty[i]), EPI);
         }
         for (int i = 0; i < NS; ++i) {
             mbar_init(sm_addr(&full[i]), 1);
@@ -289,94 +315,109 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
         }
         __syncwarp();
     } else {
-        // ---- epilogue warps: TMEM lane quadrant q (warp % 4) and a quarter
-        // of the columns each; a thread owns one tile row and 8 adjacent
-        // columns (64 contiguous bytes of each dense array), so the warps
-        // need no barrier among themselves
+        // ---- epilogue warps.  Drain: TMEM lane quadrant q (warp % 4), the
+        // warp's share of the columns, one tile row per thread, into an FP64
+        // tile in shared memory.  Pass: element (row, col) = (et / 32 + EPI u,
+        // lane), so that a warp reads and writes 256 contiguous bytes of a
+        // dense row.  With two tiles in shared memory one barrier per tile:
+        // the drain of tile it writes buffer it & 1, which the pass of tile
+        // it - 2 was the last to read; with one tile a second barrier before
+        // the drain.
+        constexpr int PER = kOzBM * kOzTN / (32 * EPI);  // elements per thread in the pass
         const int q = warp & 3;
         const int part = (warp - 2) >> 2;
-        const int r = q * 32 + lane;
+        const int r = q * 32 + lane;      // the tile row this thread drains
+        const int et = threadIdx.x - 64;  // 0 .. 32 EPI - 1 in the pass
         const double shift = st->shift;
         const double lnz = st->log_z;
         const double inv_z = exp(-lnz);
         const int e = *d_e;
+        // the entropy and log iterate of a tile's pass elements, loaded before
+        // its accumulators are drained; bit u of reps: element u is a representative
+        double hv[PER], lv[PER];
+        uint32_t reps = 0;
+        auto preload = [&](int it) {
+            const int t = tiles[blockIdx.x + it * gridDim.x];
+            const int m0 = (t / g.tiles_n) * kOzBM, n = (t % g.tiles_n) * kOzTN + lane;
+            reps = 0;
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int m = m0 + (et >> 5) + u * EPI;
+                const uint32_t xd = ((uint32_t)m << ep.n2) | (uint32_t)n;
+                const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);
+                const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
+                const bool rep = (m < g.M) && (n < g.N) && is_rep(x, ep.n);
+                reps |= (uint32_t)rep << u;
+                hv[u] = rep ? __ldg(ep.hx + xd) : 0.0;
+                lv[u] = rep ? ep.Lt[xd] : 0.0;
+            }
+        };
+        if (nmine > 0) preload(0);
         for (int it = 0; it < nmine; ++it) {
             const int tb = it & 1;
-            const int t = tiles[blockIdx.x + it * gridDim.x];
-            const int m = (t / g.tiles_n) * kOzBM + r;
-            const int n0 = (t % g.tiles_n) * kOzTN + part * kOzCols;
-            const uint32_t xd0 = ((uint32_t)m << ep.n2) | (uint32_t)n0;
-            const bool row_in = m < g.M;
-            // the row's entropy, log iterate and weighted iterate, loaded
-            // while its accumulators are produced (16-byte pieces: n0 is a
-            // multiple of 8 and the dense rows are 2^n2 >= 32 wide)
-            double2 hv[kOzCols / 2], pwv[kOzCols / 2], ltv[kOzCols / 2];
-            if (row_in) {
-#pragma unroll
-                for (int j = 0; j < kOzCols / 2; ++j) {
-                    hv[j] = __ldg((const double2*)(ep.hx + xd0) + j);
-                    pwv[j] = ((const double2*)(ep.Pw + xd0))[j];
-                    ltv[j] = ((const double2*)(ep.Lt + xd0))[j];
-                }
-            }
             const bool got = mbar_wait(sm_addr(&tfull[tb]), (it >> 1) & 1) && !aborted();
             if (!got) give_up();
             tc_fence_after();
-            double gsum[kOzCols];
-#pragma unroll
-            for (int j = 0; j < kOzCols; ++j) gsum[j] = 0.0;
+            double* gtb = gt + (g.two_tiles ? tb : 0) * (kOzBM * kOzTileLd);
+            if (!g.two_tiles) epi_sync(EPI);  // the previous pass is done with the one tile
             if (got) {
-                const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tb * kOzBuf + part * kOzCols);
+                // four columns at a time, so that few registers are held
+                // beside the preloaded values
+#pragma unroll 1
+                for (int c0 = 0; c0 < kOzCols; c0 += 4) {
+                    double gsum[4] = {0.0, 0.0, 0.0, 0.0};
+                    const uint32_t trow =
+                        tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(tb * kOzBuf + part * kOzCols + c0);
 #pragma unroll
-                for (int b = kOzW / 2 - 1; b >= 0; --b) {
-                    uint32_t v0[kOzCols], v1[kOzCols];
-                    tmem_ld8(trow + (uint32_t)(2 * b * kOzTN), v0);
-                    tmem_ld8(trow + (uint32_t)((2 * b + 1) * kOzTN), v1);
-                    // 2^{e - 7(2b+1)} from its exponent bits (e >= -900, so normal)
-                    const double w = __hiloint2double((1023 + e - 7 * (2 * b + 1)) << 20, 0);
-                    tmem_wait_ld();
+                    for (int b = kOzW / 2 - 1; b >= 0; --b) {
+                        uint32_t v0[4], v1[4];
+                        tmem_ld<4>(trow + (uint32_t)(2 * b * kOzTN), v0);
+                        tmem_ld<4>(trow + (uint32_t)((2 * b + 1) * kOzTN), v1);
+                        // 2^{e - 7(2b+1)} from its exponent bits (e >= -900, so normal)
+                        const double w = __hiloint2double((1023 + e - 7 * (2 * b + 1)) << 20, 0);
+                        tmem_wait_ld();
 #pragma unroll
-                    for (int j = 0; j < kOzCols; ++j)
-                        gsum[j] = fma((double)((int32_t)v0[j] * 128 + (int32_t)v1[j]), w, gsum[j]);
+                        for (int j = 0; j < 4; ++j)
+                            gsum[j] = fma((double)((int32_t)v0[j] * 128 + (int32_t)v1[j]), w, gsum[j]);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) gtb[r * kOzTileLd + part * kOzCols + c0 + j] = gsum[j];
                 }
             }
             // this warp's part of the TMEM buffer is free for the tile after next
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(sm_addr(&tempty[tb]));
-            if (!got || !row_in) continue;
-            // the BA update; positions that hold no representative keep their
-            // values, so every 16-byte piece is written whole
+            epi_sync(EPI);
+            if (aborted()) break;  // uniform: read after the barrier
+            const int t = tiles[blockIdx.x + it * gridDim.x];
+            const int m0 = (t / g.tiles_n) * kOzBM, n = (t % g.tiles_n) * kOzTN + lane;
 #pragma unroll
-            for (int j = 0; j < kOzCols / 2; ++j) {
-                double lo[2] = {ltv[j].x, ltv[j].y}, po[2] = {pwv[j].x, pwv[j].y};
-                const double hh[2] = {hv[j].x, hv[j].y};
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const uint32_t xd = xd0 + 2 * j + h;
-                    const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);
-                    const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
-                    if (!is_rep(x, ep.n)) continue;
-                    const double o = (double)orbit_size(x, ep.n);
-                    const double D = hh[h] - gsum[2 * j + h] * ep.inv_c;
-                    if (ep.Dout) ep.Dout[xd] = D;
-                    // exact zeros of the caller's distribution (Lt = NaN) take ln p = 0
-                    // (backend/BAA.cu:573-580)
-                    const bool zero_in = (lo[h] != lo[h]);
-                    const double lnp = zero_in ? 0.0 : lo[h] - lnz;
-                    const double lw = lnp + ep.eta * D - shift;
-                    const double ex = exp(lw);
-                    mD = fmax(mD, D);
-                    mL = fmax(mL, lw);
-                    sE = fma(o, ex, sE);
-                    sR = fma(po[h] * inv_z, D, sR);
-                    if (zero_in) zero = 1.0;
-                    lo[h] = lw;
-                    po[h] = o * ex;
-                }
-                ((double2*)(ep.Lt + xd0))[j] = make_double2(lo[0], lo[1]);
-                ((double2*)(ep.Pw + xd0))[j] = make_double2(po[0], po[1]);
+            for (int u = 0; u < PER; ++u) {
+                if (!((reps >> u) & 1u)) continue;
+                const int row = (et >> 5) + u * EPI;
+                const uint32_t xd = ((uint32_t)(m0 + row) << ep.n2) | (uint32_t)n;
+                const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);
+                const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
+                const double o = (double)orbit_size(x, ep.n);
+                const double pw = ep.Pw[xd];
+                const double D = hv[u] - gtb[row * kOzTileLd + lane] * ep.inv_c;
+                if (ep.Dout) ep.Dout[xd] = D;
+                // exact zeros of the caller's distribution (Lt = NaN) take ln p = 0
+                // (backend/BAA.cu:573-580)
+                const bool zero_in = (lv[u] != lv[u]);
+                const double lnp = zero_in ? 0.0 : lv[u] - lnz;
+                const double lw = lnp + ep.eta * D - shift;
+                const double ex = exp(lw);
+                ep.Lt[xd] = lw;
+                ep.Pw[xd] = o * ex;
+                mD = fmax(mD, D);
+                mL = fmax(mL, lw);
+                sE = fma(o, ex, sE);
+                sR = fma(pw * inv_z, D, sR);
+                if (zero_in) zero = 1.0;
             }
+            if (it + 1 < nmine) preload(it + 1);
         }
     }
 
@@ -387,7 +428,7 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
     __syncthreads();
     const bool ran = !aborted();
     if (!ran && threadIdx.x == 0) st->error = kErrOzakiWait;
-    __shared__ double red[5][kOzThreads / 32];
+    __shared__ double red[5][oz_threads(EPI) / 32];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         mD = fmax(mD, __shfl_xor_sync(0xFFFFFFFFu, mD, off));
@@ -406,7 +447,7 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
     __syncthreads();
     if (threadIdx.x == 0) {
         double a0 = red[0][0], a1 = red[1][0], a2 = red[2][0], a3 = red[3][0], a4 = red[4][0];
-        for (int w = 1; w < kOzThreads / 32; ++w) {
+        for (int w = 1; w < oz_threads(EPI) / 32; ++w) {
             a0 = fmax(a0, red[0][w]);
             a1 += red[1][w];
             a2 = fmax(a2, red[2][w]);
@@ -662,16 +703,15 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const c
     oz->bD = (2 * KLp + 127) / 128;
     int dev_smem = 0;
     BDC_CUDA_TRY(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, H->device));
-    // the deepest ring (<= kOzStages) that fits
-    for (oz->stages = kOzStages; oz->stages >= 2; --oz->stages) {
-        oz->smem = 1024 + 2 * (oz->aS * kOzBM + oz->bS * kOzTN) * 128 +
-                    oz->stages * (oz->aD * kOzBM + oz->bD * kOzTN) * 128;
-        if (oz->smem + 2048 <= dev_smem) break;
-    }
-    if (in.H2 % kOzTN) {
-        ozaki_free(oz);
-        *why = "dense rows narrower than a tile";
-        return BDC_OK;
+    // the deepest ring (<= kOzStages, >= 2) that fits beside two FP64 tiles,
+    // else beside one
+    for (oz->two_tiles = 1; oz->two_tiles >= 0; --oz->two_tiles) {
+        for (oz->stages = kOzStages; oz->stages >= 2; --oz->stages) {
+            oz->smem = 1024 + 2 * (oz->aS * kOzBM + oz->bS * kOzTN) * 128 +
+                       oz->stages * (oz->aD * kOzBM + oz->bD * kOzTN) * 128 + (1 + oz->two_tiles) * kOzTileBytes;
+            if (oz->smem + 2048 <= dev_smem) break;
+        }
+        if (oz->stages >= 2) break;
     }
     if (oz->smem + 2048 > dev_smem) {
         ozaki_free(oz);
@@ -728,7 +768,8 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const c
         *why = "tensor map encoding failed";
         return BDC_OK;
     }
-    BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smem));
+    BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smem));
+    BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smem));
     BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_slice, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sizeof(double) * KLp * 33));
     *out = oz;
@@ -749,9 +790,14 @@ cudaError_t ozaki_prepare(OzakiG* oz, DevState* st, cudaStream_t s) {
 cudaError_t ozaki_product(OzakiG* oz, const BaEpilogue& ep, DevState* st, cudaStream_t s) {
     const OzakiInput& in = oz->in;
     if (oz->tiles == 0) return cudaGetLastError();
-    const OzGeomDev gp{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_n, oz->stages};
-    k_oz_ba<<<oz->grid, kOzThreads, oz->smem, s>>>(oz->tmAs, oz->tmBs, oz->tmAd, oz->tmBd, gp,
-                                                       oz->d_tiles, oz->tiles, oz->d_e, ep, st);
+    const OzGeomDev gp{oz->KLp, oz->KRp, oz->aS, oz->bS, oz->aD, oz->bD, in.H1h, in.H2, oz->tiles_n, oz->stages,
+                       oz->two_tiles};
+    if (oz->epi == 16)
+        k_oz_ba<16><<<oz->grid, oz_threads(16), oz->smem, s>>>(oz->tmAs, oz->tmBs, oz->tmAd, oz->tmBd, gp, oz->d_tiles,
+                                                               oz->tiles, oz->d_e, ep, st);
+    else
+        k_oz_ba<8><<<oz->grid, oz_threads(8), oz->smem, s>>>(oz->tmAs, oz->tmBs, oz->tmAd, oz->tmBd, gp, oz->d_tiles,
+                                                             oz->tiles, oz->d_e, ep, st);
     return cudaGetLastError();
 }
 

@@ -29,7 +29,6 @@ constexpr int kOzP = kOzJ + 2;   // slots per row of a sliced operand: zero, x_0
 constexpr int kOzBM = 128;       // tile rows (x_hi): one TMEM lane each
 constexpr int kOzTN = 32;        // tile columns (dense x_lo): two buffers of kOzW * kOzTN TMEM columns
 constexpr int kOzStages = 6;     // deepest ring of the per-weight operands
-constexpr int kOzEpiWarps = 16;  // epilogue warps (beside one TMA producer warp and one MMA warp)
 
 // what the product reads from the factored engine (bdc_factored.cu)
 struct OzakiInput {
@@ -54,7 +53,8 @@ struct OzakiG {
     int* d_e = nullptr;             // the exponent e of this iteration's FP64 operands
     // persistent product: one CTA per SM over the 128 x 32 tiles that hold
     // representatives, two TMEM accumulator buffers
-    int smem = 0, grid = 0, stages = 0;
+    int smem = 0, grid = 0, stages = 0, two_tiles = 0;
+    int epi = 16;                   // epilogue warps: 16 (8 columns each) or 8 (16 columns each)
     int* d_tiles = nullptr;         // tile ids (tm * tiles_n + tn)
     int tiles = 0, tiles_n = 0;
     CUtensorMap tmAs, tmBs, tmAd, tmBd;
