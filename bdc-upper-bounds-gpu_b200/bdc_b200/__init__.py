@@ -62,7 +62,8 @@ class Options(ctypes.Structure):
 class Profile(ctypes.Structure):
     _fields_ = [("ms_q", ctypes.c_double), ("ms_fold", ctypes.c_double), ("ms_d", ctypes.c_double),
                 ("ms_update", ctypes.c_double), ("ms_iter", ctypes.c_double), ("ms_main", ctypes.c_double),
-                ("work_main", ctypes.c_double), ("launches", ctypes.c_int), ("iters", ctypes.c_int)]
+                ("work_main", ctypes.c_double), ("launches", ctypes.c_int), ("iters", ctypes.c_int),
+                ("main_kind", ctypes.c_int), ("bytes_main", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}

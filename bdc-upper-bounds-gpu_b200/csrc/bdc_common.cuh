@@ -82,14 +82,6 @@ __host__ __device__ inline uint32_t binom(uint32_t n, uint32_t k) {
 // on a 16-byte boundary.  The row stride is 2^{mmax+1} entries.
 // Entries are uint16 (exact: every count in a half table of length <= 17
 // is < 65536).  m == h (the whole half) is an equality test, never stored.
-#ifdef __CUDACC__
-// An unsigned 32-bit integer (a count or a table entry) as FP64 with one FP64
-// add instead of an integer-to-FP64 conversion: the double with high word
-// 0x43300000 and low word v is 2^52 + v exactly, and subtracting 2^52 leaves
-// v exactly.
-__device__ __forceinline__ double u32_to_f64(uint32_t v) { return __hiloint2double(0x43300000, (int)v) - 0x1p52; }
-#endif
-
 struct HalfTables {
     const uint16_t* rows = nullptr;  // [2^h][stride]
     int h = 0;                       // half length

@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_qpass(Spl
 #pragma unroll
             for (int t = 0; t < TL::T; ++t)
 #pragma unroll
-                for (int bb = 0; bb < TL::NB; ++bb) acc[t][bb] = fma(w, u32_to_f64(N[t][bb]), acc[t][bb]);
+                for (int bb = 0; bb < TL::NB; ++bb) acc[t][bb] = fma(w, (double)N[t][bb], acc[t][bb]);
             failed = __syncthreads_or(bad);  // buffer b is free for x_{ix+2}
             if (failed) break;
         }
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_qpass(Spl
 #pragma unroll
             for (int t = 0; t < TL::T; ++t)
 #pragma unroll
-                for (int b = 0; b < TL::NB; ++b) acc[t][b] = fma(w, u32_to_f64(N[t][b]), acc[t][b]);
+                for (int b = 0; b < TL::NB; ++b) acc[t][b] = fma(w, (double)N[t][b], acc[t][b]);
         }
     }
 
@@ -502,7 +502,7 @@ __global__ void __launch_bounds__(256, CountOcc<TB, BB>::min_blocks) k_dpass(Spl
 #pragma unroll
                 for (int b = 0; b < TL::NB; ++b) {
                     if (MODE == 0) {
-                        v = fma(u32_to_f64(N[t][b]), lq[t][b], v);
+                        v = fma((double)N[t][b], lq[t][b], v);
                     } else {
                         const uint32_t c = N[t][b];
                         if (c) {

@@ -503,6 +503,8 @@ bdc_status engine_profile(bdc_handle* H, int iters, bdc_profile_t* out) {
     out->work_main = (double)H->nonzero_pairs * (double)(H->s.jhi - H->s.jlo + 1);
     out->launches = 6;
     out->iters = iters;
+    out->main_kind = 0;
+    out->bytes_main = 0.0;
     return BDC_OK;
 }
 

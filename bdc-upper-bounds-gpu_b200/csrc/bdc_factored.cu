@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(64) k_thin_d(const ThinD* __restrict__ descs, 
                 if (wb >= d.WIDE) break;
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
-                    const double wv = u32_to_f64((pk[u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+                    const double wv = (double)((pk[u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
                     const double* lr = lqs + (wb + u) * SMALL;
 #pragma unroll
                     for (int i = 0; i < SMALL; ++i) acc[i] = fma(wv, lr[i], acc[i]);
@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(64) k_thin_d(const ThinD* __restrict__ descs, 
         }
     } else if (live) {
         for (int w = q; w < d.WIDE; w += 4) {
-            const double wv = u32_to_f64(__ldg(v + w));
+            const double wv = (double)(__ldg(v + w));
             const double* lr = lqs + w * SMALL;
 #pragma unroll
             for (int i = 0; i < SMALL; ++i) acc[i] = fma(wv, lr[i], acc[i]);
@@ -671,8 +671,8 @@ static cudaError_t launch_thin_d(int lg, const ThinD* d, int n, int ctas, int ny
 // (1 or 2) small indices x 16 / IT consecutive wide indices, the latter read
 // as 16-byte pieces of the table row; 16 FP64 FMAs per row and thread.
 __device__ __forceinline__ void unpack2(const uint32_t p, double* v) {
-    v[0] = u32_to_f64(p & 0xFFFFu);
-    v[1] = u32_to_f64(p >> 16);
+    v[0] = (double)(p & 0xFFFFu);
+    v[1] = (double)(p >> 16);
 }
 
 __device__ __forceinline__ void unpack8(const uint4 p, double* v) {
@@ -762,14 +762,23 @@ __device__ __forceinline__ void qthin_run(const ThinQ& q, int stage_bytes, uint8
         const int nr = min(kQtRows, q.s1 - (q.s0 + stg * kQtRows));
         if (i0 < q.SMALL) {
             for (int r = 0; r < nr; ++r) {
-                double v[WT];
+                double v[WT], av[IT];
                 qthin_entries<WT>(base + r * wbytes + w0 * 2, v);
+                // the IT small values in 16-byte pieces (i0 is a multiple of IT)
+                if constexpr (IT >= 2) {
 #pragma unroll
-                for (int t = 0; t < IT; ++t) {
-                    const double a = sb[r * q.SMALL + i0 + t];
-#pragma unroll
-                    for (int e = 0; e < WT; ++e) acc[t * WT + e] = fma(a, v[e], acc[t * WT + e]);
+                    for (int t = 0; t < IT; t += 2) {
+                        const double2 a2 = *reinterpret_cast<const double2*>(sb + r * q.SMALL + i0 + t);
+                        av[t] = a2.x;
+                        av[t + 1] = a2.y;
+                    }
+                } else {
+                    av[0] = sb[r * q.SMALL + i0];
                 }
+#pragma unroll
+                for (int t = 0; t < IT; ++t)
+#pragma unroll
+                    for (int e = 0; e < WT; ++e) acc[t * WT + e] = fma(av[t], v[e], acc[t * WT + e]);
             }
         }
     }
@@ -855,7 +864,7 @@ __global__ void __launch_bounds__(256) k_dthin(const ThinDF* __restrict__ descs,
             for (int u = 0; u < 8; ++u) {
                 double v[kDfRT];
 #pragma unroll
-                for (int r = 0; r < kDfRT; ++r) v[r] = u32_to_f64((pk[c][r][u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+                for (int r = 0; r < kDfRT; ++r) v[r] = (double)((pk[c][r][u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
 #pragma unroll
                 for (int i = 0; i < IT; ++i) {
                     const double l = lc[u * SMALL + i];
@@ -2150,7 +2159,10 @@ bdc_status factored_init(bdc_handle* H) {
         const bool force_fp = gk && !strcmp(gk, "dmma");
         const bool force_oz = gk && !strcmp(gk, "ozaki");
         int pick = -1, unused = 0;
-        const bool pinned = !force_oz && tf.get("oz", &pick, &unused);
+        // a pinned choice (0: FP64, 8 or 16: int8 with that many epilogue
+        // warps); a forced int8 G ignores a pinned FP64 one
+        const bool has_pick = tf.get("oz", &pick, &unused);
+        const bool pinned = has_pick && !(force_oz && pick == 0);
         if (!force_fp && !(pinned && pick == 0)) {
             // an entry of ML (NR) is ln q against a row of B_m (A_j), whose
             // entries add up to C(n2, m) (C(n1, j)); 1 for an identity table
@@ -3004,6 +3016,8 @@ bdc_status factored_profile(bdc_handle* H, int iters, bdc_profile_t* out) {
     out->work_main = 2.0 * (double)H->R * (double)(F->KL + F->KR);
     out->launches = F->launches_per_iter;
     out->iters = iters;
+    out->main_kind = F->use_oz ? 2 : 1;
+    out->bytes_main = 40.0 * (double)F->Rl;
     return BDC_OK;
 }
 

@@ -332,9 +332,10 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
         const double lnz = st->log_z;
         const double inv_z = exp(-lnz);
         const int e = *d_e;
-        // the entropy and log iterate of a tile's pass elements, loaded before
-        // its accumulators are drained; bit u of reps: element u is a representative
-        double hv[PER], lv[PER];
+        // the entropy, log iterate and weighted iterate of a tile's pass
+        // elements, loaded before its accumulators are drained; bit u of reps:
+        // element u is a representative
+        double hv[PER], lv[PER], pv[PER];
         uint32_t reps = 0;
         auto preload = [&](int it) {
             const int t = tiles[blockIdx.x + it * gridDim.x];
@@ -350,6 +351,7 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
                 reps |= (uint32_t)rep << u;
                 hv[u] = rep ? __ldg(ep.hx + xd) : 0.0;
                 lv[u] = rep ? ep.Lt[xd] : 0.0;
+                pv[u] = rep ? ep.Pw[xd] : 0.0;
             }
         };
         if (nmine > 0) preload(0);
@@ -400,7 +402,7 @@ k_oz_ba(const __grid_constant__ CUtensorMap tmAs, const __grid_constant__ CUtens
                 const uint32_t xg = xd + ((uint32_t)ep.row0 << ep.n2);
                 const uint32_t x = (xg & ~low_mask(ep.n2)) | reverse_bits(xg & low_mask(ep.n2), ep.n2);
                 const double o = (double)orbit_size(x, ep.n);
-                const double pw = ep.Pw[xd];
+                const double pw = pv[u];
                 const double D = hv[u] - gtb[row * kOzTileLd + lane] * ep.inv_c;
                 if (ep.Dout) ep.Dout[xd] = D;
                 // exact zeros of the caller's distribution (Lt = NaN) take ln p = 0

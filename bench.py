@@ -370,6 +370,19 @@ def ours_arm(args) -> None:
                     "work_per_launch": f"{pairs} nonzero (x,y) pairs x {S} split terms = "
                                        f"{prof['work_main']:.4e} multiply-adds",
                     "peak_source": "bdc_peak_probe int32 IMAD chain, measured in this run"}
+    elif prof["main_kind"] == 2:
+        # the G stage on the int8 tensor cores (k_oz_ba, the exact split of its
+        # FP64 operands): its tensor work is small, its bound is the update's
+        # device-memory traffic; ms_main is its CUDA-event time per iteration
+        achieved = prof["bytes_main"] / (prof["ms_main"] / 1e3) / 1e9
+        roofline = {"bound": "hbm",
+                    "kernel": "k_oz_ba (G = [A_L | N_R] [M_L ; B_R^T] as eight exact int8 products on tcgen05.mma "
+                              "kind::i8, TMEM accumulators, BA update in the epilogue)",
+                    "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                    "frac": achieved / peaks.get("hbm_gbs"), "traffic": profile_traffic("k_oz_ba", args.n, args.k),
+                    "work_per_launch": f"40 bytes per representative (read h, ln p, p; write ln p, p) x R = "
+                                       f"{prof['bytes_main']:.4e} bytes",
+                    "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_src})"}
     else:
         # the G stage: one k_mma_ba launch (FP64 mma.sync tiles, the BA update
         # fused in the epilogue); ms_main is its CUDA-event time per iteration
@@ -438,6 +451,7 @@ def ours_arm(args) -> None:
         "data": "synthetic (uniform start; the reference publishes no throughput)",
         "config": workload_config(args.n, args.k, R) | {"parallelism": f"replicas x{world}"},
         "engine": E.engine,
+        "g_product": {0: None, 1: "FP64 mma.sync", 2: "int8 tcgen05 (exact split)"}[prof["main_kind"]],
         "gpu_launches": launches_per_iter * args.steps,
         "profile_ms": {k2: prof[k2] for k2 in ("ms_q", "ms_fold", "ms_d", "ms_update", "ms_iter", "ms_main")},
         "roofline": roofline, "roofline_update": roofline_update,

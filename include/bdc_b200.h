@@ -281,6 +281,11 @@ typedef struct {
                            over the nonzero pairs (count) or FP64 flops (factored) */
     int launches;       /* kernel launches per iteration */
     int iters;          /* iterations averaged */
+    int main_kind;      /* the dominant kernel: 0 the count D pass, 1 G on the FP64
+                           tensor path (mma.sync), 2 G on the int8 tensor cores */
+    double bytes_main;  /* its algorithmic device-memory bytes per launch: the
+                           update's 40 bytes per representative (read h, ln p, p;
+                           write ln p, p) for G, 0 for the count D pass */
 } bdc_profile_t;
 
 /* Runs `iters` iterations (a = -inf, so none stops early) with CUDA events
