@@ -162,6 +162,11 @@ struct FactoredState {
     int n_qf = 0, qf_stage = 0;
     bdc::ThinDF* d_df[4] = {};  // by log2 IT
     int n_df[4] = {};
+    // the terms of 8 to 64 outputs on the FP64 tensor path (k_dthin_mma), in
+    // place of the IT = 8 class where that times faster
+    bdc::ThinDF* d_dm = nullptr;
+    int n_dm = 0, dm_smem = 0;
+    bool use_dm = false;
     bool use_qf = false, use_df = false;
     double* lnq_full = nullptr;  // [2^k]
     double* epart = nullptr;  // [ctas][8]
@@ -888,6 +893,91 @@ __global__ void __launch_bounds__(256) k_dthin(const ThinDF* __restrict__ descs,
     }
 }
 
+// D side on the FP64 tensor path, for the terms of 8 to 64 outputs: CTA =
+// one ThinDF entry of kDmRows table rows, warp w = rows 8w .. 8w + 7, all
+// SMALL outputs as SMALL / 8 mma.sync m8n8k4 tiles.  Lq' of the term sits in
+// shared memory at row pitch SMALL + 2 (the four row groups of a B fragment
+// land 8 doubles apart: two wavefronts, the minimum for 256 bytes); the
+// table rows stream through two buffers of kDmChunk entries with cp.async
+// (row pitch kDmPitch entries: 16-byte aligned, rows 4 banks apart).  Within
+// each 16 contraction indices, k-step j of lane column q takes index 4q + j,
+// so that a lane's four A entries are one 8-byte load (A and B use the same
+// order, and the sum does not depend on it).
+constexpr int kDmRows = 64;
+constexpr int kDmChunk = 64;
+constexpr int kDmPitch = 72;
+
+__host__ __device__ constexpr int dmma_ld(int SMALL) { return SMALL + 2; }
+static int dthin_mma_smem(int SMALL, int WIDE) {
+    return (int)sizeof(double) * WIDE * dmma_ld(SMALL) + 2 * kDmRows * kDmPitch * (int)sizeof(uint16_t);
+}
+
+template <int NB>
+__device__ __forceinline__ void dthin_mma_run(const ThinDF& t, const double* __restrict__ lnq_full, double* dsm) {
+    const int SMALL = t.SMALL, WIDE = t.WIDE, ld = dmma_ld(SMALL);
+    double* L = dsm;                                         // [WIDE][ld]
+    uint16_t* T = reinterpret_cast<uint16_t*>(dsm + WIDE * ld);  // [2][kDmRows][kDmPitch]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int gr = lane >> 2, q = lane & 3;
+    auto issue = [&](int c) {
+        uint16_t* buf = T + (c & 1) * kDmRows * kDmPitch;
+        for (int e = tid; e < kDmRows * (kDmChunk / 8); e += 256) {
+            const int r = e / (kDmChunk / 8), piece = e % (kDmChunk / 8);
+            const int row = min(t.row0 + r, t.rows - 1);
+            cp_async16(buf + r * kDmPitch + piece * 8, t.wide + (int64_t)row * t.wide_stride + c * kDmChunk + piece * 8,
+                       16);
+        }
+    };
+    const int nch = WIDE / kDmChunk;
+    issue(0);
+    cp_async_commit();
+    for (int e = tid; e < SMALL * WIDE; e += 256) {
+        const int w = e / SMALL, i = e % SMALL;
+        L[w * ld + i] = t.lq_trans ? lnq_full[w * SMALL + i] : lnq_full[i * WIDE + w];
+    }
+    double acc[NB][2];
+#pragma unroll
+    for (int nb = 0; nb < NB; ++nb) acc[nb][0] = acc[nb][1] = 0.0;
+    for (int c = 0; c < nch; ++c) {
+        if (c + 1 < nch) issue(c + 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const uint16_t* arow = T + (c & 1) * kDmRows * kDmPitch + (warp * 8 + gr) * kDmPitch;
+#pragma unroll
+        for (int ks = 0; ks < kDmChunk / 16; ++ks) {
+            const uint2 pk = *reinterpret_cast<const uint2*>(arow + ks * 16 + 4 * q);
+            const double av[4] = {(double)(pk.x & 0xFFFFu), (double)(pk.x >> 16), (double)(pk.y & 0xFFFFu),
+                                  (double)(pk.y >> 16)};
+            const double* lrow = L + (c * kDmChunk + ks * 16 + 4 * q) * ld + gr;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int nb = 0; nb < NB; ++nb) mma_f64(acc[nb][0], acc[nb][1], av[j], lrow[j * ld + nb * 8]);
+        }
+        __syncthreads();  // the buffer is free for chunk c + 2
+    }
+    const int row = t.row0 + warp * 8 + gr;
+    if (row >= t.rows) return;
+#pragma unroll
+    for (int nb = 0; nb < NB; ++nb)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) t.out[(int64_t)row * t.out_s + (int64_t)(nb * 8 + 2 * q + h) * t.out_i] = acc[nb][h];
+}
+
+__global__ void __launch_bounds__(256) k_dthin_mma(const ThinDF* __restrict__ descs, const double* __restrict__ lnq_full,
+                                                   const DevState* st) {
+    if (gated(st)) return;
+    extern __shared__ __align__(16) double dmsm[];
+    const ThinDF& t = descs[blockIdx.x];
+    switch (t.SMALL) {
+        case 8: dthin_mma_run<1>(t, lnq_full, dmsm); break;
+        case 16: dthin_mma_run<2>(t, lnq_full, dmsm); break;
+        case 32: dthin_mma_run<4>(t, lnq_full, dmsm); break;
+        default: dthin_mma_run<8>(t, lnq_full, dmsm); break;
+    }
+}
+
 // shared memory of k_qthin: the largest term's stage (table rows + small rows)
 static int qthin_stage_bytes(const std::vector<ThinQ>& v) {
     int m = 0;
@@ -912,6 +1002,12 @@ static cudaError_t launch_dthin(const ThinDF* d, int n, int it, int k, const dou
         case 8: k_dthin<8><<<n, 256, sm, s>>>(d, lnq_full, st); break;
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_dthin_mma(const ThinDF* d, int n, int smem, const double* lnq_full, cudaStream_t s,
+                                    const DevState* st) {
+    k_dthin_mma<<<n, 256, smem, s>>>(d, lnq_full, st);
     return cudaGetLastError();
 }
 
@@ -2026,9 +2122,37 @@ bdc_status factored_init(bdc_handle* H) {
                     all_d[cl].push_back(f);
                 }
             }
-        int pinned_q = -1, pinned_d = -1, unused = 0;
+        // the IT = 8 class again in 64-row blocks for k_dthin_mma
+        std::vector<ThinDF> all_m;
+        bool mok = dok && !all_d[3].empty();
+        for (int lg = 0; lg < 8 && mok; ++lg)
+            for (auto& d : td[lg]) {
+                if (d.SMALL < 8) continue;
+                if (d.SMALL > 64 || d.WIDE % kDmChunk != 0) {
+                    mok = false;
+                    break;
+                }
+                ThinDF f{};
+                f.wide = d.wide;
+                f.wide_stride = d.wide_stride;
+                f.SMALL = d.SMALL;
+                f.WIDE = d.WIDE;
+                f.rows = d.rows;
+                f.lq_trans = d.lq_trans;
+                f.out = d.out;
+                f.out_s = d.out_s;
+                f.out_i = d.out_i;
+                F->dm_smem = std::max(F->dm_smem, dthin_mma_smem(d.SMALL, d.WIDE));
+                for (int r0 = 0; r0 < d.rows; r0 += kDmRows) {
+                    f.row0 = r0;
+                    all_m.push_back(f);
+                }
+            }
+        int pinned_q = -1, pinned_d = -1, pinned_m = -1, unused = 0;
         tf.get("qf", &pinned_q, &unused);
         tf.get("df", &pinned_d, &unused);
+        tf.get("dm", &pinned_m, &unused);
+        if (const char* dm = getenv("BDC_DTHIN")) pinned_m = !strcmp(dm, "mma") ? 1 : 0;  // forces either form
         BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
         if (qok && !all_q.empty()) {
             F->qf_stage = qthin_stage_bytes(all_q);
@@ -2076,6 +2200,31 @@ bdc_status factored_init(bdc_handle* H) {
                 if (H->verbose)
                     printf("bdc: tuned D-side term products: %s (fused %.1f us, per class %.1f us)\n",
                            F->use_df ? "fused" : "per class", tfu * 1e3f, tc * 1e3f);
+            }
+            // the IT = 8 class of the fused launches on the FP64 tensor path
+            if (F->use_df && mok && F->dm_smem + 1024 <= 227 * 1024) {
+                BDC_CUDA_TRY(cudaFuncSetAttribute(k_dthin_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, F->dm_smem));
+                BDC_CUDA_TRY(cudaMalloc(&F->d_dm, sizeof(ThinDF) * all_m.size()));
+                BDC_CUDA_TRY(cudaMemcpy(F->d_dm, all_m.data(), sizeof(ThinDF) * all_m.size(), cudaMemcpyHostToDevice));
+                F->n_dm = (int)all_m.size();
+                if (pinned_m >= 0) {
+                    F->use_dm = pinned_m != 0;
+                } else {
+                    cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
+                    const float t8 = time_ms(H, [&] {
+                        return launch_dthin(F->d_df[3], F->n_df[3], 8, H->k, F->lnq_full, H->stream, nullptr);
+                    }, &e1);
+                    const float tm = time_ms(H, [&] {
+                        return launch_dthin_mma(F->d_dm, F->n_dm, F->dm_smem, F->lnq_full, H->stream, nullptr);
+                    }, &e2);
+                    BDC_CUDA_TRY(e1);
+                    BDC_CUDA_TRY(e2);
+                    F->use_dm = tm < t8;
+                    tf.put("dm", F->use_dm ? 1 : 0, 0);
+                    if (H->verbose)
+                        printf("bdc: tuned D-side terms of 8..64 outputs: %s (mma.sync %.1f us, CUDA cores %.1f us)\n",
+                               F->use_dm ? "mma.sync" : "CUDA cores", tm * 1e3f, t8 * 1e3f);
+                }
             }
         }
     }
@@ -2259,6 +2408,7 @@ void factored_free(bdc_handle* H) {
     }
     cudaFree(F->d_fold);
     ozaki_free(F->oz);
+    cudaFree(F->d_dm);
     delete F;
     H->fac = nullptr;
 }
@@ -2332,7 +2482,9 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
                 for (int cl = 0; cl < 4; ++cl) {
                     if (!F->n_df[cl]) continue;
                     if ((e = cudaStreamWaitEvent(F->side[cl], F->ev_fork, 0)) != cudaSuccess) return e;
-                    e = launch_dthin(F->d_df[cl], F->n_df[cl], 1 << cl, H->k, F->lnq_full, F->side[cl], H->d_st);
+                    e = (cl == 3 && F->use_dm)
+                            ? launch_dthin_mma(F->d_dm, F->n_dm, F->dm_smem, F->lnq_full, F->side[cl], H->d_st)
+                            : launch_dthin(F->d_df[cl], F->n_df[cl], 1 << cl, H->k, F->lnq_full, F->side[cl], H->d_st);
                     if (e != cudaSuccess) return e;
                     if ((e = cudaEventRecord(F->ev_join[cl], F->side[cl])) != cudaSuccess) return e;
                     if ((e = cudaStreamWaitEvent(s, F->ev_join[cl], 0)) != cudaSuccess) return e;

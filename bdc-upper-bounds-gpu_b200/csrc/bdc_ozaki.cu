@@ -493,21 +493,13 @@ __device__ __forceinline__ uint32_t oz_pack4(const long long (&N)[4], int s) {
     return w;
 }
 
-// 16 values -> their J digit slices as 16-byte words dst[s * pitch] (s < J)
-__device__ __forceinline__ void oz_slice16(const double (&v)[16], double scale, uint8_t* dst, int pitch) {
-    long long N[16];
+// 4 values -> their J digit slices as 4-byte words dst[s * pitch] (s < J)
+__device__ __forceinline__ void oz_slice4(const double (&v)[4], double scale, uint8_t* dst, int pitch) {
+    long long N[4];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) N[j] = __double2ll_rz(v[j] * scale);
+    for (int j = 0; j < 4; ++j) N[j] = __double2ll_rz(v[j] * scale);
 #pragma unroll
-    for (int s = 0; s < kOzJ; ++s) {
-        uint32_t w[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const long long n4[4] = {N[4 * q], N[4 * q + 1], N[4 * q + 2], N[4 * q + 3]};
-            w[q] = oz_pack4(n4, s);
-        }
-        *(uint4*)(dst + (size_t)s * pitch) = make_uint4(w[0], w[1], w[2], w[3]);
-    }
+    for (int s = 0; s < kOzJ; ++s) *(uint32_t*)(dst + (size_t)s * pitch) = oz_pack4(N, s);
 }
 
 // The operands' exponent e (max |X| < 2^e, frexp) from the bound |ML|, |NR|
@@ -515,19 +507,28 @@ __device__ __forceinline__ void oz_slice16(const double (&v)[16], double scale, 
 // whose entries add up to at most cmax.  Every block of the slicing launch
 // reduces the 2^k values of ln q (from L2) itself; false on a non-finite ln q.
 __device__ __forceinline__ bool oz_exponent(const double* __restrict__ lnq, int ny, double cmax, int* e_out) {
-    __shared__ double red[256];
-    double m = 0.0;
-    for (int y = threadIdx.x; y < ny; y += blockDim.x) m = fmax(m, fabs(lnq[y]));
-    red[threadIdx.x] = m;
-    __syncthreads();
-    for (int h = 128; h > 0; h >>= 1) {
-        if (threadIdx.x < h) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + h]);
-        __syncthreads();
+    __shared__ double red[8];
+    // eight independent maxima, so that eight loads per thread are in flight
+    double mu[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int y = threadIdx.x;
+    for (; y + 7 * 256 < ny; y += 8 * 256) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) mu[u] = fmax(mu[u], fabs(__ldg(lnq + y + u * 256)));
     }
+    for (; y < ny; y += 256) mu[0] = fmax(mu[0], fabs(__ldg(lnq + y)));
+    double m = mu[0];
+#pragma unroll
+    for (int u = 1; u < 8; ++u) m = fmax(m, mu[u]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xFFFFFFFFu, m, off));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = red[0];
+    for (int w = 1; w < 8; ++w) m = fmax(m, red[w]);
     // headroom for the rounding of the FP64 operands (sums of at most cmax
     // terms, relative error far below 2^-30), so that |X| < 2^e holds for the
     // computed values too
-    m = red[0] * cmax * (1.0 + 0x1p-30);
+    m = m * cmax * (1.0 + 0x1p-30);
     if (!isfinite(m)) return false;
     int e = 0;
     if (m > 0.0) frexp(m, &e);  // m = f 2^e, f in [0.5, 1)
@@ -536,54 +537,49 @@ __device__ __forceinline__ bool oz_exponent(const double* __restrict__ lnq, int 
     return true;
 }
 
-// NR (LA columns KL + r) -> Ad[m][slot 1 + s][r]; one thread per (row, 16 r),
+// NR (LA columns KL + r) -> Ad[m][slot 1 + s][r]; one thread per (row, 4 r),
 // over blocks [b0, b0 + nb) of the launch
 __device__ __forceinline__ void oz_slice_a(const double* __restrict__ LA, int Kp, int KL, int KR, int rows, int KRp,
                                            uint8_t* __restrict__ Ad, double scale, int b0, int nb) {
-    const int chunks = KRp / 16;
+    const int chunks = KRp / 4;
     const int64_t total = (int64_t)rows * chunks;
     for (int64_t i = (blockIdx.x - b0) * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)nb * blockDim.x) {
         const int m = (int)(i / chunks), c = (int)(i % chunks);
-        double v[16];
+        double v[4];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int r = c * 16 + j;
+        for (int j = 0; j < 4; ++j) {
+            const int r = c * 4 + j;
             v[j] = (r < KR) ? LA[(int64_t)m * Kp + KL + r] : 0.0;
         }
-        oz_slice16(v, scale, Ad + (int64_t)m * kOzP * KRp + KRp + c * 16, KRp);
+        oz_slice4(v, scale, Ad + (int64_t)m * kOzP * KRp + KRp + c * 4, KRp);
     }
 }
 
-// ML (RB rows k < KL, column n) -> Bd[n][slot 1 + s][k]: a block transposes a
-// 32-column strip of RB through shared memory; thread (column, 16 k) slices
+// ML (RB rows k < KL, column n) -> Bd[n][slot 1 + s][k]: a block covers 32
+// columns from n0 and 32 rows from k0; thread (column c, rows k0 + 4 kq ..
+// + 3) loads its four values (a warp reads 32 adjacent columns of one row at
+// a time) and writes their slices, four bytes per slot
 __device__ __forceinline__ void oz_slice_b(const double* __restrict__ RB, int KL, int cols, int KLp,
-                                           uint8_t* __restrict__ Bd, double scale, double* tile) {
-    const int n0 = blockIdx.x * 32;
-    for (int i = threadIdx.x; i < KLp * 32; i += blockDim.x) {
-        const int k = i / 32, c = i % 32;
-        tile[k * 33 + c] = (k < KL && n0 + c < cols) ? RB[(int64_t)k * cols + n0 + c] : 0.0;
-    }
-    __syncthreads();
-    const int chunks = KLp / 16;
-    for (int i = threadIdx.x; i < 32 * chunks; i += blockDim.x) {
-        const int c = i % 32, ch = i / 32;
-        if (n0 + c >= cols) continue;
-        double v[16];
+                                           uint8_t* __restrict__ Bd, double scale, int n0, int k0) {
+    const int c = threadIdx.x % 32, kq = threadIdx.x / 32;  // 256 threads: 32 columns x 8 row quads
+    if (n0 + c >= cols) return;
+    double v[4];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = tile[(ch * 16 + j) * 33 + c];
-        oz_slice16(v, scale, Bd + (int64_t)(n0 + c) * kOzP * KLp + KLp + ch * 16, KLp);
+    for (int j = 0; j < 4; ++j) {
+        const int k = k0 + 4 * kq + j;
+        v[j] = (k < KL) ? RB[(int64_t)k * cols + n0 + c] : 0.0;
     }
+    oz_slice4(v, scale, Bd + (int64_t)(n0 + c) * kOzP * KLp + KLp + k0 + 4 * kq, KLp);
 }
 
-// the exponent and both slicings in one launch: blocks [0, nb_b) the
-// 32-column strips of ML, the rest NR; block 0 publishes e for the product
+// the exponent and both slicings in one launch: blocks [0, nb_b) the 32 x 32
+// tiles of ML (strip-major), the rest NR; block 0 publishes e for the product
 __global__ void __launch_bounds__(256) k_oz_slice(const double* __restrict__ RB, const double* __restrict__ LA, int Kp,
                                                   int KL, int KR, int rows, int cols, int KLp, int KRp,
                                                   uint8_t* __restrict__ Ad, uint8_t* __restrict__ Bd, int nb_b,
                                                   const double* __restrict__ lnq, int ny, double cmax,
                                                   int* __restrict__ d_e, DevState* st) {
     if (st->done || st->error) return;
-    extern __shared__ double tile[];  // [KLp][33]
     int e = 0;
     if (!oz_exponent(lnq, ny, cmax, &e)) {
         if (blockIdx.x == 0 && threadIdx.x == 0) st->error = kErrOzakiOperand;
@@ -591,8 +587,12 @@ __global__ void __launch_bounds__(256) k_oz_slice(const double* __restrict__ RB,
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *d_e = e;
     const double scale = ldexp(1.0, 7 * kOzJ - e);
-    if ((int)blockIdx.x < nb_b) oz_slice_b(RB, KL, cols, KLp, Bd, scale, tile);
-    else oz_slice_a(LA, Kp, KL, KR, rows, KRp, Ad, scale, nb_b, (int)gridDim.x - nb_b);
+    if ((int)blockIdx.x < nb_b) {
+        const int strips = (cols + 31) / 32;
+        oz_slice_b(RB, KL, cols, KLp, Bd, scale, ((int)blockIdx.x % strips) * 32, ((int)blockIdx.x / strips) * 32);
+    } else {
+        oz_slice_a(LA, Kp, KL, KR, rows, KRp, Ad, scale, nb_b, (int)gridDim.x - nb_b);
+    }
 }
 
 // the integer operands, once: As[m] = [lo | hi] of AL[m][k] (LA columns k <
@@ -772,20 +772,17 @@ bdc_status ozaki_init(bdc_handle* H, const OzakiInput& in, OzakiG** out, const c
     }
     BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smem));
     BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_ba<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz->smem));
-    BDC_CUDA_TRY(cudaFuncSetAttribute(k_oz_slice, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sizeof(double) * KLp * 33));
     *out = oz;
     return BDC_OK;
 }
 
 cudaError_t ozaki_prepare(OzakiG* oz, DevState* st, cudaStream_t s) {
     const OzakiInput& in = oz->in;
-    const int nb_b = (in.H2 + 31) / 32;
-    const int64_t work_a = (int64_t)in.H1h * (oz->KRp / 16);
-    const int nb_a = (int)std::max<int64_t>(1, std::min<int64_t>((work_a + 255) / 256, 148 * 4));
-    k_oz_slice<<<nb_b + nb_a, 256, sizeof(double) * oz->KLp * 33, s>>>(
-        in.RB, in.LA, in.Kp, in.KL, in.KR, in.H1h, in.H2, oz->KLp, oz->KRp, oz->Ad, oz->Bd, nb_b, in.lnq, 1 << in.k,
-        in.cmax, oz->d_e, st);
+    const int nb_b = ((in.H2 + 31) / 32) * (oz->KLp / 32);
+    const int64_t work_a = (int64_t)in.H1h * (oz->KRp / 4);
+    const int nb_a = (int)std::max<int64_t>(1, std::min<int64_t>((work_a + 255) / 256, 148 * 8));
+    k_oz_slice<<<nb_b + nb_a, 256, 0, s>>>(in.RB, in.LA, in.Kp, in.KL, in.KR, in.H1h, in.H2, oz->KLp, oz->KRp, oz->Ad,
+                                          oz->Bd, nb_b, in.lnq, 1 << in.k, in.cmax, oz->d_e, st);
     return cudaGetLastError();
 }
 
