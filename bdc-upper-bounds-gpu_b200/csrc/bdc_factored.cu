@@ -160,6 +160,11 @@ struct FactoredState {
     // all per-term products of a side in one launch (used when faster)
     bdc::ThinQ* d_qf = nullptr;
     int n_qf = 0, qf_stage = 0;
+    // the fused q side split: terms of fewer than 8 small outputs on k_qthin,
+    // 8 to 64 on the FP64 tensor path (k_qthin_mma), where that times faster
+    bdc::ThinQ *d_ql = nullptr, *d_qm = nullptr;
+    int n_ql = 0, n_qm = 0, ql_stage = 0, qm_stage = 0;
+    bool use_qm = false;
     bdc::ThinDF* d_df[4] = {};  // by log2 IT
     int n_df[4] = {};
     // the terms of 8 to 64 outputs on the FP64 tensor path (k_dthin_mma), in
@@ -205,6 +210,7 @@ __device__ __forceinline__ bool gated(const DevState* st) { return st && (st->do
 
 enum Stage { ST_QBIG = 0, ST_QSMALL, ST_FOLD, ST_DSMALL, ST_G, ST_FIN, ST_COUNT };
 static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a);
+static cudaError_t enqueue_qthin_split(bdc_handle* H, cudaStream_t s, const DevState* st);
 
 // Dense layout of the iterate: row x_hi, column rev(x_lo) (the low half
 // bit-reversed).  A representative x satisfies x <= rev(x) and x <=
@@ -976,6 +982,95 @@ __global__ void __launch_bounds__(256) k_dthin_mma(const ThinDF* __restrict__ de
         case 32: dthin_mma_run<4>(t, lnq_full, dmsm); break;
         default: dthin_mma_run<8>(t, lnq_full, dmsm); break;
     }
+}
+
+// q side on the FP64 tensor path, for the terms of 8 to 64 small outputs
+// at 2^k = 4096 outputs per term: CTA = one ThinQ slice [s0, s1) of the
+// contraction, producing the term's SMALL x WIDE partial product.  Warp w
+// owns small tile ti (8 outputs i) and 64 wide outputs from c0 as eight
+// mma.sync m8n8k4 tiles; tile u's column n stands for w = c0 + 8n + u, so a
+// lane's B entries of one row (n = lane / 4, all u) are 8 adjacent table
+// entries, one 16-byte load.  Rows stream through two buffers of kQmRows
+// (table rows at pitch WIDE, small rows at pitch SMALL + 8: two wavefronts
+// for the four rows of an A fragment); rows past s1 read zero small values.
+constexpr int kQmRows = 32;
+
+__host__ __device__ constexpr int qmma_ld(int SMALL) { return SMALL >= 16 ? SMALL + 8 : SMALL; }
+__host__ __device__ constexpr int qmma_stage(int SMALL, int WIDE) {
+    return kQmRows * (qmma_ld(SMALL) * 8 + WIDE * 2);
+}
+
+__global__ void __launch_bounds__(256) k_qthin_mma(const ThinQ* __restrict__ descs, int stage_bytes,
+                                                   const DevState* st) {
+    if (gated(st)) return;
+    extern __shared__ __align__(16) uint8_t qmsm[];
+    const ThinQ& q = descs[blockIdx.x];
+    const int SMALL = q.SMALL, WIDE = q.WIDE, lds = qmma_ld(SMALL);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int gr = lane >> 2, qq = lane & 3;
+    const int groups = WIDE / 64;  // 64-column groups
+    const int ti = warp / groups, c0 = (warp % groups) * 64;
+    const uint16_t* wide = (const uint16_t*)q.wide;
+    const double* small = (const double*)q.small;
+    const int rows = q.s1 - q.s0;
+    const int nst = (rows + kQmRows - 1) / kQmRows;
+    auto issue = [&](int stg) {
+        uint8_t* base = qmsm + (stg & 1) * stage_bytes;
+        const int r0 = q.s0 + stg * kQmRows;
+        const int nr = min(kQmRows, q.s1 - r0);
+        const int wpieces = WIDE / 8;
+        for (int e = tid; e < nr * wpieces; e += 256) {
+            const int r = e / wpieces, c = e % wpieces;
+            cp_async16(base + r * WIDE * 2 + c * 16, wide + (int64_t)(r0 + r) * q.wide_stride + c * 8, 16);
+        }
+        double* sb = reinterpret_cast<double*>(base + kQmRows * WIDE * 2);
+        for (int e = tid; e < kQmRows * SMALL; e += 256) {
+            const int r = e / SMALL, c = e % SMALL;
+            if (r < nr) cp_async8(sb + r * lds + c, small + (int64_t)(r0 + r) * q.small_stride + c);
+            else sb[r * lds + c] = 0.0;  // rows past the slice contribute nothing
+        }
+    };
+    double acc[8][2];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc[u][0] = acc[u][1] = 0.0;
+    issue(0);
+    cp_async_commit();
+    for (int stg = 0; stg < nst; ++stg) {
+        if (stg + 1 < nst) issue(stg + 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const uint8_t* base = qmsm + (stg & 1) * stage_bytes;
+        const uint16_t* tb = reinterpret_cast<const uint16_t*>(base);
+        const double* sb = reinterpret_cast<const double*>(base + kQmRows * WIDE * 2);
+#pragma unroll 2
+        for (int ks = 0; ks < kQmRows / 4; ++ks) {
+            const int r = ks * 4 + qq;  // the contraction row of this lane's k index
+            const double a = sb[r * lds + ti * 8 + gr];
+            const uint4 pk = *reinterpret_cast<const uint4*>(tb + r * WIDE + c0 + 8 * gr);
+            const uint32_t pw[4] = {pk.x, pk.y, pk.z, pk.w};
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const double b = (double)((pw[u >> 1] >> (16 * (u & 1))) & 0xFFFFu);
+                mma_f64(acc[u][0], acc[u][1], a, b);
+            }
+        }
+        __syncthreads();  // the buffer is free for stage stg + 2
+    }
+    const int i = ti * 8 + gr;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int w = c0 + 8 * (2 * qq + h) + u;
+            if (q.out_trans) q.out[(int64_t)w * SMALL + i] = acc[u][h];
+            else q.out[(int64_t)i * WIDE + w] = acc[u][h];
+        }
+}
+
+static cudaError_t launch_qthin_mma(const ThinQ* d, int n, int stage_bytes, cudaStream_t s, const DevState* st) {
+    k_qthin_mma<<<n, 256, 2 * stage_bytes, s>>>(d, stage_bytes, st);
+    return cudaGetLastError();
 }
 
 // shared memory of k_qthin: the largest term's stage (table rows + small rows)
@@ -2172,6 +2267,51 @@ bdc_status factored_init(bdc_handle* H) {
                     printf("bdc: tuned q-side term products: %s (one launch %.1f us, per class %.1f us)\n",
                            F->use_qf ? "one launch" : "per class", tfu * 1e3f, tc * 1e3f);
             }
+            // the terms of 8..64 small outputs on the FP64 tensor path
+            std::vector<ThinQ> q_lo, q_hi;
+            bool qmok = ny == 4096;
+            for (const ThinQ& x : all_q) {
+                if (x.SMALL < 8) {
+                    q_lo.push_back(x);
+                    continue;
+                }
+                if (x.SMALL > 64 || x.SMALL * x.WIDE != 4096 || x.WIDE % 64 != 0) qmok = false;
+                q_hi.push_back(x);
+                F->qm_stage = std::max(F->qm_stage, qmma_stage(x.SMALL, x.WIDE));
+            }
+            F->qm_stage = (F->qm_stage + 15) & ~15;
+            if (F->use_qf && qmok && !q_hi.empty() && 2 * F->qm_stage + 1024 <= 227 * 1024) {
+                BDC_CUDA_TRY(cudaFuncSetAttribute(k_qthin_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  2 * F->qm_stage));
+                BDC_CUDA_TRY(cudaMalloc(&F->d_qm, sizeof(ThinQ) * q_hi.size()));
+                BDC_CUDA_TRY(cudaMemcpy(F->d_qm, q_hi.data(), sizeof(ThinQ) * q_hi.size(), cudaMemcpyHostToDevice));
+                F->n_qm = (int)q_hi.size();
+                if (!q_lo.empty()) {
+                    F->ql_stage = qthin_stage_bytes(q_lo);
+                    BDC_CUDA_TRY(cudaMalloc(&F->d_ql, sizeof(ThinQ) * q_lo.size()));
+                    BDC_CUDA_TRY(cudaMemcpy(F->d_ql, q_lo.data(), sizeof(ThinQ) * q_lo.size(), cudaMemcpyHostToDevice));
+                    F->n_ql = (int)q_lo.size();
+                }
+                int pinned_qm = -1;
+                tf.get("qm", &pinned_qm, &unused);
+                if (const char* qm = getenv("BDC_QTHIN")) pinned_qm = !strcmp(qm, "mma") ? 1 : 0;  // forces either form
+                if (pinned_qm >= 0) {
+                    F->use_qm = pinned_qm != 0;
+                } else {
+                    cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
+                    const float t1 = time_ms(H, [&] {
+                        return launch_qthin(F->d_qf, F->n_qf, F->qf_stage, H->stream, nullptr);
+                    }, &e1);
+                    const float t2 = time_ms(H, [&] { return enqueue_qthin_split(H, H->stream, nullptr); }, &e2);
+                    BDC_CUDA_TRY(e1);
+                    BDC_CUDA_TRY(e2);
+                    F->use_qm = t2 < t1;
+                    tf.put("qm", F->use_qm ? 1 : 0, 0);
+                    if (H->verbose)
+                        printf("bdc: tuned q-side terms of 8..64 outputs: %s (with mma.sync %.1f us, CUDA cores %.1f us)\n",
+                               F->use_qm ? "mma.sync" : "CUDA cores", t2 * 1e3f, t1 * 1e3f);
+                }
+            }
         }
         if (dok) {
             const int sm = dthin_smem(k);
@@ -2295,7 +2435,7 @@ bdc_status factored_init(bdc_handle* H) {
         nq += F->n_thinq[lg] > 0;
         nd += F->n_thind[lg] > 0;
     }
-    if (F->use_qf) nq = 1;
+    if (F->use_qf) nq = (F->use_qm && F->n_ql) ? 2 : 1;
     if (F->use_df) {
         nd = 0;
         for (int cl = 0; cl < 4; ++cl) nd += F->n_df[cl] > 0;
@@ -2387,6 +2527,8 @@ void factored_free(bdc_handle* H) {
     cudaFree(F->Bp);
     cudaFree(F->Ddense);
     cudaFree(F->d_qf);
+    cudaFree(F->d_ql);
+    cudaFree(F->d_qm);
     for (auto* d : F->d_df) cudaFree(d);
     for (int lg = 0; lg < 8; ++lg) {
         cudaFree(F->d_thinq[lg]);
@@ -2432,6 +2574,22 @@ static BaEpilogue make_epilogue(bdc_handle* H) {
 
 // the stages of one iteration (enum Stage), each gated by DevState::done / error
 
+// the fused q side split in two: the terms of fewer than 8 small outputs
+// (k_qthin) on a branch beside those of 8 to 64 (k_qthin_mma); neither fills
+// the GPU alone
+static cudaError_t enqueue_qthin_split(bdc_handle* H, cudaStream_t s, const DevState* st) {
+    FactoredState* F = H->fac;
+    cudaError_t e;
+    if (F->n_ql) {
+        if ((e = cudaEventRecord(F->ev_fork, s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(F->side[1], F->ev_fork, 0)) != cudaSuccess) return e;
+        if ((e = launch_qthin(F->d_ql, F->n_ql, F->ql_stage, F->side[1], st)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(F->ev_join[1], F->side[1])) != cudaSuccess) return e;
+    }
+    if ((e = launch_qthin_mma(F->d_qm, F->n_qm, F->qm_stage, s, st)) != cudaSuccess) return e;
+    return F->n_ql ? cudaStreamWaitEvent(s, F->ev_join[1], 0) : cudaSuccess;
+}
+
 static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
     FactoredState* F = H->fac;
     cudaStream_t s = H->stream;
@@ -2451,6 +2609,7 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
             break;
         }
         case ST_QSMALL:
+            if (F->use_qf && F->use_qm) return enqueue_qthin_split(H, s, H->d_st);
             if (F->use_qf) return launch_qthin(F->d_qf, F->n_qf, F->qf_stage, s, H->d_st);
             // fork: each size class on its own branch, joined before the fold
             if ((e = cudaEventRecord(F->ev_fork, s)) != cudaSuccess) return e;
