@@ -167,11 +167,11 @@ struct FactoredState {
     bool use_qm = false;
     bdc::ThinDF* d_df[4] = {};  // by log2 IT
     int n_df[4] = {};
-    // the terms of 8 to 64 outputs on the FP64 tensor path (k_dthin_mma), in
-    // place of the IT = 8 class where that times faster
-    bdc::ThinDF* d_dm = nullptr;
-    int n_dm = 0, dm_smem = 0;
-    bool use_dm = false;
+    // the terms of 2 to 64 outputs on the FP64 tensor path (k_dthin_mma), in
+    // place of a class of d_df where that times faster
+    bdc::ThinDF* d_dm[4] = {};  // by the class of d_df
+    int n_dm[4] = {}, dm_smem[4] = {};
+    bool use_dm[4] = {};
     bool use_qf = false, use_df = false;
     double* lnq_full = nullptr;  // [2^k]
     double* epart = nullptr;  // [ctas][8]
@@ -899,9 +899,10 @@ __global__ void __launch_bounds__(256) k_dthin(const ThinDF* __restrict__ descs,
     }
 }
 
-// D side on the FP64 tensor path, for the terms of 8 to 64 outputs: CTA =
+// D side on the FP64 tensor path, for the terms of 2 to 64 outputs: CTA =
 // one ThinDF entry of kDmRows table rows, warp w = rows 8w .. 8w + 7, all
-// SMALL outputs as SMALL / 8 mma.sync m8n8k4 tiles.  Lq' of the term sits in
+// SMALL outputs as SMALL / 8 mma.sync m8n8k4 tiles (one tile, zero-padded,
+// below 8).  Lq' of the term sits in
 // shared memory at row pitch SMALL + 2 (the four row groups of a B fragment
 // land 8 doubles apart: two wavefronts, the minimum for 256 bytes); the
 // table rows stream through two buffers of kDmChunk entries with cp.async
@@ -913,7 +914,8 @@ constexpr int kDmRows = 64;
 constexpr int kDmChunk = 64;
 constexpr int kDmPitch = 72;
 
-__host__ __device__ constexpr int dmma_ld(int SMALL) { return SMALL + 2; }
+// Lq' row pitch; terms of 2 or 4 outputs use one 8-wide tile, zero-padded
+__host__ __device__ constexpr int dmma_ld(int SMALL) { return (SMALL < 8 ? 8 : SMALL) + 2; }
 static int dthin_mma_smem(int SMALL, int WIDE) {
     return (int)sizeof(double) * WIDE * dmma_ld(SMALL) + 2 * kDmRows * kDmPitch * (int)sizeof(uint16_t);
 }
@@ -937,9 +939,10 @@ __device__ __forceinline__ void dthin_mma_run(const ThinDF& t, const double* __r
     const int nch = WIDE / kDmChunk;
     issue(0);
     cp_async_commit();
-    for (int e = tid; e < SMALL * WIDE; e += 256) {
-        const int w = e / SMALL, i = e % SMALL;
-        L[w * ld + i] = t.lq_trans ? lnq_full[w * SMALL + i] : lnq_full[i * WIDE + w];
+    const int SP = NB * 8;  // outputs of the tiles: SMALL, or 8 with zeros past SMALL
+    for (int e = tid; e < SP * WIDE; e += 256) {
+        const int w = e / SP, i = e % SP;
+        L[w * ld + i] = (i >= SMALL) ? 0.0 : t.lq_trans ? lnq_full[w * SMALL + i] : lnq_full[i * WIDE + w];
     }
     double acc[NB][2];
 #pragma unroll
@@ -968,7 +971,10 @@ __device__ __forceinline__ void dthin_mma_run(const ThinDF& t, const double* __r
 #pragma unroll
     for (int nb = 0; nb < NB; ++nb)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) t.out[(int64_t)row * t.out_s + (int64_t)(nb * 8 + 2 * q + h) * t.out_i] = acc[nb][h];
+        for (int h = 0; h < 2; ++h) {
+            const int i = nb * 8 + 2 * q + h;
+            if (i < SMALL) t.out[(int64_t)row * t.out_s + (int64_t)i * t.out_i] = acc[nb][h];
+        }
 }
 
 __global__ void __launch_bounds__(256) k_dthin_mma(const ThinDF* __restrict__ descs, const double* __restrict__ lnq_full,
@@ -977,6 +983,8 @@ __global__ void __launch_bounds__(256) k_dthin_mma(const ThinDF* __restrict__ de
     extern __shared__ __align__(16) double dmsm[];
     const ThinDF& t = descs[blockIdx.x];
     switch (t.SMALL) {
+        case 2:
+        case 4:
         case 8: dthin_mma_run<1>(t, lnq_full, dmsm); break;
         case 16: dthin_mma_run<2>(t, lnq_full, dmsm); break;
         case 32: dthin_mma_run<4>(t, lnq_full, dmsm); break;
@@ -2217,15 +2225,17 @@ bdc_status factored_init(bdc_handle* H) {
                     all_d[cl].push_back(f);
                 }
             }
-        // the IT = 8 class again in 64-row blocks for k_dthin_mma
-        std::vector<ThinDF> all_m;
-        bool mok = dok && !all_d[3].empty();
-        for (int lg = 0; lg < 8 && mok; ++lg)
+        // the classes of 2 to 64 outputs again in 64-row blocks for k_dthin_mma
+        std::vector<ThinDF> all_m[4];
+        bool mok[4] = {false, dok, dok, dok};
+        for (int lg = 0; lg < 8; ++lg)
             for (auto& d : td[lg]) {
-                if (d.SMALL < 8) continue;
+                int cl = 0;
+                while ((1 << cl) < std::min(d.SMALL, 8)) ++cl;
+                if (cl == 0 || !mok[cl]) continue;
                 if (d.SMALL > 64 || d.WIDE % kDmChunk != 0) {
-                    mok = false;
-                    break;
+                    mok[cl] = false;
+                    continue;
                 }
                 ThinDF f{};
                 f.wide = d.wide;
@@ -2237,17 +2247,17 @@ bdc_status factored_init(bdc_handle* H) {
                 f.out = d.out;
                 f.out_s = d.out_s;
                 f.out_i = d.out_i;
-                F->dm_smem = std::max(F->dm_smem, dthin_mma_smem(d.SMALL, d.WIDE));
+                F->dm_smem[cl] = std::max(F->dm_smem[cl], dthin_mma_smem(d.SMALL, d.WIDE));
                 for (int r0 = 0; r0 < d.rows; r0 += kDmRows) {
                     f.row0 = r0;
-                    all_m.push_back(f);
+                    all_m[cl].push_back(f);
                 }
             }
         int pinned_q = -1, pinned_d = -1, pinned_m = -1, unused = 0;
         tf.get("qf", &pinned_q, &unused);
         tf.get("df", &pinned_d, &unused);
-        tf.get("dm", &pinned_m, &unused);
-        if (const char* dm = getenv("BDC_DTHIN")) pinned_m = !strcmp(dm, "mma") ? 1 : 0;  // forces either form
+        tf.get("dm", &pinned_m, &unused);  // bit cl: class cl on k_dthin_mma
+        if (const char* dm = getenv("BDC_DTHIN")) pinned_m = !strcmp(dm, "mma") ? 14 : 0;  // forces either form
         BDC_CUDA_TRY(cudaMemsetAsync(H->d_st, 0, sizeof(DevState), H->stream));
         if (qok && !all_q.empty()) {
             F->qf_stage = qthin_stage_bytes(all_q);
@@ -2341,31 +2351,43 @@ bdc_status factored_init(bdc_handle* H) {
                     printf("bdc: tuned D-side term products: %s (fused %.1f us, per class %.1f us)\n",
                            F->use_df ? "fused" : "per class", tfu * 1e3f, tc * 1e3f);
             }
-            // the IT = 8 class of the fused launches on the FP64 tensor path
-            if (F->use_df && mok && F->dm_smem + 1024 <= 227 * 1024) {
-                BDC_CUDA_TRY(cudaFuncSetAttribute(k_dthin_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, F->dm_smem));
-                BDC_CUDA_TRY(cudaMalloc(&F->d_dm, sizeof(ThinDF) * all_m.size()));
-                BDC_CUDA_TRY(cudaMemcpy(F->d_dm, all_m.data(), sizeof(ThinDF) * all_m.size(), cudaMemcpyHostToDevice));
-                F->n_dm = (int)all_m.size();
+            // classes of the fused launches on the FP64 tensor path
+            int dm_bits = 0, dm_max = 0;
+            auto dm_ok = [&](int cl) {
+                return mok[cl] && !all_m[cl].empty() && F->n_df[cl] > 0 && F->dm_smem[cl] + 1024 <= 227 * 1024;
+            };
+            for (int cl = 1; cl < 4; ++cl)
+                if (dm_ok(cl)) dm_max = std::max(dm_max, F->dm_smem[cl]);
+            if (F->use_df && dm_max > 0)
+                BDC_CUDA_TRY(cudaFuncSetAttribute(k_dthin_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, dm_max));
+            for (int cl = 1; cl < 4 && F->use_df; ++cl) {
+                if (!dm_ok(cl)) continue;
+                BDC_CUDA_TRY(cudaMalloc(&F->d_dm[cl], sizeof(ThinDF) * all_m[cl].size()));
+                BDC_CUDA_TRY(cudaMemcpy(F->d_dm[cl], all_m[cl].data(), sizeof(ThinDF) * all_m[cl].size(),
+                                        cudaMemcpyHostToDevice));
+                F->n_dm[cl] = (int)all_m[cl].size();
                 if (pinned_m >= 0) {
-                    F->use_dm = pinned_m != 0;
+                    F->use_dm[cl] = (pinned_m >> cl) & 1;
                 } else {
                     cudaError_t e1 = cudaSuccess, e2 = cudaSuccess;
-                    const float t8 = time_ms(H, [&] {
-                        return launch_dthin(F->d_df[3], F->n_df[3], 8, H->k, F->lnq_full, H->stream, nullptr);
+                    const float tc = time_ms(H, [&] {
+                        return launch_dthin(F->d_df[cl], F->n_df[cl], 1 << cl, H->k, F->lnq_full, H->stream, nullptr);
                     }, &e1);
                     const float tm = time_ms(H, [&] {
-                        return launch_dthin_mma(F->d_dm, F->n_dm, F->dm_smem, F->lnq_full, H->stream, nullptr);
+                        return launch_dthin_mma(F->d_dm[cl], F->n_dm[cl], F->dm_smem[cl], F->lnq_full, H->stream,
+                                                nullptr);
                     }, &e2);
                     BDC_CUDA_TRY(e1);
                     BDC_CUDA_TRY(e2);
-                    F->use_dm = tm < t8;
-                    tf.put("dm", F->use_dm ? 1 : 0, 0);
+                    F->use_dm[cl] = tm < tc;
                     if (H->verbose)
-                        printf("bdc: tuned D-side terms of 8..64 outputs: %s (mma.sync %.1f us, CUDA cores %.1f us)\n",
-                               F->use_dm ? "mma.sync" : "CUDA cores", tm * 1e3f, t8 * 1e3f);
+                        printf("bdc: tuned D-side terms of class %d (%s outputs): %s (mma.sync %.1f us, CUDA cores %.1f us)\n",
+                               cl, cl == 3 ? "8..64" : (cl == 2 ? "4" : "2"), F->use_dm[cl] ? "mma.sync" : "CUDA cores",
+                               tm * 1e3f, tc * 1e3f);
                 }
+                dm_bits |= (int)F->use_dm[cl] << cl;
             }
+            if (F->use_df && pinned_m < 0) tf.put("dm", dm_bits, 0);
         }
     }
 
@@ -2550,7 +2572,7 @@ void factored_free(bdc_handle* H) {
     }
     cudaFree(F->d_fold);
     ozaki_free(F->oz);
-    cudaFree(F->d_dm);
+    for (auto* d : F->d_dm) cudaFree(d);
     delete F;
     H->fac = nullptr;
 }
@@ -2641,8 +2663,8 @@ static cudaError_t enqueue_stage(bdc_handle* H, int stage, double a) {
                 for (int cl = 0; cl < 4; ++cl) {
                     if (!F->n_df[cl]) continue;
                     if ((e = cudaStreamWaitEvent(F->side[cl], F->ev_fork, 0)) != cudaSuccess) return e;
-                    e = (cl == 3 && F->use_dm)
-                            ? launch_dthin_mma(F->d_dm, F->n_dm, F->dm_smem, F->lnq_full, F->side[cl], H->d_st)
+                    e = F->use_dm[cl]
+                            ? launch_dthin_mma(F->d_dm[cl], F->n_dm[cl], F->dm_smem[cl], F->lnq_full, F->side[cl], H->d_st)
                             : launch_dthin(F->d_df[cl], F->n_df[cl], 1 << cl, H->k, F->lnq_full, F->side[cl], H->d_st);
                     if (e != cudaSuccess) return e;
                     if ((e = cudaEventRecord(F->ev_join[cl], F->side[cl])) != cudaSuccess) return e;
