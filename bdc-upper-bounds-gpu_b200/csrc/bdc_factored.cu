@@ -831,9 +831,20 @@ __global__ void __launch_bounds__(256) k_dthin(const ThinDF* __restrict__ descs,
     const ThinDF& t = descs[blockIdx.x];
     const int SMALL = t.SMALL, WIDE = t.WIDE;
     const int cs = 8 * SMALL + 1;  // padded chunk of 8 contraction indices
-    for (int e = threadIdx.x; e < SMALL * WIDE; e += blockDim.x) {
-        const int w = e / SMALL, i = e % SMALL;
-        lq[(w >> 3) * cs + (w & 7) * SMALL + i] = t.lq_trans ? lnq_full[w * SMALL + i] : lnq_full[i * WIDE + w];
+    // eight loads per thread in flight, then their stores
+    for (int e0 = threadIdx.x; e0 < SMALL * WIDE; e0 += 8 * blockDim.x) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * (int)blockDim.x, w = e / SMALL, i = e % SMALL;
+            v[u] = (e < SMALL * WIDE) ? (t.lq_trans ? __ldg(lnq_full + w * SMALL + i) : __ldg(lnq_full + i * WIDE + w))
+                                      : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * (int)blockDim.x, w = e / SMALL, i = e % SMALL;
+            if (e < SMALL * WIDE) lq[(w >> 3) * cs + (w & 7) * SMALL + i] = v[u];
+        }
     }
     __syncthreads();
     const int LPR = t.LPR;
@@ -937,13 +948,16 @@ __device__ __forceinline__ void dthin_mma_run(const ThinDF& t, const double* __r
         }
     };
     const int nch = WIDE / kDmChunk;
-    issue(0);
-    cp_async_commit();
+    // Lq' by 8-byte asynchronous copies in the first chunk's group (all of a
+    // thread's copies in flight at once), zeros past SMALL by plain stores
     const int SP = NB * 8;  // outputs of the tiles: SMALL, or 8 with zeros past SMALL
     for (int e = tid; e < SP * WIDE; e += 256) {
         const int w = e / SP, i = e % SP;
-        L[w * ld + i] = (i >= SMALL) ? 0.0 : t.lq_trans ? lnq_full[w * SMALL + i] : lnq_full[i * WIDE + w];
+        if (i >= SMALL) L[w * ld + i] = 0.0;
+        else cp_async8(L + w * ld + i, t.lq_trans ? lnq_full + w * SMALL + i : lnq_full + i * WIDE + w);
     }
+    issue(0);
+    cp_async_commit();
     double acc[NB][2];
 #pragma unroll
     for (int nb = 0; nb < NB; ++nb) acc[nb][0] = acc[nb][1] = 0.0;
