@@ -82,6 +82,34 @@ __host__ __device__ inline uint32_t binom(uint32_t n, uint32_t k) {
 // on a 16-byte boundary.  The row stride is 2^{mmax+1} entries.
 // Entries are uint16 (exact: every count in a half table of length <= 17
 // is < 65536).  m == h (the whole half) is an equality test, never stored.
+#ifdef __CUDACC__
+// The sum (MAX = false) or maximum (MAX = true) of n block partials v[i *
+// stride] by one whole warp, in a fixed order: lane l combines i = l, l + 32,
+// ... (eight loads in flight at a time), then a shuffle tree; every lane
+// returns the result.  Replaces one thread walking the partials, whose loads
+// would wait on one another.
+template <bool MAX>
+__device__ __forceinline__ double warp_parts(const double* __restrict__ v, int n, int stride) {
+    const int lane = threadIdx.x & 31;
+    double a = MAX ? -1.7976931348623157e308 : 0.0;
+    int i = lane;
+    for (; i + 7 * 32 < n; i += 8 * 32) {
+        double t[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) t[u] = v[(size_t)(i + 32 * u) * stride];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a = MAX ? fmax(a, t[u]) : a + t[u];
+    }
+    for (; i < n; i += 32) a = MAX ? fmax(a, v[(size_t)i * stride]) : a + v[(size_t)i * stride];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double b = __shfl_xor_sync(0xFFFFFFFFu, a, o);
+        a = MAX ? fmax(a, b) : a + b;
+    }
+    return a;
+}
+#endif
+
 struct HalfTables {
     const uint16_t* rows = nullptr;  // [2^h][stride]
     int h = 0;                       // half length

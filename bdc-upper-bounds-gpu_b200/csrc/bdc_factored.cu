@@ -3126,11 +3126,11 @@ __global__ void __launch_bounds__(256) k_acc_extrap(const uint32_t* __restrict__
     if (threadIdx.x == 0) part[blockIdx.x] = mx;
 }
 
+// one warp
 __global__ void k_acc_max(const double* __restrict__ part, int nb, DevState* st) {
-    if (acc_gated(st) || threadIdx.x != 0) return;
-    double m = -DBL_MAX;
-    for (int b = 0; b < nb; ++b) m = fmax(m, part[b]);
-    st->ng_max = m;
+    if (acc_gated(st)) return;
+    const double m = warp_parts<true>(part, nb, 1);
+    if (threadIdx.x == 0) st->ng_max = m;
 }
 
 // Lt -= max, Pw = |O| exp(Lt); block sums of |O| exp(Lt)
@@ -3154,10 +3154,11 @@ __global__ void __launch_bounds__(256) k_acc_pw(const uint32_t* __restrict__ rep
 }
 
 // ln Z of y and the exp shift of the next update (max ln y + eta * last bound)
+// one warp
 __global__ void k_acc_setz(const double* __restrict__ part, int nb, double eta, DevState* st) {
-    if (acc_gated(st) || threadIdx.x != 0) return;
-    double s = 0.0;
-    for (int b = 0; b < nb; ++b) s += part[b];
+    if (acc_gated(st)) return;
+    const double s = warp_parts<false>(part, nb, 1);
+    if (threadIdx.x != 0) return;
     const double lnz = log(s);
     st->log_z = lnz;
     st->shift = -lnz + eta * st->max_d;

@@ -106,13 +106,12 @@ __global__ void __launch_bounds__(256) k_aa_dots(int64_t L, const uint8_t* __res
     }
 }
 
+// one warp per output a (blockIdx.x)
 __global__ void k_aa_dots_finish(const double* __restrict__ part, int nb, int m, double* __restrict__ out) {
-    const int a = threadIdx.x;
-    if (a >= 2 * kAAMax) return;
-    if ((a % kAAMax) >= m) return;
-    double s = 0.0;
-    for (int b = 0; b < nb; ++b) s += part[(size_t)b * 2 * kAAMax + a];
-    out[a] = s;
+    const int a = blockIdx.x;
+    if (a >= 2 * kAAMax || (a % kAAMax) >= m) return;
+    const double s = warp_parts<false>(part + a, nb, 2 * kAAMax);
+    if (threadIdx.x == 0) out[a] = s;
 }
 
 // x = g_last - sum_a gamma_a dG_a, clipped at 0; partial sums of w x
@@ -137,10 +136,9 @@ __global__ void __launch_bounds__(256) k_aa_mix(int64_t L, const uint8_t* __rest
 // x /= sum of the partials (every block re-adds them: nb is small)
 __global__ void k_scale_by_sum(int64_t L, double* __restrict__ x, const double* __restrict__ part, int nb) {
     __shared__ double inv;
-    if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int b = 0; b < nb; ++b) s += part[b];
-        inv = s > 0.0 ? 1.0 / s : 0.0;
+    if (threadIdx.x < 32) {
+        const double s = warp_parts<false>(part, nb, 1);
+        if (threadIdx.x == 0) inv = s > 0.0 ? 1.0 / s : 0.0;
     }
     __syncthreads();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x)
@@ -249,8 +247,22 @@ __global__ void __launch_bounds__(256) k_rs_acc(int S, int ny, const float* __re
     const int c = blockIdx.y;
     if (y >= ny) return;
     const int s0 = c * kRsChunk, s1 = min(S, s0 + kRsChunk);
+    // eight members' loads in flight, then their multiply-adds in member
+    // order (the same sum, bit for bit, as one member at a time)
     double a = 0.0;
-    for (int s = s0; s < s1; ++s) a = fma((double)w[s] * p[s], (double)rows[(int64_t)s * ny + y], a);
+    int s = s0;
+    for (; s + 8 <= s1; s += 8) {
+        float r[8];
+        double wp[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            r[u] = rows[(int64_t)(s + u) * ny + y];
+            wp[u] = (double)w[s + u] * p[s + u];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a = fma(wp[u], (double)r[u], a);
+    }
+    for (; s < s1; ++s) a = fma((double)w[s] * p[s], (double)rows[(int64_t)s * ny + y], a);
     part[(int64_t)c * ny + y] = a;
 }
 
@@ -265,7 +277,26 @@ __global__ void k_rs_sum_lnq(int k, int nc, const double* __restrict__ part, dou
     if (y >= ny) return;
     const uint32_t r = reverse_bits((uint32_t)y, k), c = complement_bits((uint32_t)y, k), rc = reverse_bits(c, k);
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    for (int ch = 0; ch < nc; ++ch) {
+    int ch = 0;
+    for (; ch + 4 <= nc; ch += 4) {  // four chunks' loads in flight, added in chunk order
+        double v[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const double* pc = part + (int64_t)(ch + u) * ny;
+            v[u][0] = pc[y];
+            v[u][1] = pc[r];
+            v[u][2] = pc[c];
+            v[u][3] = pc[rc];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            a0 += v[u][0];
+            a1 += v[u][1];
+            a2 += v[u][2];
+            a3 += v[u][3];
+        }
+    }
+    for (; ch < nc; ++ch) {
         const double* pc = part + (int64_t)ch * ny;
         a0 += pc[y];
         a1 += pc[r];
@@ -292,7 +323,19 @@ __global__ void __launch_bounds__(256) k_rs_div(int S, int ny, const float* __re
     if (s < S) {
         const float* row = rows + (int64_t)s * ny;
         double a = 0.0;
-        for (int y = lane; y < ny; y += 32) a = fma((double)row[y], lnq[y], a);
+        int y = lane;
+        for (; y + 7 * 32 < ny; y += 8 * 32) {  // eight loads in flight, summed in order
+            float r[8];
+            double l[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                r[u] = row[y + 32 * u];
+                l[u] = lnq[y + 32 * u];
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) a = fma((double)r[u], l[u], a);
+        }
+        for (; y < ny; y += 32) a = fma((double)row[y], lnq[y], a);
         for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
         d = h[s] - a * inv_c;
         r = (double)w[s] * p[s] * d;
@@ -327,7 +370,21 @@ __global__ void __launch_bounds__(1024) k_rs_update(int S, const double* __restr
     __shared__ double mD, Zs;
     if (threadIdx.x == 0) {
         double m = -DBL_MAX, r = 0.0;
-        for (int b = 0; b < nb; ++b) {
+        int b = 0;
+        for (; b + 8 <= nb; b += 8) {  // eight partials' loads in flight, combined in order
+            double pm[8], pr[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                pm[u] = part[2 * (b + u)];
+                pr[u] = part[2 * (b + u) + 1];
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                m = fmax(m, pm[u]);
+                r += pr[u];
+            }
+        }
+        for (; b < nb; ++b) {
             m = fmax(m, part[2 * b]);
             r += part[2 * b + 1];
         }
@@ -677,7 +734,7 @@ struct Anderson {
         BDC_CUDA_TRY(cudaGetLastError());
         AAPtrs P = ptrs();
         k_aa_dots<<<nb, 256, 0, s>>>(L, w, P, dF[sl].get<double>(), f_last.get<double>(), part.get<double>());
-        k_aa_dots_finish<<<1, 32, 0, s>>>(part.get<double>(), nb, count, dots.get<double>());
+        k_aa_dots_finish<<<2 * kAAMax, 32, 0, s>>>(part.get<double>(), nb, count, dots.get<double>());
         BDC_CUDA_TRY(cudaGetLastError());
         double hd[2 * kAAMax];
         BDC_CUDA_TRY(cudaMemcpyAsync(hd, dots.get<double>(), sizeof(hd), cudaMemcpyDeviceToHost, s));
