@@ -228,6 +228,14 @@ __host__ __device__ __forceinline__ uint32_t fac_loc(uint32_t x, int n, int row0
     return fac_pos(x, n >> 1) - ((uint32_t)row0 << (n >> 1));
 }
 
+// the string at dense position xd of the held rows (fac_pos is an
+// involution), and whether it is a representative: kernels that touch every
+// representative walk the dense arrays in memory order this way, coalesced,
+// instead of the ascending list (whose positions are bit-reversed in a row)
+__device__ __forceinline__ uint32_t fac_str(uint32_t xd, int n, int row0) {
+    return fac_pos(xd + ((uint32_t)row0 << (n >> 1)), n >> 1);
+}
+
 
 // ------------------------------------------------ products: plain store
 // LAYOUT < 0: register-staged mainloop (any operand kind); otherwise the
@@ -3097,17 +3105,17 @@ __global__ void k_acc_decide(DevState* st) {
 
 // x_{t-1}, x_t (dense, at representatives) and the extrapolated ln y into Lt;
 // block max of ln y
-__global__ void __launch_bounds__(256) k_acc_extrap(const uint32_t* __restrict__ reps, int64_t R, int n, int row0,
-                                                    double* __restrict__ xa, double* __restrict__ xb,
-                                                    double* __restrict__ Lt, double* __restrict__ part,
-                                                    const DevState* st) {
+__global__ void __launch_bounds__(256) k_acc_extrap(int64_t nx, int n, int row0, double* __restrict__ xa,
+                                                    double* __restrict__ xb, double* __restrict__ Lt,
+                                                    double* __restrict__ part, const DevState* st) {
     if (acc_gated(st)) return;
     const int mode = st->ng_mode;
     const double lnz = st->log_z;
     const double beta = (double)st->ng_t / ((double)st->ng_t + 3.0);
     double mx = -DBL_MAX;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t xd = fac_loc(reps[i], n, row0);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nx; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t xd = (uint32_t)i;
+        if (!is_rep(fac_str(xd, n, row0), n)) continue;
         double y;
         if (mode == 1) {
             const double a_old = xa[xd], a_new = Lt[xd] - lnz;
@@ -3134,14 +3142,14 @@ __global__ void k_acc_max(const double* __restrict__ part, int nb, DevState* st)
 }
 
 // Lt -= max, Pw = |O| exp(Lt); block sums of |O| exp(Lt)
-__global__ void __launch_bounds__(256) k_acc_pw(const uint32_t* __restrict__ reps, int64_t R, int n, int row0,
-                                                double* __restrict__ Lt, double* __restrict__ Pw,
-                                                double* __restrict__ part, const DevState* st) {
+__global__ void __launch_bounds__(256) k_acc_pw(int64_t nx, int n, int row0, double* __restrict__ Lt,
+                                                double* __restrict__ Pw, double* __restrict__ part, const DevState* st) {
     if (acc_gated(st)) return;
     const double m = st->ng_max;
     double sum = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i], xd = fac_loc(x, n, row0);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nx; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t xd = (uint32_t)i, x = fac_str(xd, n, row0);
+        if (!is_rep(x, n)) continue;
         const double l = Lt[xd] - m;
         const double o = (double)orbit_size(x, n);
         const double e = exp(l);
@@ -3176,9 +3184,10 @@ static cudaError_t enqueue_acc_step(bdc_handle* H, double eta) {
     cudaStream_t s = H->stream;
     const int nb = H->nb_upd;
     k_acc_decide<<<1, 32, 0, s>>>(H->d_st);
-    k_acc_extrap<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->snap0, F->snap1, F->Lt, F->epart, H->d_st);
+    const int64_t nx = (int64_t)F->H1h << H->s.n2;  // the dense positions of the held rows
+    k_acc_extrap<<<nb, 256, 0, s>>>(nx, H->n, F->row0, F->snap0, F->snap1, F->Lt, F->epart, H->d_st);
     k_acc_max<<<1, 32, 0, s>>>(F->epart, nb, H->d_st);
-    k_acc_pw<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Lt, F->Pw, F->epart, H->d_st);
+    k_acc_pw<<<nb, 256, 0, s>>>(nx, H->n, F->row0, F->Lt, F->Pw, F->epart, H->d_st);
     k_acc_setz<<<1, 32, 0, s>>>(F->epart, nb, eta, H->d_st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -3211,12 +3220,13 @@ bdc_status factored_acc_buffers(bdc_handle* H) {
 }
 
 // x_t = x_{t-1} = the current normalised log iterate; nothing evaluated yet
-__global__ void __launch_bounds__(256) k_acc_init(const uint32_t* __restrict__ reps, int64_t R, int n, int row0,
-                                                  const double* __restrict__ Lt, double* __restrict__ xa,
-                                                  double* __restrict__ xb, DevState* st, double gap_nats) {
+__global__ void __launch_bounds__(256) k_acc_init(int64_t nx, int n, int row0, const double* __restrict__ Lt,
+                                                  double* __restrict__ xa, double* __restrict__ xb, DevState* st,
+                                                  double gap_nats) {
     const double lnz = st->log_z;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t xd = fac_loc(reps[i], n, row0);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nx; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t xd = (uint32_t)i;
+        if (!is_rep(fac_str(xd, n, row0), n)) continue;
         const double l = Lt[xd] - lnz;
         xa[xd] = l;
         xb[xd] = l;
@@ -3232,7 +3242,7 @@ bdc_status factored_acc_start(bdc_handle* H, double gap_bits) {
     bdc_status rc = factored_acc_buffers(H);
     if (rc != BDC_OK) return rc;
     FactoredState* F = H->fac;
-    k_acc_init<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Lt, F->snap0, F->snap1, H->d_st,
+    k_acc_init<<<H->nb_upd, 256, 0, H->stream>>>((int64_t)F->H1h << H->s.n2, H->n, F->row0, F->Lt, F->snap0, F->snap1, H->d_st,
                                                  gap_bits * 0.69314718055994530942);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
