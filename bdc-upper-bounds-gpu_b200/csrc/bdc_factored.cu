@@ -129,6 +129,9 @@ struct FactoredState {
     int H1h = 0;              // rows held: x_hi in [row0, row0 + H1h) (all x_hi < H1 / 2 on one GPU)
     int row0 = 0;             // first row held (a shard of the rows over several GPUs; 0 on one GPU)
     int64_t i0 = 0, Rl = 0;   // the representatives in those rows: [i0, i0 + Rl) of the ascending list
+    int64_t* d_rowstart = nullptr;  // [H1h + 1]: held row r's representatives are [i0 + rowstart[r], i0 + rowstart[r + 1])
+    double* rpart = nullptr;        // [2 H1h]: per-row partials of the load
+    int rows_smem = 0;              // dynamic shared memory of the row kernels
     std::vector<bdc::Term> terms;
     double* Pw = nullptr;     // [2^{n-1}]  |O(x)| e(x) at representatives, 0 elsewhere
     double* Lt = nullptr;     // [2^{n-1}]  ln e(x) (p = e / Z)
@@ -1373,73 +1376,148 @@ __global__ void k_fac_rescale_finish(const double* part, int nb, double a, DevSt
     st->done = !(mx >= a);
 }
 
-// p -> (Pw, Lt) at representatives; block max of ln p for the first shift
-__global__ void __launch_bounds__(256)
-k_fac_load(const uint32_t* __restrict__ reps, int64_t R, int n, int row0, const double* __restrict__ p,
-           double* Pw, double* Lt, double* part, int strict_zero, DevState* st) {
-    double mx = -DBL_MAX;
-    int zero = 0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i], xd = fac_loc(x, n, row0);
-        const double v = p[i];
-        Pw[xd] = (double)orbit_size(x, n) * v;
-        if (strict_zero) {
-            // p = 0 stays 0 (ln p = -inf): the map of the BA update itself
-            Lt[xd] = (v > 0.0) ? log(v) : -INFINITY;
-            if (v > 0.0) mx = fmax(mx, log(v));
-            continue;
-        }
-        // ln 0 = 0 (backend/BAA.cu:573-580): marked with NaN for the epilogue
-        const double l = (v != 0.0) ? log(v) : 0.0;
-        Lt[xd] = (v != 0.0) ? l : __longlong_as_double(0x7ff8000000000000ll);
-        mx = fmax(mx, l);
-        if (v == 0.0) zero = 1;
-    }
-    __shared__ double red[256];
-    __shared__ int zr[256];
-    red[threadIdx.x] = mx;
-    zr[threadIdx.x] = zero;
-    __syncthreads();
-    for (int t = 128; t > 0; t >>= 1) {
-        if (threadIdx.x < t) {
-            red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + t]);
-            zr[threadIdx.x] |= zr[threadIdx.x + t];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        part[2 * blockIdx.x] = red[0];
-        part[2 * blockIdx.x + 1] = (double)zr[0];
-    }
-}
-
+// one warp
 __global__ void k_fac_load_finish(const double* part, int nb, int k, DevState* st) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double mx = -DBL_MAX, z = 0.0;
-    for (int b = 0; b < nb; ++b) {
-        mx = fmax(mx, part[2 * b]);
-        z = fmax(z, part[2 * b + 1]);
-    }
+    if (blockIdx.x != 0) return;
+    const double mx = warp_parts<true>(part, nb, 2);
+    const double z = warp_parts<true>(part + 1, nb, 2);
+    if (threadIdx.x != 0) return;
     st->log_z = 0.0;
     st->shift = mx + (double)k * 0.69314718055994530942;  // first guess; re-scaled if off
     st->zero_p = (z != 0.0);
 }
 
-// p per representative from the dense state: p = Pw / (|O| Z)
-__global__ void k_fac_store(const uint32_t* __restrict__ reps, int64_t R, int n, int row0,
-                            const double* __restrict__ Pw, double* __restrict__ p, const DevState* st) {
-    const double inv_z = exp(-st->log_z);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint32_t x = reps[i];
-        p[i] = Pw[fac_loc(x, n, row0)] * inv_z / (double)orbit_size(x, n);
+// ---- per-representative vectors <-> dense rows, one CTA per held row.
+// The representatives of row x_hi are a contiguous run of the ascending list
+// in ascending x_lo, while the dense row stores column rev(x_lo): the CTA
+// ranks the row's representatives by a block scan of the flags in x_lo order
+// and moves the run through shared memory, so that both sides are read and
+// written in memory order.  Shared memory: the run (8 bytes per column) and
+// the ranks (2 bytes per column, 0xFFFF where no representative).
+constexpr uint16_t kNoRank = 0xFFFF;
+
+__host__ __device__ constexpr int rows_smem_bytes(int n2) { return (8 + 2) << n2; }
+
+// ranks of the representatives of row xh in x_lo order into rk; returns their
+// number (every thread)
+__device__ __forceinline__ int row_ranks(uint32_t xh, int n, int n2, uint16_t* rk) {
+    __shared__ int wsum[8];
+    const int H2 = 1 << n2, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int C = H2 >= 256 ? H2 / 256 : 1;  // consecutive x_lo per thread
+    const int lo0 = tid * C;
+    int cnt = 0;
+    for (int j = 0; j < C && lo0 + j < H2; ++j) cnt += is_rep((xh << n2) | (uint32_t)(lo0 + j), n) ? 1 : 0;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    int base = incl - cnt, total = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        if (w < warp) base += wsum[w];
+        total += wsum[w];
+    }
+    for (int j = 0; j < C && lo0 + j < H2; ++j) {
+        const bool rep = is_rep((xh << n2) | (uint32_t)(lo0 + j), n);
+        rk[lo0 + j] = rep ? (uint16_t)base : kNoRank;
+        base += rep ? 1 : 0;
+    }
+    __syncthreads();
+    return total;
+}
+
+// p -> (Pw, Lt) on the held rows, per-row partials [max ln p, zero flag]
+// (k_fac_load's per-element rules)
+__global__ void __launch_bounds__(256) k_fac_load_rows(const int64_t* __restrict__ rs, int n, int row0,
+                                                       const double* __restrict__ p, double* __restrict__ Pw,
+                                                       double* __restrict__ Lt, double* __restrict__ part,
+                                                       int strict_zero) {
+    extern __shared__ double rsm[];
+    const int n2 = n >> 1, H2 = 1 << n2, r = blockIdx.x;
+    uint16_t* rk = reinterpret_cast<uint16_t*>(rsm + H2);
+    const uint32_t xh = (uint32_t)(row0 + r);
+    const int cnt = row_ranks(xh, n, n2, rk);
+    const int64_t b0 = rs[r];
+    for (int j = threadIdx.x; j < cnt; j += 256) rsm[j] = p[b0 + j];
+    __syncthreads();
+    double mx = -DBL_MAX;
+    int zero = 0;
+    double* pw = Pw + ((int64_t)r << n2);
+    double* lt = Lt + ((int64_t)r << n2);
+    for (int c = threadIdx.x; c < H2; c += 256) {
+        const uint32_t xl = reverse_bits((uint32_t)c, n2);
+        const uint16_t k = rk[xl];
+        if (k == kNoRank) continue;
+        const double v = rsm[k];
+        pw[c] = (double)orbit_size((xh << n2) | xl, n) * v;
+        if (strict_zero) {
+            lt[c] = (v > 0.0) ? log(v) : -INFINITY;
+            if (v > 0.0) mx = fmax(mx, log(v));
+            continue;
+        }
+        const double l = (v != 0.0) ? log(v) : 0.0;
+        lt[c] = (v != 0.0) ? l : __longlong_as_double(0x7ff8000000000000ll);
+        mx = fmax(mx, l);
+        if (v == 0.0) zero = 1;
+    }
+    __shared__ double red[8];
+    __shared__ int zr[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+        zero |= __shfl_xor_sync(0xFFFFFFFFu, zero, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[threadIdx.x >> 5] = mx;
+        zr[threadIdx.x >> 5] = zero;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; ++w) {
+            red[0] = fmax(red[0], red[w]);
+            zr[0] |= zr[w];
+        }
+        part[2 * r] = red[0];
+        part[2 * r + 1] = (double)zr[0];
     }
 }
 
-// scatter h per representative into the dense layout
-__global__ void k_scatter(const uint32_t* __restrict__ reps, int64_t R, int n, int row0, const double* __restrict__ v,
-                          double* __restrict__ dense) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
-        dense[fac_loc(reps[i], n, row0)] = v[i];
+// MODE 0: p = Pw / (|O| Z) (k_fac_store's rule); MODE 1: out = dense (a
+// gather of D); MODE 2: dense = v (a scatter of h), on the held rows
+template <int MODE>
+__global__ void __launch_bounds__(256) k_fac_rows(const int64_t* __restrict__ rs, int n, int row0,
+                                                  const double* __restrict__ src, double* __restrict__ dst,
+                                                  const DevState* st) {
+    extern __shared__ double rsm[];
+    const int n2 = n >> 1, H2 = 1 << n2, r = blockIdx.x;
+    uint16_t* rk = reinterpret_cast<uint16_t*>(rsm + H2);
+    const uint32_t xh = (uint32_t)(row0 + r);
+    const int cnt = row_ranks(xh, n, n2, rk);
+    const int64_t b0 = rs[r];
+    const double inv_z = (MODE == 0) ? exp(-st->log_z) : 1.0;
+    if (MODE == 2) {
+        for (int j = threadIdx.x; j < cnt; j += 256) rsm[j] = src[b0 + j];
+        __syncthreads();
+        double* d = dst + ((int64_t)r << n2);
+        for (int c = threadIdx.x; c < H2; c += 256) {
+            const uint16_t k = rk[reverse_bits((uint32_t)c, n2)];
+            if (k != kNoRank) d[c] = rsm[k];
+        }
+        return;
+    }
+    const double* d = src + ((int64_t)r << n2);
+    for (int c = threadIdx.x; c < H2; c += 256) {
+        const uint32_t xl = reverse_bits((uint32_t)c, n2);
+        const uint16_t k = rk[xl];
+        if (k == kNoRank) continue;
+        rsm[k] = (MODE == 0) ? d[c] * inv_z / (double)orbit_size((xh << n2) | xl, n) : d[c];
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < cnt; j += 256) dst[b0 + j] = rsm[j];
 }
 
 // constant parts of LA (AL columns) and RB (BR^T rows) from the bundles
@@ -1896,6 +1974,19 @@ bdc_status factored_init(bdc_handle* H) {
         F->H1h = c1 - c0;
         F->i0 = below(c0);
         F->Rl = below(c1) - F->i0;
+        // where each held row's run of representatives starts (k_fac_rows)
+        std::vector<int64_t> rs((size_t)F->H1h + 1);
+        for (int q = 0; q <= F->H1h; ++q) rs[(size_t)q] = below(c0 + q) - F->i0;
+        BDC_CUDA_TRY(cudaMalloc(&F->d_rowstart, sizeof(int64_t) * rs.size()));
+        BDC_CUDA_TRY(cudaMemcpy(F->d_rowstart, rs.data(), sizeof(int64_t) * rs.size(), cudaMemcpyHostToDevice));
+        BDC_CUDA_TRY(cudaMalloc(&F->rpart, sizeof(double) * 2 * (size_t)F->H1h));
+        F->rows_smem = rows_smem_bytes(s.n2);
+        if (F->rows_smem > 48 * 1024) {
+            BDC_CUDA_TRY(cudaFuncSetAttribute(k_fac_load_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, F->rows_smem));
+            BDC_CUDA_TRY(cudaFuncSetAttribute(k_fac_rows<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, F->rows_smem));
+            BDC_CUDA_TRY(cudaFuncSetAttribute(k_fac_rows<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, F->rows_smem));
+            BDC_CUDA_TRY(cudaFuncSetAttribute(k_fac_rows<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, F->rows_smem));
+        }
     }
     const int k = H->k;
     int KL = 0, KR = 0;
@@ -1978,7 +2069,8 @@ bdc_status factored_init(bdc_handle* H) {
         BDC_CUDA_TRY(cudaStreamSynchronize(H->stream));
         cudaFree(d_cm);
     }
-    k_scatter<<<H->num_sms * 8, 256, 0, H->stream>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, H->d_h + F->i0, F->hx);
+    k_fac_rows<2><<<F->H1h, 256, F->rows_smem, H->stream>>>(F->d_rowstart, H->n, F->row0, H->d_h + F->i0, F->hx,
+                                                            nullptr);
     BDC_CUDA_TRY(cudaGetLastError());
 
     // ---- the two thin products: U^T (H2 x KL) = (AL^T Pw)^T, V (H1h x KR) = Pw BR
@@ -2570,6 +2662,8 @@ void factored_free(bdc_handle* H) {
         cudaFree(p);
     cudaFree(F->Bp);
     cudaFree(F->Ddense);
+    cudaFree(F->d_rowstart);
+    cudaFree(F->rpart);
     cudaFree(F->d_qf);
     cudaFree(F->d_ql);
     cudaFree(F->d_qm);
@@ -2766,10 +2860,15 @@ bdc_status factored_load_p(bdc_handle* H, int strict_zero) {
     const int64_t NX = (int64_t)F->H1h * F->H2;  // the dense rows held
     BDC_CUDA_TRY(cudaMemsetAsync(F->Pw, 0, sizeof(double) * NX, H->stream));
     const int nb = H->nb_upd;
-    k_fac_load<<<nb, 256, 0, H->stream>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, H->d_p[0] + F->i0, F->Pw, F->Lt,
-                                          F->epart, strict_zero, H->d_st);
-    if (H->shard_world > 1) k_lnp_all<<<nb, 256, 0, H->stream>>>(H->d_p[0], H->R, strict_zero, F->epart);
-    k_fac_load_finish<<<1, 32, 0, H->stream>>>(F->epart, nb, H->k, H->d_st);
+    k_fac_load_rows<<<F->H1h, 256, F->rows_smem, H->stream>>>(F->d_rowstart, H->n, F->row0, H->d_p[0] + F->i0, F->Pw,
+                                                              F->Lt, F->rpart, strict_zero);
+    if (H->shard_world > 1) {
+        // the first shift from every rank's p, not only the held rows
+        k_lnp_all<<<nb, 256, 0, H->stream>>>(H->d_p[0], H->R, strict_zero, F->epart);
+        k_fac_load_finish<<<1, 32, 0, H->stream>>>(F->epart, nb, H->k, H->d_st);
+    } else {
+        k_fac_load_finish<<<1, 32, 0, H->stream>>>(F->rpart, F->H1h, H->k, H->d_st);
+    }
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
 }
@@ -2855,16 +2954,12 @@ bdc_status factored_shard_finish(bdc_handle* H, const double* part5, double a) {
 
 bdc_status factored_store_p(bdc_handle* H, double* p_out) {
     FactoredState* F = H->fac;
-    k_fac_store<<<H->nb_upd, 256, 0, H->stream>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Pw, p_out + F->i0, H->d_st);
+    k_fac_rows<0><<<F->H1h, 256, F->rows_smem, H->stream>>>(F->d_rowstart, H->n, F->row0, F->Pw, p_out + F->i0,
+                                                            H->d_st);
     BDC_CUDA_TRY(cudaGetLastError());
     return BDC_OK;
 }
 
-__global__ void k_gather_dense(const uint32_t* __restrict__ reps, int64_t R, int n, int row0, const double* __restrict__ dense,
-                               double* __restrict__ out) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < R; i += (int64_t)gridDim.x * blockDim.x)
-        out[i] = dense[fac_loc(reps[i], n, row0)];
-}
 
 static bdc_status rescale(bdc_handle* H, double a);
 
@@ -2883,8 +2978,9 @@ static cudaError_t enqueue_map(bdc_handle* H, const double* p_in, double* p_out,
     // (Pw is zero away from the representatives from set-up on: every kernel
     // writes it only there, and the load below rewrites all of them)
     const int nb = H->nb_upd;
-    k_fac_load<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, p_in + F->i0, F->Pw, F->Lt, F->epart, 1, H->d_st);
-    k_fac_load_finish<<<1, 32, 0, s>>>(F->epart, nb, H->k, H->d_st);
+    k_fac_load_rows<<<F->H1h, 256, F->rows_smem, s>>>(F->d_rowstart, H->n, F->row0, p_in + F->i0, F->Pw, F->Lt,
+                                                      F->rpart, 1);
+    k_fac_load_finish<<<1, 32, 0, s>>>(F->rpart, F->H1h, H->k, H->d_st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     F->dout = D_out ? F->Ddense : nullptr;
@@ -2893,8 +2989,9 @@ static cudaError_t enqueue_map(bdc_handle* H, const double* p_in, double* p_out,
     if (e != cudaSuccess) return e;
     k_fac_rescale<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Lt, F->Pw, F->epart, H->d_st, 1);
     k_fac_rescale_finish<<<1, 32, 0, s>>>(F->epart, nb, -INFINITY, H->d_st, 1);
-    if (D_out) k_gather_dense<<<H->num_sms * 8, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Ddense, D_out + F->i0);
-    k_fac_store<<<nb, 256, 0, s>>>(H->d_reps + F->i0, F->Rl, H->n, F->row0, F->Pw, p_out + F->i0, H->d_st);
+    if (D_out)
+        k_fac_rows<1><<<F->H1h, 256, F->rows_smem, s>>>(F->d_rowstart, H->n, F->row0, F->Ddense, D_out + F->i0, H->d_st);
+    k_fac_rows<0><<<F->H1h, 256, F->rows_smem, s>>>(F->d_rowstart, H->n, F->row0, F->Pw, p_out + F->i0, H->d_st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return cudaMemcpyAsync(H->h_st, H->d_st, sizeof(DevState), cudaMemcpyDeviceToHost, s);
