@@ -207,8 +207,6 @@ __global__ void k_orbit_weights(int64_t R, const uint32_t* __restrict__ reps, in
 }
 
 // ---------------------------------------------------- the restricted BA map
-// acc_part[c][y] = sum_{s in chunk c} |O_s| p_s N(x_s, y)
-constexpr int kRsChunk = 64;
 
 // Device state of the restricted problem's accelerated loop (rs_accelerated):
 // the Anderson Gram matrix by physical history slot, the mixing weights, the
@@ -239,121 +237,123 @@ __device__ __forceinline__ bool rs_skip(const RsAAState* st, int gate) {
     return gate >= 3 && !st->solve_ok;
 }
 
-__global__ void __launch_bounds__(256) k_rs_acc(int S, int ny, const float* __restrict__ rows,
-                                                const uint8_t* __restrict__ w, const double* __restrict__ p,
-                                                double* __restrict__ part, const RsAAState* st, int gate) {
+// acc(y) = sum_s |O_s| p_s N(x_s, y) for a slab of 32 outputs per block: lane
+// = output, warp w = members w, w + 32, ... (eight loads in flight, the
+// multiply-adds in member order), the 32 warps' sums added in warp order.
+// The last block to finish then forms ln q(y) with q(y) = (1/(4C)) sum over
+// the group {id, rev, comp, rev comp} of acc(g y) (ln 0 = 0) and re-arms the
+// ticket.
+constexpr int kRsQThreads = 1024;
+__global__ void __launch_bounds__(kRsQThreads) k_rs_q(int S, int k, const float* __restrict__ rows,
+                                                      const uint8_t* __restrict__ w, const double* __restrict__ p,
+                                                      double inv_c, double* __restrict__ acc,
+                                                      double* __restrict__ lnq, unsigned* __restrict__ ticket,
+                                                      const RsAAState* st, int gate) {
     if (rs_skip(st, gate)) return;
-    const int y = blockIdx.x * blockDim.x + threadIdx.x;
-    const int c = blockIdx.y;
-    if (y >= ny) return;
-    const int s0 = c * kRsChunk, s1 = min(S, s0 + kRsChunk);
-    // eight members' loads in flight, then their multiply-adds in member
-    // order (the same sum, bit for bit, as one member at a time)
-    double a = 0.0;
-    int s = s0;
-    for (; s + 8 <= s1; s += 8) {
-        float r[8];
-        double wp[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            r[u] = rows[(int64_t)(s + u) * ny + y];
-            wp[u] = (double)w[s + u] * p[s + u];
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) a = fma(wp[u], (double)r[u], a);
-    }
-    for (; s < s1; ++s) a = fma((double)w[s] * p[s], (double)rows[(int64_t)s * ny + y], a);
-    part[(int64_t)c * ny + y] = a;
-}
-
-// acc(y) = sum of the chunk partials; ln q(y) with q(y) = (1/(4C)) sum over
-// the group {id, rev, comp, rev comp} of acc(g y) (each thread adds the
-// partials of its y's four images itself); ln 0 = 0
-__global__ void k_rs_sum_lnq(int k, int nc, const double* __restrict__ part, double inv_c, double* __restrict__ acc,
-                             double* __restrict__ lnq, const RsAAState* st, int gate) {
-    if (rs_skip(st, gate)) return;
+    __shared__ double sh[kRsQThreads / 32][33];
+    __shared__ bool last;
     const int ny = 1 << k;
-    const int y = blockIdx.x * blockDim.x + threadIdx.x;
-    if (y >= ny) return;
-    const uint32_t r = reverse_bits((uint32_t)y, k), c = complement_bits((uint32_t)y, k), rc = reverse_bits(c, k);
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    int ch = 0;
-    for (; ch + 4 <= nc; ch += 4) {  // four chunks' loads in flight, added in chunk order
-        double v[4][4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const double* pc = part + (int64_t)(ch + u) * ny;
-            v[u][0] = pc[y];
-            v[u][1] = pc[r];
-            v[u][2] = pc[c];
-            v[u][3] = pc[rc];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            a0 += v[u][0];
-            a1 += v[u][1];
-            a2 += v[u][2];
-            a3 += v[u][3];
-        }
-    }
-    for (; ch < nc; ++ch) {
-        const double* pc = part + (int64_t)ch * ny;
-        a0 += pc[y];
-        a1 += pc[r];
-        a2 += pc[c];
-        a3 += pc[rc];
-    }
-    acc[y] = a0;
-    const double q = 0.25 * inv_c * (a0 + a1 + a2 + a3);
-    lnq[y] = q > 0.0 ? log(q) : 0.0;
-}
-
-// D_s = h_s - (1/C) sum_y N(x_s, y) ln q(y): one warp per member; block
-// partials [max D, sum |O| p D]
-__global__ void __launch_bounds__(256) k_rs_div(int S, int ny, const float* __restrict__ rows,
-                                                const double* __restrict__ lnq, const double* __restrict__ h,
-                                                const uint8_t* __restrict__ w, const double* __restrict__ p,
-                                                double inv_c, double* __restrict__ D, double* __restrict__ part,
-                                                const RsAAState* st, int gate) {
-    if (rs_skip(st, gate)) return;
-    __shared__ double smax[8], ssum[8];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int s = blockIdx.x * 8 + warp;
-    double d = -DBL_MAX, r = 0.0;
-    if (s < S) {
-        const float* row = rows + (int64_t)s * ny;
-        double a = 0.0;
-        int y = lane;
-        for (; y + 7 * 32 < ny; y += 8 * 32) {  // eight loads in flight, summed in order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int y = blockIdx.x * 32 + lane;
+    double a = 0.0;
+    if (y < ny) {
+        for (int s = warp; s < S; s += 8 * 32) {
             float r[8];
-            double l[8];
+            double wp[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                r[u] = row[y + 32 * u];
-                l[u] = lnq[y + 32 * u];
+                const int t = s + 32 * u;
+                r[u] = t < S ? rows[(int64_t)t * ny + y] : 0.0f;
+                wp[u] = t < S ? (double)w[t] * p[t] : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < 8; ++u) a = fma((double)r[u], l[u], a);
+            for (int u = 0; u < 8; ++u) a = fma(wp[u], (double)r[u], a);
         }
-        for (; y < ny; y += 32) a = fma((double)row[y], lnq[y], a);
-        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
-        d = h[s] - a * inv_c;
-        r = (double)w[s] * p[s] * d;
-        if (lane == 0) D[s] = d;
     }
-    if (lane == 0) {
-        smax[warp] = d;
-        ssum[warp] = r;
+    sh[warp][lane] = a;
+    __syncthreads();
+    if (warp == 0) {
+        double t = 0.0;
+#pragma unroll 8
+        for (int i = 0; i < kRsQThreads / 32; ++i) t += sh[i][lane];
+        if (y < ny) acc[y] = t;
+        __threadfence();
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double m = smax[0], t = ssum[0];
-        for (int i = 1; i < 8; ++i) {
-            m = fmax(m, smax[i]);
-            t += ssum[i];
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int yy = threadIdx.x; yy < ny; yy += blockDim.x) {
+        const uint32_t r = reverse_bits((uint32_t)yy, k), c = complement_bits((uint32_t)yy, k),
+                       rc = reverse_bits(c, k);
+        const double q = 0.25 * inv_c * (__ldcg(acc + yy) + __ldcg(acc + r) + __ldcg(acc + c) + __ldcg(acc + rc));
+        lnq[yy] = q > 0.0 ? log(q) : 0.0;
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// D_s = h_s - (1/C) sum_y N(x_s, y) ln q(y): one block per member, each thread
+// V consecutive outputs per vector load and up to eight vectors in flight,
+// summed in order; the block's threads added as a warp tree, then the warps
+// in order
+template <int V>
+__global__ void __launch_bounds__(256) k_rs_div(int ny, const float* __restrict__ rows,
+                                                const double* __restrict__ lnq, const double* __restrict__ h,
+                                                double inv_c, double* __restrict__ D, const RsAAState* st,
+                                                int gate) {
+    if (rs_skip(st, gate)) return;
+    __shared__ double sh[8];
+    const int s = blockIdx.x;
+    const float* __restrict__ row = rows + (int64_t)s * ny;
+    const int step = blockDim.x * V;
+    double a = 0.0;
+    for (int y0 = threadIdx.x * V; y0 < ny; y0 += 8 * step) {
+        float r[8][V];
+        double l[8][V];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int yy = y0 + u * step;
+            if (yy < ny) {
+                if constexpr (V == 4) {
+                    const float4 f = *reinterpret_cast<const float4*>(row + yy);
+                    const double2 l0 = *reinterpret_cast<const double2*>(lnq + yy);
+                    const double2 l1 = *reinterpret_cast<const double2*>(lnq + yy + 2);
+                    r[u][0] = f.x;
+                    r[u][1] = f.y;
+                    r[u][2] = f.z;
+                    r[u][3] = f.w;
+                    l[u][0] = l0.x;
+                    l[u][1] = l0.y;
+                    l[u][2] = l1.x;
+                    l[u][3] = l1.y;
+                } else {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        r[u][v] = row[yy + v];
+                        l[u][v] = lnq[yy + v];
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    r[u][v] = 0.0f;
+                    l[u][v] = 0.0;
+                }
+            }
         }
-        part[2 * blockIdx.x] = m;
-        part[2 * blockIdx.x + 1] = t;
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int v = 0; v < V; ++v) a = fma((double)r[u][v], l[u][v], a);
+    }
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = sh[0];
+        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) t += sh[i];
+        D[s] = h[s] - t * inv_c;
     }
 }
 
@@ -361,32 +361,35 @@ __global__ void __launch_bounds__(256) k_rs_div(int S, int ny, const float* __re
 // out[1] = rate of p (nats).  rec 1 / 2 records them in st as the step's
 // plain / mixed evaluation, adds them to the bracket and sets the stop flag
 // when the bracket is below the target.
-__global__ void __launch_bounds__(1024) k_rs_update(int S, const double* __restrict__ part, int nb,
-                                                    const double* __restrict__ D, const uint8_t* __restrict__ w,
-                                                    const double* __restrict__ p, double* __restrict__ pn,
-                                                    double* __restrict__ out, RsAAState* st, int gate, int rec) {
+__global__ void __launch_bounds__(1024) k_rs_update(int S, const double* __restrict__ D,
+                                                    const uint8_t* __restrict__ w, const double* __restrict__ p,
+                                                    double* __restrict__ pn, double* __restrict__ out,
+                                                    RsAAState* st, int gate, int rec) {
     if (rs_skip(st, gate)) return;
-    __shared__ double sh[32];
+    __shared__ double sh[32], shm[32];
     __shared__ double mD, Zs;
-    if (threadIdx.x == 0) {
+    {  // max D and sum |O| p D: each thread's members in order, a warp tree, the warps in order
         double m = -DBL_MAX, r = 0.0;
-        int b = 0;
-        for (; b + 8 <= nb; b += 8) {  // eight partials' loads in flight, combined in order
-            double pm[8], pr[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                pm[u] = part[2 * (b + u)];
-                pr[u] = part[2 * (b + u) + 1];
-            }
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                m = fmax(m, pm[u]);
-                r += pr[u];
-            }
+        for (int s = threadIdx.x; s < S; s += blockDim.x) {
+            const double d = D[s];
+            m = fmax(m, d);
+            r += (double)w[s] * p[s] * d;
         }
-        for (; b < nb; ++b) {
-            m = fmax(m, part[2 * b]);
-            r += part[2 * b + 1];
+        for (int o = 16; o > 0; o >>= 1) {
+            m = fmax(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+            r += __shfl_xor_sync(0xFFFFFFFFu, r, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            shm[threadIdx.x >> 5] = m;
+            sh[threadIdx.x >> 5] = r;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = shm[0], r = sh[0];
+        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
+            m = fmax(m, shm[i]);
+            r += sh[i];
         }
         mD = m;
         out[0] = m;
@@ -806,24 +809,22 @@ struct Bracket {
 
 // The restricted problem on S: rows, weights, h, and its BA map
 struct Restricted {
-    int S = 0, ny = 0, nc = 0, nbd = 0;
-    DevBuf idx, rows, w, h, part, acc, lnq, D, dpart, out;
+    int S = 0, ny = 0;
+    DevBuf idx, rows, w, h, acc, lnq, D, out, ticket;
 
     bdc_status build(bdc_handle* H, const std::vector<uint32_t>& members) {
         S = (int)members.size();
         ny = 1 << H->k;
-        nc = (S + kRsChunk - 1) / kRsChunk;
-        nbd = (S + 7) / 8;
         BDC_CUDA_TRY(dalloc(idx, sizeof(uint32_t) * S));
         BDC_CUDA_TRY(dalloc(rows, sizeof(float) * (size_t)S * ny));
         BDC_CUDA_TRY(dalloc(w, S));
         BDC_CUDA_TRY(dalloc(h, sizeof(double) * S));
-        BDC_CUDA_TRY(dalloc(part, sizeof(double) * (size_t)nc * ny));
         BDC_CUDA_TRY(dalloc(acc, sizeof(double) * ny));
         BDC_CUDA_TRY(dalloc(lnq, sizeof(double) * ny));
         BDC_CUDA_TRY(dalloc(D, sizeof(double) * S));
-        BDC_CUDA_TRY(dalloc(dpart, sizeof(double) * 2 * nbd));
         BDC_CUDA_TRY(dalloc(out, sizeof(double) * 2));
+        BDC_CUDA_TRY(dalloc(ticket, sizeof(unsigned)));
+        BDC_CUDA_TRY(cudaMemsetAsync(ticket.p, 0, sizeof(unsigned), H->stream));
         BDC_CUDA_TRY(cudaMemcpyAsync(idx.p, members.data(), sizeof(uint32_t) * S, cudaMemcpyHostToDevice, H->stream));
         const int g = std::max(1, std::min(H->num_sms * 8, (int)(((int64_t)S * ny + 255) / 256)));
         k_rows<<<g, 256, 0, H->stream>>>(H->s, H->A, H->B, H->d_reps, idx.get<uint32_t>(), S, rows.get<float>());
@@ -832,18 +833,21 @@ struct Restricted {
         BDC_CUDA_TRY(cudaGetLastError());
         return BDC_OK;
     }
-    // queues p -> pn (four kernels, gated by st / gate, recorded by rec; see
+    // queues p -> pn (three kernels, gated by st / gate, recorded by rec; see
     // k_rs_update)
     cudaError_t enqueue_map(bdc_handle* H, const double* p, double* pn, RsAAState* st, int gate, int rec) {
         cudaStream_t s = H->stream;
-        k_rs_acc<<<dim3((ny + 255) / 256, nc), 256, 0, s>>>(S, ny, rows.get<float>(), w.get<uint8_t>(), p,
-                                                            part.get<double>(), st, gate);
-        k_rs_sum_lnq<<<(ny + 255) / 256, 256, 0, s>>>(H->k, nc, part.get<double>(), H->inv_c, acc.get<double>(),
-                                                      lnq.get<double>(), st, gate);
-        k_rs_div<<<nbd, 256, 0, s>>>(S, ny, rows.get<float>(), lnq.get<double>(), h.get<double>(), w.get<uint8_t>(),
-                                     p, H->inv_c, D.get<double>(), dpart.get<double>(), st, gate);
-        k_rs_update<<<1, 1024, 0, s>>>(S, dpart.get<double>(), nbd, D.get<double>(), w.get<uint8_t>(), p, pn,
-                                       out.get<double>(), st, gate, rec);
+        k_rs_q<<<(ny + 31) / 32, kRsQThreads, 0, s>>>(S, H->k, rows.get<float>(), w.get<uint8_t>(), p, H->inv_c,
+                                                      acc.get<double>(), lnq.get<double>(), ticket.get<unsigned>(),
+                                                      st, gate);
+        if (ny >= 128)
+            k_rs_div<4><<<S, std::max(32, std::min(256, ny / 32)), 0, s>>>(ny, rows.get<float>(), lnq.get<double>(),
+                                                               h.get<double>(), H->inv_c, D.get<double>(), st, gate);
+        else
+            k_rs_div<1><<<S, 32, 0, s>>>(ny, rows.get<float>(), lnq.get<double>(), h.get<double>(), H->inv_c,
+                                         D.get<double>(), st, gate);
+        k_rs_update<<<1, 1024, 0, s>>>(S, D.get<double>(), w.get<uint8_t>(), p, pn, out.get<double>(), st, gate,
+                                       rec);
         return cudaGetLastError();
     }
     // p -> pn; ub / rate (nats) of p
@@ -864,7 +868,8 @@ struct Restricted {
 // the restricted problem, with every decision taken on the device from
 // RsAAState: one step is the plain map, the push of the new differences with
 // their Gram products, the least-squares weights, the mixed point, its map and
-// the choice of the next iterate -- fourteen kernels, captured kRsGraphSteps
+// the choice of the next iterate -- nine kernels (two maps of three, three
+// single-block steps between and after them), captured kRsGraphSteps
 // steps to a CUDA graph; the host reads the state once per graph.
 constexpr int kRsGraphSteps = 16;
 
@@ -873,23 +878,35 @@ struct RsSlots {
     double* dG[kAAMax];
 };
 
-// f = g - x.  After a previous pair: the differences dF = f - f_last and
-// dG = g - g_last go to physical slot sl = npush % m, with block partials of
-// w dF_a . dF_sl and w dF_a . f over the slots in use after the push; then
-// f_last = f, g_last = g.
-__global__ void __launch_bounds__(256) k_rs_push_dots(int L, int m, const uint8_t* __restrict__ wts,
-                                                      const double* __restrict__ x, const double* __restrict__ g,
-                                                      double* __restrict__ f_last, double* __restrict__ g_last,
-                                                      RsSlots P, double* __restrict__ part, const RsAAState* st) {
+// the rate guard: the mixed point is kept when it has weights, a finite
+// bound and a rate at least the plain step's
+__device__ __forceinline__ bool rs_mixed_kept(const RsAAState* st) {
+    return st->solve_ok && isfinite(st->ua) && st->ra >= st->r;
+}
+
+// ---- the step's small kernels merged, one block each (L = |S| is small):
+// push + dot products + the Anderson solve, mix + normalise, accept + state.
+constexpr int kRsBlock = 1024;
+
+// f = g - x; with a last pair, dF = f - f_last and dG = g - g_last go to the
+// ring slot sl = npush % m, with the dot products w dF_a . dF_sl and
+// w dF_a . f over the slots in use; then f_last = f, g_last = g.  Thread 0
+// then writes the new Gram row and right side and solves (A + lambda I)
+// gamma = b by Cholesky with the ridge lambda = 1e-12 tr(A) / c over the c
+// slots in use; solve_ok = 0 when the system is degenerate or this was the
+// first pair after a clear.
+__global__ void __launch_bounds__(kRsBlock) k_rs_push_solve(int L, int m, const uint8_t* __restrict__ wts,
+                                                           const double* __restrict__ x, const double* __restrict__ g,
+                                                           double* __restrict__ f_last, double* __restrict__ g_last,
+                                                           RsSlots P, RsAAState* st) {
     if (rs_skip(st, 2)) return;
-    __shared__ double sh[8];
     const bool diff = st->have_last != 0;
     const int sl = st->npush % m;
     const int act = min(st->npush + 1, m);
     double a1[kAAMax], a2[kAAMax];
 #pragma unroll
     for (int a = 0; a < kAAMax; ++a) a1[a] = a2[a] = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) {
+    for (int i = threadIdx.x; i < L; i += kRsBlock) {
         const double gi = g[i], fi = gi - x[i];
         if (diff) {
             const double dn = fi - f_last[i];
@@ -907,54 +924,70 @@ __global__ void __launch_bounds__(256) k_rs_push_dots(int L, int m, const uint8_
         f_last[i] = fi;
         g_last[i] = gi;
     }
-    if (!diff) return;  // uniform
-    for (int a = 0; a < act; ++a) {
-        const double r1 = block_reduce_sum(a1[a], sh);
-        const double r2 = block_reduce_sum(a2[a], sh);
-        if (threadIdx.x == 0) {
-            part[(size_t)blockIdx.x * 2 * kAAMax + a] = r1;
-            part[(size_t)blockIdx.x * 2 * kAAMax + kAAMax + a] = r2;
+    // the dot products: a warp tree per warp, then thread a (a < act) adds
+    // the warps' w dF_a . dF_sl in warp order and thread kAAMax + a the
+    // w dF_a . f; the Gram matrix comes to shared memory at the same time
+    __shared__ double wp[kRsBlock / 32][2 * kAAMax];
+    __shared__ double sA[kAAMax][kAAMax], sb[kAAMax];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (diff) {
+#pragma unroll
+        for (int a = 0; a < kAAMax; ++a)
+            if (a < act) {
+                double v1 = a1[a], v2 = a2[a];
+                for (int o = 16; o > 0; o >>= 1) {
+                    v1 += __shfl_xor_sync(0xFFFFFFFFu, v1, o);
+                    v2 += __shfl_xor_sync(0xFFFFFFFFu, v2, o);
+                }
+                if (lane == 0) {
+                    wp[warp][a] = v1;
+                    wp[warp][kAAMax + a] = v2;
+                }
+            }
+    }
+    if (threadIdx.x < kAAMax * kAAMax) {
+        const int i = threadIdx.x / kAAMax, j = threadIdx.x % kAAMax;
+        sA[i][j] = st->A[i][j];
+    } else if (threadIdx.x < kAAMax * kAAMax + kAAMax) {
+        sb[threadIdx.x - kAAMax * kAAMax] = st->b[threadIdx.x - kAAMax * kAAMax];
+    }
+    __syncthreads();  // every thread has read st
+    if (diff && threadIdx.x < 2 * kAAMax && threadIdx.x % kAAMax < act) {
+        const int a = threadIdx.x % kAAMax;
+        double t = 0.0;
+        for (int i = 0; i < kRsBlock / 32; ++i) t += wp[i][threadIdx.x];
+        if (threadIdx.x < kAAMax) {
+            sA[sl][a] = t;
+            sA[a][sl] = t;
+            st->A[sl][a] = t;
+            st->A[a][sl] = t;
+        } else {
+            sb[a] = t;
+            st->b[a] = t;
         }
     }
-}
-
-// one thread: the new Gram row and right side from the partials, then the
-// weights gamma of (A + lambda I) gamma = b by Cholesky with the ridge
-// lambda = 1e-12 tr(A) / c over the c slots in use; solve_ok = 0 when the
-// system is degenerate or this was the first pair after a clear
-__global__ void k_rs_aa_solve(int m, int nb, const double* __restrict__ part, RsAAState* st) {
-    if (rs_skip(st, 2) || threadIdx.x != 0) return;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
     st->solve_ok = 0;
     if (!st->have_last) {
         st->have_last = 1;
         return;
     }
-    const int sl = st->npush % m;
-    const int c = min(st->npush + 1, m);
-    for (int a = 0; a < c; ++a) {
-        double r1 = 0.0, r2 = 0.0;
-        for (int bb = 0; bb < nb; ++bb) {
-            r1 += part[(size_t)bb * 2 * kAAMax + a];
-            r2 += part[(size_t)bb * 2 * kAAMax + kAAMax + a];
-        }
-        st->A[sl][a] = r1;
-        st->A[a][sl] = r1;
-        st->b[a] = r2;
-    }
+    const int c = act;
     st->npush += 1;
     // the system in ring order, oldest difference first: position j holds
     // physical slot (npush - c + j) % m.  Products and differences are
     // rounded separately (no FMA contraction), as in the host-side solve of
-    // the full-space loop, so both loops take the same steps on equal data.
+    // the full-space loop.
     int ph[kAAMax];
     for (int j = 0; j < c; ++j) ph[j] = (st->npush - c + j) % m;
     double M[kAAMax][kAAMax], y[kAAMax], gam[kAAMax];
     double tr = 0.0;
-    for (int a = 0; a < c; ++a) tr += st->A[ph[a]][ph[a]];
+    for (int a = 0; a < c; ++a) tr += sA[ph[a]][ph[a]];
     if (!(tr > 0.0) || !isfinite(tr)) return;
     const double lam = 1e-12 * tr / c;
     for (int a = 0; a < c; ++a)
-        for (int d = 0; d < c; ++d) M[a][d] = st->A[ph[a]][ph[d]] + (a == d ? lam : 0.0);
+        for (int d = 0; d < c; ++d) M[a][d] = sA[ph[a]][ph[d]] + (a == d ? lam : 0.0);
     for (int j = 0; j < c; ++j) {
         double dsum = M[j][j];
         for (int t = 0; t < j; ++t) dsum = __dsub_rn(dsum, __dmul_rn(M[j][t], M[j][t]));
@@ -967,7 +1000,7 @@ __global__ void k_rs_aa_solve(int m, int nb, const double* __restrict__ part, Rs
         }
     }
     for (int i = 0; i < c; ++i) {
-        double v = st->b[ph[i]];
+        double v = sb[ph[i]];
         for (int t = 0; t < i; ++t) v = __dsub_rn(v, __dmul_rn(M[i][t], y[t]));
         y[i] = v / M[i][i];
     }
@@ -982,14 +1015,14 @@ __global__ void k_rs_aa_solve(int m, int nb, const double* __restrict__ part, Rs
     st->solve_ok = 1;
 }
 
-// xa = g_last - sum_a gamma_a dG_a, clipped at 0; block partials of w xa
-__global__ void __launch_bounds__(256) k_rs_mix(int L, int m, const uint8_t* __restrict__ wts, RsSlots P,
-                                                const double* __restrict__ g_last, double* __restrict__ xa,
-                                                double* __restrict__ part, const RsAAState* st) {
+// xa = g_last - sum_a gamma_a dG_a, clipped at 0, normalised to sum w xa = 1
+__global__ void __launch_bounds__(kRsBlock) k_rs_mix_scale(int L, int m, const uint8_t* __restrict__ wts, RsSlots P,
+                                                          const double* __restrict__ g_last, double* __restrict__ xa,
+                                                          const RsAAState* st) {
     if (rs_skip(st, 3)) return;
-    __shared__ double sh[8];
+    __shared__ double sh[kRsBlock / 32];
+    __shared__ double inv;
     const int c = min(st->npush, m);
-    // ring order, oldest first (the order of gamma)
     double gam[kAAMax];
     const double* dg[kAAMax];
 #pragma unroll
@@ -998,7 +1031,7 @@ __global__ void __launch_bounds__(256) k_rs_mix(int L, int m, const uint8_t* __r
         dg[a] = P.dG[(a < c) ? (st->npush - c + a) % m : 0];
     }
     double sum = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) {
+    for (int i = threadIdx.x; i < L; i += kRsBlock) {
         double v = g_last[i];
 #pragma unroll
         for (int a = 0; a < kAAMax; ++a)
@@ -1007,41 +1040,23 @@ __global__ void __launch_bounds__(256) k_rs_mix(int L, int m, const uint8_t* __r
         xa[i] = v;
         sum = fma((double)wts[i], v, sum);
     }
-    const double r = block_reduce_sum(sum, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = r;
-}
-
-__global__ void k_rs_scale(int L, double* __restrict__ xa, const double* __restrict__ part, int nb,
-                           const RsAAState* st) {
-    if (rs_skip(st, 3)) return;
-    __shared__ double inv;
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int bb = 0; bb < nb; ++bb) t += part[bb];
-        inv = t > 0.0 ? 1.0 / t : 0.0;
-    }
+    const double t = block_reduce_sum(sum, sh);
+    if (threadIdx.x == 0) inv = t > 0.0 ? 1.0 / t : 0.0;
     __syncthreads();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) xa[i] *= inv;
+    for (int i = threadIdx.x; i < L; i += kRsBlock) xa[i] *= inv;
 }
 
-// the rate guard: the mixed point is kept when it has weights, a finite
-// bound and a rate at least the plain step's
-__device__ __forceinline__ bool rs_mixed_kept(const RsAAState* st) {
-    return st->solve_ok && isfinite(st->ua) && st->ra >= st->r;
-}
-
-// next iterate: the mixed map's image when kept, else the plain image
-__global__ void k_rs_accept_copy(int L, double* __restrict__ x, const double* __restrict__ g,
-                                 const double* __restrict__ ga, const RsAAState* st) {
+// the next iterate (the mixed image when kept, else the plain one); then a
+// rejected mixed point clears the history (when it holds a difference) and a
+// stop flag ends the loop
+__global__ void __launch_bounds__(kRsBlock) k_rs_accept(int L, int m, double* __restrict__ x,
+                                                       const double* __restrict__ g, const double* __restrict__ ga,
+                                                       RsAAState* st) {
     if (rs_skip(st, 1)) return;
     const double* __restrict__ src = (!st->stop_plain && rs_mixed_kept(st)) ? ga : g;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L; i += gridDim.x * blockDim.x) x[i] = src[i];
-}
-
-// a rejected mixed point clears the history (when it holds a difference);
-// a stop flag ends the loop
-__global__ void k_rs_accept_state(int m, RsAAState* st) {
-    if (rs_skip(st, 1) || threadIdx.x != 0) return;
+    for (int i = threadIdx.x; i < L; i += kRsBlock) x[i] = src[i];
+    __syncthreads();  // every thread has read st
+    if (threadIdx.x != 0) return;
     if (st->stop_plain) {
         st->fin = 1;
         return;
@@ -1055,8 +1070,8 @@ __global__ void k_rs_accept_state(int m, RsAAState* st) {
 }
 
 struct RsAA {
-    int L = 0, m = 0, nb = 0;
-    DevBuf f_last, g_last, part, mpart, st;
+    int L = 0, m = 0;
+    DevBuf f_last, g_last, st;
     DevBuf dF[kAAMax], dG[kAAMax];
     RsAAState* host[2] = {nullptr, nullptr};  // pinned copies of the state, one per graph in flight
     cudaEvent_t copied[2] = {nullptr, nullptr};
@@ -1067,10 +1082,9 @@ struct RsAA {
             if (copied[i]) cudaEventDestroy(copied[i]);
         }
     }
-    cudaError_t init(int len, int mem, int sms) {
+    cudaError_t init(int len, int mem) {
         L = len;
         m = mem;
-        nb = std::max(1, std::min(sms * 4, (L + 255) / 256));
         cudaError_t e = cudaSuccess;
         for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
             e = cudaMallocHost(&host[i], sizeof(RsAAState));
@@ -1078,8 +1092,6 @@ struct RsAA {
         }
         if (e == cudaSuccess) e = dalloc(f_last, sizeof(double) * L);
         if (e == cudaSuccess) e = dalloc(g_last, sizeof(double) * L);
-        if (e == cudaSuccess) e = dalloc(part, sizeof(double) * nb * 2 * kAAMax);
-        if (e == cudaSuccess) e = dalloc(mpart, sizeof(double) * nb);
         if (e == cudaSuccess) e = dalloc(st, sizeof(RsAAState));
         for (int i = 0; i < m && e == cudaSuccess; ++i) {
             e = dalloc(dF[i], sizeof(double) * L);
@@ -1104,18 +1116,14 @@ static cudaError_t rs_enqueue_step(bdc_handle* H, Restricted& rs, RsAA& aa, doub
     const uint8_t* w = rs.w.get<uint8_t>();
     cudaError_t e = rs.enqueue_map(H, x, g, st, 1, 1);
     if (e != cudaSuccess) return e;
-    k_rs_push_dots<<<aa.nb, 256, 0, s>>>(aa.L, aa.m, w, x, g, aa.f_last.get<double>(), aa.g_last.get<double>(),
-                                         aa.slots(), aa.part.get<double>(), st);
-    k_rs_aa_solve<<<1, 32, 0, s>>>(aa.m, aa.nb, aa.part.get<double>(), st);
-    k_rs_mix<<<aa.nb, 256, 0, s>>>(aa.L, aa.m, w, aa.slots(), aa.g_last.get<double>(), xa, aa.mpart.get<double>(),
-                                   st);
-    k_rs_scale<<<aa.nb, 256, 0, s>>>(aa.L, xa, aa.mpart.get<double>(), aa.nb, st);
+    k_rs_push_solve<<<1, kRsBlock, 0, s>>>(aa.L, aa.m, w, x, g, aa.f_last.get<double>(), aa.g_last.get<double>(),
+                                           aa.slots(), st);
+    k_rs_mix_scale<<<1, kRsBlock, 0, s>>>(aa.L, aa.m, w, aa.slots(), aa.g_last.get<double>(), xa, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     e = rs.enqueue_map(H, xa, ga, st, 3, 2);
     if (e != cudaSuccess) return e;
-    k_rs_accept_copy<<<aa.nb, 256, 0, s>>>(aa.L, x, g, ga, st);
-    k_rs_accept_state<<<1, 32, 0, s>>>(aa.m, st);
+    k_rs_accept<<<1, kRsBlock, 0, s>>>(aa.L, aa.m, x, g, ga, st);
     return cudaGetLastError();
 }
 
@@ -1558,7 +1566,7 @@ bdc_status solve_impl(bdc_handle_t H, double gap_bits, int64_t max_evals, bdc_st
             BDC_CUDA_TRY(cudaMemcpyAsync(ps.p, hx.data(), sizeof(double) * Sn, cudaMemcpyHostToDevice, s));
         }
         RsAA aa;
-        BDC_CUDA_TRY(aa.init(Sn, kAAMax, sms));
+        BDC_CUDA_TRY(aa.init(Sn, kAAMax));
         DevBuf pbak;
         BDC_CUDA_TRY(dalloc(pbak, sizeof(double) * Sn));
         Bracket rb;
