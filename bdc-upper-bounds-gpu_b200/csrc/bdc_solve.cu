@@ -238,12 +238,13 @@ __device__ __forceinline__ bool rs_skip(const RsAAState* st, int gate) {
 }
 
 // acc(y) = sum_s |O_s| p_s N(x_s, y) for a slab of 32 outputs per block: lane
-// = output, warp w = members w, w + 32, ... (eight loads in flight, the
+// = output, warp w = members w, w + 32, ... (kRsQLoads loads in flight, the
 // multiply-adds in member order), the 32 warps' sums added in warp order.
 // The last block to finish then forms ln q(y) with q(y) = (1/(4C)) sum over
 // the group {id, rev, comp, rev comp} of acc(g y) (ln 0 = 0) and re-arms the
 // ticket.
 constexpr int kRsQThreads = 1024;
+constexpr int kRsQLoads = 12;
 __global__ void __launch_bounds__(kRsQThreads) k_rs_q(int S, int k, const float* __restrict__ rows,
                                                       const uint8_t* __restrict__ w, const double* __restrict__ p,
                                                       double inv_c, double* __restrict__ acc,
@@ -257,17 +258,17 @@ __global__ void __launch_bounds__(kRsQThreads) k_rs_q(int S, int k, const float*
     const int y = blockIdx.x * 32 + lane;
     double a = 0.0;
     if (y < ny) {
-        for (int s = warp; s < S; s += 8 * 32) {
-            float r[8];
-            double wp[8];
+        for (int s = warp; s < S; s += kRsQLoads * 32) {
+            float r[kRsQLoads];
+            double wp[kRsQLoads];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
+            for (int u = 0; u < kRsQLoads; ++u) {
                 const int t = s + 32 * u;
                 r[u] = t < S ? rows[(int64_t)t * ny + y] : 0.0f;
                 wp[u] = t < S ? (double)w[t] * p[t] : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < 8; ++u) a = fma(wp[u], (double)r[u], a);
+            for (int u = 0; u < kRsQLoads; ++u) a = fma(wp[u], (double)r[u], a);
         }
     }
     sh[warp][lane] = a;
@@ -361,10 +362,9 @@ __global__ void __launch_bounds__(256) k_rs_div(int ny, const float* __restrict_
 // out[1] = rate of p (nats).  rec 1 / 2 records them in st as the step's
 // plain / mixed evaluation, adds them to the bracket and sets the stop flag
 // when the bracket is below the target.
-__global__ void __launch_bounds__(1024) k_rs_update(int S, const double* __restrict__ D,
-                                                    const uint8_t* __restrict__ w, const double* __restrict__ p,
-                                                    double* __restrict__ pn, double* __restrict__ out,
-                                                    RsAAState* st, int gate, int rec) {
+__device__ __forceinline__ void rs_update_body(int S, const double* __restrict__ D, const uint8_t* __restrict__ w,
+                                               const double* __restrict__ p, double* __restrict__ pn,
+                                               double* __restrict__ out, RsAAState* st, int gate, int rec) {
     if (rs_skip(st, gate)) return;
     __shared__ double sh[32], shm[32];
     __shared__ double mD, Zs;
@@ -429,6 +429,13 @@ __global__ void __launch_bounds__(1024) k_rs_update(int S, const double* __restr
     __syncthreads();
     const double inv = 1.0 / Zs;
     for (int s = threadIdx.x; s < S; s += blockDim.x) pn[s] *= inv;
+}
+
+__global__ void __launch_bounds__(1024) k_rs_update(int S, const double* __restrict__ D,
+                                                    const uint8_t* __restrict__ w, const double* __restrict__ p,
+                                                    double* __restrict__ pn, double* __restrict__ out,
+                                                    RsAAState* st, int gate, int rec) {
+    rs_update_body(S, D, w, p, pn, out, st, gate, rec);
 }
 
 // ------------------------------------------------- Newton on the support
@@ -835,7 +842,8 @@ struct Restricted {
     }
     // queues p -> pn (three kernels, gated by st / gate, recorded by rec; see
     // k_rs_update)
-    cudaError_t enqueue_map(bdc_handle* H, const double* p, double* pn, RsAAState* st, int gate, int rec) {
+    // queues acc, ln q and D of p (two kernels, gated by st / gate)
+    cudaError_t enqueue_qd(bdc_handle* H, const double* p, RsAAState* st, int gate) {
         cudaStream_t s = H->stream;
         k_rs_q<<<(ny + 31) / 32, kRsQThreads, 0, s>>>(S, H->k, rows.get<float>(), w.get<uint8_t>(), p, H->inv_c,
                                                       acc.get<double>(), lnq.get<double>(), ticket.get<unsigned>(),
@@ -846,6 +854,12 @@ struct Restricted {
         else
             k_rs_div<1><<<S, 32, 0, s>>>(ny, rows.get<float>(), lnq.get<double>(), h.get<double>(), H->inv_c,
                                          D.get<double>(), st, gate);
+        return cudaGetLastError();
+    }
+    cudaError_t enqueue_map(bdc_handle* H, const double* p, double* pn, RsAAState* st, int gate, int rec) {
+        cudaStream_t s = H->stream;
+        const cudaError_t e = enqueue_qd(H, p, st, gate);
+        if (e != cudaSuccess) return e;
         k_rs_update<<<1, 1024, 0, s>>>(S, D.get<double>(), w.get<uint8_t>(), p, pn, out.get<double>(), st, gate,
                                        rec);
         return cudaGetLastError();
@@ -868,8 +882,9 @@ struct Restricted {
 // the restricted problem, with every decision taken on the device from
 // RsAAState: one step is the plain map, the push of the new differences with
 // their Gram products, the least-squares weights, the mixed point, its map and
-// the choice of the next iterate -- nine kernels (two maps of three, three
-// single-block steps between and after them), captured kRsGraphSteps
+// the choice of the next iterate -- six kernels (per map the member sums
+// and D, then one block that updates and, after the plain map, pushes,
+// solves and mixes, after the mixed map accepts), captured kRsGraphSteps
 // steps to a CUDA graph; the host reads the state once per graph.
 constexpr int kRsGraphSteps = 16;
 
@@ -895,10 +910,10 @@ constexpr int kRsBlock = 1024;
 // gamma = b by Cholesky with the ridge lambda = 1e-12 tr(A) / c over the c
 // slots in use; solve_ok = 0 when the system is degenerate or this was the
 // first pair after a clear.
-__global__ void __launch_bounds__(kRsBlock) k_rs_push_solve(int L, int m, const uint8_t* __restrict__ wts,
-                                                           const double* __restrict__ x, const double* __restrict__ g,
-                                                           double* __restrict__ f_last, double* __restrict__ g_last,
-                                                           RsSlots P, RsAAState* st) {
+__device__ __forceinline__ void rs_push_solve_body(int L, int m, const uint8_t* __restrict__ wts,
+                                                   const double* __restrict__ x, const double* __restrict__ g,
+                                                   double* __restrict__ f_last, double* __restrict__ g_last,
+                                                   RsSlots P, RsAAState* st) {
     if (rs_skip(st, 2)) return;
     const bool diff = st->have_last != 0;
     const int sl = st->npush % m;
@@ -1016,9 +1031,9 @@ __global__ void __launch_bounds__(kRsBlock) k_rs_push_solve(int L, int m, const 
 }
 
 // xa = g_last - sum_a gamma_a dG_a, clipped at 0, normalised to sum w xa = 1
-__global__ void __launch_bounds__(kRsBlock) k_rs_mix_scale(int L, int m, const uint8_t* __restrict__ wts, RsSlots P,
-                                                          const double* __restrict__ g_last, double* __restrict__ xa,
-                                                          const RsAAState* st) {
+__device__ __forceinline__ void rs_mix_scale_body(int L, int m, const uint8_t* __restrict__ wts, RsSlots P,
+                                                  const double* __restrict__ g_last, double* __restrict__ xa,
+                                                  const RsAAState* st) {
     if (rs_skip(st, 3)) return;
     __shared__ double sh[kRsBlock / 32];
     __shared__ double inv;
@@ -1049,9 +1064,8 @@ __global__ void __launch_bounds__(kRsBlock) k_rs_mix_scale(int L, int m, const u
 // the next iterate (the mixed image when kept, else the plain one); then a
 // rejected mixed point clears the history (when it holds a difference) and a
 // stop flag ends the loop
-__global__ void __launch_bounds__(kRsBlock) k_rs_accept(int L, int m, double* __restrict__ x,
-                                                       const double* __restrict__ g, const double* __restrict__ ga,
-                                                       RsAAState* st) {
+__device__ __forceinline__ void rs_accept_body(int L, int m, double* __restrict__ x, const double* __restrict__ g,
+                                               const double* __restrict__ ga, RsAAState* st) {
     if (rs_skip(st, 1)) return;
     const double* __restrict__ src = (!st->stop_plain && rs_mixed_kept(st)) ? ga : g;
     for (int i = threadIdx.x; i < L; i += kRsBlock) x[i] = src[i];
@@ -1067,6 +1081,32 @@ __global__ void __launch_bounds__(kRsBlock) k_rs_accept(int L, int m, double* __
     }
     if (st->stop_mixed) st->fin = 1;
     st->solve_ok = 0;
+}
+
+// the plain map's update (gate 1), then push + solve (gate 2), then the
+// mixed point (gate 3), one block: each part reads what the one before it
+// left in st and in the vectors after a block barrier
+__global__ void __launch_bounds__(kRsBlock) k_rs_step_plain(int L, int m, const double* __restrict__ D,
+                                                           const uint8_t* __restrict__ w, const double* __restrict__ x,
+                                                           double* __restrict__ g, double* __restrict__ out,
+                                                           double* __restrict__ f_last, double* __restrict__ g_last,
+                                                           RsSlots P, double* __restrict__ xa, RsAAState* st) {
+    rs_update_body(L, D, w, x, g, out, st, 1, 1);
+    __syncthreads();
+    rs_push_solve_body(L, m, w, x, g, f_last, g_last, P, st);
+    __syncthreads();
+    rs_mix_scale_body(L, m, w, P, g_last, xa, st);
+}
+
+// the mixed map's update (gate 3), then the next iterate (gate 1)
+__global__ void __launch_bounds__(kRsBlock) k_rs_step_mixed(int L, int m, const double* __restrict__ D,
+                                                           const uint8_t* __restrict__ w, const double* __restrict__ xa,
+                                                           double* __restrict__ ga, double* __restrict__ out,
+                                                           double* __restrict__ x, const double* __restrict__ g,
+                                                           RsAAState* st) {
+    rs_update_body(L, D, w, xa, ga, out, st, 3, 2);
+    __syncthreads();
+    rs_accept_body(L, m, x, g, ga, st);
 }
 
 struct RsAA {
@@ -1114,16 +1154,16 @@ static cudaError_t rs_enqueue_step(bdc_handle* H, Restricted& rs, RsAA& aa, doub
     cudaStream_t s = H->stream;
     RsAAState* st = aa.st.get<RsAAState>();
     const uint8_t* w = rs.w.get<uint8_t>();
-    cudaError_t e = rs.enqueue_map(H, x, g, st, 1, 1);
+    cudaError_t e = rs.enqueue_qd(H, x, st, 1);
     if (e != cudaSuccess) return e;
-    k_rs_push_solve<<<1, kRsBlock, 0, s>>>(aa.L, aa.m, w, x, g, aa.f_last.get<double>(), aa.g_last.get<double>(),
-                                           aa.slots(), st);
-    k_rs_mix_scale<<<1, kRsBlock, 0, s>>>(aa.L, aa.m, w, aa.slots(), aa.g_last.get<double>(), xa, st);
+    k_rs_step_plain<<<1, kRsBlock, 0, s>>>(aa.L, aa.m, rs.D.get<double>(), w, x, g, rs.out.get<double>(),
+                                           aa.f_last.get<double>(), aa.g_last.get<double>(), aa.slots(), xa, st);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    e = rs.enqueue_map(H, xa, ga, st, 3, 2);
+    e = rs.enqueue_qd(H, xa, st, 3);
     if (e != cudaSuccess) return e;
-    k_rs_accept<<<1, kRsBlock, 0, s>>>(aa.L, aa.m, x, g, ga, st);
+    k_rs_step_mixed<<<1, kRsBlock, 0, s>>>(aa.L, aa.m, rs.D.get<double>(), w, xa, ga, rs.out.get<double>(), x, g,
+                                           st);
     return cudaGetLastError();
 }
 
