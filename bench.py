@@ -325,7 +325,7 @@ def ours_arm(args) -> None:
     barrier()
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_steps = max(1, min(args.steps, 10))
+    e2e_steps = max(1, min(args.steps, 50))
     f0.record(stream)
     for _ in range(e2e_steps):
         E.baa_iteration_ptr(p_in.data_ptr(), p_out.data_ptr())
